@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Residual + Jacobian evaluations per second on the ternary spline EAM workload.
+
+Workload (one "step"): one residual + analytic Jacobian + JᵀJ/Jᵀr evaluation
+over 500 periodic configurations × 256 atoms (Zr/Cu/Al random packings at
+0.060 Å⁻³), 6 φ + 3 ρ + 3 F makima splines × 20 knots (D = 240),
+w_e = 1, w_s = 0.1 — rows = 388,000.  FP32 compute, FP64 sums.
+
+  value     device-timed throughput (CUDA events on the library's stream,
+            inputs resident in HBM, L2 flushed between timed steps)
+  e2e       the same step through the C ABI with host buffers: x uploaded
+            (H2D) and JᵀJ, Jᵀr, ‖F‖² read back (D2H) every step
+  roofline  the dominant kernel's algorithmic bytes (or FLOPs) ÷ its measured
+            per-launch time, against MEASURED_PEAKS.json
+  cpu_baseline  the oracle (FP64 CPU restatement of the reference path,
+            OpenMP over configurations) running the reference's own method —
+            a central-difference Jacobian of 2·D + 1 residual evaluations —
+            on a bounded sample of FD columns, extrapolated to one Jacobian
+
+`--impl reference` times that CPU path alone as the reference arm.
+Multi-GPU (torchrun): every rank evaluates its own 500-configuration shard
+(weak scaling) and the normal equations are summed over ranks with one
+NCCL all-reduce per step (the exchange an LM step needs).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+W_E, W_S = 1.0, 0.1
+N_CFG, N_ATOMS = 500, 256
+WORKLOAD = "ternary Zr-Cu-Al makima-spline EAM, 500 configs x 256 atoms, D=240, w_e=1, w_s=0.1"
+METRIC = "residual+Jacobian evals/s (ternary EAM, 500x256 atoms, D=240)"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    p.add_argument("--e2e-steps", type=int, default=50)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-columns", type=int, default=4)
+    p.add_argument("--small", action="store_true", help="small case for profiler captures")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def workload(rank=0, small=False):
+    from forcesmith_b200 import synth
+    n_cfg, n_at = (20, 256) if small else (N_CFG, N_ATOMS)
+    ds = synth.packing(np.full(n_cfg, n_at, np.int32), seed=20261204 + 7919 * rank)
+    true = synth.ternary_true_model(20)
+    start = synth.perturb(true, 0.95, 1.05, seed=7)
+    return ds, true, start
+
+
+def label_on_gpu(ds, true, device):
+    from forcesmith_b200.gpu import GpuSession
+    g = GpuSession(device, "fp64")
+    g.upload(ds)
+    g.set_model(true)
+    out = g.eval(W_E, W_S, want=("forces", "energy", "stress"))
+    g.close()
+    return ds.with_labels(out["forces"], out["energy"], out["stress"])
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic(g, phase, M, D, P, N, ndens=60):
+    """Algorithmic bytes (or FLOPs) of one launch of each phase's main kernel."""
+    if phase == "residual":
+        # 4-B (j, image) word per directed pair, per-atom position/type/ref force in
+        # and force out, per-row residual out
+        return "hbm", P * 4 + N * (24 + 4 + 24 + 24) + M * 8
+    if phase == "jac_forces":
+        # column-major FP32 J written once, pairs and ∂ρ/∂y rows read once
+        return "hbm", M * D * 4 + P * 4 + N * ndens * 4 + N * 40
+    if phase == "jac_atoms":
+        return "hbm", P * 4 + N * (ndens * 4 + 40) + 2 * D * 8
+    # JᵀJ: 2·m·D² FLOPs (dense contraction), plus Jᵀr
+    return "tensor", 2.0 * M * D * D + 2.0 * M * D
+
+
+def cpu_baseline(ds, start, columns):
+    """Reference method on the host: FD Jacobian = 1 + 2·D residual evaluations."""
+    from oracle.api import Oracle, set_threads
+    threads = set_threads(os.cpu_count() or 1)
+    o = Oracle()
+    o.upload(ds)
+    o.set_model(start)
+    D = o.D
+    o.eval(W_E, W_S, want=("obj",))  # warm
+    t0 = time.perf_counter()
+    o.eval(W_E, W_S, want=("F",))
+    t_res = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.jacobian_fd(W_E, W_S, 0, columns)
+    t_col = (time.perf_counter() - t0) / columns
+    t_jac = t_res + D * t_col
+    return {"value": 1.0 / t_jac, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": f"1 residual + {columns} of {D} central-difference columns (h=1e-5) over "
+                      f"{ds.n_cfg} configs; one evaluation = residual + {D} columns "
+                      f"(t_res={t_res*1e3:.1f} ms, t_col={t_col*1e3:.1f} ms)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ds, true, start = workload(0, args.small)
+    from oracle.api import Oracle, set_threads
+    threads = set_threads(os.cpu_count() or 1)
+    o = Oracle()
+    o.upload(ds)
+    o.set_model(true)
+    lab = o.eval(W_E, W_S)
+    ds = ds.with_labels(lab["forces"], lab["energy"], lab["stress"])
+    o.set_references(ds)
+    o.set_model(start)
+    D = o.D
+    for _ in range(args.warmup):
+        o.jacobian_fd(W_E, W_S, 0, 1)
+    t0 = time.perf_counter()
+    o.eval(W_E, W_S, want=("F",))
+    t_res = time.perf_counter() - t0
+    cols = []
+    for k in range(args.steps):
+        c = k % D
+        t0 = time.perf_counter()
+        o.jacobian_fd(W_E, W_S, c, c + 1)
+        cols.append(time.perf_counter() - t0)
+    t_jac = t_res + D * float(np.mean(cols))
+    v = 1.0 / t_jac
+    sample = (f"per step one central-difference column (2 residual evaluations over {ds.n_cfg} "
+              f"configs); evaluation = residual + {D} columns, t_res={t_res*1e3:.1f} ms, "
+              f"t_col={np.mean(cols)*1e3:.1f} ms")
+    line = {"metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_jac * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "method": "central-difference Jacobian, h=1e-5",
+                       "threads": threads},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    from forcesmith_b200 import gpu as G
+
+    ds, true, start = workload(rank, args.small)
+    ds = label_on_gpu(ds, true, local)
+    g = G.GpuSession(local, args.precision)
+    g.upload(ds)
+    g.set_model(start)
+    M, D, P, N = g.residual_count(W_S), g.D, g.num_pairs(), ds.n_atoms
+    stream = torch.cuda.ExternalStream(g.stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    ne = torch.empty(D * D + D + 1, dtype=torch.float64, device=f"cuda:{local}")
+
+    def step():
+        g.jacobian_async(W_E, W_S)
+        if dist is not None:
+            G.copy_normal_equations(g, ne.data_ptr())
+            with torch.cuda.stream(stream):
+                dist.all_reduce(ne)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    G.set_profiling(g, args.steps)
+    l0 = G.launch_count(g)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # L2 flush between timed steps, outside the step events
+            ev[k][0].record(stream)
+        step()
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t_wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    launches = G.launch_count(g) - l0
+    phases, nprof = G.phase_times(g)
+    G.set_profiling(g, 0)
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * 1000.0 / ms
+
+    # e2e through the C ABI with host buffers (x in pinned memory)
+    x = torch.from_numpy(g.gather_params()).pin_memory().numpy()
+    JtJ, Jtr = np.zeros((D, D)), np.zeros(D)
+    import ctypes as C
+    from forcesmith_b200.abi import _dp
+    obj = C.c_double()
+    for _ in range(3):
+        g.set_params(x)
+        g._lib.fs_gpu_eval_jacobian(g._h, W_E, W_S, None, None, _dp(JtJ), _dp(Jtr), C.byref(obj))
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        g.set_params(x)
+        rc = g._lib.fs_gpu_eval_jacobian(g._h, W_E, W_S, None, None, _dp(JtJ), _dp(Jtr), C.byref(obj))
+        assert rc == 0
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    assert np.isfinite(obj.value) and np.all(np.isfinite(JtJ))
+
+    hbm, bf16, src = peaks()
+    per = {k: v / max(nprof, 1) for k, v in phases.items()}
+    dom = max(per, key=per.get)
+    bound, alg = algorithmic(g, dom, M, D, P, N)
+    t_dom = per[dom] * 1e-3
+    if bound == "hbm":
+        achieved, peak, unit = alg / t_dom / 1e9, hbm, "GB/s"
+    else:
+        achieved, peak, unit = alg / t_dom / 1e12, bf16, "TFLOP/s"
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.precision.replace("fp", "f") + "+f64acc",
+        "data": "synthetic (seeded packings; labels from a seeded true model in FP64)",
+        "config": {"workload": WORKLOAD, "rows": M, "params": D, "pairs": P, "atoms": N,
+                   "parallelism": f"weak dp{world}" if world > 1 else "1 GPU",
+                   "l2": "flushed by a 256 MiB write between timed steps",
+                   "wall_s_timed": t_wall},
+        "e2e": {"value": world / e2e_s, "unit": "evals/s", "h2d_bytes_per_step": D * 8,
+                "d2h_bytes_per_step": (D * D + D + 1) * 8},
+        "gpu_launches": int(launches),
+        "phases_ms": {k: round(v, 5) for k, v in per.items()},
+        "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                     "frac": achieved / peak, "peak_source": src, "traffic": None,
+                     "algorithmic": alg},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(ds, start, args.cpu_columns)
+    if dist is not None:
+        dist.barrier()
+    g.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

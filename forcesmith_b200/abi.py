@@ -1,0 +1,296 @@
+"""ctypes mirror of include/forcesmith_gpu.h and a thin session wrapper.
+
+The same `Session` class drives any library that exports the `fs_gpu_*`
+call set under some prefix, so host code (and the parity tests) read the
+same for the device library and for any CPU implementation of the ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+FS_OK = 0
+FS_ERR_ARG = -1
+FS_ERR_CUDA = -2
+FS_ERR_STATE = -3
+FS_ERR_UNSUPPORTED = -4
+FS_ERR_NOMEM = -5
+FS_ERR_DEVICE = -6
+FS_ERR_NUMERIC = -7
+
+FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW = 0, 1, 2, 3
+FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA = 0, 1, 2, 3
+FS_PREC_FP32, FS_PREC_FP64 = 0, 1
+
+FORMS = {
+    "lj": (0, 2), "morse": (1, 3), "exp_decay": (2, 2), "sqrt": (3, 2),
+    "power_decay": (4, 2), "mexp_decay": (5, 3), "harmonic": (6, 2),
+    "exp_plus": (7, 3), "parabola": (8, 3), "const": (9, 1),
+    "buckingham": (10, 3), "born": (11, 5),
+}
+
+
+class FsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+class fs_table(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("form", C.c_int32), ("n", C.c_int32),
+                ("reserved", C.c_int32), ("rmin", C.c_double), ("rmax", C.c_double),
+                ("values", C.POINTER(C.c_double)), ("fixed", C.POINTER(C.c_uint8)),
+                ("lower", C.POINTER(C.c_double)), ("upper", C.POINTER(C.c_double))]
+
+
+class fs_model(C.Structure):
+    _fields_ = [("family", C.c_int32), ("ntypes", C.c_int32), ("n_tables", C.c_int32),
+                ("reserved", C.c_int32), ("tables", C.POINTER(fs_table))]
+
+
+class fs_gpu_opts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32),
+                ("lanes_per_atom", C.c_int32), ("reserved", C.c_int32)]
+
+
+def _dp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+@dataclass
+class Table:
+    """One table of a calculator, in the reference's gather order."""
+    kind: int
+    values: np.ndarray
+    rmin: float = 0.0
+    rmax: float = 0.0
+    form: int = 0
+    fixed: Optional[np.ndarray] = None
+    lower: Optional[np.ndarray] = None
+    upper: Optional[np.ndarray] = None
+
+    @staticmethod
+    def spline(rmin, rmax, knots, fixed=None):
+        return Table(FS_TABLE_SPLINE, np.ascontiguousarray(knots, dtype=np.float64),
+                     float(rmin), float(rmax), 0,
+                     None if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8))
+
+    @staticmethod
+    def analytic(name, params, rmin, rmax, fixed=None, lower=None, upper=None):
+        form, npar = FORMS[name]
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        assert p.size == npar, (name, p.size, npar)
+        f = lambda a, dt: None if a is None else np.ascontiguousarray(a, dtype=dt)
+        return Table(FS_TABLE_ANALYTIC, p, float(rmin), float(rmax), form,
+                     f(fixed, np.uint8), f(lower, np.float64), f(upper, np.float64))
+
+    @staticmethod
+    def sw(A, B, p, q, delta, a1, gamma, a2, fixed=None):
+        v = np.array([A, B, p, q, delta, a1, gamma, a2], dtype=np.float64)
+        return Table(FS_TABLE_SW, v, 0.0, 0.0, 0,
+                     None if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8))
+
+    @staticmethod
+    def lam(values, fixed=None):
+        return Table(FS_TABLE_LAMBDA, np.ascontiguousarray(values, dtype=np.float64),
+                     fixed=None if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8))
+
+    def copy(self):
+        c = lambda a: None if a is None else a.copy()
+        return Table(self.kind, self.values.copy(), self.rmin, self.rmax, self.form,
+                     c(self.fixed), c(self.lower), c(self.upper))
+
+
+@dataclass
+class Model:
+    family: int
+    ntypes: int
+    tables: list = field(default_factory=list)
+
+    def to_c(self):
+        """Returns (fs_model, keepalive) — keep the second alive while in use."""
+        arr = (fs_table * len(self.tables))()
+        keep = [arr]
+        for k, t in enumerate(self.tables):
+            ft = arr[k]
+            ft.kind, ft.form, ft.n = t.kind, t.form, int(t.values.size)
+            ft.rmin, ft.rmax = t.rmin, t.rmax
+            ft.values = _dp(t.values)
+            ft.fixed = None if t.fixed is None else t.fixed.ctypes.data_as(C.POINTER(C.c_uint8))
+            ft.lower = _dp(t.lower)
+            ft.upper = _dp(t.upper)
+            keep.append(t)
+        m = fs_model(self.family, self.ntypes, len(self.tables), 0, arr)
+        return m, keep
+
+    def free_values(self) -> np.ndarray:
+        out = []
+        for t in self.tables:
+            fx = t.fixed if t.fixed is not None else np.zeros(t.values.size, np.uint8)
+            out.append(t.values[fx == 0])
+        return np.concatenate(out) if out else np.zeros(0)
+
+    def with_values(self, x: np.ndarray) -> "Model":
+        m = Model(self.family, self.ntypes, [t.copy() for t in self.tables])
+        o = 0
+        for t in m.tables:
+            fx = t.fixed if t.fixed is not None else np.zeros(t.values.size, np.uint8)
+            k = int((fx == 0).sum())
+            t.values[fx == 0] = x[o:o + k]
+            o += k
+        return m
+
+    def copy(self):
+        return Model(self.family, self.ntypes, [t.copy() for t in self.tables])
+
+
+@dataclass
+class Dataset:
+    """Concatenated periodic configurations (shapes of fs_gpu_upload_configs)."""
+    natoms: np.ndarray            # int32[n_cfg]
+    box9: np.ndarray              # float64[n_cfg, 9] row-major, lattice vectors as columns
+    pos: np.ndarray               # float64[N, 3]
+    type: np.ndarray              # int32[N]
+    ref_force: Optional[np.ndarray] = None   # float64[N, 3]
+    ref_energy: Optional[np.ndarray] = None  # float64[n_cfg]
+    ref_stress9: Optional[np.ndarray] = None  # float64[n_cfg, 9]
+
+    @property
+    def n_cfg(self):
+        return int(self.natoms.size)
+
+    @property
+    def n_atoms(self):
+        return int(self.natoms.sum())
+
+    def rows(self, w_s: float) -> int:
+        return int(3 * self.n_atoms + self.n_cfg * (2 + (6 if w_s > 0 else 0)))
+
+    def subset(self, idx):
+        idx = np.asarray(idx)
+        starts = np.concatenate([[0], np.cumsum(self.natoms)])
+        sel = np.concatenate([np.arange(starts[i], starts[i + 1]) for i in idx]) \
+            if idx.size else np.zeros(0, np.int64)
+        g = lambda a, s: None if a is None else np.ascontiguousarray(a[s])
+        return Dataset(np.ascontiguousarray(self.natoms[idx]), np.ascontiguousarray(self.box9[idx]),
+                       np.ascontiguousarray(self.pos[sel]), np.ascontiguousarray(self.type[sel]),
+                       g(self.ref_force, sel), g(self.ref_energy, idx), g(self.ref_stress9, idx))
+
+    def with_labels(self, forces, energy, stress9):
+        return Dataset(self.natoms, self.box9, self.pos, self.type,
+                       np.ascontiguousarray(forces, np.float64).reshape(-1, 3),
+                       np.ascontiguousarray(energy, np.float64),
+                       np.ascontiguousarray(stress9, np.float64).reshape(-1, 9))
+
+
+class Session:
+    """Handle-based wrapper over an `fs_gpu_*`-shaped C ABI (`prefix_*`)."""
+
+    def __init__(self, lib: C.CDLL, prefix: str, handle: C.c_void_p, err_fn=None):
+        self._lib = lib
+        self._p = prefix
+        self._h = handle
+        self._err_fn = err_fn
+        self._keep = None
+        self.D = None
+
+    def _f(self, name):
+        return getattr(self._lib, f"{self._p}_{name}")
+
+    def _check(self, rc, what):
+        if rc != FS_OK:
+            msg = what
+            if self._err_fn is not None:
+                msg = f"{what}: {self._err_fn(self._h)}"
+            raise FsError(rc, msg)
+
+    def upload(self, ds: Dataset):
+        self._ds = ds
+        rc = self._f("upload_configs")(self._h, C.c_int32(ds.n_cfg), _ip(ds.natoms),
+                                       _dp(np.ascontiguousarray(ds.box9, np.float64)),
+                                       _dp(np.ascontiguousarray(ds.pos, np.float64)), _ip(ds.type),
+                                       _dp(ds.ref_force), _dp(ds.ref_energy), _dp(ds.ref_stress9))
+        self._check(rc, "upload_configs")
+
+    def set_references(self, ds: Dataset):
+        rc = self._f("set_references")(self._h, _dp(ds.ref_force), _dp(ds.ref_energy),
+                                       _dp(ds.ref_stress9))
+        self._check(rc, "set_references")
+
+    def set_model(self, model: Model, prepare=True):
+        m, keep = model.to_c()
+        self._keep = keep
+        self._check(self._f("set_model")(self._h, C.byref(m)), "set_model")
+        d = C.c_int32()
+        self._check(self._f("param_count")(self._h, C.byref(d)), "param_count")
+        self.D = d.value
+        if prepare:
+            self._check(self._f("prepare")(self._h), "prepare")
+
+    def prepare(self):
+        self._check(self._f("prepare")(self._h), "prepare")
+
+    def num_pairs(self):
+        n = C.c_int64()
+        self._check(self._f("num_pairs")(self._h, C.byref(n)), "num_pairs")
+        return n.value
+
+    def neighbor_counts(self, n_atoms):
+        out = np.zeros(n_atoms, np.int32)
+        self._check(self._f("get_neighbor_counts")(self._h, _ip(out)), "get_neighbor_counts")
+        return out
+
+    def gather_params(self):
+        x = np.zeros(self.D, np.float64)
+        self._check(self._f("gather_params")(self._h, _dp(x)), "gather_params")
+        return x
+
+    def gather_bounds(self):
+        lo = np.zeros(self.D, np.float64)
+        hi = np.zeros(self.D, np.float64)
+        self._check(self._f("gather_bounds")(self._h, _dp(lo), _dp(hi)), "gather_bounds")
+        return lo, hi
+
+    def set_params(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        self._check(self._f("set_params")(self._h, _dp(x), C.c_int32(x.size)), "set_params")
+
+    def residual_count(self, w_s):
+        m = C.c_int64()
+        self._check(self._f("residual_count")(self._h, C.c_double(w_s), C.byref(m)),
+                    "residual_count")
+        return m.value
+
+    def eval(self, w_e=1.0, w_s=0.0, want=("F", "forces", "energy", "stress", "limit", "obj")):
+        ds = self._ds
+        m = self.residual_count(w_s)
+        out = {}
+        F = np.zeros(m) if "F" in want else None
+        fo = np.zeros((ds.n_atoms, 3)) if "forces" in want else None
+        en = np.zeros(ds.n_cfg) if "energy" in want else None
+        st = np.zeros((ds.n_cfg, 9)) if "stress" in want else None
+        li = np.zeros(ds.n_cfg) if "limit" in want else None
+        ob = C.c_double()
+        rc = self._f("eval")(self._h, C.c_double(w_e), C.c_double(w_s), _dp(F), _dp(fo), _dp(en),
+                             _dp(st), _dp(li), C.byref(ob) if "obj" in want else None)
+        self._check(rc, "eval")
+        for k, v in (("F", F), ("forces", fo), ("energy", en), ("stress", st), ("limit", li)):
+            if v is not None:
+                out[k] = v
+        if "obj" in want:
+            out["obj"] = ob.value
+        return out
+
+
+def load_library(path: str) -> C.CDLL:
+    if not os.path.exists(path):
+        raise FileNotFoundError(path)
+    return C.CDLL(path, mode=C.RTLD_GLOBAL)

@@ -1,0 +1,899 @@
+// EAM and tabulated-pair calculators on the device: the residual vector and
+// its analytic Jacobian with respect to the free spline knots.
+//
+//   residual   EAMForceCalculator::eval_forces (src/force/eam_force.cpp:45-102),
+//              PairForceCalculator::eval_forces (src/force/pair_force.cpp:21-60),
+//              with_eval_scope (include/forcesmith/force/eval_scope.hpp:13-31)
+//              and write_config_residuals
+//              (include/forcesmith/optimization/residual_layout.hpp:37-54).
+//   Jacobian   the chain rule of EAMForceCalculator::write_param_jacobian
+//              (src/force/eam_force.cpp:108-279) and
+//              PairForceCalculator::write_param_jacobian (pair_force.cpp:80-111),
+//              with ∂(spline)/∂(knots) taken through the makima slopes.  The
+//              reference differentiates splines by central differences
+//              (forcesmith_functor.cpp:279-286); this is the exact derivative
+//              of the same function.
+//
+// One CTA per configuration.  The configuration's wrapped positions, its
+// periodic image shifts and the spline segment tables sit in shared memory;
+// the neighbour list is a 4-byte (j, image) word per directed pair, and each
+// pair vector is rebuilt in FP64 then rounded to the working precision T.
+#include "spline_dev.cuh"
+
+#include <algorithm>
+
+namespace fsg {
+namespace {
+
+struct Smem {
+  unsigned char *p;
+  __device__ explicit Smem(unsigned char *base) : p(base) {}
+  template <class X> __device__ X *take(size_t n, size_t align = 16) {
+    uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    a = (a + align - 1) & ~(uintptr_t)(align - 1);
+    X *r = reinterpret_cast<X *>(a);
+    p = reinterpret_cast<unsigned char *>(a + n * sizeof(X));
+    return r;
+  }
+};
+
+inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+
+struct Common {
+  const CfgDev *cfg;
+  const double *wpos;
+  const int32_t *type;
+  const double *ref_force;
+  const int32_t *nb_start;
+  const uint32_t *nb_pack;
+  const TableDesc *desc;
+  const int32_t *cmap;
+  int n_tables, n_segs, n_cmap, ntypes;
+  int family; // FS_FAMILY_EAM or FS_FAMILY_PAIR
+};
+
+// Stage the configuration geometry: wrapped positions (FP64), species, and
+// the image shift table ix·a + iy·b + iz·c.
+__device__ void stage_geometry(const CfgDev &cd, const Common &A, double *wpos, double *shift, uint8_t *typ) {
+  const int N = cd.natoms;
+  for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) wpos[k] = A.wpos[3 * static_cast<int64_t>(cd.atom0) + k];
+  for (int k = threadIdx.x; k < N; k += blockDim.x) typ[k] = static_cast<uint8_t>(A.type[cd.atom0 + k]);
+  const int wx = 2 * cd.sx + 1, wy = 2 * cd.sy + 1, wz = 2 * cd.sz + 1;
+  for (int k = threadIdx.x; k < wx * wy * wz; k += blockDim.x) {
+    const double ix = k / (wy * wz) - cd.sx, iy = (k / wz) % wy - cd.sy, iz = k % wz - cd.sz;
+    for (int a = 0; a < 3; ++a) shift[3 * k + a] = ix * cd.box[3 * a] + iy * cd.box[3 * a + 1] + iz * cd.box[3 * a + 2];
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void pair_vec(const double *wpos, const double *shift, int i, uint32_t pk, int &j,
+                                         T &dx, T &dy, T &dz) {
+  j = static_cast<int>(pk & 0xFFFFFu);
+  const int img = static_cast<int>(pk >> 20);
+  dx = static_cast<T>((wpos[3 * j] - wpos[3 * i]) + shift[3 * img]);
+  dy = static_cast<T>((wpos[3 * j + 1] - wpos[3 * i + 1]) + shift[3 * img + 1]);
+  dz = static_cast<T>((wpos[3 * j + 2] - wpos[3 * i + 2]) + shift[3 * img + 2]);
+}
+
+template <class T> __device__ __forceinline__ T sqrt_t(T x) { return sqrt(x); }
+
+template <class T> struct ResArgs {
+  Common c;
+  const typename Vec4T<T>::type *seg_a;
+  double w_e, w_s;
+  double *F, *forces, *energy, *stress9, *limit, *obj_part;
+};
+
+template <class T> size_t residual_smem(int n_tables, int n_segs, int max_atoms, int max_img) {
+  size_t b = 0;
+  b += align16(n_tables * sizeof(STab<T>));
+  b += align16(n_segs * 4 * sizeof(T));
+  b += align16(3 * max_atoms * sizeof(double));
+  b += align16(3 * max_img * sizeof(double));
+  b += align16(max_atoms);
+  b += align16(2 * max_atoms * sizeof(T));
+  b += 64 * sizeof(double) + 64;
+  return b + 64;
+}
+
+// ---------------------------------------------------------------------------
+// Residual: ρ pass → embedding → force/energy/stress pass → residual rows.
+// ---------------------------------------------------------------------------
+template <class T, int LPA, bool EAM>
+__global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
+  using T4 = typename Vec4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x;
+  const CfgDev &cd = A.c.cfg[c];
+  const int N = cd.natoms;
+  const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
+  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  Smem S(smem_raw);
+  STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
+  T4 *seg = S.take<T4>(A.c.n_segs);
+  double *wpos = S.take<double>(3 * N);
+  double *shift = S.take<double>(3 * nimg);
+  uint8_t *typ = S.take<uint8_t>(N);
+  T *rho = S.take<T>(N);
+  T *gradF = S.take<T>(N);
+  double *red = S.take<double>(64);
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) seg[k] = A.seg_a[k];
+  stage_geometry(cd, A.c, wpos, shift, typ);
+  __syncthreads();
+
+  const int ngroups = blockDim.x / LPA, g = threadIdx.x / LPA, l = threadIdx.x % LPA;
+  const int32_t *start = A.c.nb_start + cd.atom0;
+  double e_emb = 0.0, lim = 0.0;
+  if constexpr (EAM) {
+    // ρ_i = Σ_j ρ_{t(j)}(r_ij), closed gate (eam_force.cpp:59-66)
+    for (int i0 = 0; i0 < N; i0 += ngroups) {
+      const int i = i0 + g;
+      T acc = T(0);
+      if (i < N) {
+        for (int p = start[i] + l; p < start[i + 1]; p += LPA) {
+          int j;
+          T dx, dy, dz;
+          pair_vec(wpos, shift, i, A.c.nb_pack[p], j, dx, dy, dz);
+          const T r = sqrt_t(dx * dx + dy * dy + dz * dz);
+          const STab<T> &tb = tabs[np + typ[j]];
+          if (in_span(tb, r)) {
+            T t;
+            const int e = seg_of(tb, r, t);
+            acc += seg_val<T>(seg[e], t);
+          }
+        }
+      }
+      acc = warp_sum_group(acc, LPA);
+      if (i < N && l == 0) rho[i] = acc;
+    }
+    __syncthreads();
+    // clamp_embedding + F(ρ), F'(ρ) (kernels.hpp:19-31; eam_force.cpp:68-73)
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const STab<T> &tb = tabs[np + nt + typ[i]];
+      T rr = rho[i];
+      if (rr > tb.xmax) {
+        const double d = static_cast<double>(rr) - static_cast<double>(tb.xmax);
+        lim += 100.0 * 10.0 * d * d;
+        rr = tb.xmax;
+      } else if (rr < tb.x0) {
+        const double d = static_cast<double>(tb.x0) - static_cast<double>(rr);
+        lim += 100.0 * 10.0 * d * d;
+        rr = tb.x0;
+      }
+      T t;
+      const int e = seg_of(tb, rr, t);
+      e_emb += static_cast<double>(seg_val<T>(seg[e], t));
+      gradF[i] = seg_der<T>(seg[e], t, tb.inv_h);
+    }
+    __syncthreads();
+  }
+  // forces, ½φ energy and −½ d fᵀ stress (eam_force.cpp:75-100; kernels.hpp:33-38)
+  double e_pair = 0.0, objp = 0.0;
+  double sg[6] = {0, 0, 0, 0, 0, 0};
+  const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
+  const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
+  for (int i0 = 0; i0 < N; i0 += ngroups) {
+    const int i = i0 + g;
+    T f[3] = {0, 0, 0}, ep = T(0), s[6] = {0, 0, 0, 0, 0, 0};
+    if (i < N) {
+      const int ti = typ[i];
+      for (int p = start[i] + l; p < start[i + 1]; p += LPA) {
+        int j;
+        T d[3];
+        pair_vec(wpos, shift, i, A.c.nb_pack[p], j, d[0], d[1], d[2]);
+        const T r = sqrt_t(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        if (r < T(1e-14)) continue;
+        const int tj = typ[j];
+        const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
+        T phi = T(0), dphi = T(0);
+        if constexpr (EAM) {
+          if (in_span(tp, r)) {
+            T t;
+            const int e = seg_of(tp, r, t);
+            phi = seg_val<T>(seg[e], t);
+            dphi = seg_der<T>(seg[e], t, tp.inv_h);
+          }
+        } else {
+          // make_pair_bond's half-open gate [rmin, rmax) (pair_force.cpp:28)
+          if (r < tp.x0 || r >= tp.xmax) continue;
+          T t;
+          const int e = seg_of(tp, r, t);
+          phi = seg_val<T>(seg[e], t);
+          dphi = seg_der<T>(seg[e], t, tp.inv_h);
+        }
+        T fs = dphi;
+        if constexpr (EAM) {
+          const STab<T> &gj = tabs[np + tj], &gi = tabs[np + ti];
+          T drho_j = T(0), drho_i = T(0);
+          if (in_span(gj, r)) {
+            T t;
+            const int e = seg_of(gj, r, t);
+            drho_j = seg_der<T>(seg[e], t, gj.inv_h);
+          }
+          if (in_span(gi, r)) {
+            T t;
+            const int e = seg_of(gi, r, t);
+            drho_i = seg_der<T>(seg[e], t, gi.inv_h);
+          }
+          fs = dphi + gradF[i] * drho_j + gradF[j] * drho_i;
+        }
+        fs = fs * (T(1) / r);
+        const T fx = fs * d[0], fy = fs * d[1], fz = fs * d[2];
+        f[0] += fx;
+        f[1] += fy;
+        f[2] += fz;
+        ep += phi;
+        const T hx = T(0.5) * d[0], hy = T(0.5) * d[1], hz = T(0.5) * d[2];
+        s[0] -= hx * fx;
+        s[1] -= hy * fy;
+        s[2] -= hz * fz;
+        s[3] -= hx * fy;
+        s[4] -= hx * fz;
+        s[5] -= hy * fz;
+      }
+    }
+    for (int a = 0; a < 3; ++a) f[a] = warp_sum_group(f[a], LPA);
+    ep = warp_sum_group(ep, LPA);
+    for (int a = 0; a < 6; ++a) s[a] = warp_sum_group(s[a], LPA);
+    if (i < N && l == 0) {
+      const int64_t ga = static_cast<int64_t>(cd.atom0) + i;
+      for (int a = 0; a < 3; ++a) {
+        const double fa = static_cast<double>(f[a]);
+        const double res = fa - A.c.ref_force[3 * ga + a];
+        A.F[row0 + 3 * i + a] = res;
+        if (A.forces) A.forces[3 * ga + a] = fa;
+        objp += res * res;
+      }
+      e_pair += 0.5 * static_cast<double>(ep);
+      for (int a = 0; a < 6; ++a) sg[a] += static_cast<double>(s[a]);
+    }
+  }
+  const double E = block_sum(e_emb + e_pair, red);
+  const double L = block_sum(lim, red);
+  double st[6];
+  for (int a = 0; a < 6; ++a) st[a] = block_sum(sg[a], red);
+  const double op = block_sum(objp, red);
+  if (threadIdx.x == 0) {
+    const double iv = 1.0 / cd.volume;
+    for (int a = 0; a < 6; ++a) st[a] = st[a] * iv; // σ /= V (eval_scope.hpp:28)
+    int64_t row = row0 + 3 * N;
+    double o = op;
+    const double re = A.w_e * (E - cd.ref_energy);
+    A.F[row++] = re;
+    o += re * re;
+    static constexpr int vi[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    if (A.w_s > 0.0) {
+      for (int v = 0; v < 6; ++v) {
+        const double rs = A.w_s * (st[v] - cd.ref_stress[3 * vi[v][0] + vi[v][1]]);
+        A.F[row++] = rs;
+        o += rs * rs;
+      }
+    }
+    A.F[row++] = L;
+    o += L * L;
+    A.obj_part[c] = o;
+    if (A.energy) A.energy[c] = E;
+    if (A.limit) A.limit[c] = L;
+    if (A.stress9) {
+      double *s9 = A.stress9 + 9 * static_cast<int64_t>(c);
+      s9[0] = st[0];
+      s9[4] = st[1];
+      s9[8] = st[2];
+      s9[1] = s9[3] = st[3];
+      s9[2] = s9[6] = st[4];
+      s9[5] = s9[7] = st[5];
+    }
+  }
+}
+
+// Σ over configurations in a fixed order (deterministic objective).
+__global__ void sum_kernel(const double *__restrict__ part, int n, double *__restrict__ out) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) s += part[k];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// ---------------------------------------------------------------------------
+// Jacobian, kernel 1 (EAM): per atom ρ̄, ∂ρ/∂y^ρ, the clamp, F'(ρ̄), F''(ρ̄),
+// the embedding knot windows, and the energy / limit rows
+// (eam_force.cpp:121-210).
+// ---------------------------------------------------------------------------
+template <class T> struct JacArgs {
+  Common c;
+  const typename Vec4T<T>::type *seg_a;
+  const T *seg_g;       // [seg][4][kWin]
+  const int32_t *seg_ws;
+  double w_e, w_s;
+  int64_t M;            // rows of J (leading dimension)
+  int D;
+  int dens_c0, ndens;   // contiguous density columns
+  T *J;                 // column-major M × D
+  T *scal;              // [atom][4]: gradF, curvF, over (0 = unclamped), unused
+  T *drho;              // [atom][ndens]
+  T *dgd;               // [atom][kWin]: ∂F'(ρ̄)/∂y over the embedding window
+  int32_t *wsF;         // [atom]: embedding window start (knot)
+};
+
+template <class T> size_t jac_common_smem(int n_tables, int n_segs, int n_cmap, int max_atoms, int max_img) {
+  size_t b = 0;
+  b += align16(n_tables * sizeof(STab<T>));
+  b += align16(n_segs * 4 * sizeof(T));
+  b += align16(n_segs * 4 * kWin * sizeof(T));
+  b += align16(n_segs * sizeof(int32_t));
+  b += align16(n_cmap * sizeof(int32_t));
+  b += align16(3 * max_atoms * sizeof(double));
+  b += align16(3 * max_img * sizeof(double));
+  b += align16(max_atoms);
+  return b + 128;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
+  using T4 = typename Vec4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x;
+  const CfgDev &cd = A.c.cfg[c];
+  const int N = cd.natoms;
+  const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
+  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  Smem S(smem_raw);
+  STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
+  T4 *seg = S.take<T4>(A.c.n_segs);
+  T *segg = S.take<T>(A.c.n_segs * 4 * kWin);
+  int32_t *segws = S.take<int32_t>(A.c.n_segs);
+  int32_t *cmap = S.take<int32_t>(A.c.n_cmap);
+  double *wpos = S.take<double>(3 * N);
+  double *shift = S.take<double>(3 * nimg);
+  uint8_t *typ = S.take<uint8_t>(N);
+  double *erow = S.take<double>(A.D);
+  double *lrow = S.take<double>(A.D);
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
+    seg[k] = A.seg_a[k];
+    segws[k] = A.seg_ws[k];
+  }
+  for (int k = threadIdx.x; k < A.c.n_segs * 4 * kWin; k += blockDim.x) segg[k] = A.seg_g[k];
+  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
+  for (int k = threadIdx.x; k < A.D; k += blockDim.x) erow[k] = lrow[k] = 0.0;
+  stage_geometry(cd, A.c, wpos, shift, typ);
+  __syncthreads();
+  const int32_t *start = A.c.nb_start + cd.atom0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int64_t ga = static_cast<int64_t>(cd.atom0) + i;
+    T *dr = A.drho + ga * A.ndens;
+    for (int m = 0; m < A.ndens; ++m) dr[m] = T(0);
+    T rho = T(0);
+    for (int p = start[i]; p < start[i + 1]; ++p) {
+      int j;
+      T dx, dy, dz;
+      pair_vec(wpos, shift, i, A.c.nb_pack[p], j, dx, dy, dz);
+      const T r = sqrt_t(dx * dx + dy * dy + dz * dz);
+      const STab<T> &tb = tabs[np + typ[j]];
+      if (!in_span(tb, r)) continue;
+      T t;
+      const int e = seg_of(tb, r, t);
+      rho += seg_val<T>(seg[e], t);
+      const int ws = segws[e];
+      const T *G = segg + e * 4 * kWin;
+      for (int q = 0; q < kWin && ws + q < tb.n; ++q) {
+        const int col = cmap[tb.cmap0 + ws + q];
+        if (col < 0) continue;
+        dr[col - A.dens_c0] += G[q] + t * (G[kWin + q] + t * (G[2 * kWin + q] + t * G[3 * kWin + q]));
+      }
+    }
+    const int ti = typ[i];
+    const STab<T> &te = tabs[np + nt + ti];
+    T rb = rho;
+    double over = 0.0;
+    if (rb > te.xmax) {
+      over = 2.0 * 100.0 * 10.0 * (static_cast<double>(rb) - static_cast<double>(te.xmax));
+      rb = te.xmax;
+    } else if (rb < te.x0) {
+      over = -2.0 * 100.0 * 10.0 * (static_cast<double>(te.x0) - static_cast<double>(rb));
+      rb = te.x0;
+    }
+    T t;
+    const int e = seg_of(te, rb, t);
+    const T gF = seg_der<T>(seg[e], t, te.inv_h);
+    const T cF = seg_der2<T>(seg[e], t, te.inv_h);
+    T *sc = A.scal + 4 * ga;
+    sc[0] = gF;
+    sc[1] = cF;
+    sc[2] = static_cast<T>(over);
+    sc[3] = T(0);
+    const int ws = segws[e];
+    A.wsF[ga] = ws;
+    const T *G = segg + e * 4 * kWin;
+    for (int q = 0; q < kWin; ++q) {
+      const bool ok = ws + q < te.n;
+      const T dv = G[q] + t * (G[kWin + q] + t * (G[2 * kWin + q] + t * G[3 * kWin + q]));
+      const T dd = (G[kWin + q] + t * (T(2) * G[2 * kWin + q] + T(3) * t * G[3 * kWin + q])) * te.inv_h;
+      A.dgd[ga * kWin + q] = ok ? dd : T(0);
+      if (!ok) continue;
+      const int col = cmap[te.cmap0 + ws + q];
+      if (col >= 0) atomicAdd(&erow[col], A.w_e * static_cast<double>(dv));
+    }
+    for (int m = 0; m < A.ndens; ++m) {
+      const double dv = static_cast<double>(dr[m]);
+      if (dv == 0.0) continue;
+      if (over != 0.0)
+        atomicAdd(&lrow[A.dens_c0 + m], over * dv);
+      else
+        atomicAdd(&erow[A.dens_c0 + m], A.w_e * static_cast<double>(gF) * dv);
+    }
+    if (over != 0.0)
+      for (int m = 0; m < A.ndens; ++m) dr[m] = T(0);
+  }
+  __syncthreads();
+  const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
+  const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
+  const int64_t rE = row0 + 3 * N, rL = rE + 1 + (A.w_s > 0.0 ? 6 : 0);
+  for (int col = threadIdx.x; col < A.D; col += blockDim.x) {
+    A.J[col * A.M + rE] = static_cast<T>(erow[col]);
+    A.J[col * A.M + rL] = static_cast<T>(lrow[col]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobian, kernel 2: force rows of every atom and the stress rows
+// (eam_force.cpp:212-278 / pair_force.cpp:89-110, add_force_column and
+// add_radial_bond of include/forcesmith/force/param_jacobian.hpp:91-122).
+//
+// A warp owns an atom i.  Per chunk of ≤ 32 neighbours the lanes build pair
+// records; then, pair by pair, 24 lanes scatter the knot-window terms
+//   φ'       (col window of φ_{t_i t_j})         weight 1
+//   ρ'_{tj}  (window of ρ_{t_j})                 weight F'_i
+//   ρ'_{ti}  (window of ρ_{t_i})                 weight F'_j
+//   F'_j     (embedding window of j)             weight ρ'_{t_i}(r)
+// into the warp's row buffer (distinct columns per pair, no atomics), and
+// every lane adds the dense ρ-chain term Σ_j F''_j ρ'_{t_i}(r) u drho_j for
+// the density columns it owns.  The stress rows use the pair symmetry of the
+// full list for the chain terms: Σ_pairs v (F''_i drho_i ρ'_{tj} + F''_j
+// drho_j ρ'_{ti}) = 2 Σ_i P_i F''_i drho_i with P_i = Σ_j v_ij ρ'_{tj}(r_ij).
+// ---------------------------------------------------------------------------
+template <class T> struct PairRec {
+  T u[3], v[6];
+  T tphi, trj, tri;
+  T dgj, dgi;      // ρ'_{tj}(r), ρ'_{ti}(r) (gated)
+  T gFj, cFj;      // F'_j, F''_j
+  int ephi, erj, eri; // extended segment (−1: gated out)
+  int j, tj, wsj;
+};
+
+template <class T, bool EAM>
+__global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps) {
+  using T4 = typename Vec4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x;
+  const CfgDev &cd = A.c.cfg[c];
+  const int N = cd.natoms;
+  const int D = A.D;
+  const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
+  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  Smem S(smem_raw);
+  STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
+  T4 *seg = S.take<T4>(A.c.n_segs);
+  T *segg = S.take<T>(A.c.n_segs * 4 * kWin);
+  int32_t *segws = S.take<int32_t>(A.c.n_segs);
+  int32_t *cmap = S.take<int32_t>(A.c.n_cmap);
+  double *wpos = S.take<double>(3 * N);
+  double *shift = S.take<double>(3 * nimg);
+  uint8_t *typ = S.take<uint8_t>(N);
+  T *rowb = S.take<T>(static_cast<size_t>(warps) * 10 * D); // per warp: 3 force + 6 stress + 1 energy
+  PairRec<T> *recs = S.take<PairRec<T>>(static_cast<size_t>(warps) * 32);
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
+    seg[k] = A.seg_a[k];
+    segws[k] = A.seg_ws[k];
+  }
+  for (int k = threadIdx.x; k < A.c.n_segs * 4 * kWin; k += blockDim.x) segg[k] = A.seg_g[k];
+  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
+  for (int k = threadIdx.x; k < warps * 10 * D; k += blockDim.x) rowb[k] = T(0);
+  stage_geometry(cd, A.c, wpos, shift, typ);
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  T *frow = rowb + static_cast<size_t>(w) * 10 * D; // [3][D]
+  T *srow = frow + 3 * D;                            // [6][D] (accumulated over the warp's atoms)
+  T *erow = frow + 9 * D;                            // [D]    (φ energy part)
+  PairRec<T> *rec = recs + w * 32;
+  const int32_t *start = A.c.nb_start + cd.atom0;
+  const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
+  const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
+  const T half_we = static_cast<T>(0.5 * A.w_e);
+  const bool want_stress = A.w_s > 0.0;
+
+  for (int i = w; i < N; i += warps) {
+    for (int k = lane; k < 3 * D; k += 32) frow[k] = T(0);
+    const int ti = typ[i];
+    const int64_t gi = static_cast<int64_t>(cd.atom0) + i;
+    T gFi = T(0), cFi = T(0);
+    int wsFi = 0;
+    if constexpr (EAM) {
+      gFi = A.scal[4 * gi];
+      cFi = A.scal[4 * gi + 1];
+      wsFi = A.wsF[gi];
+    }
+    T V[3] = {0, 0, 0}, P[6] = {0, 0, 0, 0, 0, 0};
+    T dacc[2][3] = {{0, 0, 0}, {0, 0, 0}}; // dense ρ-chain, columns m = lane, lane + 32
+    __syncwarp();
+    for (int p0 = start[i]; p0 < start[i + 1]; p0 += 32) {
+      const int cnt = min(32, start[i + 1] - p0);
+      if (lane < cnt) {
+        PairRec<T> R;
+        int j;
+        T d[3];
+        pair_vec(wpos, shift, i, A.c.nb_pack[p0 + lane], j, d[0], d[1], d[2]);
+        const T r = sqrt_t(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        const int tj = typ[j];
+        R.j = j;
+        R.tj = tj;
+        R.ephi = R.erj = R.eri = -1;
+        R.dgj = R.dgi = R.gFj = R.cFj = T(0);
+        R.wsj = 0;
+        R.tphi = R.trj = R.tri = T(0);
+        if (r >= T(1e-14)) {
+          const T ir = T(1) / r;
+          for (int a = 0; a < 3; ++a) R.u[a] = d[a] * ir;
+          R.v[0] = d[0] * d[0] * ir;
+          R.v[1] = d[1] * d[1] * ir;
+          R.v[2] = d[2] * d[2] * ir;
+          R.v[3] = d[0] * d[1] * ir;
+          R.v[4] = d[0] * d[2] * ir;
+          R.v[5] = d[1] * d[2] * ir;
+          const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
+          const bool phi_in = EAM ? in_span(tp, r) : (r >= tp.x0 && r < tp.xmax);
+          if (phi_in) R.ephi = seg_of(tp, r, R.tphi);
+          if constexpr (EAM) {
+            const STab<T> &gj = tabs[np + tj], &gi_ = tabs[np + ti];
+            if (in_span(gj, r)) {
+              R.erj = seg_of(gj, r, R.trj);
+              R.dgj = seg_der<T>(seg[R.erj], R.trj, gj.inv_h);
+            }
+            if (in_span(gi_, r)) {
+              R.eri = seg_of(gi_, r, R.tri);
+              R.dgi = seg_der<T>(seg[R.eri], R.tri, gi_.inv_h);
+            }
+            const int64_t gj_ = static_cast<int64_t>(cd.atom0) + j;
+            R.gFj = A.scal[4 * gj_];
+            R.cFj = A.scal[4 * gj_ + 1];
+            R.wsj = A.wsF[gj_];
+          }
+        } else {
+          for (int a = 0; a < 3; ++a) R.u[a] = T(0);
+          for (int a = 0; a < 6; ++a) R.v[a] = T(0);
+        }
+        rec[lane] = R;
+        for (int a = 0; a < 3; ++a) V[a] += R.dgj * R.u[a];
+        for (int a = 0; a < 6; ++a) P[a] += R.dgj * R.v[a];
+      }
+      __syncwarp();
+      // sparse knot-window scatter, one pair at a time
+      const int slot = lane / kWin, q = lane % kWin;
+      for (int k = 0; k < cnt; ++k) {
+        const PairRec<T> &R = rec[k];
+        if (lane < 4 * kWin) {
+          int e = -1, tab = -1, col = -1;
+          T tt = T(0), weight = T(0), ih = T(0);
+          bool stress = true, energy = false;
+          if (slot == 0) {
+            e = R.ephi;
+            tab = pair_ord(ti, R.tj, nt);
+            tt = R.tphi;
+            weight = T(1);
+            energy = true;
+          } else if (EAM && slot == 1) {
+            e = R.erj;
+            tab = np + R.tj;
+            tt = R.trj;
+            weight = (R.tj == ti) ? gFi + R.gFj : gFi;
+          } else if (EAM && slot == 2) {
+            e = (R.tj == ti) ? -1 : R.eri;
+            tab = np + ti;
+            tt = R.tri;
+            weight = R.gFj;
+          } else if (EAM && slot == 3) {
+            const STab<T> &te = tabs[np + nt + R.tj];
+            const int knot = R.wsj + q;
+            if (knot < te.n) col = cmap[te.cmap0 + knot];
+            const T cf = A.dgd[(static_cast<int64_t>(cd.atom0) + R.j) * kWin + q] * R.dgi;
+            if (col >= 0 && cf != T(0)) {
+              for (int a = 0; a < 3; ++a) frow[a * D + col] += cf * R.u[a];
+            }
+            stress = false;
+          }
+          if (slot < 3 && e >= 0) {
+            const STab<T> &tb = tabs[tab];
+            ih = tb.inv_h;
+            const int knot = segws[e] + q;
+            if (knot < tb.n) col = cmap[tb.cmap0 + knot];
+            if (col >= 0) {
+              const T *G = segg + e * 4 * kWin;
+              const T dd = (G[kWin + q] + tt * (T(2) * G[2 * kWin + q] + T(3) * tt * G[3 * kWin + q])) * ih;
+              const T cf = weight * dd;
+              for (int a = 0; a < 3; ++a) frow[a * D + col] += cf * R.u[a];
+              if (stress && want_stress)
+                for (int a = 0; a < 6; ++a) srow[a * D + col] += cf * R.v[a];
+              if (energy) {
+                const T dv = G[q] + tt * (G[kWin + q] + tt * (G[2 * kWin + q] + tt * G[3 * kWin + q]));
+                erow[col] += half_we * dv;
+              }
+            }
+          }
+        }
+        __syncwarp();
+      }
+      if constexpr (EAM) {
+        // dense ρ-chain: Σ_j F''_j ρ'_{ti}(r) u drho_j[m]
+        for (int k = 0; k < cnt; ++k) {
+          const PairRec<T> &R = rec[k];
+          const T wgt = R.cFj * R.dgi;
+          if (wgt == T(0)) continue;
+          const T *drj = A.drho + (static_cast<int64_t>(cd.atom0) + R.j) * A.ndens;
+          for (int s2 = 0; s2 < 2; ++s2) {
+            const int m = lane + 32 * s2;
+            if (m < A.ndens) {
+              const T dv = wgt * drj[m];
+              for (int a = 0; a < 3; ++a) dacc[s2][a] += dv * R.u[a];
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+    for (int a = 0; a < 3; ++a) V[a] = warp_sum_group(V[a], 32);
+    for (int a = 0; a < 6; ++a) P[a] = warp_sum_group(P[a], 32);
+    if constexpr (EAM) {
+      const T *dri = A.drho + gi * A.ndens;
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const int m = lane + 32 * s2;
+        if (m < A.ndens) {
+          const T gim = cFi * dri[m];
+          const int col = A.dens_c0 + m;
+          for (int a = 0; a < 3; ++a) frow[a * D + col] += dacc[s2][a] + gim * V[a];
+          if (want_stress)
+            for (int a = 0; a < 6; ++a) srow[a * D + col] += T(2) * P[a] * gim;
+        }
+      }
+      if (lane < kWin) {
+        const STab<T> &te = tabs[np + nt + ti];
+        const int knot = wsFi + lane;
+        const int col = knot < te.n ? cmap[te.cmap0 + knot] : -1;
+        const T dg = A.dgd[gi * kWin + lane];
+        if (col >= 0 && dg != T(0)) {
+          for (int a = 0; a < 3; ++a) frow[a * D + col] += dg * V[a];
+          if (want_stress)
+            for (int a = 0; a < 6; ++a) srow[a * D + col] += T(2) * P[a] * dg;
+        }
+      }
+    }
+    __syncwarp();
+    for (int col = lane; col < D; col += 32) {
+      T *Jc = A.J + static_cast<int64_t>(col) * A.M + row0 + 3 * i;
+      Jc[0] = frow[col];
+      Jc[1] = frow[D + col];
+      Jc[2] = frow[2 * D + col];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  const int64_t rE = row0 + 3 * N;
+  const double sc = -A.w_s * 0.5 / cd.volume;
+  for (int col = threadIdx.x; col < D; col += blockDim.x) {
+    double e = 0.0;
+    for (int ww = 0; ww < warps; ++ww) e += static_cast<double>(rowb[static_cast<size_t>(ww) * 10 * D + 9 * D + col]);
+    T *Jc = A.J + static_cast<int64_t>(col) * A.M;
+    if constexpr (EAM)
+      Jc[rE] = static_cast<T>(static_cast<double>(Jc[rE]) + e);
+    else
+      Jc[rE] = static_cast<T>(e);
+    if (want_stress) {
+      for (int v = 0; v < 6; ++v) {
+        double s = 0.0;
+        for (int ww = 0; ww < warps; ++ww) s += static_cast<double>(rowb[static_cast<size_t>(ww) * 10 * D + (3 + v) * D + col]);
+        Jc[rE + 1 + v] = static_cast<T>(sc * s);
+      }
+    }
+    if constexpr (!EAM) Jc[rE + 1 + (want_stress ? 6 : 0)] = T(0); // limit row: no embedding
+  }
+}
+
+template <class T> Common make_common(fs_gpu *h) {
+  Common c;
+  c.cfg = h->d_cfg;
+  c.wpos = h->d_wpos;
+  c.type = h->d_type;
+  c.ref_force = h->d_ref_force;
+  c.nb_start = h->d_nb_start;
+  c.nb_pack = h->d_nb_pack;
+  c.desc = h->d_desc;
+  c.cmap = h->d_cmap;
+  c.n_tables = static_cast<int>(h->desc.size());
+  c.n_segs = h->n_segs;
+  c.n_cmap = h->n_cmap;
+  c.ntypes = h->ntypes;
+  c.family = h->family;
+  return c;
+}
+
+int max_images(const fs_gpu *h) {
+  int m = 1;
+  for (const CfgDev &cd : h->cfg_host) m = std::max(m, (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1));
+  return m;
+}
+
+int choose_lpa(const fs_gpu *h) {
+  if (h->lanes_per_atom) return h->lanes_per_atom;
+  const double avg = h->n_atoms ? static_cast<double>(h->n_pairs) / h->n_atoms : 0.0;
+  if (avg > 24) return 16;
+  if (avg > 10) return 8;
+  return 4;
+}
+
+template <class T, int LPA, bool EAM> int launch_residual_t(fs_gpu *h, double w_e, double w_s) {
+  using T4 = typename Vec4T<T>::type;
+  ResArgs<T> a;
+  a.c = make_common<T>(h);
+  a.seg_a = static_cast<const T4 *>(h->d_seg_a);
+  a.w_e = w_e;
+  a.w_s = w_s;
+  a.F = h->d_F;
+  a.forces = h->d_forces;
+  a.energy = h->d_energy;
+  a.stress9 = h->d_stress9;
+  a.limit = h->d_limit;
+  a.obj_part = h->d_obj_part;
+  const size_t sm = residual_smem<T>(a.c.n_tables, h->n_segs, h->max_natoms, max_images(h));
+  if (sm > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "residual: configuration too large for shared memory");
+  auto k = residual_kernel<T, LPA, EAM>;
+  FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+  k<<<h->n_cfg, 256, sm, h->stream>>>(a);
+  FS_CUDA(cudaGetLastError());
+  sum_kernel<<<1, 1024, 0, h->stream>>>(h->d_obj_part, h->n_cfg, h->d_obj);
+  FS_CUDA(cudaGetLastError());
+  h->launches += 2;
+  return FS_OK;
+}
+
+template <class T, bool EAM> int launch_residual_lpa(fs_gpu *h, double w_e, double w_s) {
+  switch (choose_lpa(h)) {
+  case 4: return launch_residual_t<T, 4, EAM>(h, w_e, w_s);
+  case 8: return launch_residual_t<T, 8, EAM>(h, w_e, w_s);
+  case 16: return launch_residual_t<T, 16, EAM>(h, w_e, w_s);
+  default: return launch_residual_t<T, 32, EAM>(h, w_e, w_s);
+  }
+}
+
+template <class X> int grow(fs_gpu *h, X **p, size_t n, size_t &have) {
+  if (have >= n && *p) return FS_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(n, 1) * sizeof(X)) != cudaSuccess)
+    return set_error(h, FS_ERR_NOMEM, "cudaMalloc (Jacobian)");
+  have = n;
+  return FS_OK;
+}
+
+template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
+  using T4 = typename Vec4T<T>::type;
+  const bool eam = h->family == FS_FAMILY_EAM;
+  const int64_t M = rows_of(h, w_s);
+  const int D = h->D;
+  // buffers
+  const size_t jn = static_cast<size_t>(M) * D;
+  if (static_cast<size_t>(h->jac_alloc) < jn || !h->d_J) {
+    if (h->d_J) cudaFree(h->d_J);
+    h->d_J = nullptr;
+    if (cudaMalloc(&h->d_J, std::max<size_t>(jn, 1) * sizeof(T)) != cudaSuccess)
+      return set_error(h, FS_ERR_NOMEM, "cudaMalloc (J)");
+    h->jac_alloc = static_cast<int64_t>(jn);
+  }
+  if (!h->d_JtJ) {
+    FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
+    FS_CUDA(cudaMalloc(&h->d_Jtr, std::max(D, 1) * sizeof(double)));
+  }
+  // density columns: tables [np, np+nt) are contiguous in the column space
+  const int nt = h->ntypes, np = npair_of(nt);
+  int dens_c0 = 0, ndens = 0;
+  if (eam) {
+    int lo = 1 << 30, hi = -1;
+    for (int t = np; t < np + nt; ++t)
+      for (int col : h->tables[t].cols)
+        if (col >= 0) {
+          lo = std::min(lo, col);
+          hi = std::max(hi, col);
+        }
+    if (hi >= 0) {
+      dens_c0 = lo;
+      ndens = hi - lo + 1;
+    }
+    if (ndens > 64) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: more than 64 free density knots");
+    const size_t na = static_cast<size_t>(h->n_atoms);
+    if (static_cast<size_t>(h->atom_scratch_alloc) < na || !h->d_atom_scalars) {
+      size_t dummy = 0;
+      if (h->d_atom_scalars) cudaFree(h->d_atom_scalars);
+      if (h->d_drho) cudaFree(h->d_drho);
+      if (h->d_dgd) cudaFree(h->d_dgd);
+      if (h->d_wsF) cudaFree(h->d_wsF);
+      h->d_atom_scalars = h->d_drho = h->d_dgd = nullptr;
+      h->d_wsF = nullptr;
+      FS_TRY(grow(h, reinterpret_cast<T **>(&h->d_atom_scalars), 4 * na, dummy));
+      dummy = 0;
+      FS_TRY(grow(h, reinterpret_cast<T **>(&h->d_drho), 64 * na, dummy));
+      dummy = 0;
+      FS_TRY(grow(h, reinterpret_cast<T **>(&h->d_dgd), kWin * na, dummy));
+      dummy = 0;
+      FS_TRY(grow(h, &h->d_wsF, na, dummy));
+      h->atom_scratch_alloc = static_cast<int64_t>(na);
+    }
+  }
+  JacArgs<T> a;
+  a.c = make_common<T>(h);
+  a.seg_a = static_cast<const T4 *>(h->d_seg_a);
+  a.seg_g = static_cast<const T *>(h->d_seg_g);
+  a.seg_ws = h->d_seg_ws;
+  a.w_e = w_e;
+  a.w_s = w_s;
+  a.M = M;
+  a.D = D;
+  a.dens_c0 = dens_c0;
+  a.ndens = ndens;
+  a.J = static_cast<T *>(h->d_J);
+  a.scal = static_cast<T *>(h->d_atom_scalars);
+  a.drho = static_cast<T *>(h->d_drho);
+  a.dgd = static_cast<T *>(h->d_dgd);
+  a.wsF = h->d_wsF;
+  const size_t common = jac_common_smem<T>(a.c.n_tables, h->n_segs, h->n_cmap, h->max_natoms, max_images(h));
+  if (eam) {
+    const size_t sm1 = common + align16(2 * D * sizeof(double)) + 32;
+    if (sm1 > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: configuration too large");
+    FS_CUDA(cudaFuncSetAttribute(jac_atoms_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sm1)));
+    jac_atoms_kernel<T><<<h->n_cfg, 256, sm1, h->stream>>>(a);
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+  }
+  mark(h, 2);
+  int warps = 8;
+  size_t sm2 = 0;
+  for (; warps >= 1; warps >>= 1) {
+    sm2 = common + align16(static_cast<size_t>(warps) * 10 * D * sizeof(T)) +
+          align16(static_cast<size_t>(warps) * 32 * sizeof(PairRec<T>)) + 64;
+    if (sm2 <= 227 * 1024) break;
+  }
+  if (warps < 1) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: configuration too large");
+  auto k2 = eam ? jac_forces_kernel<T, true> : jac_forces_kernel<T, false>;
+  FS_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm2)));
+  k2<<<h->n_cfg, 32 * warps, sm2, h->stream>>>(a, warps);
+  FS_CUDA(cudaGetLastError());
+  ++h->launches;
+  mark(h, 3);
+  return FS_OK;
+}
+
+} // namespace
+
+int eval_residual(fs_gpu *h, double w_e, double w_s) {
+  if (h->family != FS_FAMILY_EAM && h->family != FS_FAMILY_PAIR) {
+    extern int eval_residual_other(fs_gpu * h, double w_e, double w_s);
+    return eval_residual_other(h, w_e, w_s);
+  }
+  const bool eam = h->family == FS_FAMILY_EAM;
+  if (h->precision == FS_PREC_FP64)
+    return eam ? launch_residual_lpa<double, true>(h, w_e, w_s) : launch_residual_lpa<double, false>(h, w_e, w_s);
+  return eam ? launch_residual_lpa<float, true>(h, w_e, w_s) : launch_residual_lpa<float, false>(h, w_e, w_s);
+}
+
+int eval_jacobian(fs_gpu *h, double w_e, double w_s) {
+  if (h->family != FS_FAMILY_EAM && h->family != FS_FAMILY_PAIR) {
+    extern int eval_jacobian_other(fs_gpu * h, double w_e, double w_s);
+    return eval_jacobian_other(h, w_e, w_s);
+  }
+  return h->precision == FS_PREC_FP64 ? launch_jacobian_t<double>(h, w_e, w_s)
+                                      : launch_jacobian_t<float>(h, w_e, w_s);
+}
+
+} // namespace fsg

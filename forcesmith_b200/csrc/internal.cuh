@@ -1,0 +1,221 @@
+// Internal declarations shared by the translation units of
+// libforcesmith_b200.so (the fs_gpu context, device table layout, launchers).
+#pragma once
+
+#include "forcesmith_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+namespace fsg {
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+struct Status {
+  int code = FS_OK;
+  std::string msg;
+};
+
+#define FS_CUDA(call)                                                          \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(e_);             \
+      return FS_ERR_CUDA;                                                      \
+    }                                                                          \
+  } while (0)
+
+#define FS_TRY(expr)                                                           \
+  do {                                                                         \
+    int rc_ = (expr);                                                          \
+    if (rc_ != FS_OK) return rc_;                                              \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Device table layout.
+//
+// A spline of n knots is stored as n+1 "extended segments": e = 0 is the
+// linear extrapolation below x0, e = 1..n-1 the interior cubic (or linear,
+// n < 4) pieces, e = n the linear extrapolation above x_{n-1}.  Segment e
+// holds the power-basis coefficients a[0..3] in t = (r - origin_e)/h, the
+// knot-derivative block G[4][6] = ∂a_k/∂y_{ws+q}, and its window start ws.
+// ---------------------------------------------------------------------------
+constexpr int kWin = 6;      // knots a segment depends on (makima: 6)
+constexpr int kMaxTables = 64;
+constexpr int kMaxSegs = 4096;
+
+struct TableDesc {
+  int kind;    // fs_table_kind
+  int form;    // fs_form (analytic)
+  int n;       // knots / parameters
+  int seg0;    // first extended segment (splines)
+  int cmap0;   // first entry of the knot/param → column map
+  int pv0;     // first value in the parameter-value array
+  int pad0, pad1;
+  double x0, h, inv_h, xmax; // spline grid (x0, spacing, 1/h, last knot)
+  double rmin, rmax;         // gate span
+};
+
+// Per-config geometry on the device.
+struct CfgDev {
+  int atom0;      // first atom (global)
+  int natoms;
+  int pair0;      // first pair (global) of the config
+  int sx, sy, sz; // image shells
+  double box[9];  // row-major, lattice vectors as columns
+  double inv[9];
+  double volume;
+  double ref_energy;
+  double ref_stress[9];
+};
+
+// ---------------------------------------------------------------------------
+// The context behind the opaque fs_gpu handle.
+// ---------------------------------------------------------------------------
+template <class X> struct DBuf {
+  X *p = nullptr;
+  size_t n = 0;
+};
+
+struct HostTable {
+  int kind = 0, form = 0, n = 0;
+  double rmin = 0, rmax = 0;
+  std::vector<double> v, lo, hi;
+  std::vector<uint8_t> fixed;
+  std::vector<int> cols; // column per value (-1 if fixed)
+};
+
+} // namespace fsg
+
+struct fs_gpu {
+  int device = 0;
+  int precision = FS_PREC_FP32;
+  int lanes_per_atom = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // configs (host)
+  int n_cfg = 0;
+  int64_t n_atoms = 0;
+  int max_natoms = 0;
+  std::vector<int32_t> natoms;
+  std::vector<int64_t> atom0;
+  std::vector<fsg::CfgDev> cfg_host;
+  // configs (device)
+  fsg::CfgDev *d_cfg = nullptr;
+  double *d_pos = nullptr;       // raw positions, 3 per atom
+  double *d_wpos = nullptr;      // wrapped positions, 3 per atom
+  int32_t *d_type = nullptr;
+  double *d_ref_force = nullptr; // 3 per atom
+
+  // neighbours
+  double rcut_built = -1.0;
+  int64_t n_pairs = 0;
+  int32_t *d_nb_start = nullptr; // n_atoms + 1 (global pair offsets)
+  uint32_t *d_nb_pack = nullptr; // j_local (20 bits) | image index (12 bits)
+  int32_t *d_nb_count = nullptr; // per atom
+
+  // model
+  bool have_model = false;
+  int family = 0, ntypes = 1;
+  std::vector<fsg::HostTable> tables;
+  int D = 0;                // free parameters
+  std::vector<fsg::TableDesc> desc;
+  int n_segs = 0, n_cmap = 0, n_vals = 0;
+  fsg::TableDesc *d_desc = nullptr;
+  int32_t *d_cmap = nullptr;     // knot/param → column (-1 fixed)
+  double *d_vals = nullptr;      // all table values (FP64, current params)
+  // segment tables in the working precision (FP32 or FP64)
+  void *d_seg_a = nullptr;       // [n_segs][4]
+  void *d_seg_g = nullptr;       // [n_segs][4][kWin]
+  int32_t *d_seg_ws = nullptr;   // [n_segs]
+  double *d_x = nullptr;         // current parameter vector (D)
+  bool params_dirty = true;
+
+  // evaluation buffers
+  int64_t rows_alloc = 0;
+  double *d_F = nullptr;         // residual (rows)
+  double *d_forces = nullptr;    // 3 per atom
+  double *d_energy = nullptr, *d_stress9 = nullptr, *d_limit = nullptr;
+  double *d_obj_part = nullptr;  // per config
+  double *d_obj = nullptr;       // scalar
+  // Jacobian buffers
+  int64_t jac_alloc = 0;         // elements of J
+  void *d_J = nullptr;           // column-major rows × D, FP32 or FP64
+  double *d_JtJ = nullptr;       // D × D
+  double *d_Jtr = nullptr;       // D
+  double *d_gram_part = nullptr; // split partials
+  size_t gram_part_alloc = 0;
+  // per-atom Jacobian scratch
+  void *d_atom_scalars = nullptr; // [n_atoms][4]: gradF, curvF, (ws as float), over
+  void *d_drho = nullptr;         // [n_atoms][ndens]
+  void *d_dgd = nullptr;          // [n_atoms][kWin]
+  int32_t *d_wsF = nullptr;       // [n_atoms]
+  int64_t atom_scratch_alloc = 0;
+  double last_ws = -1.0, last_we = 0.0;
+  bool jac_valid = false;
+
+  // LM solve scratch
+  double *d_chol = nullptr;
+  double *d_dx = nullptr;
+  int32_t *d_flag = nullptr;
+
+  // live per-phase timing (CUDA events on `stream`) and kernel launch count
+  std::vector<cudaEvent_t> prof_ev; // prof_slots × (kPhases + 1)
+  int prof_slots = 0, prof_used = 0;
+  int64_t launches = 0;
+
+  // population scratch
+  void *d_pop_seg_a = nullptr;
+  double *d_pop_vals = nullptr;
+  double *d_pop_obj = nullptr;
+  int pop_alloc = 0;
+};
+
+namespace fsg {
+
+int set_error(fs_gpu *h, int code, const std::string &m);
+
+// Phases of one residual + Jacobian evaluation, timed with CUDA events
+// when profiling is on: residual, per-atom Jacobian, force/stress rows,
+// normal-equation products.
+constexpr int kPhases = 4;
+enum { kPhResidual = 0, kPhJacAtoms = 1, kPhJacForces = 2, kPhGram = 3 };
+inline void mark(fs_gpu *h, int boundary) {
+  if (h->prof_slots > 0 && h->prof_used < h->prof_slots)
+    cudaEventRecord(h->prof_ev[h->prof_used * (kPhases + 1) + boundary], h->stream);
+}
+
+// neighbour.cu
+int build_neighbors(fs_gpu *h, double rcut);
+
+// tables.cu
+int upload_tables(fs_gpu *h);          // structure + values (after set_model)
+int refresh_segments(fs_gpu *h);       // recompute segment data from d_vals
+double model_max_cutoff(const fs_gpu *h);
+
+// eam.cu / pair
+int eval_residual(fs_gpu *h, double w_e, double w_s);
+int eval_jacobian(fs_gpu *h, double w_e, double w_s);
+
+// gram.cu
+int gram(fs_gpu *h, int64_t m, double *JtJ_dev, double *Jtr_dev);
+
+// solve.cu
+int lm_solve(fs_gpu *h, double lambda, int mode, double *dx_host);
+
+// population.cu
+int eval_population(fs_gpu *h, double w_e, double w_s, const double *xs, int NP, double *obj);
+
+inline int64_t rows_of(const fs_gpu *h, double w_s) {
+  return 3 * h->n_atoms + static_cast<int64_t>(h->n_cfg) * (2 + (w_s > 0.0 ? 6 : 0));
+}
+
+inline int npair_of(int nt) { return nt * (nt + 1) / 2; }
+
+} // namespace fsg

@@ -1,0 +1,182 @@
+"""ctypes binding of libforcesmith_b200.so (include/forcesmith_gpu.h).
+
+The device library is the only implementation behind this class: if the
+shared object is missing or no CUDA device is visible, construction raises —
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
+                  fs_model, load_library)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libforcesmith_b200.so")
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is not built; run `python -m forcesmith_b200.build` (nvcc, sm_100a)")
+        L = load_library(LIB_PATH)
+        vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        pd, pi = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+        L.fs_gpu_create.argtypes = [C.POINTER(fs_gpu_opts), C.POINTER(vp)]
+        L.fs_gpu_destroy.argtypes = [vp]
+        L.fs_gpu_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        L.fs_gpu_get_stream.argtypes = [vp, C.POINTER(vp)]
+        L.fs_gpu_upload_configs.argtypes = [vp, i32, pi, pd, pd, pi, pd, pd, pd]
+        L.fs_gpu_set_references.argtypes = [vp, pd, pd, pd]
+        L.fs_gpu_set_model.argtypes = [vp, C.POINTER(fs_model)]
+        L.fs_gpu_prepare.argtypes = [vp]
+        L.fs_gpu_num_pairs.argtypes = [vp, C.POINTER(i64)]
+        L.fs_gpu_get_neighbor_counts.argtypes = [vp, pi]
+        L.fs_gpu_get_neighbors.argtypes = [vp, pi, C.POINTER(C.c_int8)]
+        L.fs_gpu_param_count.argtypes = [vp, pi]
+        L.fs_gpu_gather_params.argtypes = [vp, pd]
+        L.fs_gpu_gather_bounds.argtypes = [vp, pd, pd]
+        L.fs_gpu_set_params.argtypes = [vp, pd, i32]
+        L.fs_gpu_residual_count.argtypes = [vp, dbl, C.POINTER(i64)]
+        L.fs_gpu_eval.argtypes = [vp, dbl, dbl, pd, pd, pd, pd, pd, pd]
+        L.fs_gpu_eval_jacobian.argtypes = [vp, dbl, dbl, pd, pd, pd, pd, pd]
+        L.fs_gpu_eval_jacobian_async.argtypes = [vp, dbl, dbl]
+        L.fs_gpu_fetch_normal_equations.argtypes = [vp, pd, pd, pd]
+        L.fs_gpu_lm_step.argtypes = [vp, dbl, i32, pd]
+        L.fs_gpu_lsq_step.argtypes = [vp, dbl, pd]
+        L.fs_gpu_eval_population.argtypes = [vp, dbl, dbl, pd, i32, pd]
+        _LIB = L
+    return _LIB
+
+
+def _err(h) -> str:
+    buf = C.create_string_buffer(512)
+    if h:
+        lib().fs_gpu_last_error(h, buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+class GpuSession(Session):
+    """One fs_gpu context (one device, one stream)."""
+
+    def __init__(self, device: int = 0, precision: str = "fp32", lanes_per_atom: int = 0):
+        L = lib()
+        opts = fs_gpu_opts(device, FS_PREC_FP64 if precision == "fp64" else FS_PREC_FP32,
+                           lanes_per_atom, 0)
+        h = C.c_void_p()
+        rc = L.fs_gpu_create(C.byref(opts), C.byref(h))
+        if rc != FS_OK:
+            raise FsError(rc, "fs_gpu_create (is a CUDA device visible?)")
+        super().__init__(L, "fs_gpu", h, err_fn=_err)
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fs_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self._lib.fs_gpu_get_stream(self._h, C.byref(s)), "get_stream")
+        return s.value or 0
+
+    def neighbors(self):
+        P = self.num_pairs()
+        j = np.zeros(P, np.int32)
+        img = np.zeros(3 * P, np.int8)
+        self._check(self._lib.fs_gpu_get_neighbors(self._h, _ip(j),
+                                                   img.ctypes.data_as(C.POINTER(C.c_int8))),
+                    "get_neighbors")
+        return j, img.reshape(-1, 3)
+
+    def jacobian(self, w_e=1.0, w_s=0.0, want_J=True):
+        m = self.residual_count(w_s)
+        D = self.D
+        F = np.zeros(m)
+        J = np.zeros((D, m)) if want_J else None  # column-major m × D
+        JtJ = np.zeros((D, D))
+        Jtr = np.zeros(D)
+        obj = C.c_double()
+        rc = self._lib.fs_gpu_eval_jacobian(self._h, w_e, w_s, _dp(F), _dp(J), _dp(JtJ), _dp(Jtr),
+                                            C.byref(obj))
+        self._check(rc, "eval_jacobian")
+        return dict(F=F, J=None if J is None else J.T, JtJ=JtJ, Jtr=Jtr, obj=obj.value)
+
+    def jacobian_async(self, w_e=1.0, w_s=0.0):
+        self._check(self._lib.fs_gpu_eval_jacobian_async(self._h, w_e, w_s), "eval_jacobian_async")
+
+    def normal_equations(self):
+        D = self.D
+        JtJ, Jtr, obj = np.zeros((D, D)), np.zeros(D), C.c_double()
+        self._check(self._lib.fs_gpu_fetch_normal_equations(self._h, _dp(JtJ), _dp(Jtr),
+                                                            C.byref(obj)), "fetch_normal_equations")
+        return JtJ, Jtr, obj.value
+
+    def lm_step(self, lam, mode=0):
+        dx = np.zeros(self.D)
+        self._check(self._lib.fs_gpu_lm_step(self._h, lam, mode, _dp(dx)), "lm_step")
+        return dx
+
+    def lsq_step(self, ridge=0.0):
+        dx = np.zeros(self.D)
+        self._check(self._lib.fs_gpu_lsq_step(self._h, ridge, _dp(dx)), "lsq_step")
+        return dx
+
+    def eval_population(self, xs, w_e=1.0, w_s=0.0):
+        xs = np.ascontiguousarray(xs, np.float64)
+        obj = np.zeros(xs.shape[0])
+        self._check(self._lib.fs_gpu_eval_population(self._h, w_e, w_s, _dp(xs), xs.shape[0],
+                                                     _dp(obj)), "eval_population")
+        return obj
+
+
+def _bind_instrumentation():
+    L = lib()
+    L.fs_gpu_set_profiling.argtypes = [C.c_void_p, C.c_int32]
+    L.fs_gpu_phase_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int32,
+                                     C.POINTER(C.c_int32)]
+    L.fs_gpu_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.fs_gpu_copy_normal_equations.argtypes = [C.c_void_p, C.c_void_p]
+
+
+PHASES = ("residual", "jac_atoms", "jac_forces", "gram")
+
+
+def set_profiling(sess: GpuSession, max_steps: int):
+    _bind_instrumentation()
+    sess._check(sess._lib.fs_gpu_set_profiling(sess._h, max_steps), "set_profiling")
+
+
+def phase_times(sess: GpuSession):
+    _bind_instrumentation()
+    ms = np.zeros(8)
+    steps = C.c_int32()
+    sess._check(sess._lib.fs_gpu_phase_times(sess._h, _dp(ms), 8, C.byref(steps)), "phase_times")
+    return dict(zip(PHASES, ms[:4].tolist())), steps.value
+
+
+def launch_count(sess: GpuSession) -> int:
+    _bind_instrumentation()
+    n = C.c_int64()
+    sess._check(sess._lib.fs_gpu_launch_count(sess._h, C.byref(n)), "launch_count")
+    return n.value
+
+
+def copy_normal_equations(sess: GpuSession, dst_ptr: int):
+    _bind_instrumentation()
+    sess._check(sess._lib.fs_gpu_copy_normal_equations(sess._h, C.c_void_p(dst_ptr)),
+                "copy_normal_equations")

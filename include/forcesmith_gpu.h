@@ -1,0 +1,244 @@
+/*
+ * forcesmith_gpu.h — C ABI of the B200 objective-evaluation path.
+ *
+ * This is the drop-in boundary between Forcesmith's C++ host code and the
+ * sm_100a kernels.  Every entry point is `extern "C"`, takes plain pointers
+ * and sizes, returns an int status (FS_OK == 0, negative on error) and never
+ * throws.  Host pointers are ordinary pageable or pinned memory; the library
+ * owns every device allocation behind the opaque `fs_gpu` handle.
+ *
+ * Each entry point replaces one interface of the reference's CPU path
+ * (paths are relative to the Forcesmith source tree):
+ *
+ *   fs_gpu_upload_configs      Forcesmith::add_configuration / the per-config
+ *                              `Configuration` data model
+ *                              (include/forcesmith/core/atom.hpp:38-100,
+ *                               src/io/config_reader.cpp:58-130)
+ *   fs_gpu_set_model           Forcesmith::seed_force_model + the calculator
+ *                              tables (include/forcesmith/api/forcesmith.hpp:125,
+ *                               include/forcesmith/force/eam_force.hpp:24-32,
+ *                               pair_force.hpp:27-29, adp_force.hpp:34-54,
+ *                               stiweb_force.hpp:19-62)
+ *   fs_gpu_prepare             CForceCalculator::prepare → build_all_neighbor_lists
+ *                              (src/core/neighbor_list.cpp:105-147,
+ *                               src/force/eam_force.cpp:281-296)
+ *   fs_gpu_get_neighbor_counts / fs_gpu_get_neighbors
+ *                              the integer neighbour sets of build_periodic
+ *                              (src/core/neighbor_list.cpp:59-92)
+ *   fs_gpu_param_count / fs_gpu_gather_params / fs_gpu_gather_bounds /
+ *   fs_gpu_set_params          CFittable param_count / gather_params /
+ *                              gather_bounds / scatter_params, table order
+ *                              (include/forcesmith/force/force_calculator_concept.hpp:171-208,
+ *                               src/force/stiweb_force.cpp:169-195,
+ *                               src/potentials/spline.cpp:191-203)
+ *   fs_gpu_residual_count      opt::count_residuals
+ *                              (include/forcesmith/optimization/residual_layout.hpp:18-31)
+ *   fs_gpu_eval                ForcesmithFunctor::operator() → eval_into:
+ *                              scatter + eval_forces per config + write_config_residuals
+ *                              (src/optimization/forcesmith_functor.cpp:35-57,221-231)
+ *                              and force::evaluate / Forcesmith::evaluate_all
+ *                              (src/force/evaluate.cpp:5-20, src/api/forcesmith.cpp:587-614)
+ *   fs_gpu_eval_jacobian       ForcesmithFunctor::df (src/optimization/forcesmith_functor.cpp:252-292)
+ *                              — the analytic chain rule of write_param_jacobian
+ *                              (src/force/eam_force.cpp:108-279, pair_force.cpp:80-111)
+ *                              extended to spline knots, in place of opt::fd_jacobian
+ *                              (include/forcesmith/optimization/fd_jacobian.hpp:37-49);
+ *                              plus the JᵀJ / Jᵀr products that
+ *                              NormalEquationsSolver and LM consume
+ *                              (src/optimization/solver.cpp:242-266)
+ *   fs_gpu_lm_step / fs_gpu_lsq_step
+ *                              the LM / lsq step of EigenLMSolver and
+ *                              NormalEquationsSolver (src/optimization/solver.cpp:67-85,242-266)
+ *   fs_gpu_de_*                BoostDESolver's population evaluation
+ *                              (src/optimization/solver.cpp:113-155)
+ *   fs_gpu_surrogate_*         (no reference counterpart: the learned
+ *                              pre-screen of DE trial vectors)
+ */
+#ifndef FORCESMITH_GPU_H
+#define FORCESMITH_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  FS_OK = 0,
+  FS_ERR_ARG = -1,         /* bad argument (null handle, size mismatch …)   */
+  FS_ERR_CUDA = -2,        /* a CUDA runtime call failed                    */
+  FS_ERR_STATE = -3,       /* call out of order (no configs / no model …)   */
+  FS_ERR_UNSUPPORTED = -4, /* valid input this build does not handle        */
+  FS_ERR_NOMEM = -5,       /* device allocation failed                      */
+  FS_ERR_DEVICE = -6,      /* a kernel reported an error word               */
+  FS_ERR_NUMERIC = -7      /* non-finite result / failed factorisation      */
+};
+
+/* ---- model description ------------------------------------------------- */
+enum fs_family {
+  FS_FAMILY_PAIR = 0, /* tables: pair[npair]                                */
+  FS_FAMILY_EAM = 1,  /* tables: pair[npair], density[nt], embedding[nt]    */
+  FS_FAMILY_ADP = 2,  /* tables: EAM + dipole[npair], quadrupole[npair]     */
+  FS_FAMILY_SW = 3    /* tables: sw[npair] (8 params each), lambda[1]       */
+};
+
+enum fs_table_kind {
+  FS_TABLE_SPLINE = 0,   /* uniform-grid makima spline: n knot values       */
+  FS_TABLE_ANALYTIC = 1, /* closed form `form` with n parameters            */
+  FS_TABLE_SW = 2,       /* SWParams {A,B,p,q,delta,a1,gamma,a2}, n == 8    */
+  FS_TABLE_LAMBDA = 3    /* SW triplet strengths, n == nt * npair           */
+};
+
+/* Analytic radial forms (include/forcesmith/potentials/analytic_potential.hpp). */
+enum fs_form {
+  FS_FORM_LJ = 0,          /* 4ε((σ/r)^12 − (σ/r)^6)             {eps,sigma} */
+  FS_FORM_MORSE = 1,       /* De(1−e^{−a(r−re)})² − De           {De,a,re}   */
+  FS_FORM_EXP_DECAY = 2,   /* A e^{−Br}                          {A,B}       */
+  FS_FORM_SQRT = 3,        /* A sqrt(r/B)                        {A,B}       */
+  FS_FORM_POWER_DECAY = 4, /* A / r^n                            {A,n}       */
+  FS_FORM_MEXP_DECAY = 5,  /* A e^{−B(r−r0)}                     {A,B,r0}    */
+  FS_FORM_HARMONIC = 6,    /* k (r−r0)²                          {k,r0}      */
+  FS_FORM_EXP_PLUS = 7,    /* A e^{−Br} + C                      {A,B,C}     */
+  FS_FORM_PARABOLA = 8,    /* A r² + B r + C                     {A,B,C}     */
+  FS_FORM_CONST = 9,       /* C                                  {C}         */
+  FS_FORM_BUCKINGHAM = 10, /* A e^{−r/ρ} − C (ρ²/r²)³            {A,rho,C}   */
+  FS_FORM_BORN = 11,       /* A e^{(C−r)/B} − D/r^6 + E/r^8      {A,B,C,D,E} */
+  FS_FORM_COUNT = 12
+};
+
+typedef struct fs_table {
+  int32_t kind;          /* fs_table_kind                                   */
+  int32_t form;          /* fs_form for FS_TABLE_ANALYTIC, else ignored     */
+  int32_t n;             /* knots / parameters                              */
+  int32_t reserved;
+  double rmin, rmax;     /* knot domain (spline) or gate span (analytic)    */
+  const double *values;  /* knot values y[n] or parameters[n]               */
+  const uint8_t *fixed;  /* nullable: 1 = value is fixed (takes no column)  */
+  const double *lower;   /* nullable: per-value lower bound (−inf if null)  */
+  const double *upper;   /* nullable: per-value upper bound (+inf if null)  */
+} fs_table;
+
+typedef struct fs_model {
+  int32_t family;   /* fs_family                                            */
+  int32_t ntypes;   /* species slots (Z-sorted)                             */
+  int32_t n_tables; /* must equal the family's table count                  */
+  int32_t reserved;
+  const fs_table *tables; /* in the reference's gather order                */
+} fs_model;
+
+/* ---- context ----------------------------------------------------------- */
+enum fs_precision { FS_PREC_FP32 = 0, FS_PREC_FP64 = 1 };
+
+typedef struct fs_gpu_opts {
+  int32_t device;         /* CUDA ordinal                                  */
+  int32_t precision;      /* fs_precision: FP32 compute + FP64 sums, or FP64 */
+  int32_t lanes_per_atom; /* 0 = autotuned schedule, else 8 / 16 / 32      */
+  int32_t reserved;
+} fs_gpu_opts;
+
+typedef struct fs_gpu fs_gpu;
+
+int fs_gpu_create(const fs_gpu_opts *opts, fs_gpu **out);
+int fs_gpu_destroy(fs_gpu *h);
+/* Copies the last error message (NUL-terminated, truncated) into buf. */
+int fs_gpu_last_error(const fs_gpu *h, char *buf, size_t size);
+/* The CUDA stream every launch of this context is enqueued on. */
+int fs_gpu_get_stream(fs_gpu *h, void **stream);
+
+/*
+ * Configurations, concatenated.  box9 is row-major 3×3 per config whose
+ * COLUMNS are the lattice vectors X, Y, Z (config_reader.cpp:58-68).
+ * pos / ref_force: 3 doubles per atom.  type: species slot per atom.
+ * ref_stress9: row-major 3×3 per config.  ref_* may be NULL (zeros).
+ */
+int fs_gpu_upload_configs(fs_gpu *h, int32_t n_cfg, const int32_t *natoms,
+                          const double *box9, const double *pos,
+                          const int32_t *type, const double *ref_force,
+                          const double *ref_energy, const double *ref_stress9);
+/* Replace only the reference labels (same shapes as the upload). */
+int fs_gpu_set_references(fs_gpu *h, const double *ref_force,
+                          const double *ref_energy, const double *ref_stress9);
+
+int fs_gpu_set_model(fs_gpu *h, const fs_model *model);
+/* Builds the device neighbour lists at the model's max cutoff. */
+int fs_gpu_prepare(fs_gpu *h);
+
+int fs_gpu_num_pairs(fs_gpu *h, int64_t *n_pairs);
+/* counts[total_atoms]; neighbours in the reference order (i, then j, then
+ * image ix, iy, iz lexicographic): j is the config-local atom index,
+ * img3 holds (ix, iy, iz) per pair. */
+int fs_gpu_get_neighbor_counts(fs_gpu *h, int32_t *counts);
+int fs_gpu_get_neighbors(fs_gpu *h, int32_t *j, int8_t *img3);
+
+int fs_gpu_param_count(fs_gpu *h, int32_t *D);
+int fs_gpu_gather_params(fs_gpu *h, double *x);
+int fs_gpu_gather_bounds(fs_gpu *h, double *lo, double *hi);
+int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D);
+
+/* rows = Σ_c 3N_c + 2 + (w_s > 0 ? 6 : 0)  (residual_layout.hpp:18-31) */
+int fs_gpu_residual_count(fs_gpu *h, double w_s, int64_t *m);
+
+/*
+ * One residual evaluation over every configuration at the current params.
+ * Every output is nullable.  F[m]: residual vector in the reference's row
+ * order.  forces[3·Ntot], energy[n_cfg], stress9[9·n_cfg] (already /V),
+ * limit[n_cfg]: the calculator outputs.  obj: ‖F‖² (FP64 sum).
+ */
+int fs_gpu_eval(fs_gpu *h, double w_e, double w_s, double *F, double *forces,
+                double *energy, double *stress9, double *limit, double *obj);
+
+/*
+ * Residual + Jacobian.  J is column-major m × D (Eigen's fjac layout) in
+ * FP64; JtJ is D × D and Jtr is D (FP64 accumulation).  Every output is
+ * nullable; with J == NULL the Jacobian stays on the device.
+ */
+int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F,
+                         double *J, double *JtJ, double *Jtr, double *obj);
+
+/* Device-resident variant: enqueues residual + Jacobian + JᵀJ + Jᵀr on the
+ * context stream and returns without synchronising.  Results stay on the
+ * device (fetch them with fs_gpu_fetch_normal_equations). */
+int fs_gpu_eval_jacobian_async(fs_gpu *h, double w_e, double w_s);
+int fs_gpu_fetch_normal_equations(fs_gpu *h, double *JtJ, double *Jtr,
+                                  double *obj);
+
+/*
+ * Damped Gauss–Newton step from the last eval_jacobian:
+ * solve (JᵀJ + λ·diag) dx = −Jᵀr by FP64 Cholesky on the device.
+ * mode 0: diag = I (Levenberg); mode 1: diag = diag(JᵀJ) (Marquardt).
+ */
+int fs_gpu_lm_step(fs_gpu *h, double lambda, int32_t mode, double *dx);
+/* NormalEquationsSolver step: λ = ridge > 0 ? ridge : 1e-8·max(mean diag,1);
+ * dx = −(JᵀJ + λI)⁻¹ Jᵀr. */
+int fs_gpu_lsq_step(fs_gpu *h, double ridge, double *dx);
+
+/* Copies [JᵀJ (D·D), Jᵀr (D), ‖F‖² (1)] as FP64 into a caller-owned DEVICE
+ * buffer, ordered on the context stream (for a collective over ranks). */
+int fs_gpu_copy_normal_equations(fs_gpu *h, void *dst_device);
+
+/*
+ * Instrumentation.  With profiling on, every eval_jacobian records CUDA
+ * events on the context stream between its phases (residual, per-atom
+ * Jacobian, force/stress rows, JᵀJ/Jᵀr), for up to max_steps calls.
+ * fs_gpu_phase_times synchronises, returns the summed milliseconds per phase
+ * and the number of recorded calls, and resets.  fs_gpu_launch_count is the
+ * number of kernels this context has launched.
+ */
+int fs_gpu_set_profiling(fs_gpu *h, int32_t max_steps);
+int fs_gpu_phase_times(fs_gpu *h, double *ms, int32_t n, int32_t *steps);
+int fs_gpu_launch_count(fs_gpu *h, int64_t *count);
+
+/*
+ * Batched objective: obj[k] = ‖F(x_k)‖² for NP parameter vectors xs[NP·D]
+ * (row-major), all configurations, one launch.  The DE population kernel.
+ */
+int fs_gpu_eval_population(fs_gpu *h, double w_e, double w_s, const double *xs,
+                           int32_t NP, double *obj);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* FORCESMITH_GPU_H */

@@ -1,0 +1,72 @@
+"""CPU-only checks of the boundary: the sm_100a library loads and exports
+every entry point include/*.h declares; host-side marshalling and the
+synthetic workloads are deterministic."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from forcesmith_b200 import build, synth
+from forcesmith_b200.abi import Model, Table, fs_table, fs_model, FS_FAMILY_EAM
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        names |= set(re.findall(r"\b(fs_gpu_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    path = build.build_gpu()
+    lib = C.CDLL(path)  # loading needs only libcudart, not a device
+    missing = [n for n in _declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert len(_declared_symbols()) >= 20
+
+
+def test_create_without_device_fails_cleanly():
+    from forcesmith_b200 import gpu
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a device is visible")
+    except Exception:
+        pass
+    with pytest.raises(Exception):
+        gpu.GpuSession(0)
+
+
+def test_struct_layout_matches_header():
+    assert C.sizeof(fs_table) == 4 * 4 + 2 * 8 + 4 * 8
+    assert C.sizeof(fs_model) == 4 * 4 + 8
+
+
+def test_synthetic_workloads_are_deterministic():
+    a = synth.packing(np.array([40, 33], np.int32), seed=3)
+    b = synth.packing(np.array([40, 33], np.int32), seed=3)
+    assert np.array_equal(a.pos, b.pos) and np.array_equal(a.type, b.type)
+    f = synth.fcc(2)
+    assert f.natoms.tolist() == [108, 108]
+    d = synth.diamond(5)
+    assert set(d.natoms.tolist()) <= {64, 216, 512}
+
+
+def test_model_parameter_layout_follows_table_order():
+    """TableParams gather order (force_calculator_concept.hpp:171-208): tables
+    in declaration order, free values only."""
+    true = synth.ternary_true_model(20)
+    x = true.free_values()
+    assert x.size == 240
+    fixed = np.zeros(20, np.uint8)
+    fixed[[0, 5]] = 1
+    true.tables[3].fixed = fixed
+    assert true.free_values().size == 238
+    m2 = true.with_values(true.free_values() * 2)
+    assert np.allclose(m2.tables[3].values[[0, 5]], true.tables[3].values[[0, 5]])

@@ -1,0 +1,233 @@
+"""Parity of the sm_100a path (called through the C ABI) with the oracle.
+
+Tolerances (stated here, as the comparison bar):
+  neighbour sets              bit-exact (counts, j, image) in the reference order
+  FP64 mode  forces / stress  |Δ| ≤ 1e-9·(1 + |x|)       (bar: 1e-5 relative)
+             energy, F rows   |Δ| ≤ 1e-9·(1 + |x|)
+             objective        relative 1e-9
+             Jacobian         vs analytic oracle 1e-9·(1 + |J|); vs the
+                              reference's central differences 1e-5·|J| + 1e-8
+  FP32 mode  forces           |Δ| ≤ 2e-5·max|F_ref|  (FP32 spline arithmetic;
+                              pair vectors rebuilt in FP64)
+             objective        relative 1e-4
+             Jacobian         |Δ| ≤ 1e-4·max|J column| per column
+"""
+import math
+
+import numpy as np
+import pytest
+
+from forcesmith_b200 import synth
+from forcesmith_b200.abi import Model, Table, FS_FAMILY_EAM, FS_FAMILY_PAIR
+from oracle import api as O
+from tests.helpers import cluster, concat, label, small_ternary, ternary_models, spline_pair_model
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(precision="fp64", lpa=0):
+    from forcesmith_b200.gpu import GpuSession
+    return GpuSession(0, precision, lpa)
+
+
+def _pair(ds, model, precision="fp64", lpa=0):
+    g = _gpu(precision, lpa)
+    g.upload(ds)
+    g.set_model(model)
+    o = O.Oracle()
+    o.upload(ds)
+    o.set_model(model)
+    return g, o
+
+
+def _close(a, b, rel, what):
+    a, b = np.asarray(a), np.asarray(b)
+    err = np.max(np.abs(a - b) / (1.0 + np.abs(b))) if a.size else 0.0
+    assert err <= rel, f"{what}: max rel err {err:.3e} > {rel:.1e}"
+
+
+@pytest.fixture(scope="module")
+def ternary_small():
+    true, start = ternary_models(20)
+    ds = small_ternary(6, 48, seed=99)
+    ds = label(ds, true, O.Oracle, 1.0, 0.1)
+    return ds, true, start
+
+
+def _geometries():
+    a = 3.615
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]]) * a
+    fcc = cluster(np.array([np.array([x, y, z]) * a + b for x in range(2) for y in range(2)
+                            for z in range(2) for b in basis]), 2 * a)
+    tri = cluster(np.random.default_rng(1).uniform(-3, 14, (40, 3)), 10.0)
+    tri.box9[0] = [10.0, 5.0, 0.0, 0.0, 8.66, 0.0, 0.0, 0.0, 10.0]
+    small = synth.packing(np.array([32, 40], np.int32), seed=5)
+    mi = cluster([[0, 0, 0], [9.5, 0, 0]], 10.0)
+    return concat(fcc, tri, small.subset([0]), small.subset([1]), mi)
+
+
+@pytest.mark.parametrize("rcut", [1.0, 0.75 * 3.615, 6.0])
+def test_neighbor_sets_bit_exact(rcut):
+    ds = _geometries()
+    model = Model(FS_FAMILY_PAIR, 1, [Table.spline(0.0, rcut, np.zeros(4))])
+    g, o = _pair(ds, model)
+    assert g.num_pairs() == o.num_pairs()
+    assert np.array_equal(g.neighbor_counts(ds.n_atoms), o.neighbor_counts(ds.n_atoms))
+    gj, gimg = g.neighbors()
+    oj, oimg, _ = o.neighbors()
+    assert np.array_equal(gj, oj)
+    assert np.array_equal(gimg, oimg)
+
+
+def test_neighbor_sets_ternary_bit_exact(ternary_small):
+    ds, true, _ = ternary_small
+    g, o = _pair(ds, true)
+    gj, gimg = g.neighbors()
+    oj, oimg, _ = o.neighbors()
+    assert np.array_equal(gj, oj) and np.array_equal(gimg, oimg)
+
+
+@pytest.mark.parametrize("lpa", [0, 4, 8, 16, 32])
+def test_eam_residual_fp64(ternary_small, lpa):
+    ds, _, start = ternary_small
+    g, o = _pair(ds, start, "fp64", lpa)
+    rg, ro = g.eval(1.0, 0.1), o.eval(1.0, 0.1)
+    _close(rg["forces"], ro["forces"], 1e-9, "forces")
+    _close(rg["energy"], ro["energy"], 1e-9, "energy")
+    _close(rg["stress"], ro["stress"], 1e-9, "stress")
+    _close(rg["F"], ro["F"], 1e-9, "F")
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-9 * ro["obj"]
+
+
+def test_eam_residual_fp32(ternary_small):
+    ds, _, start = ternary_small
+    g, o = _pair(ds, start, "fp32")
+    rg, ro = g.eval(1.0, 0.1), o.eval(1.0, 0.1)
+    scale = np.max(np.abs(ro["forces"]))
+    assert np.max(np.abs(rg["forces"] - ro["forces"])) <= 2e-5 * scale
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-4 * ro["obj"]
+    assert np.max(np.abs(rg["energy"] - ro["energy"]) / np.abs(ro["energy"])) <= 1e-5
+
+
+def test_pair_residual_half_open_gate():
+    ds = small_ternary(3, 40, seed=12)
+    ds.type[:] = ds.type % 2
+    model = spline_pair_model(2, rmax=5.5)
+    ds = label(ds, model.with_values(model.free_values() * 1.02), O.Oracle, 1.0, 0.3)
+    g, o = _pair(ds, model)
+    rg, ro = g.eval(1.0, 0.3), o.eval(1.0, 0.3)
+    _close(rg["F"], ro["F"], 1e-9, "F")
+
+
+def test_eam_clamp_limit_rows():
+    """ρ beyond the embedding span: limit rows and the clamped embedding
+    (kernels.hpp:19-31; eam_force.cpp:151-190)."""
+    true, start = ternary_models(12)
+    ds = small_ternary(3, 40, seed=21)
+    for t in start.tables[9:]:  # shrink the embedding span below the observed ρ
+        t.rmax = 9.0
+    g, o = _pair(ds, start)
+    rg, ro = g.eval(1.0, 0.0), o.eval(1.0, 0.0)
+    assert np.all(ro["limit"] > 0)
+    _close(rg["limit"], ro["limit"], 1e-9, "limit")
+    _close(rg["F"], ro["F"], 1e-9, "F")
+    jg = g.jacobian(1.0, 0.0)["J"]
+    ja = o.jacobian_analytic(1.0, 0.0)
+    _close(jg, ja, 1e-8, "J with clamped atoms")
+
+
+def test_eam_jacobian_fp64_vs_oracle(ternary_small):
+    ds, _, start = ternary_small
+    sub = ds.subset([0, 1])
+    g, o = _pair(sub, start, "fp64")
+    res = g.jacobian(1.0, 0.1)
+    Ja = o.jacobian_analytic(1.0, 0.1)
+    _close(res["J"], Ja, 1e-9, "J vs analytic oracle")
+    Jf = o.jacobian_fd(1.0, 0.1)
+    assert np.all(np.abs(res["J"] - Jf) <= 1e-5 * np.abs(Jf) + 1e-8 + 1e-6 * np.abs(Jf).max())
+    F = o.eval(1.0, 0.1)["F"]
+    JtJ, Jtr = O.normal_equations(Ja, F)
+    _close(res["JtJ"], JtJ, 1e-9, "JtJ")
+    _close(res["Jtr"], Jtr, 1e-9, "Jtr")
+    assert abs(res["obj"] - float(F @ F)) <= 1e-9 * float(F @ F)
+
+
+def test_eam_jacobian_fp32(ternary_small):
+    ds, _, start = ternary_small
+    sub = ds.subset([0, 1, 2])
+    g, o = _pair(sub, start, "fp32")
+    res = g.jacobian(1.0, 0.1)
+    Ja = o.jacobian_analytic(1.0, 0.1)
+    colmax = np.abs(Ja).max(axis=0) + 1e-30
+    err = np.max(np.abs(res["J"] - Ja) / colmax)
+    assert err <= 1e-4, err
+    F = o.eval(1.0, 0.1)["F"]
+    JtJ, Jtr = O.normal_equations(Ja, F)
+    d = np.sqrt(np.outer(np.diag(JtJ), np.diag(JtJ)))
+    assert np.max(np.abs(res["JtJ"] - JtJ) / d) <= 1e-4
+    assert np.max(np.abs(res["Jtr"] - Jtr)) <= 1e-4 * np.max(np.abs(Jtr))
+
+
+def test_pair_jacobian_fp64():
+    ds = small_ternary(2, 40, seed=13)
+    ds.type[:] = ds.type % 2
+    model = spline_pair_model(2)
+    ds = label(ds, model.with_values(model.free_values() * 1.03), O.Oracle, 1.0, 0.2)
+    g, o = _pair(ds, model)
+    res = g.jacobian(0.7, 0.2)
+    _close(res["J"], o.jacobian_analytic(0.7, 0.2), 1e-9, "pair J")
+
+
+def test_lm_and_lsq_steps_fp64(ternary_small):
+    ds, _, start = ternary_small
+    g = _gpu("fp64")
+    g.upload(ds)
+    g.set_model(start)
+    res = g.jacobian(1.0, 0.1, want_J=False)
+    for lam, mode in ((1e-3, 0), (1e-2, 1), (10.0, 0)):
+        dx = g.lm_step(lam, mode)
+        ref = O.lm_step(res["JtJ"], res["Jtr"], lam, mode)
+        _close(dx, ref, 1e-8, f"lm_step λ={lam}")
+    dx = g.lsq_step(0.0)
+    _close(dx, O.lsq_step(res["JtJ"], res["Jtr"], 0.0), 1e-6, "lsq_step")
+
+
+def test_population_objective(ternary_small):
+    ds, _, start = ternary_small
+    g, o = _pair(ds.subset([0, 1, 2]), start, "fp64")
+    x0 = g.gather_params()
+    xs = np.stack([x0 * synth.uniform(x0.size, 0.98, 1.02, 100 + k) for k in range(5)])
+    og = g.eval_population(xs, 1.0, 0.1)
+    oo = o.eval_population(xs, 1.0, 0.1)
+    _close(og, oo, 1e-9, "population objective")
+
+
+def test_gradient_directional_full_size():
+    """Size-independent property at the full ternary workload (500 × 256):
+    d/dε ‖F(x + εv)‖² = 2 vᵀJᵀF, with J from the FP32 analytic path and the
+    objective from the FP64 path."""
+    true, start = ternary_models(20)
+    ds = synth.ternary_geometry()
+    g64 = _gpu("fp64")
+    g64.upload(ds)
+    g64.set_model(true)
+    lab = g64.eval(1.0, 0.1)
+    ds = ds.with_labels(lab["forces"], lab["energy"], lab["stress"])
+    g64.set_references(ds)
+    g64.set_model(start)
+    g32 = _gpu("fp32")
+    g32.upload(ds)
+    g32.set_model(start)
+    res = g32.jacobian(1.0, 0.1, want_J=False)
+    x = g64.gather_params()
+    v = synth.uniform(x.size, -1.0, 1.0, 77)
+    eps = 1e-4
+    g64.set_params(x + eps * v)
+    op = g64.eval(1.0, 0.1, want=("obj",))["obj"]
+    g64.set_params(x - eps * v)
+    om = g64.eval(1.0, 0.1, want=("obj",))["obj"]
+    fd = (op - om) / (2 * eps)
+    an = 2.0 * float(v @ res["Jtr"])
+    assert abs(fd - an) <= 1e-3 * abs(fd), (fd, an)
+    assert np.allclose(res["JtJ"], res["JtJ"].T, rtol=0, atol=1e-12 * np.abs(res["JtJ"]).max())
+    assert np.all(np.linalg.eigvalsh(res["JtJ"]) > -1e-8 * np.abs(res["JtJ"]).max())
