@@ -122,6 +122,8 @@ void free_jacobian(fs_gpu *h) {
   dfree(h->d_JtJ);
   dfree(h->d_Jtr);
   dfree(h->d_gram_part);
+  dfree(h->d_jtr_part);
+  h->jtr_part_alloc = 0;
   dfree(h->d_atom_scalars);
   dfree(h->d_drho);
   dfree(h->d_dgd);
@@ -135,6 +137,14 @@ void free_jacobian(fs_gpu *h) {
 int sync(fs_gpu *h) {
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return set_error(h, FS_ERR_CUDA, std::string("kernel: ") + cudaGetErrorString(e));
+  if (h->d_err) { // a bounded device wait gave up
+    int32_t flag = 0;
+    cudaMemcpy(&flag, h->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (flag) {
+      cudaMemset(h->d_err, 0, sizeof(int32_t));
+      return set_error(h, FS_ERR_DEVICE, "a device-side wait timed out (results discarded)");
+    }
+  }
   return FS_OK;
 }
 
@@ -210,6 +220,7 @@ int fs_gpu_destroy(fs_gpu *h) {
   dfree(h->d_pop_seg_a);
   dfree(h->d_pop_vals);
   dfree(h->d_pop_obj);
+  dfree(h->d_err);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -271,8 +282,11 @@ int fs_gpu_upload_configs(fs_gpu *h, int32_t n_cfg, const int32_t *natoms, const
     return set_error(h, FS_ERR_UNSUPPORTED, "upload_configs: too many atoms");
   h->n_atoms = off;
   h->max_natoms = maxn;
-  for (int64_t i = 0; i < off; ++i)
+  h->max_type = 0;
+  for (int64_t i = 0; i < off; ++i) {
     if (type[i] < 0 || type[i] > 255) return set_error(h, FS_ERR_ARG, "upload_configs: bad type");
+    h->max_type = std::max(h->max_type, static_cast<int>(type[i]));
+  }
   FS_TRY(dalloc(h, &h->d_cfg, n_cfg));
   FS_TRY(dalloc(h, &h->d_pos, 3 * off));
   FS_TRY(dalloc(h, &h->d_wpos, 3 * off));
@@ -374,6 +388,8 @@ int fs_gpu_prepare(fs_gpu *h) {
   if (!h) return FS_ERR_ARG;
   if (h->n_cfg == 0) return set_error(h, FS_ERR_STATE, "prepare: no configurations");
   if (!h->have_model) return set_error(h, FS_ERR_STATE, "prepare: no model");
+  if (h->max_type >= h->ntypes)
+    return set_error(h, FS_ERR_ARG, "prepare: an atom's species slot is >= the model's ntypes");
   cudaSetDevice(h->device);
   FS_TRY(build_neighbors(h, model_max_cutoff(h)));
   FS_TRY(ensure_eval_buffers(h, 1.0));
@@ -538,13 +554,16 @@ int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F, double *J
   const int64_t m = rows_of(h, w_s);
   if (F) FS_CUDA(cudaMemcpyAsync(F, h->d_F, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (J) {
+    // column-major m × D, from the device's padded leading dimension
     const size_t n = static_cast<size_t>(m) * h->D;
     if (h->precision == FS_PREC_FP64) {
-      FS_CUDA(cudaMemcpyAsync(J, h->d_J, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      FS_CUDA(cudaMemcpy2DAsync(J, m * sizeof(double), h->d_J, h->ldj * sizeof(double), m * sizeof(double),
+                                h->D, cudaMemcpyDeviceToHost, h->stream));
       FS_TRY(sync(h));
     } else {
       std::vector<float> tmp(n);
-      FS_CUDA(cudaMemcpyAsync(tmp.data(), h->d_J, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+      FS_CUDA(cudaMemcpy2DAsync(tmp.data(), m * sizeof(float), h->d_J, h->ldj * sizeof(float), m * sizeof(float),
+                                h->D, cudaMemcpyDeviceToHost, h->stream));
       FS_TRY(sync(h));
       for (size_t k = 0; k < n; ++k) J[k] = tmp[k];
     }

@@ -307,11 +307,15 @@ template <class T> struct JacArgs {
   const T *seg_g;       // [seg][4][kWin]
   const int32_t *seg_ws;
   double w_e, w_s;
-  int64_t M;            // rows of J (leading dimension)
+  int64_t M;            // rows of J
+  int64_t ld;           // leading dimension of J (≥ M)
   int D;
+  const double *F;      // residual (for the fused Jᵀr)
+  double *jtr_part;     // [config][D] Jᵀr partials (FP64)
   int dens_c0, ndens;   // contiguous density columns
+  int stage;            // 1: the per-atom Jacobian data of a config fits in shared memory
   T *J;                 // column-major M × D
-  T *scal;              // [atom][4]: gradF, curvF, over (0 = unclamped), unused
+  T *gF, *cF, *over;    // [atom]: F'(ρ̄), F''(ρ̄), clamp overshoot term (0 = unclamped)
   T *drho;              // [atom][ndens]
   T *dgd;               // [atom][kWin]: ∂F'(ρ̄)/∂y over the embedding window
   int32_t *wsF;         // [atom]: embedding window start (knot)
@@ -330,6 +334,26 @@ template <class T> size_t jac_common_smem(int n_tables, int n_segs, int n_cmap, 
   return b + 128;
 }
 
+// Shared-memory copy of the per-atom Jacobian data of one configuration
+// (row stride ndens + 1 keeps a warp's column reads on distinct banks).
+template <class T> size_t atom_stage_smem(int max_atoms, int ndens) {
+  return align16(static_cast<size_t>(max_atoms) * (ndens + 1) * sizeof(T)) +
+         3 * align16(max_atoms * sizeof(T)) + align16(max_atoms * sizeof(int32_t)) +
+         align16(static_cast<size_t>(max_atoms) * kWin * sizeof(T)) + 96;
+}
+
+template <class T>
+__device__ void stage_tables(const JacArgs<T> &A, STab<T> *tabs, typename Vec4T<T>::type *seg, T *segg,
+                             int32_t *segws, int32_t *cmap) {
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
+    seg[k] = A.seg_a[k];
+    segws[k] = A.seg_ws[k];
+  }
+  for (int k = threadIdx.x; k < A.c.n_segs * 4 * kWin; k += blockDim.x) segg[k] = A.seg_g[k];
+  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   using T4 = typename Vec4T<T>::type;
@@ -339,6 +363,7 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   const int N = cd.natoms;
   const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
   const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  const int nd = A.ndens, ds = nd + 1;
   Smem S(smem_raw);
   STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
   T4 *seg = S.take<T4>(A.c.n_segs);
@@ -350,21 +375,18 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   uint8_t *typ = S.take<uint8_t>(N);
   double *erow = S.take<double>(A.D);
   double *lrow = S.take<double>(A.D);
-  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
-  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
-    seg[k] = A.seg_a[k];
-    segws[k] = A.seg_ws[k];
-  }
-  for (int k = threadIdx.x; k < A.c.n_segs * 4 * kWin; k += blockDim.x) segg[k] = A.seg_g[k];
-  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
+  T *drs = S.take<T>(static_cast<size_t>(N) * ds); // ∂ρ_i/∂y rows (staged)
+  T *sgf = S.take<T>(N);
+  T *sov = S.take<T>(N);
+  stage_tables(A, tabs, seg, segg, segws, cmap);
   for (int k = threadIdx.x; k < A.D; k += blockDim.x) erow[k] = lrow[k] = 0.0;
+  for (int k = threadIdx.x; k < N * ds; k += blockDim.x) drs[k] = T(0);
   stage_geometry(cd, A.c, wpos, shift, typ);
   __syncthreads();
   const int32_t *start = A.c.nb_start + cd.atom0;
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int64_t ga = static_cast<int64_t>(cd.atom0) + i;
-    T *dr = A.drho + ga * A.ndens;
-    for (int m = 0; m < A.ndens; ++m) dr[m] = T(0);
+    T *dr = drs + i * ds;
     T rho = T(0);
     for (int p = start[i]; p < start[i + 1]; ++p) {
       int j;
@@ -398,12 +420,11 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
     T t;
     const int e = seg_of(te, rb, t);
     const T gF = seg_der<T>(seg[e], t, te.inv_h);
-    const T cF = seg_der2<T>(seg[e], t, te.inv_h);
-    T *sc = A.scal + 4 * ga;
-    sc[0] = gF;
-    sc[1] = cF;
-    sc[2] = static_cast<T>(over);
-    sc[3] = T(0);
+    A.gF[ga] = gF;
+    A.cF[ga] = seg_der2<T>(seg[e], t, te.inv_h);
+    A.over[ga] = static_cast<T>(over);
+    sgf[i] = gF;
+    sov[i] = static_cast<T>(over);
     const int ws = segws[e];
     A.wsF[ga] = ws;
     const T *G = segg + e * 4 * kWin;
@@ -416,24 +437,34 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
       const int col = cmap[te.cmap0 + ws + q];
       if (col >= 0) atomicAdd(&erow[col], A.w_e * static_cast<double>(dv));
     }
-    for (int m = 0; m < A.ndens; ++m) {
-      const double dv = static_cast<double>(dr[m]);
-      if (dv == 0.0) continue;
-      if (over != 0.0)
-        atomicAdd(&lrow[A.dens_c0 + m], over * dv);
-      else
-        atomicAdd(&erow[A.dens_c0 + m], A.w_e * static_cast<double>(gF) * dv);
-    }
-    if (over != 0.0)
-      for (int m = 0; m < A.ndens; ++m) dr[m] = T(0);
   }
   __syncthreads();
+  // energy row: Σ_i w_e F'_i ∂ρ_i/∂y (unclamped atoms); limit row: Σ over_i ∂ρ_i/∂y
+  for (int m = threadIdx.x; m < nd; m += blockDim.x) {
+    double e = 0.0, l = 0.0;
+    for (int i = 0; i < N; ++i) {
+      const double v = static_cast<double>(drs[i * ds + m]);
+      const double ov = static_cast<double>(sov[i]);
+      if (ov != 0.0)
+        l += ov * v;
+      else
+        e += static_cast<double>(sgf[i]) * v;
+    }
+    erow[A.dens_c0 + m] += A.w_e * e;
+    lrow[A.dens_c0 + m] = l;
+  }
+  __syncthreads();
+  // ∂ρ/∂y of clamped atoms is dropped from the force chain (eam_force.cpp:188-190)
+  for (int k = threadIdx.x; k < N * nd; k += blockDim.x) {
+    const int i = k / nd, m = k % nd;
+    A.drho[(static_cast<int64_t>(cd.atom0) + i) * nd + m] = sov[i] != T(0) ? T(0) : drs[i * ds + m];
+  }
   const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
   const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
   const int64_t rE = row0 + 3 * N, rL = rE + 1 + (A.w_s > 0.0 ? 6 : 0);
   for (int col = threadIdx.x; col < A.D; col += blockDim.x) {
-    A.J[col * A.M + rE] = static_cast<T>(erow[col]);
-    A.J[col * A.M + rL] = static_cast<T>(lrow[col]);
+    A.J[col * A.ld + rE] = static_cast<T>(erow[col]);
+    A.J[col * A.ld + rL] = static_cast<T>(lrow[col]);
   }
 }
 
@@ -453,19 +484,29 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
 // the density columns it owns.  The stress rows use the pair symmetry of the
 // full list for the chain terms: Σ_pairs v (F''_i drho_i ρ'_{tj} + F''_j
 // drho_j ρ'_{ti}) = 2 Σ_i P_i F''_i drho_i with P_i = Σ_j v_ij ρ'_{tj}(r_ij).
+// The configuration's per-atom data (∂ρ/∂y rows, F', F'', embedding windows)
+// is staged in shared memory when it fits, so the inner loops never wait on
+// global memory.
 // ---------------------------------------------------------------------------
 template <class T> struct PairRec {
+  // per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window)
+  int e[4];        // extended segment (−1: no contribution)
+  int cbase[4];    // column-map index of the window's first knot
+  int nv[4];       // valid knots in the window
+  T t[4], w[4], ih[4];
   T u[3], v[6];
-  T tphi, trj, tri;
-  T dgj, dgi;      // ρ'_{tj}(r), ρ'_{ti}(r) (gated)
-  T gFj, cFj;      // F'_j, F''_j
-  int ephi, erj, eri; // extended segment (−1: gated out)
-  int j, tj, wsj;
+  T dgi, cFj;      // ρ'_{ti}(r), F''_j
+  int j;
 };
 
+template <class T> struct V2T;
+template <> struct V2T<float> { using type = float2; };
+template <> struct V2T<double> { using type = double2; };
+
 template <class T, bool EAM>
-__global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps) {
+__global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
   using T4 = typename Vec4T<T>::type;
+  using T2 = typename V2T<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int c = blockIdx.x;
   const CfgDev &cd = A.c.cfg[c];
@@ -473,6 +514,7 @@ __global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps
   const int D = A.D;
   const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
   const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  const int nd = A.ndens;
   Smem S(smem_raw);
   STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
   T4 *seg = S.take<T4>(A.c.n_segs);
@@ -482,40 +524,70 @@ __global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps
   double *wpos = S.take<double>(3 * N);
   double *shift = S.take<double>(3 * nimg);
   uint8_t *typ = S.take<uint8_t>(N);
-  T *rowb = S.take<T>(static_cast<size_t>(warps) * 10 * D); // per warp: 3 force + 6 stress + 1 energy
+  // per warp: force rows + φ energy as [col] × (x, y, z, e); stress as
+  // [col] × 3 pairs (xx,yy)(zz,xy)(xz,yz); energy row; pair records
+  T4 *frow_all = S.take<T4>(static_cast<size_t>(warps) * D);
+  T2 *srow_all = S.take<T2>(static_cast<size_t>(warps) * 3 * D);
+  T *erow_all = S.take<T>(static_cast<size_t>(warps) * D);
   PairRec<T> *recs = S.take<PairRec<T>>(static_cast<size_t>(warps) * 32);
-  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
-  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
-    seg[k] = A.seg_a[k];
-    segws[k] = A.seg_ws[k];
+  double *jtr_all = S.take<double>(static_cast<size_t>(warps) * D);
+  const T *drho = A.drho + static_cast<int64_t>(cd.atom0) * nd;
+  int dstr = nd;
+  const T *gFa = A.gF + cd.atom0, *cFa = A.cF + cd.atom0, *dgda = A.dgd + static_cast<int64_t>(cd.atom0) * kWin;
+  const int32_t *wsFa = A.wsF + cd.atom0;
+  if (EAM && A.stage) {
+    T *s_dr = S.take<T>(static_cast<size_t>(N) * (nd + 1));
+    T *s_gf = S.take<T>(N);
+    T *s_cf = S.take<T>(N);
+    T *s_pad = S.take<T>(N);
+    int32_t *s_ws = S.take<int32_t>(N);
+    T *s_dgd = S.take<T>(static_cast<size_t>(N) * kWin);
+    (void)s_pad;
+    for (int k = threadIdx.x; k < N * nd; k += blockDim.x) s_dr[(k / nd) * (nd + 1) + k % nd] = drho[k];
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+      s_gf[k] = gFa[k];
+      s_cf[k] = cFa[k];
+      s_ws[k] = wsFa[k];
+    }
+    for (int k = threadIdx.x; k < N * kWin; k += blockDim.x) s_dgd[k] = dgda[k];
+    drho = s_dr;
+    dstr = nd + 1;
+    gFa = s_gf;
+    cFa = s_cf;
+    wsFa = s_ws;
+    dgda = s_dgd;
   }
-  for (int k = threadIdx.x; k < A.c.n_segs * 4 * kWin; k += blockDim.x) segg[k] = A.seg_g[k];
-  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
-  for (int k = threadIdx.x; k < warps * 10 * D; k += blockDim.x) rowb[k] = T(0);
+  stage_tables(A, tabs, seg, segg, segws, cmap);
+  for (int k = threadIdx.x; k < warps * 3 * D; k += blockDim.x) srow_all[k] = T2{T(0), T(0)};
+  for (int k = threadIdx.x; k < warps * D; k += blockDim.x) {
+    erow_all[k] = T(0);
+    jtr_all[k] = 0.0;
+  }
   stage_geometry(cd, A.c, wpos, shift, typ);
   __syncthreads();
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  T *frow = rowb + static_cast<size_t>(w) * 10 * D; // [3][D]
-  T *srow = frow + 3 * D;                            // [6][D] (accumulated over the warp's atoms)
-  T *erow = frow + 9 * D;                            // [D]    (φ energy part)
+  T4 *frow = frow_all + static_cast<size_t>(w) * D;
+  T2 *srow = srow_all + static_cast<size_t>(w) * 3 * D;
+  T *erow = erow_all + static_cast<size_t>(w) * D;
+  double *jtr = jtr_all + static_cast<size_t>(w) * D;
   PairRec<T> *rec = recs + w * 32;
   const int32_t *start = A.c.nb_start + cd.atom0;
   const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
   const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
   const T half_we = static_cast<T>(0.5 * A.w_e);
   const bool want_stress = A.w_s > 0.0;
+  const int slot = lane / kWin, q = lane % kWin;
 
   for (int i = w; i < N; i += warps) {
-    for (int k = lane; k < 3 * D; k += 32) frow[k] = T(0);
+    for (int k = lane; k < D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
     const int ti = typ[i];
-    const int64_t gi = static_cast<int64_t>(cd.atom0) + i;
     T gFi = T(0), cFi = T(0);
     int wsFi = 0;
     if constexpr (EAM) {
-      gFi = A.scal[4 * gi];
-      cFi = A.scal[4 * gi + 1];
-      wsFi = A.wsF[gi];
+      gFi = gFa[i];
+      cFi = cFa[i];
+      wsFi = wsFa[i];
     }
     T V[3] = {0, 0, 0}, P[6] = {0, 0, 0, 0, 0, 0};
     T dacc[2][3] = {{0, 0, 0}, {0, 0, 0}}; // dense ρ-chain, columns m = lane, lane + 32
@@ -530,11 +602,14 @@ __global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps
         const T r = sqrt_t(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         const int tj = typ[j];
         R.j = j;
-        R.tj = tj;
-        R.ephi = R.erj = R.eri = -1;
-        R.dgj = R.dgi = R.gFj = R.cFj = T(0);
-        R.wsj = 0;
-        R.tphi = R.trj = R.tri = T(0);
+        for (int s = 0; s < 4; ++s) {
+          R.e[s] = -1;
+          R.cbase[s] = 0;
+          R.nv[s] = 0;
+          R.t[s] = R.w[s] = R.ih[s] = T(0);
+        }
+        R.dgi = R.cFj = T(0);
+        T dgj = T(0);
         if (r >= T(1e-14)) {
           const T ir = T(1) / r;
           for (int a = 0; a < 3; ++a) R.u[a] = d[a] * ir;
@@ -544,83 +619,85 @@ __global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps
           R.v[3] = d[0] * d[1] * ir;
           R.v[4] = d[0] * d[2] * ir;
           R.v[5] = d[1] * d[2] * ir;
+          auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt) {
+            T t;
+            const int e = seg_of(tb, rr, t);
+            R.e[s] = e;
+            R.t[s] = t;
+            R.w[s] = wgt;
+            R.ih[s] = tb.inv_h;
+            R.cbase[s] = tb.cmap0 + segws[e];
+            R.nv[s] = tb.n - segws[e];
+            return e;
+          };
           const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
           const bool phi_in = EAM ? in_span(tp, r) : (r >= tp.x0 && r < tp.xmax);
-          if (phi_in) R.ephi = seg_of(tp, r, R.tphi);
+          if (phi_in) set_slot(0, tp, r, T(1));
           if constexpr (EAM) {
             const STab<T> &gj = tabs[np + tj], &gi_ = tabs[np + ti];
+            const T gFj = gFa[j];
+            R.cFj = cFa[j];
             if (in_span(gj, r)) {
-              R.erj = seg_of(gj, r, R.trj);
-              R.dgj = seg_der<T>(seg[R.erj], R.trj, gj.inv_h);
+              const int e = set_slot(1, gj, r, tj == ti ? gFi + gFj : gFi);
+              dgj = seg_der<T>(seg[e], R.t[1], gj.inv_h);
             }
             if (in_span(gi_, r)) {
-              R.eri = seg_of(gi_, r, R.tri);
-              R.dgi = seg_der<T>(seg[R.eri], R.tri, gi_.inv_h);
+              T t;
+              const int e = seg_of(gi_, r, t);
+              R.dgi = seg_der<T>(seg[e], t, gi_.inv_h);
+              if (tj != ti) set_slot(2, gi_, r, gFj);
             }
-            const int64_t gj_ = static_cast<int64_t>(cd.atom0) + j;
-            R.gFj = A.scal[4 * gj_];
-            R.cFj = A.scal[4 * gj_ + 1];
-            R.wsj = A.wsF[gj_];
+            // F_j window: coefficient dgd_j[q]·ρ'_{ti}(r)
+            const STab<T> &te = tabs[np + nt + tj];
+            const int wsj = wsFa[j];
+            R.e[3] = -2;
+            R.w[3] = R.dgi;
+            R.cbase[3] = te.cmap0 + wsj;
+            R.nv[3] = te.n - wsj;
           }
         } else {
           for (int a = 0; a < 3; ++a) R.u[a] = T(0);
           for (int a = 0; a < 6; ++a) R.v[a] = T(0);
         }
         rec[lane] = R;
-        for (int a = 0; a < 3; ++a) V[a] += R.dgj * R.u[a];
-        for (int a = 0; a < 6; ++a) P[a] += R.dgj * R.v[a];
+        for (int a = 0; a < 3; ++a) V[a] += dgj * R.u[a];
+        for (int a = 0; a < 6; ++a) P[a] += dgj * R.v[a];
       }
       __syncwarp();
-      // sparse knot-window scatter, one pair at a time
-      const int slot = lane / kWin, q = lane % kWin;
+      // sparse knot-window scatter, one pair at a time, 24 lanes = 4 slots × 6 knots
       for (int k = 0; k < cnt; ++k) {
         const PairRec<T> &R = rec[k];
         if (lane < 4 * kWin) {
-          int e = -1, tab = -1, col = -1;
-          T tt = T(0), weight = T(0), ih = T(0);
-          bool stress = true, energy = false;
-          if (slot == 0) {
-            e = R.ephi;
-            tab = pair_ord(ti, R.tj, nt);
-            tt = R.tphi;
-            weight = T(1);
-            energy = true;
-          } else if (EAM && slot == 1) {
-            e = R.erj;
-            tab = np + R.tj;
-            tt = R.trj;
-            weight = (R.tj == ti) ? gFi + R.gFj : gFi;
-          } else if (EAM && slot == 2) {
-            e = (R.tj == ti) ? -1 : R.eri;
-            tab = np + ti;
-            tt = R.tri;
-            weight = R.gFj;
-          } else if (EAM && slot == 3) {
-            const STab<T> &te = tabs[np + nt + R.tj];
-            const int knot = R.wsj + q;
-            if (knot < te.n) col = cmap[te.cmap0 + knot];
-            const T cf = A.dgd[(static_cast<int64_t>(cd.atom0) + R.j) * kWin + q] * R.dgi;
-            if (col >= 0 && cf != T(0)) {
-              for (int a = 0; a < 3; ++a) frow[a * D + col] += cf * R.u[a];
-            }
-            stress = false;
-          }
-          if (slot < 3 && e >= 0) {
-            const STab<T> &tb = tabs[tab];
-            ih = tb.inv_h;
-            const int knot = segws[e] + q;
-            if (knot < tb.n) col = cmap[tb.cmap0 + knot];
-            if (col >= 0) {
+          const int e = R.e[slot];
+          const int col = (e != -1 && q < R.nv[slot]) ? cmap[R.cbase[slot] + q] : -1;
+          if (col >= 0) {
+            const T tt = R.t[slot];
+            T cf, dv = T(0);
+            if (e >= 0) {
               const T *G = segg + e * 4 * kWin;
-              const T dd = (G[kWin + q] + tt * (T(2) * G[2 * kWin + q] + T(3) * tt * G[3 * kWin + q])) * ih;
-              const T cf = weight * dd;
-              for (int a = 0; a < 3; ++a) frow[a * D + col] += cf * R.u[a];
-              if (stress && want_stress)
-                for (int a = 0; a < 6; ++a) srow[a * D + col] += cf * R.v[a];
-              if (energy) {
-                const T dv = G[q] + tt * (G[kWin + q] + tt * (G[2 * kWin + q] + tt * G[3 * kWin + q]));
-                erow[col] += half_we * dv;
-              }
+              const T g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
+              cf = R.w[slot] * ((g1 + tt * (T(2) * g2 + T(3) * tt * g3)) * R.ih[slot]);
+              if (slot == 0) dv = half_we * (G[q] + tt * (g1 + tt * (g2 + tt * g3)));
+            } else {
+              cf = R.w[slot] * dgda[R.j * kWin + q];
+            }
+            T4 fr = frow[col];
+            fr.x += cf * R.u[0];
+            fr.y += cf * R.u[1];
+            fr.z += cf * R.u[2];
+            fr.w += dv;
+            frow[col] = fr;
+            if (want_stress && e >= 0) {
+              T2 s0 = srow[3 * col], s1 = srow[3 * col + 1], s2 = srow[3 * col + 2];
+              s0.x += cf * R.v[0];
+              s0.y += cf * R.v[1];
+              s1.x += cf * R.v[2];
+              s1.y += cf * R.v[3];
+              s2.x += cf * R.v[4];
+              s2.y += cf * R.v[5];
+              srow[3 * col] = s0;
+              srow[3 * col + 1] = s1;
+              srow[3 * col + 2] = s2;
             }
           }
         }
@@ -632,12 +709,15 @@ __global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps
           const PairRec<T> &R = rec[k];
           const T wgt = R.cFj * R.dgi;
           if (wgt == T(0)) continue;
-          const T *drj = A.drho + (static_cast<int64_t>(cd.atom0) + R.j) * A.ndens;
+          const T *drj = drho + R.j * dstr;
+          const T u0 = R.u[0], u1 = R.u[1], u2 = R.u[2];
           for (int s2 = 0; s2 < 2; ++s2) {
             const int m = lane + 32 * s2;
-            if (m < A.ndens) {
+            if (m < nd) {
               const T dv = wgt * drj[m];
-              for (int a = 0; a < 3; ++a) dacc[s2][a] += dv * R.u[a];
+              dacc[s2][0] += dv * u0;
+              dacc[s2][1] += dv * u1;
+              dacc[s2][2] += dv * u2;
             }
           }
         }
@@ -647,58 +727,110 @@ __global__ void __launch_bounds__(256) jac_forces_kernel(JacArgs<T> A, int warps
     for (int a = 0; a < 3; ++a) V[a] = warp_sum_group(V[a], 32);
     for (int a = 0; a < 6; ++a) P[a] = warp_sum_group(P[a], 32);
     if constexpr (EAM) {
-      const T *dri = A.drho + gi * A.ndens;
+      const T *dri = drho + i * dstr;
       for (int s2 = 0; s2 < 2; ++s2) {
         const int m = lane + 32 * s2;
-        if (m < A.ndens) {
+        if (m < nd) {
           const T gim = cFi * dri[m];
           const int col = A.dens_c0 + m;
-          for (int a = 0; a < 3; ++a) frow[a * D + col] += dacc[s2][a] + gim * V[a];
-          if (want_stress)
-            for (int a = 0; a < 6; ++a) srow[a * D + col] += T(2) * P[a] * gim;
+          T4 fr = frow[col];
+          fr.x += dacc[s2][0] + gim * V[0];
+          fr.y += dacc[s2][1] + gim * V[1];
+          fr.z += dacc[s2][2] + gim * V[2];
+          frow[col] = fr;
+          if (want_stress) {
+            const T g2 = T(2) * gim;
+            srow[3 * col].x += g2 * P[0];
+            srow[3 * col].y += g2 * P[1];
+            srow[3 * col + 1].x += g2 * P[2];
+            srow[3 * col + 1].y += g2 * P[3];
+            srow[3 * col + 2].x += g2 * P[4];
+            srow[3 * col + 2].y += g2 * P[5];
+          }
         }
       }
+      __syncwarp();
       if (lane < kWin) {
         const STab<T> &te = tabs[np + nt + ti];
         const int knot = wsFi + lane;
         const int col = knot < te.n ? cmap[te.cmap0 + knot] : -1;
-        const T dg = A.dgd[gi * kWin + lane];
+        const T dg = dgda[i * kWin + lane];
         if (col >= 0 && dg != T(0)) {
-          for (int a = 0; a < 3; ++a) frow[a * D + col] += dg * V[a];
-          if (want_stress)
-            for (int a = 0; a < 6; ++a) srow[a * D + col] += T(2) * P[a] * dg;
+          T4 fr = frow[col];
+          fr.x += dg * V[0];
+          fr.y += dg * V[1];
+          fr.z += dg * V[2];
+          frow[col] = fr;
+          if (want_stress) {
+            const T g2 = T(2) * dg;
+            srow[3 * col].x += g2 * P[0];
+            srow[3 * col].y += g2 * P[1];
+            srow[3 * col + 1].x += g2 * P[2];
+            srow[3 * col + 1].y += g2 * P[3];
+            srow[3 * col + 2].x += g2 * P[4];
+            srow[3 * col + 2].y += g2 * P[5];
+          }
         }
       }
     }
     __syncwarp();
+    const double F0 = A.F[row0 + 3 * i], F1 = A.F[row0 + 3 * i + 1], F2 = A.F[row0 + 3 * i + 2];
     for (int col = lane; col < D; col += 32) {
-      T *Jc = A.J + static_cast<int64_t>(col) * A.M + row0 + 3 * i;
-      Jc[0] = frow[col];
-      Jc[1] = frow[D + col];
-      Jc[2] = frow[2 * D + col];
+      const T4 fr = frow[col];
+      T *Jc = A.J + static_cast<int64_t>(col) * A.ld + row0 + 3 * i;
+      Jc[0] = fr.x;
+      Jc[1] = fr.y;
+      Jc[2] = fr.z;
+      erow[col] += fr.w;
+      jtr[col] += static_cast<double>(fr.x) * F0 + static_cast<double>(fr.y) * F1 + static_cast<double>(fr.z) * F2;
     }
     __syncwarp();
   }
   __syncthreads();
   const int64_t rE = row0 + 3 * N;
   const double sc = -A.w_s * 0.5 / cd.volume;
+  const int64_t rL = rE + 1 + (want_stress ? 6 : 0);
   for (int col = threadIdx.x; col < D; col += blockDim.x) {
-    double e = 0.0;
-    for (int ww = 0; ww < warps; ++ww) e += static_cast<double>(rowb[static_cast<size_t>(ww) * 10 * D + 9 * D + col]);
-    T *Jc = A.J + static_cast<int64_t>(col) * A.M;
+    double e = 0.0, jr = 0.0;
+    for (int ww = 0; ww < warps; ++ww) {
+      e += static_cast<double>(erow_all[static_cast<size_t>(ww) * D + col]);
+      jr += jtr_all[static_cast<size_t>(ww) * D + col];
+    }
+    T *Jc = A.J + static_cast<int64_t>(col) * A.ld;
     if constexpr (EAM)
       Jc[rE] = static_cast<T>(static_cast<double>(Jc[rE]) + e);
     else
       Jc[rE] = static_cast<T>(e);
+    // Jᵀr over this configuration's rows: force rows (above), energy, stress, limit
+    jr += static_cast<double>(Jc[rE]) * A.F[rE];
+    if constexpr (EAM) jr += static_cast<double>(Jc[rL]) * A.F[rL];
     if (want_stress) {
+      double s[6] = {0, 0, 0, 0, 0, 0};
+      for (int ww = 0; ww < warps; ++ww) {
+        const T2 *sr = srow_all + static_cast<size_t>(ww) * 3 * D + 3 * col;
+        s[0] += static_cast<double>(sr[0].x);
+        s[1] += static_cast<double>(sr[0].y);
+        s[2] += static_cast<double>(sr[1].x);
+        s[3] += static_cast<double>(sr[1].y);
+        s[4] += static_cast<double>(sr[2].x);
+        s[5] += static_cast<double>(sr[2].y);
+      }
       for (int v = 0; v < 6; ++v) {
-        double s = 0.0;
-        for (int ww = 0; ww < warps; ++ww) s += static_cast<double>(rowb[static_cast<size_t>(ww) * 10 * D + (3 + v) * D + col]);
-        Jc[rE + 1 + v] = static_cast<T>(sc * s);
+        Jc[rE + 1 + v] = static_cast<T>(sc * s[v]);
+        jr += static_cast<double>(Jc[rE + 1 + v]) * A.F[rE + 1 + v];
       }
     }
-    if constexpr (!EAM) Jc[rE + 1 + (want_stress ? 6 : 0)] = T(0); // limit row: no embedding
+    if constexpr (!EAM) Jc[rL] = T(0); // limit row: no embedding
+    A.jtr_part[static_cast<int64_t>(c) * D + col] = jr;
   }
+}
+
+__global__ void jtr_reduce_kernel(const double *__restrict__ part, int n_cfg, int D, double *__restrict__ Jtr) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= D) return;
+  double s = 0.0;
+  for (int c = 0; c < n_cfg; ++c) s += part[static_cast<int64_t>(c) * D + col];
+  Jtr[col] = s;
 }
 
 template <class T> Common make_common(fs_gpu *h) {
@@ -782,14 +914,27 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   const bool eam = h->family == FS_FAMILY_EAM;
   const int64_t M = rows_of(h, w_s);
   const int D = h->D;
-  // buffers
-  const size_t jn = static_cast<size_t>(M) * D;
-  if (static_cast<size_t>(h->jac_alloc) < jn || !h->d_J) {
+  // J: column-major with the leading dimension rounded up to 32 rows (a
+  // 16-byte multiple, as a TMA row stride needs); padding rows stay zero
+  const int64_t ldj = (M + 31) / 32 * 32;
+  const size_t jn = static_cast<size_t>(ldj) * D;
+  if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J) {
     if (h->d_J) cudaFree(h->d_J);
     h->d_J = nullptr;
     if (cudaMalloc(&h->d_J, std::max<size_t>(jn, 1) * sizeof(T)) != cudaSuccess)
       return set_error(h, FS_ERR_NOMEM, "cudaMalloc (J)");
+    FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     h->jac_alloc = static_cast<int64_t>(jn);
+    h->ldj = ldj;
+  }
+  {
+    const size_t need = static_cast<size_t>(h->n_cfg) * D;
+    if (h->jtr_part_alloc < need || !h->d_jtr_part) {
+      if (h->d_jtr_part) cudaFree(h->d_jtr_part);
+      h->d_jtr_part = nullptr;
+      FS_CUDA(cudaMalloc(&h->d_jtr_part, std::max<size_t>(need, 1) * sizeof(double)));
+      h->jtr_part_alloc = need;
+    }
   }
   if (!h->d_JtJ) {
     FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
@@ -838,17 +983,27 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   a.w_e = w_e;
   a.w_s = w_s;
   a.M = M;
+  a.ld = ldj;
   a.D = D;
+  a.F = h->d_F;
+  a.jtr_part = h->d_jtr_part;
   a.dens_c0 = dens_c0;
   a.ndens = ndens;
   a.J = static_cast<T *>(h->d_J);
-  a.scal = static_cast<T *>(h->d_atom_scalars);
+  {
+    T *sc = static_cast<T *>(h->d_atom_scalars);
+    const size_t na = static_cast<size_t>(h->n_atoms);
+    a.gF = sc;
+    a.cF = sc ? sc + na : nullptr;
+    a.over = sc ? sc + 2 * na : nullptr;
+  }
   a.drho = static_cast<T *>(h->d_drho);
   a.dgd = static_cast<T *>(h->d_dgd);
   a.wsF = h->d_wsF;
+  a.stage = 0;
   const size_t common = jac_common_smem<T>(a.c.n_tables, h->n_segs, h->n_cmap, h->max_natoms, max_images(h));
   if (eam) {
-    const size_t sm1 = common + align16(2 * D * sizeof(double)) + 32;
+    const size_t sm1 = common + align16(2 * D * sizeof(double)) + atom_stage_smem<T>(h->max_natoms, ndens) + 64;
     if (sm1 > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: configuration too large");
     FS_CUDA(cudaFuncSetAttribute(jac_atoms_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sm1)));
@@ -857,19 +1012,38 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
     ++h->launches;
   }
   mark(h, 2);
-  int warps = 8;
+  // per-warp buffers + (optionally) the configuration's staged per-atom data;
+  // prefer the most warps that fit with staging, else the most without
+  auto k2_smem = [&](int wp) {
+    return common + align16(static_cast<size_t>(wp) * D * 4 * sizeof(T)) +
+           align16(static_cast<size_t>(wp) * 3 * D * 2 * sizeof(T)) + align16(static_cast<size_t>(wp) * D * sizeof(T)) +
+           align16(static_cast<size_t>(wp) * 32 * sizeof(PairRec<T>)) +
+           align16(static_cast<size_t>(wp) * D * sizeof(double)) + 112;
+  };
+  const size_t stage_b = eam ? atom_stage_smem<T>(h->max_natoms, ndens) : 0;
+  const size_t cap = 227 * 1024;
+  int warps = 0;
   size_t sm2 = 0;
-  for (; warps >= 1; warps >>= 1) {
-    sm2 = common + align16(static_cast<size_t>(warps) * 10 * D * sizeof(T)) +
-          align16(static_cast<size_t>(warps) * 32 * sizeof(PairRec<T>)) + 64;
-    if (sm2 <= 227 * 1024) break;
-  }
+  if (eam)
+    for (int wp = 8; wp >= 4 && !warps; --wp)
+      if (k2_smem(wp) + stage_b <= cap) {
+        warps = wp;
+        sm2 = k2_smem(wp) + stage_b;
+        a.stage = 1;
+      }
+  for (int wp = 8; wp >= 1 && !warps; --wp)
+    if (k2_smem(wp) <= cap) {
+      warps = wp;
+      sm2 = k2_smem(wp);
+    }
   if (warps < 1) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: configuration too large");
   auto k2 = eam ? jac_forces_kernel<T, true> : jac_forces_kernel<T, false>;
   FS_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm2)));
   k2<<<h->n_cfg, 32 * warps, sm2, h->stream>>>(a, warps);
   FS_CUDA(cudaGetLastError());
-  ++h->launches;
+  jtr_reduce_kernel<<<(D + 127) / 128, 128, 0, h->stream>>>(h->d_jtr_part, h->n_cfg, D, h->d_Jtr);
+  FS_CUDA(cudaGetLastError());
+  h->launches += 2;
   mark(h, 3);
   return FS_OK;
 }

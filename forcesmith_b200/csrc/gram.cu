@@ -1,8 +1,9 @@
-// Normal-equation products JᵀJ (D × D) and Jᵀr (D) with FP64 accumulation,
-// the inputs of NormalEquationsSolver and the LM step
-// (src/optimization/solver.cpp:242-266).
+// Normal-equation product JᵀJ (D × D) with FP64 accumulation, an input of
+// NormalEquationsSolver and the LM step (src/optimization/solver.cpp:242-266);
+// Jᵀr is accumulated in FP64 by the Jacobian kernels themselves.
 //
-// SIMT path: 64 × 64 output tiles (upper triangle only) × a split of the rows.
+// SIMT path (FP64 mode, or D > 256): 64 × 64 output tiles (upper triangle
+// only) × a split of the rows.
 // Each 32-row slab is multiplied in the working precision and folded into
 // FP64 accumulators, so the FP32 partial sums never exceed 32 terms.
 // Split partials are reduced in a fixed order (deterministic result).
@@ -16,13 +17,11 @@ namespace {
 constexpr int TB = 64, KS = 32;
 
 template <class T>
-__global__ void __launch_bounds__(256) gram_partial_kernel(const T *__restrict__ J, const double *__restrict__ F,
-                                                           int64_t M, int D, int64_t rows_per_split,
-                                                           const int2 *__restrict__ tiles,
-                                                           double *__restrict__ part, double *__restrict__ part_r) {
+__global__ void __launch_bounds__(256) gram_partial_kernel(const T *__restrict__ J, int64_t ld, int64_t M, int D,
+                                                           int64_t rows_per_split, const int2 *__restrict__ tiles,
+                                                           double *__restrict__ part) {
   __shared__ T As[KS][TB + 1];
   __shared__ T Bs[KS][TB + 1];
-  __shared__ double Fs[KS];
   const int2 tp = tiles[blockIdx.x];
   const int split = blockIdx.y;
   const int a0 = tp.x * TB, b0 = tp.y * TB;
@@ -30,22 +29,16 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(const T *__restrict__
   const int64_t r_begin = static_cast<int64_t>(split) * rows_per_split;
   const int64_t r_end = min(M, r_begin + rows_per_split);
   double acc[4][4];
-  double accr[4] = {0, 0, 0, 0};
   for (int x = 0; x < 4; ++x)
     for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
-  const bool diag = tp.x == tp.y;
   for (int64_t r0 = r_begin; r0 < r_end; r0 += KS) {
     // load As[k][c] = J[r0+k, a0+c]; column-major: consecutive k are contiguous
     for (int idx = threadIdx.x; idx < KS * TB; idx += blockDim.x) {
       const int k = idx % KS, cc = idx / KS;
       const int64_t r = r0 + k;
       const int ca = a0 + cc, cb = b0 + cc;
-      As[k][cc] = (r < r_end && ca < D) ? J[static_cast<int64_t>(ca) * M + r] : T(0);
-      Bs[k][cc] = (r < r_end && cb < D) ? J[static_cast<int64_t>(cb) * M + r] : T(0);
-    }
-    if (diag && threadIdx.x < KS) {
-      const int64_t r = r0 + threadIdx.x;
-      Fs[threadIdx.x] = r < r_end ? F[r] : 0.0;
+      As[k][cc] = (r < r_end && ca < D) ? J[static_cast<int64_t>(ca) * ld + r] : T(0);
+      Bs[k][cc] = (r < r_end && cb < D) ? J[static_cast<int64_t>(cb) * ld + r] : T(0);
     }
     __syncthreads();
     T s[4][4];
@@ -61,10 +54,6 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(const T *__restrict__
     }
     for (int x = 0; x < 4; ++x)
       for (int y = 0; y < 4; ++y) acc[x][y] += static_cast<double>(s[x][y]);
-    if (diag && ty == 0) {
-      for (int k = 0; k < KS; ++k)
-        for (int x = 0; x < 4; ++x) accr[x] += static_cast<double>(As[k][tx * 4 + x]) * Fs[k];
-    }
     __syncthreads();
   }
   double *P = part + static_cast<size_t>(split) * D * D;
@@ -73,15 +62,9 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(const T *__restrict__
       const int a = a0 + tx * 4 + x, b = b0 + ty * 4 + y;
       if (a < D && b < D) P[static_cast<size_t>(a) * D + b] = acc[x][y];
     }
-  if (diag && ty == 0)
-    for (int x = 0; x < 4; ++x) {
-      const int a = a0 + tx * 4 + x;
-      if (a < D) part_r[static_cast<size_t>(split) * D + a] = accr[x];
-    }
 }
 
-__global__ void gram_reduce_kernel(const double *__restrict__ part, const double *__restrict__ part_r, int splits,
-                                   int D, double *__restrict__ JtJ, double *__restrict__ Jtr) {
+__global__ void gram_reduce_kernel(const double *__restrict__ part, int splits, int D, double *__restrict__ JtJ) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx < D * D) {
     const int a = idx / D, b = idx % D;
@@ -92,18 +75,14 @@ __global__ void gram_reduce_kernel(const double *__restrict__ part, const double
       if (a / TB < b / TB) JtJ[static_cast<size_t>(b) * D + a] = s;
     }
   }
-  if (idx < D) {
-    double s = 0.0;
-    for (int k = 0; k < splits; ++k) s += part_r[static_cast<size_t>(k) * D + idx];
-    Jtr[idx] = s;
-  }
 }
 
 } // namespace
 
-int gram(fs_gpu *h, int64_t M, double *JtJ, double *Jtr) {
+int gram(fs_gpu *h, int64_t M, double *JtJ, double *) {
   const int D = h->D;
   if (D == 0) return FS_OK;
+  if (h->precision == FS_PREC_FP32 && D <= 256) return gram_tc(h, M, JtJ);
   const int T = (D + TB - 1) / TB;
   std::vector<int2> tiles;
   for (int a = 0; a < T; ++a)
@@ -113,7 +92,7 @@ int gram(fs_gpu *h, int64_t M, double *JtJ, double *Jtr) {
   int64_t rps = (M + splits - 1) / splits;
   rps = (rps + KS - 1) / KS * KS;
   splits = static_cast<int>((M + rps - 1) / rps);
-  const size_t need = static_cast<size_t>(splits) * D * D + static_cast<size_t>(splits) * D + 2 * nt;
+  const size_t need = static_cast<size_t>(splits) * D * D + 2 * nt;
   if (h->gram_part_alloc < need || !h->d_gram_part) {
     if (h->d_gram_part) cudaFree(h->d_gram_part);
     h->d_gram_part = nullptr;
@@ -121,18 +100,17 @@ int gram(fs_gpu *h, int64_t M, double *JtJ, double *Jtr) {
     h->gram_part_alloc = need;
   }
   double *part = h->d_gram_part;
-  double *part_r = part + static_cast<size_t>(splits) * D * D;
-  int2 *d_tiles = reinterpret_cast<int2 *>(part_r + static_cast<size_t>(splits) * D);
+  int2 *d_tiles = reinterpret_cast<int2 *>(part + static_cast<size_t>(splits) * D * D);
   FS_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, h->stream));
   dim3 grid(nt, splits);
   if (h->precision == FS_PREC_FP64)
-    gram_partial_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<const double *>(h->d_J), h->d_F, M, D,
-                                                              rps, d_tiles, part, part_r);
+    gram_partial_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<const double *>(h->d_J), h->ldj, M, D,
+                                                              rps, d_tiles, part);
   else
-    gram_partial_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<const float *>(h->d_J), h->d_F, M, D, rps,
-                                                            d_tiles, part, part_r);
+    gram_partial_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<const float *>(h->d_J), h->ldj, M, D, rps,
+                                                            d_tiles, part);
   FS_CUDA(cudaGetLastError());
-  gram_reduce_kernel<<<(D * D + 255) / 256, 256, 0, h->stream>>>(part, part_r, splits, D, JtJ, Jtr);
+  gram_reduce_kernel<<<(D * D + 255) / 256, 256, 0, h->stream>>>(part, splits, D, JtJ);
   FS_CUDA(cudaGetLastError());
   h->launches += 2;
   return FS_OK;

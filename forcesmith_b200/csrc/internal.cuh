@@ -146,7 +146,11 @@ struct fs_gpu {
   double *d_obj = nullptr;       // scalar
   // Jacobian buffers
   int64_t jac_alloc = 0;         // elements of J
-  void *d_J = nullptr;           // column-major rows × D, FP32 or FP64
+  void *d_J = nullptr;           // column-major ldj × D, FP32 or FP64 (rows ≥ M are zero)
+  int64_t ldj = 0;               // leading dimension of J (rows rounded up to 32)
+  double *d_jtr_part = nullptr;  // per-config Jᵀr partials (FP64)
+  size_t jtr_part_alloc = 0;
+  int32_t *d_err = nullptr;      // device error word (bounded waits that gave up)
   double *d_JtJ = nullptr;       // D × D
   double *d_Jtr = nullptr;       // D
   double *d_gram_part = nullptr; // split partials
@@ -162,6 +166,8 @@ struct fs_gpu {
 
   // LM solve scratch
   double *d_chol = nullptr;
+  int chol_D = 0;
+  int max_type = 0;
   double *d_dx = nullptr;
   int32_t *d_flag = nullptr;
 
@@ -205,6 +211,7 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s);
 
 // gram.cu
 int gram(fs_gpu *h, int64_t m, double *JtJ_dev, double *Jtr_dev);
+int gram_tc(fs_gpu *h, int64_t m, double *JtJ_dev); // tcgen05 (FP32 J)
 
 // solve.cu
 int lm_solve(fs_gpu *h, double lambda, int mode, double *dx_host);

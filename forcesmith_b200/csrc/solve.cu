@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(1024) chol_solve_kernel(const double *__restri
   for (int k = tid; k < D * D; k += nth) {
     const int i = k / D, j = k % D;
     double v = JtJ[k];
-    if (i == j) v += lambda * (mode == 1 ? JtJ[k] : 1.0);
+    if (i == j) v += lambda * (mode == 1 ? (JtJ[k] > 0.0 ? JtJ[k] : 1.0) : 1.0); // zero column → 1
     A[k] = v;
   }
   __syncthreads();
@@ -66,7 +66,11 @@ __global__ void __launch_bounds__(1024) chol_solve_kernel(const double *__restri
 
 int lm_solve(fs_gpu *h, double lambda, int mode, double *dx_host) {
   const int D = h->D;
-  if (!h->d_chol) {
+  if (!h->d_chol || h->chol_D != D) {
+    if (h->d_chol) cudaFree(h->d_chol);
+    if (h->d_dx) cudaFree(h->d_dx);
+    if (h->d_flag) cudaFree(h->d_flag);
+    h->chol_D = D;
     FS_CUDA(cudaMalloc(&h->d_chol, static_cast<size_t>(std::max(D, 1)) * std::max(D, 1) * sizeof(double)));
     FS_CUDA(cudaMalloc(&h->d_dx, std::max(D, 1) * sizeof(double)));
     FS_CUDA(cudaMalloc(&h->d_flag, sizeof(int32_t)));

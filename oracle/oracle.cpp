@@ -1161,7 +1161,11 @@ int orc_normal_equations(const double *J, const double *F, int64_t m, int32_t D,
 int orc_lm_step(const double *JtJ, const double *Jtr, int32_t D, double lambda, int32_t mode,
                 double *dx) {
   std::vector<double> A(JtJ, JtJ + static_cast<int64_t>(D) * D);
-  for (int i = 0; i < D; ++i) A[i * D + i] += lambda * (mode == 1 ? JtJ[i * D + i] : 1.0);
+  // Marquardt scaling by diag(JᵀJ), with 1 where a column is zero (MINPACK's rule)
+  for (int i = 0; i < D; ++i) {
+    const double dii = JtJ[i * D + i];
+    A[i * D + i] += lambda * (mode == 1 ? (dii > 0.0 ? dii : 1.0) : 1.0);
+  }
   if (!cholesky(A, D)) return FS_ERR_NUMERIC;
   for (int i = 0; i < D; ++i) dx[i] = -Jtr[i];
   chol_solve(A, D, dx);

@@ -21,6 +21,7 @@ def cluster(pos, box, types=None, ref_force=None):
 
 
 def concat(*dss):
+    dss = [d if d.ref_force is not None else with_zero_labels(d) for d in dss]
     return Dataset(np.concatenate([d.natoms for d in dss]).astype(np.int32),
                    np.concatenate([d.box9 for d in dss]),
                    np.concatenate([d.pos for d in dss]),
