@@ -68,11 +68,11 @@ __global__ void gram_reduce_kernel(const double *__restrict__ part, int splits, 
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx < D * D) {
     const int a = idx / D, b = idx % D;
-    if (a / TB <= b / TB) { // computed tile (upper block triangle)
+    if (a <= b) { // upper triangle, mirrored: JᵀJ is exactly symmetric
       double s = 0.0;
       for (int k = 0; k < splits; ++k) s += part[static_cast<size_t>(k) * D * D + idx];
       JtJ[idx] = s;
-      if (a / TB < b / TB) JtJ[static_cast<size_t>(b) * D + a] = s;
+      JtJ[static_cast<size_t>(b) * D + a] = s;
     }
   }
 }

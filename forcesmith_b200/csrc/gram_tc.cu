@@ -4,7 +4,11 @@
 // rows as the contraction dimension K — K-major for both operands.  Each CTA
 // owns a contiguous slab of rows (split-K over 148 SMs):
 //   - a TMA producer thread streams 32-row × 256-column tiles of Jᵀ
-//     (32 KB, 128-byte swizzle) through a 4-stage mbarrier ring;
+//     (32 KB, 128-byte swizzle) through a 3-stage mbarrier ring;
+//   - two warps split every landed tile into hi = TF32(x) (round to nearest)
+//     in place and lo = x − hi beside it (3×TF32: hi·hi + hi·lo + lo·hi keeps
+//     ≈ 2⁻²¹ relative accuracy, where plain TF32 truncation biases JᵀJ by
+//     ≈ −1e-3);
 //   - one thread issues the MMAs: rows [0,128) of Jᵀ against all 256 columns
 //     (M=128, N=256) and rows [128,256) against columns [128,256) (M=128,
 //     N=128) — the lower-left block is the transpose of the upper-right;
@@ -25,10 +29,11 @@
 namespace fsg {
 namespace {
 
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kKChunk = 32;                                  // rows of J per stage (128 B of FP32)
 constexpr int kTileN = 256;                                  // columns of J per stage
-constexpr uint32_t kStageBytes = kKChunk * kTileN * 4;       // 32 KB
+constexpr uint32_t kTileBytes = kKChunk * kTileN * 4;        // 32 KB landed by TMA (then hi)
+constexpr uint32_t kStageBytes = 2 * kTileBytes;             // + 32 KB lo
 constexpr int kThreads = 128;
 constexpr uint32_t kTmemCols = 512;
 constexpr long long kWaitCycles = 4000000000ll;              // ≈ 2 s at 2 GHz
@@ -72,6 +77,10 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
           smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
       : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -142,9 +151,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char *stage = base;
   uint64_t *full = reinterpret_cast<uint64_t *>(base + kStages * kStageBytes);
   uint64_t *empty = full + kStages;
-  uint64_t *done = empty + kStages;
+  uint64_t *conv = empty + kStages;
+  uint64_t *done = conv + kStages;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
-  __shared__ int failed;
+  __shared__ volatile int failed;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t r0 = static_cast<int64_t>(blockIdx.x) * rows_per_cta;
   const int64_t r1 = min(ld, r0 + rows_per_cta);
@@ -154,6 +164,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
+      mbar_init(&conv[s], 2);
     }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -173,30 +184,63 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int kc = 0; kc < nchunks; ++kc) {
       const int s = kc % kStages;
       if (kc >= kStages && !mbar_wait(&empty[s], ((kc / kStages) - 1) & 1)) {
-        atomicExch(&failed, 1);
+        atomicExch(const_cast<int *>(&failed), 1);
         break;
       }
-      mbar_expect_tx(&full[s], kStageBytes);
+      mbar_expect_tx(&full[s], kTileBytes);
       tma_load_2d(stage + static_cast<size_t>(s) * kStageBytes, &tmap, &full[s],
                   static_cast<int>(r0 + static_cast<int64_t>(kc) * kKChunk), 0);
     }
+  } else if (warp >= 2) {
+    // hi/lo split of every landed tile (element-wise, so the swizzle is kept)
+    for (int kc = 0; kc < nchunks && !failed; ++kc) {
+      const int s = kc % kStages;
+      if (!mbar_wait(&full[s], (kc / kStages) & 1)) {
+        atomicExch(const_cast<int *>(&failed), 1);
+        break;
+      }
+      float4 *hi = reinterpret_cast<float4 *>(stage + static_cast<size_t>(s) * kStageBytes);
+      float4 *lo = reinterpret_cast<float4 *>(stage + static_cast<size_t>(s) * kStageBytes + kTileBytes);
+      for (int k = threadIdx.x - 64; k < static_cast<int>(kTileBytes / 16); k += 64) {
+        const float4 x = hi[k];
+        float4 a, b;
+        const float *xs = &x.x;
+        float *as = &a.x, *bs = &b.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float h = __uint_as_float((__float_as_uint(xs[e]) + 0x1000u) & 0xFFFFE000u);
+          as[e] = h;
+          bs[e] = xs[e] - h;
+        }
+        hi[k] = a;
+        lo[k] = b;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&conv[s]);
+    }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer
+    // MMA issuer: per 8-element K step, hi·hi + hi·lo + lo·hi for both blocks
     constexpr uint32_t id_full = idesc_tf32(128, 256), id_half = idesc_tf32(128, 128);
     for (int kc = 0; kc < nchunks; ++kc) {
       const int s = kc % kStages;
-      if (!mbar_wait(&full[s], (kc / kStages) & 1)) {
-        atomicExch(&failed, 1);
+      if (!mbar_wait(&conv[s], (kc / kStages) & 1)) {
+        atomicExch(const_cast<int *>(&failed), 1);
         break;
       }
       tc_fence_after();
-      const uint32_t sa = smem_u32(stage + static_cast<size_t>(s) * kStageBytes);
+      const uint32_t sh = smem_u32(stage + static_cast<size_t>(s) * kStageBytes);
+      const uint32_t sl = sh + kTileBytes;
 #pragma unroll
       for (int ks = 0; ks < kKChunk / 8; ++ks) {
-        const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
         const uint32_t k_off = ks * 32; // 8 TF32 elements of K = 32 bytes inside the swizzle row
-        umma_tf32(tmem, desc_sw128(sa + k_off), desc_sw128(sa + k_off), id_full, acc);
-        umma_tf32(tmem + 256, desc_sw128(sa + 16384 + k_off), desc_sw128(sa + 16384 + k_off), id_half, acc);
+        const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
+        umma_tf32(tmem, desc_sw128(sh + k_off), desc_sw128(sh + k_off), id_full, acc);
+        umma_tf32(tmem, desc_sw128(sh + k_off), desc_sw128(sl + k_off), id_full, 1u);
+        umma_tf32(tmem, desc_sw128(sl + k_off), desc_sw128(sh + k_off), id_full, 1u);
+        umma_tf32(tmem + 256, desc_sw128(sh + 16384 + k_off), desc_sw128(sh + 16384 + k_off), id_half, acc);
+        umma_tf32(tmem + 256, desc_sw128(sh + 16384 + k_off), desc_sw128(sl + 16384 + k_off), id_half, 1u);
+        umma_tf32(tmem + 256, desc_sw128(sl + 16384 + k_off), desc_sw128(sh + 16384 + k_off), id_half, 1u);
       }
       umma_commit(&empty[s]);
     }
@@ -205,7 +249,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncwarp();
   // epilogue: every warp drains its 32 TMEM lanes
   const bool ok = mbar_wait(done, 0);
-  if (!ok) atomicExch(&failed, 1);
+  if (!ok) atomicExch(const_cast<int *>(&failed), 1);
   tc_fence_after();
   __syncthreads();
   if (!failed) {
@@ -244,12 +288,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
-// Σ over CTAs in a fixed order; (a ≥ 128, b < 128) is mirrored from (b, a).
+// Σ over CTAs in a fixed order; the lower triangle mirrors the upper one, so
+// JᵀJ is exactly symmetric.
 __global__ void gram_tc_reduce_kernel(const double *__restrict__ part, int nparts, int D, double *__restrict__ JtJ) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= D * D) return;
   const int a = idx / D, b = idx % D;
-  const size_t src = (a >= 128 && b < 128) ? static_cast<size_t>(b) * D + a : static_cast<size_t>(idx);
+  const size_t src = (a > b) ? static_cast<size_t>(b) * D + a : static_cast<size_t>(idx);
   double s = 0.0;
   for (int k = 0; k < nparts; ++k) s += part[static_cast<size_t>(k) * D * D + src];
   JtJ[idx] = s;
@@ -299,7 +344,7 @@ int gram_tc(fs_gpu *h, int64_t M, double *JtJ) {
     FS_CUDA(cudaMalloc(&h->d_err, sizeof(int32_t)));
     FS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), h->stream));
   }
-  const size_t smem = kStages * kStageBytes + 1024 + 256;
+  const size_t smem = kStages * kStageBytes + 1024 + 256; // 3 × 64 KB + barriers
   FS_CUDA(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   gram_tc_kernel<<<ncta, kThreads, smem, h->stream>>>(map, D, rows_per_cta, ld, h->d_gram_part, h->d_err);
   FS_CUDA(cudaGetLastError());
