@@ -57,6 +57,12 @@ class fs_gpu_opts(C.Structure):
                 ("lanes_per_atom", C.c_int32), ("reserved", C.c_int32)]
 
 
+class fs_de_opts(C.Structure):
+    _fields_ = [("NP", C.c_int32), ("reserved", C.c_int32), ("mutation", C.c_double),
+                ("crossover", C.c_double), ("seed", C.c_uint64), ("w_e", C.c_double),
+                ("w_s", C.c_double)]
+
+
 def _dp(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
 
@@ -183,6 +189,10 @@ class Dataset:
         return Dataset(np.ascontiguousarray(self.natoms[idx]), np.ascontiguousarray(self.box9[idx]),
                        np.ascontiguousarray(self.pos[sel]), np.ascontiguousarray(self.type[sel]),
                        g(self.ref_force, sel), g(self.ref_energy, idx), g(self.ref_stress9, idx))
+
+    def with_types(self, type_):
+        return Dataset(self.natoms, self.box9, self.pos, np.ascontiguousarray(type_, np.int32),
+                       self.ref_force, self.ref_energy, self.ref_stress9)
 
     def with_labels(self, forces, energy, stress9):
         return Dataset(self.natoms, self.box9, self.pos, self.type,

@@ -47,16 +47,24 @@ def build_gpu(force=False, verbose=False, extra=()):
         return GPU_LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    headers = [d for d in deps if not d.endswith(".cu")]
+    objs, jobs = [], []
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s) + ".o")
-        cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-               "-I", INC, "-I", CSRC, "--expt-relaxed-constexpr", "-rdc=false",
-               *extra, "-c", s, "-o", o]
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
         objs.append(o)
+        if force or _stale(o, [s, *headers]):
+            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                   "-I", INC, "-I", CSRC, "--expt-relaxed-constexpr", "-rdc=false",
+                   *extra, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            jobs.append(cmd)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), jobs)):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     cmd = [NVCC, *ARCH, "-shared", *objs, "-o", GPU_LIB + ".tmp", "-lcudart"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)

@@ -111,6 +111,10 @@ void free_configs(fs_gpu *h) {
   dfree(h->d_limit);
   dfree(h->d_obj_part);
   dfree(h->d_obj);
+  dfree(h->d_pop_seg_a);
+  h->pop_alloc = 0;
+  fsg::de_free(h->de);
+  h->de = nullptr;
   h->rows_alloc = 0;
   h->rcut_built = -1.0;
   h->n_pairs = 0;
@@ -217,7 +221,7 @@ int fs_gpu_destroy(fs_gpu *h) {
   dfree(h->d_chol);
   dfree(h->d_dx);
   dfree(h->d_flag);
-  dfree(h->d_pop_seg_a);
+  dfree(h->d_pop_spl);
   dfree(h->d_pop_vals);
   dfree(h->d_pop_obj);
   dfree(h->d_err);
@@ -379,6 +383,10 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
   h->rcut_built = -1.0;
   h->jac_valid = false;
   free_jacobian(h);
+  fsg::de_free(h->de);
+  h->de = nullptr;
+  dfree(h->d_pop_spl);
+  h->pop_spl_count = 0;
   FS_TRY(upload_tables(h));
   h->params_dirty = true;
   return FS_OK;
@@ -519,8 +527,6 @@ int fs_gpu_eval(fs_gpu *h, double w_e, double w_s, double *F, double *forces, do
 
 int fs_gpu_eval_jacobian_async(fs_gpu *h, double w_e, double w_s) {
   FS_TRY(check_ready(h));
-  if (h->family == FS_FAMILY_ADP)
-    return set_error(h, FS_ERR_UNSUPPORTED, "eval_jacobian: ADP Jacobian is not handled by this build");
   cudaSetDevice(h->device);
   FS_TRY(ensure_eval_buffers(h, w_s));
   FS_TRY(ensure_params(h));

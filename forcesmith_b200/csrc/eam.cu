@@ -18,64 +18,12 @@
 // periodic image shifts and the spline segment tables sit in shared memory;
 // the neighbour list is a 4-byte (j, image) word per directed pair, and each
 // pair vector is rebuilt in FP64 then rounded to the working precision T.
-#include "spline_dev.cuh"
+#include "kern_common.cuh"
 
 #include <algorithm>
 
 namespace fsg {
 namespace {
-
-struct Smem {
-  unsigned char *p;
-  __device__ explicit Smem(unsigned char *base) : p(base) {}
-  template <class X> __device__ X *take(size_t n, size_t align = 16) {
-    uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    a = (a + align - 1) & ~(uintptr_t)(align - 1);
-    X *r = reinterpret_cast<X *>(a);
-    p = reinterpret_cast<unsigned char *>(a + n * sizeof(X));
-    return r;
-  }
-};
-
-inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
-
-struct Common {
-  const CfgDev *cfg;
-  const double *wpos;
-  const int32_t *type;
-  const double *ref_force;
-  const int32_t *nb_start;
-  const uint32_t *nb_pack;
-  const TableDesc *desc;
-  const int32_t *cmap;
-  int n_tables, n_segs, n_cmap, ntypes;
-  int family; // FS_FAMILY_EAM or FS_FAMILY_PAIR
-};
-
-// Stage the configuration geometry: wrapped positions (FP64), species, and
-// the image shift table ix·a + iy·b + iz·c.
-__device__ void stage_geometry(const CfgDev &cd, const Common &A, double *wpos, double *shift, uint8_t *typ) {
-  const int N = cd.natoms;
-  for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) wpos[k] = A.wpos[3 * static_cast<int64_t>(cd.atom0) + k];
-  for (int k = threadIdx.x; k < N; k += blockDim.x) typ[k] = static_cast<uint8_t>(A.type[cd.atom0 + k]);
-  const int wx = 2 * cd.sx + 1, wy = 2 * cd.sy + 1, wz = 2 * cd.sz + 1;
-  for (int k = threadIdx.x; k < wx * wy * wz; k += blockDim.x) {
-    const double ix = k / (wy * wz) - cd.sx, iy = (k / wz) % wy - cd.sy, iz = k % wz - cd.sz;
-    for (int a = 0; a < 3; ++a) shift[3 * k + a] = ix * cd.box[3 * a] + iy * cd.box[3 * a + 1] + iz * cd.box[3 * a + 2];
-  }
-}
-
-template <class T>
-__device__ __forceinline__ void pair_vec(const double *wpos, const double *shift, int i, uint32_t pk, int &j,
-                                         T &dx, T &dy, T &dz) {
-  j = static_cast<int>(pk & 0xFFFFFu);
-  const int img = static_cast<int>(pk >> 20);
-  dx = static_cast<T>((wpos[3 * j] - wpos[3 * i]) + shift[3 * img]);
-  dy = static_cast<T>((wpos[3 * j + 1] - wpos[3 * i + 1]) + shift[3 * img + 1]);
-  dz = static_cast<T>((wpos[3 * j + 2] - wpos[3 * i + 2]) + shift[3 * img + 2]);
-}
-
-template <class T> __device__ __forceinline__ T sqrt_t(T x) { return sqrt(x); }
 
 template <class T> struct ResArgs {
   Common c;
@@ -99,29 +47,15 @@ template <class T> size_t residual_smem(int n_tables, int n_segs, int max_atoms,
 // ---------------------------------------------------------------------------
 // Residual: ρ pass → embedding → force/energy/stress pass → residual rows.
 // ---------------------------------------------------------------------------
-template <class T, int LPA, bool EAM>
-__global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
-  using T4 = typename Vec4T<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int c = blockIdx.x;
-  const CfgDev &cd = A.c.cfg[c];
+// The residual of one configuration from staged tables and geometry: writes
+// its rows when ROWS, and returns Σ rows² (valid on thread 0) — shared by the
+// residual kernel and the population kernel.
+template <class T, int LPA, bool EAM, bool ROWS>
+__device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, const STab<T> *tabs,
+                              const typename Vec4T<T>::type *seg, const double *wpos, const double *shift,
+                              const uint8_t *typ, T *rho, T *gradF, double *red) {
   const int N = cd.natoms;
   const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
-  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
-  Smem S(smem_raw);
-  STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
-  T4 *seg = S.take<T4>(A.c.n_segs);
-  double *wpos = S.take<double>(3 * N);
-  double *shift = S.take<double>(3 * nimg);
-  uint8_t *typ = S.take<uint8_t>(N);
-  T *rho = S.take<T>(N);
-  T *gradF = S.take<T>(N);
-  double *red = S.take<double>(64);
-  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
-  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) seg[k] = A.seg_a[k];
-  stage_geometry(cd, A.c, wpos, shift, typ);
-  __syncthreads();
-
   const int ngroups = blockDim.x / LPA, g = threadIdx.x / LPA, l = threadIdx.x % LPA;
   const int32_t *start = A.c.nb_start + cd.atom0;
   double e_emb = 0.0, lim = 0.0;
@@ -241,8 +175,10 @@ __global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
       for (int a = 0; a < 3; ++a) {
         const double fa = static_cast<double>(f[a]);
         const double res = fa - A.c.ref_force[3 * ga + a];
-        A.F[row0 + 3 * i + a] = res;
-        if (A.forces) A.forces[3 * ga + a] = fa;
+        if constexpr (ROWS) {
+          A.F[row0 + 3 * i + a] = res;
+          if (A.forces) A.forces[3 * ga + a] = fa;
+        }
         objp += res * res;
       }
       e_pair += 0.5 * static_cast<double>(ep);
@@ -254,28 +190,31 @@ __global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
   double st[6];
   for (int a = 0; a < 6; ++a) st[a] = block_sum(sg[a], red);
   const double op = block_sum(objp, red);
+  double out = 0.0;
   if (threadIdx.x == 0) {
     const double iv = 1.0 / cd.volume;
     for (int a = 0; a < 6; ++a) st[a] = st[a] * iv; // σ /= V (eval_scope.hpp:28)
     int64_t row = row0 + 3 * N;
     double o = op;
     const double re = A.w_e * (E - cd.ref_energy);
-    A.F[row++] = re;
+    if constexpr (ROWS) A.F[row] = re;
+    ++row;
     o += re * re;
     static constexpr int vi[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
     if (A.w_s > 0.0) {
       for (int v = 0; v < 6; ++v) {
         const double rs = A.w_s * (st[v] - cd.ref_stress[3 * vi[v][0] + vi[v][1]]);
-        A.F[row++] = rs;
+        if constexpr (ROWS) A.F[row] = rs;
+        ++row;
         o += rs * rs;
       }
     }
-    A.F[row++] = L;
+    if constexpr (ROWS) A.F[row] = L;
     o += L * L;
-    A.obj_part[c] = o;
-    if (A.energy) A.energy[c] = E;
-    if (A.limit) A.limit[c] = L;
-    if (A.stress9) {
+    out = o;
+    if (ROWS && A.energy) A.energy[c] = E;
+    if (ROWS && A.limit) A.limit[c] = L;
+    if (ROWS && A.stress9) {
       double *s9 = A.stress9 + 9 * static_cast<int64_t>(c);
       s9[0] = st[0];
       s9[4] = st[1];
@@ -284,6 +223,67 @@ __global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
       s9[2] = s9[6] = st[4];
       s9[5] = s9[7] = st[5];
     }
+  }
+  return out;
+}
+
+template <class T, int LPA, bool EAM>
+__global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
+  using T4 = typename Vec4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x;
+  const CfgDev &cd = A.c.cfg[c];
+  const int N = cd.natoms;
+  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  Smem S(smem_raw);
+  STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
+  T4 *seg = S.take<T4>(A.c.n_segs);
+  double *wpos = S.take<double>(3 * N);
+  double *shift = S.take<double>(3 * nimg);
+  uint8_t *typ = S.take<uint8_t>(N);
+  T *rho = S.take<T>(N);
+  T *gradF = S.take<T>(N);
+  double *red = S.take<double>(64);
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) seg[k] = A.seg_a[k];
+  stage_geometry(cd, A.c, wpos, shift, typ);
+  __syncthreads();
+  const double o = config_pass<T, LPA, EAM, true>(A, c, cd, tabs, seg, wpos, shift, typ, rho, gradF, red);
+  if (threadIdx.x == 0) A.obj_part[c] = o;
+}
+
+// Population objective: one CTA per (configuration, tile of trial vectors).
+// The configuration's geometry is staged once; each trial's spline segments
+// (built by pop_setup_kernel) are swapped in and the configuration's Σ rows²
+// is written to part[trial][config].
+template <class T, int LPA, bool EAM>
+__global__ void __launch_bounds__(256) pop_eval_kernel(ResArgs<T> A, const typename Vec4T<T>::type *pop_seg,
+                                                       int NP, int tile, int n_tiles, const int32_t *order,
+                                                       double *part) {
+  using T4 = typename Vec4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = order[blockIdx.x / n_tiles];
+  const int k0 = (blockIdx.x % n_tiles) * tile, k1 = min(NP, k0 + tile);
+  const CfgDev &cd = A.c.cfg[c];
+  const int N = cd.natoms;
+  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  Smem S(smem_raw);
+  STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
+  T4 *seg = S.take<T4>(A.c.n_segs);
+  double *wpos = S.take<double>(3 * N);
+  double *shift = S.take<double>(3 * nimg);
+  uint8_t *typ = S.take<uint8_t>(N);
+  T *rho = S.take<T>(N);
+  T *gradF = S.take<T>(N);
+  double *red = S.take<double>(64);
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  stage_geometry(cd, A.c, wpos, shift, typ);
+  for (int k = k0; k < k1; ++k) {
+    for (int q = threadIdx.x; q < A.c.n_segs; q += blockDim.x) seg[q] = pop_seg[static_cast<int64_t>(k) * A.c.n_segs + q];
+    __syncthreads();
+    const double o = config_pass<T, LPA, EAM, false>(A, c, cd, tabs, seg, wpos, shift, typ, rho, gradF, red);
+    if (threadIdx.x == 0) part[static_cast<int64_t>(k) * A.c.cfg_count + c] = o;
+    __syncthreads();
   }
 }
 
@@ -848,6 +848,7 @@ template <class T> Common make_common(fs_gpu *h) {
   c.n_cmap = h->n_cmap;
   c.ntypes = h->ntypes;
   c.family = h->family;
+  c.cfg_count = h->n_cfg;
   return c;
 }
 
@@ -1048,6 +1049,154 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   return FS_OK;
 }
 
+
+// Per-trial makima segments for the population kernel: block (table, trial)
+// rebuilds the knot values from the trial vector (fixed knots from the model)
+// and computes the slopes and power-basis coefficients with the same
+// arithmetic as the single-model setup.
+template <class T>
+__global__ void pop_setup_kernel(const TableDesc *__restrict__ desc, const int *__restrict__ spl,
+                                 const double *__restrict__ vals, const int32_t *__restrict__ cmap,
+                                 const double *__restrict__ xs, int D, int n_segs,
+                                 typename Vec4T<T>::type *__restrict__ pop_seg) {
+  using T4 = typename Vec4T<T>::type;
+  const TableDesc td = desc[spl[blockIdx.x]];
+  const int k = blockIdx.y, n = td.n;
+  __shared__ double y[512], s[512];
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int col = cmap[td.cmap0 + q];
+    y[q] = col >= 0 ? xs[static_cast<int64_t>(k) * D + col] : vals[td.pv0 + q];
+  }
+  __syncthreads();
+  const double h = td.h;
+  auto sec = [&](int q) { return (y[q + 1] - y[q]) / h; };
+  auto wgt = [](double u, double v) { return fabs(u - v) + fabs(u + v) / 2; };
+  auto slope = [&](double p1, double p2, double p3, double p4) {
+    const double w1 = wgt(p4, p3), w2 = wgt(p2, p1);
+    const double r = (w1 * p2 + w2 * p3) / (w1 + w2);
+    return (isnan(r) || w1 + w2 == 0.0) ? 0.0 : r;
+  };
+  if (n >= 4)
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      double v;
+      if (q == 0 || q == 1) {
+        const double m0 = sec(0), m1 = sec(1);
+        const double mm1 = 2.0 * m0 + -1.0 * m1;
+        v = q == 0 ? slope(2.0 * mm1 + -1.0 * m0, mm1, m0, m1) : slope(mm1, m0, m1, sec(2));
+      } else if (q >= n - 2) {
+        const double mnm3 = sec(n - 3), mnm2 = sec(n - 2);
+        const double mnm1 = 2.0 * mnm2 + -1.0 * mnm3;
+        v = q == n - 2 ? slope(sec(n - 4), mnm3, mnm2, mnm1) : slope(mnm3, mnm2, mnm1, 2.0 * mnm1 + -1.0 * mnm2);
+      } else {
+        v = slope(sec(q - 2), sec(q - 1), sec(q), sec(q + 1));
+      }
+      s[q] = v;
+    }
+  __syncthreads();
+  for (int e = threadIdx.x; e <= n; e += blockDim.x) {
+    double a[4] = {0, 0, 0, 0};
+    if (e == 0) {
+      a[0] = y[0];
+      a[1] = y[1] - y[0];
+    } else if (e == n) {
+      a[0] = y[n - 1];
+      a[1] = y[n - 1] - y[n - 2];
+    } else {
+      const int i = e - 1;
+      if (n < 4) {
+        a[0] = y[i];
+        a[1] = y[i + 1] - y[i];
+      } else {
+        const double s0 = s[i], s1 = s[i + 1];
+        a[0] = y[i];
+        a[1] = h * s0;
+        a[2] = -3.0 * y[i] - 2.0 * h * s0 + 3.0 * y[i + 1] - h * s1;
+        a[3] = 2.0 * y[i] + h * s0 - 2.0 * y[i + 1] + h * s1;
+      }
+    }
+    T4 o;
+    o.x = static_cast<T>(a[0]);
+    o.y = static_cast<T>(a[1]);
+    o.z = static_cast<T>(a[2]);
+    o.w = static_cast<T>(a[3]);
+    pop_seg[static_cast<int64_t>(k) * n_segs + td.seg0 + e] = o;
+  }
+}
+
+__global__ void pop_reduce_kernel(const double *__restrict__ part, int n_cfg, int NP, double *__restrict__ obj) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= NP) return;
+  double s = 0.0;
+  for (int c = 0; c < n_cfg; ++c) s += part[static_cast<int64_t>(k) * n_cfg + c];
+  obj[k] = s;
+}
+
+template <class T, int LPA, bool EAM>
+int launch_population_t(fs_gpu *h, double w_e, double w_s, const double *d_xs, int NP, double *d_obj) {
+  using T4 = typename Vec4T<T>::type;
+  ResArgs<T> a;
+  a.c = make_common<T>(h);
+  a.seg_a = nullptr;
+  a.w_e = w_e;
+  a.w_s = w_s;
+  a.F = a.forces = a.energy = a.stress9 = a.limit = a.obj_part = nullptr;
+  // layout: config order (n_cfg int32, fixed offset 0) | per-trial segments | per-(trial, config) Σ rows²
+  const size_t ordb = (h->n_cfg * sizeof(int32_t) + 255) / 256 * 256;
+  const size_t segb = (static_cast<size_t>(NP) * h->n_segs * sizeof(T4) + 255) / 256 * 256;
+  const size_t partb = static_cast<size_t>(NP) * h->n_cfg * sizeof(double);
+  const size_t need = ordb + segb + partb;
+  if (static_cast<size_t>(h->pop_alloc) < need || !h->d_pop_seg_a) {
+    if (h->d_pop_seg_a) cudaFree(h->d_pop_seg_a);
+    h->d_pop_seg_a = nullptr;
+    FS_CUDA(cudaMalloc(&h->d_pop_seg_a, need));
+    h->pop_alloc = static_cast<int64_t>(need);
+    // configurations in decreasing atom count (largest work items first)
+    std::vector<int32_t> ord(h->n_cfg);
+    for (int c = 0; c < h->n_cfg; ++c) ord[c] = c;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return h->natoms[x] > h->natoms[y]; });
+    FS_CUDA(cudaMemcpy(h->d_pop_seg_a, ord.data(), h->n_cfg * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  const int32_t *order = static_cast<const int32_t *>(h->d_pop_seg_a);
+  T4 *pop_seg = reinterpret_cast<T4 *>(static_cast<char *>(h->d_pop_seg_a) + ordb);
+  double *part = reinterpret_cast<double *>(static_cast<char *>(h->d_pop_seg_a) + ordb + segb);
+  std::vector<int> spl;
+  for (int t = 0; t < static_cast<int>(h->desc.size()); ++t)
+    if (h->desc[t].kind == FS_TABLE_SPLINE) spl.push_back(t);
+  if (h->pop_spl_count != static_cast<int>(spl.size()) || !h->d_pop_spl) {
+    if (h->d_pop_spl) cudaFree(h->d_pop_spl);
+    FS_CUDA(cudaMalloc(&h->d_pop_spl, std::max<size_t>(spl.size(), 1) * sizeof(int)));
+    FS_CUDA(cudaMemcpy(h->d_pop_spl, spl.data(), spl.size() * sizeof(int), cudaMemcpyHostToDevice));
+    h->pop_spl_count = static_cast<int>(spl.size());
+  }
+  if (!spl.empty()) {
+    dim3 g(static_cast<unsigned>(spl.size()), static_cast<unsigned>(NP));
+    pop_setup_kernel<T><<<g, 32, 0, h->stream>>>(h->d_desc, h->d_pop_spl, h->d_vals, h->d_cmap, d_xs, h->D,
+                                                 h->n_segs, pop_seg);
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+  }
+  const int tile = std::max(1, std::min(16, NP));
+  const int n_tiles = (NP + tile - 1) / tile;
+  const size_t sm = residual_smem<T>(a.c.n_tables, h->n_segs, h->max_natoms, max_images(h));
+  auto k = pop_eval_kernel<T, LPA, EAM>;
+  FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+  k<<<static_cast<unsigned>(h->n_cfg) * n_tiles, 256, sm, h->stream>>>(a, pop_seg, NP, tile, n_tiles, order, part);
+  FS_CUDA(cudaGetLastError());
+  pop_reduce_kernel<<<(NP + 127) / 128, 128, 0, h->stream>>>(part, h->n_cfg, NP, d_obj);
+  FS_CUDA(cudaGetLastError());
+  h->launches += 2;
+  return FS_OK;
+}
+
+template <class T, bool EAM> int launch_population_lpa(fs_gpu *h, double w_e, double w_s, const double *xs, int NP, double *obj) {
+  switch (choose_lpa(h)) {
+  case 4: return launch_population_t<T, 4, EAM>(h, w_e, w_s, xs, NP, obj);
+  case 8: return launch_population_t<T, 8, EAM>(h, w_e, w_s, xs, NP, obj);
+  case 16: return launch_population_t<T, 16, EAM>(h, w_e, w_s, xs, NP, obj);
+  default: return launch_population_t<T, 32, EAM>(h, w_e, w_s, xs, NP, obj);
+  }
+}
+
 } // namespace
 
 int eval_residual(fs_gpu *h, double w_e, double w_s) {
@@ -1070,4 +1219,20 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s) {
                                       : launch_jacobian_t<float>(h, w_e, w_s);
 }
 
+} // namespace fsg
+
+namespace fsg {
+// Σ‖F(x_k)‖² for NP device-resident trial vectors (EAM / pair families).
+int eval_population_device(fs_gpu *h, double w_e, double w_s, const double *d_xs, int NP, double *d_obj) {
+  if (h->family != FS_FAMILY_EAM && h->family != FS_FAMILY_PAIR)
+    return set_error(h, FS_ERR_UNSUPPORTED, "population kernel: EAM and pair families");
+  for (const HostTable &t : h->tables)
+    if (t.kind != FS_TABLE_SPLINE) return set_error(h, FS_ERR_UNSUPPORTED, "population kernel: spline tables");
+  const bool eam = h->family == FS_FAMILY_EAM;
+  if (h->precision == FS_PREC_FP64)
+    return eam ? launch_population_lpa<double, true>(h, w_e, w_s, d_xs, NP, d_obj)
+               : launch_population_lpa<double, false>(h, w_e, w_s, d_xs, NP, d_obj);
+  return eam ? launch_population_lpa<float, true>(h, w_e, w_s, d_xs, NP, d_obj)
+             : launch_population_lpa<float, false>(h, w_e, w_s, d_xs, NP, d_obj);
+}
 } // namespace fsg

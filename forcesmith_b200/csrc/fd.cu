@@ -1,0 +1,99 @@
+// Central-difference Jacobian on the device — the reference's own method
+// (opt::fd_jacobian, include/forcesmith/optimization/fd_jacobian.hpp:37-49:
+// h = 1e-5, x restored by the same add/subtract sequence), used for families
+// without an analytic device Jacobian in this build (ADP).  2·D residual
+// launches; FP64 contexts only (FP32 residuals are too coarse for h = 1e-5).
+#include "internal.cuh"
+
+#include <vector>
+
+namespace fsg {
+namespace {
+
+__global__ void fd_column(const double *__restrict__ Fp, const double *__restrict__ Fm, int64_t M, double inv2h,
+                          double *__restrict__ col) {
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < M;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    col[r] = (Fp[r] - Fm[r]) * inv2h;
+}
+
+__global__ void jtr_dense(const double *__restrict__ J, int64_t ld, int64_t M, const double *__restrict__ F,
+                          double *__restrict__ Jtr) {
+  __shared__ double red[32];
+  const int col = blockIdx.x;
+  double s = 0.0;
+  for (int64_t r = threadIdx.x; r < M; r += blockDim.x) s += J[col * ld + r] * F[r];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) t += red[k];
+    Jtr[col] = t;
+  }
+}
+
+} // namespace
+
+int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s) {
+  if (h->precision != FS_PREC_FP64)
+    return set_error(h, FS_ERR_UNSUPPORTED, "central-difference Jacobian needs an FP64 context");
+  const int D = h->D;
+  const int64_t M = rows_of(h, w_s);
+  const int64_t ldj = (M + 31) / 32 * 32;
+  const size_t jn = static_cast<size_t>(ldj) * D;
+  if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J) {
+    if (h->d_J) cudaFree(h->d_J);
+    h->d_J = nullptr;
+    FS_CUDA(cudaMalloc(&h->d_J, std::max<size_t>(jn, 1) * sizeof(double)));
+    FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(double), h->stream));
+    h->jac_alloc = static_cast<int64_t>(jn);
+    h->ldj = ldj;
+  }
+  if (!h->d_JtJ) {
+    FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
+    FS_CUDA(cudaMalloc(&h->d_Jtr, std::max(D, 1) * sizeof(double)));
+  }
+  double *Fbase = nullptr, *Fp = nullptr;
+  FS_CUDA(cudaMallocAsync(&Fbase, M * sizeof(double), h->stream));
+  FS_CUDA(cudaMallocAsync(&Fp, M * sizeof(double), h->stream));
+  FS_CUDA(cudaMemcpyAsync(Fbase, h->d_F, M * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  std::vector<double> x(D), xp;
+  FS_TRY(fs_gpu_gather_params(h, x.data()));
+  xp = x;
+  const double hh = 1e-5;
+  int rc = FS_OK;
+  for (int j = 0; j < D && rc == FS_OK; ++j) {
+    xp[j] += hh;
+    rc = fs_gpu_set_params(h, xp.data(), D);
+    if (rc == FS_OK) rc = refresh_segments(h);
+    if (rc == FS_OK) rc = eval_residual(h, w_e, w_s);
+    if (rc != FS_OK) break;
+    FS_CUDA(cudaMemcpyAsync(Fp, h->d_F, M * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    xp[j] -= 2.0 * hh;
+    rc = fs_gpu_set_params(h, xp.data(), D);
+    if (rc == FS_OK) rc = refresh_segments(h);
+    if (rc == FS_OK) rc = eval_residual(h, w_e, w_s);
+    if (rc != FS_OK) break;
+    xp[j] += hh;
+    fd_column<<<256, 256, 0, h->stream>>>(Fp, h->d_F, M, 1.0 / (2.0 * hh),
+                                          static_cast<double *>(h->d_J) + static_cast<int64_t>(j) * ldj);
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+  }
+  const int rc2 = fs_gpu_set_params(h, x.data(), D);
+  if (rc == FS_OK) rc = rc2;
+  if (rc == FS_OK) rc = refresh_segments(h);
+  h->params_dirty = false;
+  FS_CUDA(cudaMemcpyAsync(h->d_F, Fbase, M * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  if (rc == FS_OK) {
+    jtr_dense<<<D, 256, 0, h->stream>>>(static_cast<const double *>(h->d_J), ldj, M, h->d_F, h->d_Jtr);
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+  }
+  cudaFreeAsync(Fbase, h->stream);
+  cudaFreeAsync(Fp, h->stream);
+  return rc;
+}
+
+} // namespace fsg

@@ -92,6 +92,11 @@ struct HostTable {
 
 } // namespace fsg
 
+namespace fsg {
+struct DeState;
+void de_free(DeState *s);
+} // namespace fsg
+
 struct fs_gpu {
   int device = 0;
   int precision = FS_PREC_FP32;
@@ -177,10 +182,15 @@ struct fs_gpu {
   int64_t launches = 0;
 
   // population scratch
-  void *d_pop_seg_a = nullptr;
+  void *d_pop_seg_a = nullptr;   // per-trial segments | per-(trial, config) Σ rows² | config order
+  int64_t pop_alloc = 0;
+  int *d_pop_spl = nullptr;      // spline table indices
+  int pop_spl_count = 0;
   double *d_pop_vals = nullptr;
   double *d_pop_obj = nullptr;
-  int pop_alloc = 0;
+
+  // device differential evolution (population.cu)
+  fsg::DeState *de = nullptr;
 };
 
 namespace fsg {
@@ -216,8 +226,9 @@ int gram_tc(fs_gpu *h, int64_t m, double *JtJ_dev); // tcgen05 (FP32 J)
 // solve.cu
 int lm_solve(fs_gpu *h, double lambda, int mode, double *dx_host);
 
-// population.cu
+// population.cu / eam.cu
 int eval_population(fs_gpu *h, double w_e, double w_s, const double *xs, int NP, double *obj);
+int eval_population_device(fs_gpu *h, double w_e, double w_s, const double *d_xs, int NP, double *d_obj);
 
 inline int64_t rows_of(const fs_gpu *h, double w_s) {
   return 3 * h->n_atoms + static_cast<int64_t>(h->n_cfg) * (2 + (w_s > 0.0 ? 6 : 0));

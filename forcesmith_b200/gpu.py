@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import (FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
+from .abi import (fs_de_opts, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
                   fs_model, load_library)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -52,6 +52,9 @@ def lib() -> C.CDLL:
         L.fs_gpu_lm_step.argtypes = [vp, dbl, i32, pd]
         L.fs_gpu_lsq_step.argtypes = [vp, dbl, pd]
         L.fs_gpu_eval_population.argtypes = [vp, dbl, dbl, pd, i32, pd]
+        L.fs_gpu_de_init.argtypes = [vp, C.POINTER(fs_de_opts), pd, pd, pd]
+        L.fs_gpu_de_run.argtypes = [vp, i32, i32, pd, pd, pd]
+        L.fs_gpu_de_population.argtypes = [vp, pd, pd]
         _LIB = L
     return _LIB
 
@@ -142,6 +145,37 @@ class GpuSession(Session):
         self._check(self._lib.fs_gpu_eval_population(self._h, w_e, w_s, _dp(xs), xs.shape[0],
                                                      _dp(obj)), "eval_population")
         return obj
+
+    # -- differential evolution on the device ---------------------------------
+    def de_init(self, lo, hi, x0=None, NP=None, mutation=0.65, crossover=0.5, seed=42,
+                w_e=1.0, w_s=0.0):
+        lo = np.ascontiguousarray(lo, np.float64)
+        hi = np.ascontiguousarray(hi, np.float64)
+        NP = int(NP if NP is not None else 15 * lo.size)
+        o = fs_de_opts(NP, 0, float(mutation), float(crossover), int(seed), float(w_e), float(w_s))
+        px = None
+        if x0 is not None:
+            x0 = np.ascontiguousarray(x0, np.float64)
+            px = _dp(x0)
+        self._check(self._lib.fs_gpu_de_init(self._h, C.byref(o), _dp(lo), _dp(hi), px), "de_init")
+        self._de_np = NP
+
+    def de_run(self, generations, use_graph=True, history=False):
+        D = self.param_count()
+        best = np.zeros(1)
+        x = np.zeros(D)
+        hist = np.zeros(max(int(generations), 1)) if history else None
+        self._check(self._lib.fs_gpu_de_run(self._h, int(generations), 1 if use_graph else 0,
+                                            _dp(best), _dp(x), _dp(hist) if history else None),
+                    "de_run")
+        return (best[0], x, hist[:generations]) if history else (best[0], x)
+
+    def de_population(self):
+        D = self.param_count()
+        pop = np.zeros((self._de_np, D))
+        obj = np.zeros(self._de_np)
+        self._check(self._lib.fs_gpu_de_population(self._h, _dp(pop), _dp(obj)), "de_population")
+        return pop, obj
 
 
 def _bind_instrumentation():

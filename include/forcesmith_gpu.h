@@ -237,6 +237,39 @@ int fs_gpu_launch_count(fs_gpu *h, int64_t *count);
 int fs_gpu_eval_population(fs_gpu *h, double w_e, double w_s, const double *xs,
                            int32_t NP, double *obj);
 
+/*
+ * Differential evolution on the device — replaces BoostDESolver::solve
+ * (src/optimization/solver.cpp:113-155; DEParams: NP, mutation F, crossover
+ * CR, seed, max_generations).  DE/rand/1/bin with box clamping and greedy
+ * selection; a generation is trial construction, the batched objective
+ * (fs_gpu_eval_population's kernels) and selection, captured once as a CUDA
+ * graph and replayed when use_graph != 0.  Random numbers are a counter hash
+ * of (seed, generation, member), so a run is reproducible for a given seed;
+ * it does not reproduce Boost.Math's random stream.
+ *
+ * fs_gpu_de_init: population member 0 = clamp(x0) when x0 != NULL, the rest
+ * uniform in [lo, hi]; evaluates the initial population.  Any later
+ * fs_gpu_upload_configs / fs_gpu_set_model discards the DE state.
+ * fs_gpu_de_run: `generations` more generations; writes the best objective
+ * and vector, and when history != NULL the best objective after each
+ * generation (that adds one host sync per generation).
+ * fs_gpu_de_population: copies the population (NP·D) and its objectives.
+ */
+typedef struct fs_de_opts {
+    int32_t NP;        /* population size, >= 4 */
+    int32_t reserved;
+    double mutation;   /* F  (reference default 0.65) */
+    double crossover;  /* CR (reference default 0.5)  */
+    uint64_t seed;
+    double w_e, w_s;   /* energy / stress weights of the objective */
+} fs_de_opts;
+
+int fs_gpu_de_init(fs_gpu *h, const fs_de_opts *opts, const double *lo,
+                   const double *hi, const double *x0);
+int fs_gpu_de_run(fs_gpu *h, int32_t generations, int32_t use_graph,
+                  double *best_obj, double *best_x, double *history);
+int fs_gpu_de_population(fs_gpu *h, double *pop, double *obj);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

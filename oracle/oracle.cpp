@@ -974,6 +974,8 @@ int orc_set_model(orc_state *h, const fs_model *m) {
 
 int orc_prepare(orc_state *h) {
   if (!h || !h->S.have_model) return FS_ERR_STATE;
+  for (const auto t : h->S.type)
+    if (t < 0 || t >= h->S.ntypes) return FS_ERR_ARG; // species slot outside the model
   build_neighbors(h->S, max_cutoff(h->S));
   prime_sites(h->S);
   return FS_OK;
@@ -1025,6 +1027,13 @@ int orc_gather_bounds(orc_state *h, double *lo, double *hi) {
 int orc_set_params(orc_state *h, const double *x, int32_t D) {
   if (!h || !x || D != param_count(h->S)) return FS_ERR_ARG;
   scatter(h->S, x);
+  // with_eval_scope rebuilds the lists whenever the cutoff changes
+  // (eval_scope.hpp:13-20); pairs beyond a shorter cutoff contribute zero, so
+  // only a longer one needs new lists.
+  if (h->S.rcut_built >= 0 && max_cutoff(h->S) > h->S.rcut_built) {
+    build_neighbors(h->S, max_cutoff(h->S));
+    prime_sites(h->S);
+  }
   return FS_OK;
 }
 int orc_residual_count(orc_state *h, double w_s, int64_t *m) {
@@ -1078,12 +1087,19 @@ int orc_eval_jacobian_fd(orc_state *h, double w_e, double w_s, double *J, int32_
   gather(S, x.data());
   xp = x;
   const double hh = 1e-5;
+  auto scatter_fit = [&](const double *xx) {
+    scatter(S, xx);
+    if (max_cutoff(S) > S.rcut_built) {
+      build_neighbors(S, max_cutoff(S));
+      prime_sites(S);
+    }
+  };
   for (int j = c0; j < c1; ++j) {
     xp[j] += hh;
-    scatter(S, xp.data());
+    scatter_fit(xp.data());
     residual(S, w_e, w_s, fp.data(), ro);
     xp[j] -= 2.0 * hh;
-    scatter(S, xp.data());
+    scatter_fit(xp.data());
     residual(S, w_e, w_s, fm.data(), ro);
     xp[j] += hh;
     double *col = J + static_cast<int64_t>(j) * m;

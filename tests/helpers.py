@@ -65,3 +65,34 @@ def spline_pair_model(nt=2, nknots=12, rmin=1.5, rmax=5.5, seed=3):
             y = 0.4 * (np.exp(-2.0 * (r - 2.6)) - 2.0 * np.exp(-(r - 2.6))) * f * (1 - (r / rmax) ** 4)
             tabs.append(Table.spline(rmin, rmax, y))
     return Model(FS_FAMILY_PAIR, nt, tabs)
+
+
+def small_diamond(n_cfg=4, cells=(2,), seed=31):
+    return synth.diamond(n_cfg, cells=cells, seed=seed)
+
+
+def adp_spline_model(nt=2, nknots=10, seed=5):
+    """Spline ADP tables: pair[np], density[nt], embedding[nt], dipole[np], quadrupole[np]."""
+    r = np.linspace(1.8, 5.5, nknots)
+    rho = np.linspace(0.0, 30.0, nknots)
+    np_ = nt * (nt + 1) // 2
+    tabs = []
+    k = 0
+
+    def f(lo, hi):
+        nonlocal k
+        k += 1
+        return synth.uniform(nknots, lo, hi, seed + k)
+    for _ in range(np_):
+        tabs.append(Table.spline(1.8, 5.5, 0.3 * (np.exp(-2 * (r - 2.7)) - 2 * np.exp(-(r - 2.7))) * f(0.9, 1.1)
+                                 * (1 - (r / 5.5) ** 4)))
+    for _ in range(nt):
+        tabs.append(Table.spline(1.8, 5.5, np.exp(-1.2 * (r - 2.5)) * f(0.9, 1.1) * (1 - (r / 5.5) ** 4)))
+    for _ in range(nt):
+        tabs.append(Table.spline(0.0, 30.0, -np.sqrt(rho) * f(0.9, 1.1)))
+    for _ in range(np_):
+        tabs.append(Table.spline(1.8, 5.5, 0.05 * np.exp(-(r - 2.5)) * f(0.5, 1.5) * (1 - (r / 5.5) ** 4)))
+    for _ in range(np_):
+        tabs.append(Table.spline(1.8, 5.5, 0.02 * np.exp(-1.5 * (r - 2.5)) * f(0.5, 1.5) * (1 - (r / 5.5) ** 4)))
+    from forcesmith_b200.abi import FS_FAMILY_ADP
+    return Model(FS_FAMILY_ADP, nt, tabs)

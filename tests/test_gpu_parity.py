@@ -236,3 +236,64 @@ def test_gradient_directional_full_size():
     assert abs(fd - an) <= 2e-4 * abs(fd), (fd, an)
     assert np.allclose(res["JtJ"], res["JtJ"].T, rtol=0, atol=1e-12 * np.abs(res["JtJ"]).max())
     assert np.all(np.linalg.eigvalsh(res["JtJ"]) > -1e-8 * np.abs(res["JtJ"]).max())
+
+
+# ---------------------------------------------------------------- SW ---
+
+@pytest.fixture(scope="module")
+def sw_case():
+    from tests.helpers import small_diamond
+    ds = small_diamond(4, (2, 3), seed=31)
+    ds = label(ds, synth.sw_model(), O.Oracle, 1.0, 0.2)
+    return ds, synth.sw_start_model()
+
+
+def test_sw_residual_fp64(sw_case):
+    ds, start = sw_case
+    g, o = _pair(ds, start, "fp64")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    _close(rg["forces"], ro["forces"], 1e-9, "SW forces")
+    _close(rg["F"], ro["F"], 1e-9, "SW F")
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-9 * ro["obj"]
+
+
+def test_sw_residual_fp32(sw_case):
+    ds, start = sw_case
+    g, o = _pair(ds, start, "fp32")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    assert np.max(np.abs(rg["forces"] - ro["forces"])) <= 2e-5 * np.max(np.abs(ro["forces"]))
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-4 * ro["obj"]
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-5), ("fp32", 2e-3)])
+def test_sw_jacobian_vs_central_differences(sw_case, precision, tol):
+    """The analytic SW Jacobian against the reference's own method for SW —
+    central differences (stiweb has no analytic Jacobian in the reference)."""
+    ds, start = sw_case
+    g, o = _pair(ds, start, precision)
+    res = g.jacobian(1.0, 0.2)
+    Jf = o.jacobian_fd(1.0, 0.2)
+    colmax = np.abs(Jf).max(axis=0)
+    err = np.abs(res["J"] - Jf) / (tol * np.abs(Jf) + 1e-8 + 1e-7 * colmax)
+    assert err.max() <= 1.0, err.max()
+    F = o.eval(1.0, 0.2)["F"]
+    JtJ, Jtr = O.normal_equations(Jf, F)
+    assert np.max(np.abs(res["Jtr"] - Jtr)) <= 10 * tol * np.max(np.abs(Jtr))
+
+
+# --------------------------------------------------------------- ADP ---
+
+def test_adp_residual_and_fd_jacobian_fp64():
+    from tests.helpers import adp_spline_model
+    ds = small_ternary(3, 32, seed=41)
+    ds.type[:] = ds.type % 2
+    model = adp_spline_model(2)
+    ds = label(ds, model.with_values(model.free_values() * 1.02), O.Oracle, 1.0, 0.1)
+    g, o = _pair(ds, model, "fp64")
+    rg, ro = g.eval(1.0, 0.1), o.eval(1.0, 0.1)
+    _close(rg["forces"], ro["forces"], 1e-9, "ADP forces")
+    _close(rg["energy"], ro["energy"], 1e-9, "ADP energy")
+    _close(rg["F"], ro["F"], 1e-9, "ADP F")
+    res = g.jacobian(1.0, 0.1)
+    Jf = o.jacobian_fd(1.0, 0.1)
+    assert np.max(np.abs(res["J"] - Jf)) <= 1e-6 * (1 + np.abs(Jf).max())

@@ -216,6 +216,7 @@ def test_neighbor_small_box_multiple_images():
     (neighbor_list.cpp:65-90): in a box smaller than 2·rc one j appears at
     several images, and the list is symmetric under (i,j,n) ↔ (j,i,−n)."""
     ds = synth.packing(np.array([32], np.int32), seed=5)
+    ds = ds.with_types(np.zeros(32, np.int32))
     o = O.Oracle()
     o.upload(ds)
     o.set_model(Model(FS_FAMILY_PAIR, 1, [Table.spline(0.0, 6.0, np.zeros(4))]))
