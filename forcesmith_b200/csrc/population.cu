@@ -60,11 +60,15 @@ __global__ void de_trial_kernel(const double *__restrict__ pop, double *__restri
   if (threadIdx.x == 0) {
     uint64_t draw = 0;
     for (int q = 0; q < 3; ++q) {
-      int c;
-      do {
-        c = static_cast<int>(urand(seed, gen, i, draw++) * NP);
-        if (c >= NP) c = NP - 1;
-      } while (c == i || (q > 0 && c == r[0]) || (q > 1 && c == r[1]));
+      // up to 64 random draws, then the first free index (NP >= 4 leaves one)
+      int c = -1;
+      for (int t = 0; t < 64 && c < 0; ++t) {
+        int v = static_cast<int>(urand(seed, gen, i, draw++) * NP);
+        if (v >= NP) v = NP - 1;
+        if (!(v == i || (q > 0 && v == r[0]) || (q > 1 && v == r[1]))) c = v;
+      }
+      for (int v = 0; v < NP && c < 0; ++v)
+        if (!(v == i || (q > 0 && v == r[0]) || (q > 1 && v == r[1]))) c = v;
       r[q] = c;
     }
     jrand = static_cast<int>(urand(seed, gen, i, 1ull << 33) * D);

@@ -161,7 +161,7 @@ class GpuSession(Session):
         self._de_np = NP
 
     def de_run(self, generations, use_graph=True, history=False):
-        D = self.param_count()
+        D = self.D
         best = np.zeros(1)
         x = np.zeros(D)
         hist = np.zeros(max(int(generations), 1)) if history else None
@@ -171,7 +171,7 @@ class GpuSession(Session):
         return (best[0], x, hist[:generations]) if history else (best[0], x)
 
     def de_population(self):
-        D = self.param_count()
+        D = self.D
         pop = np.zeros((self._de_np, D))
         obj = np.zeros(self._de_np)
         self._check(self._lib.fs_gpu_de_population(self._h, _dp(pop), _dp(obj)), "de_population")

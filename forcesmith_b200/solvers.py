@@ -58,12 +58,17 @@ class LMSolver:
     """Levenberg–Marquardt with FP64 damped Cholesky steps on the device.
 
     Per iteration: one residual+Jacobian evaluation (normal equations formed
-    on the device), then `n_trials` damping values λ·trial_factors solved
-    by device Cholesky and their objectives evaluated together in one
-    population launch.  The best trial with a positive gain ratio is taken;
-    when none is, λ grows ×`reject_factor` and the trials repeat without a
-    new Jacobian.  Marquardt scaling (λ·diag JᵀJ, zero column → 1) by
-    default, as MINPACK scales by the column norms.
+    on the device), then damping values λ·trial_factors solved by device
+    Cholesky and their objectives evaluated together in one population
+    launch.  The trial with the lowest objective among those with a
+    positive gain ratio ρ is taken and λ is updated from it by Nielsen's
+    rule λ·max(1/3, 1 − (2ρ − 1)³); when no trial decreases the objective, λ
+    grows ×`reject_factor` and the trials repeat without a new Jacobian.
+
+    Damping is Levenberg's λ·I (mode 0) starting from λ₀ = τ·max diag(JᵀJ)
+    (Madsen–Nielsen).  Marquardt's λ·diag(JᵀJ) (mode 1, τ used as λ₀) is
+    available but leaves knots that the data barely constrains almost
+    undamped, and on spline fits those steps run away.
 
     Termination follows MINPACK's tests: `ftol` on the actual and predicted
     relative reduction (status 1), `xtol` on the relative step (status 2),
@@ -74,10 +79,10 @@ class LMSolver:
     max_iter: int = 500
     xtol: float = 1e-7
     ftol: float = 1e-7
-    lam0: float = 1e-3
-    mode: int = 1
-    trial_factors: tuple = (0.1, 1.0, 10.0)
-    reject_factor: float = 100.0
+    tau: float = 1e-3
+    mode: int = 0
+    trial_factors: tuple = (0.25, 1.0, 4.0)
+    reject_factor: float = 16.0
 
     def honors_bounds(self):
         return False
@@ -92,7 +97,7 @@ class LMSolver:
         if D == 0:
             return LM_IMPROPER_INPUT, x, info
         maxfev = max(self.max_iter, 1) * 100 + 100
-        lam = self.lam0
+        lam = None
         sess.set_params(x)
         status = None
         for it in range(self.max_iter):
@@ -103,6 +108,8 @@ class LMSolver:
             if it == 0:
                 info["obj"].append(obj)
             diag = np.diag(JtJ).copy()
+            if lam is None:
+                lam = self.tau * (max(float(diag.max()), 1e-300) if self.mode == 0 else 1.0)
             if self.mode == 1:
                 diag[diag <= 0.0] = 1.0
             else:
@@ -126,10 +133,10 @@ class LMSolver:
                     x_new = x + s
                     act_rel = (obj - o) / obj if obj > 0 else 0.0
                     pred_rel = pred / obj if obj > 0 else 0.0
-                    dnorm = math.sqrt(float(s @ (np.sqrt(diag) ** 2 * s)))
-                    xnorm = math.sqrt(float(x_new @ (np.sqrt(diag) ** 2 * x_new)))
+                    dnorm = math.sqrt(float(s @ s))
+                    xnorm = math.sqrt(float(x_new @ x_new))
                     x, obj = x_new, o
-                    lam = l * (1.0 / 3.0 if best_rho > 0.75 else (2.0 if best_rho < 0.25 else 1.0))
+                    lam = l * max(1.0 / 3.0, 1.0 - (2.0 * best_rho - 1.0) ** 3)
                     info["obj"].append(obj)
                     info["lam"].append(l)
                     f_conv = abs(act_rel) <= self.ftol and pred_rel <= self.ftol and best_rho <= 2.0
@@ -163,17 +170,22 @@ class LMSolver:
 class HybridSolver:
     """Trust-region dogleg on the Gauss–Newton model of ‖F‖².
 
-    Each accepted point costs one residual+Jacobian evaluation; the
-    Gauss–Newton step is the device Cholesky solve of JᵀJ p = −Jᵀr (tiny
-    ridge), the Cauchy point uses g = Jᵀr and JᵀJ read back (D×D).  The
-    radius grows ×2 on a gain ratio > 0.75 at the boundary and shrinks ×¼
-    below 0.25; a rejected step shrinks it without a new Jacobian.
-    `max_iter` bounds the Jacobians, maxfev = max_iter·D as in the
-    reference (solver.cpp:108).
+    Each accepted point costs one residual+Jacobian evaluation.  The
+    Gauss–Newton point is the device Cholesky solve of (JᵀJ + μI) p = −Jᵀr
+    with a small Levenberg regulariser μ (from τ·max diag JᵀJ, ÷3 after a
+    very successful step, ×2 after a poor or rejected one) so that knots the
+    data barely constrain do not dominate it; the Cauchy point uses g = Jᵀr
+    and JᵀJ read back (D×D).  The dogleg path is cut at the trust radius
+    (initially radius0·max(‖x‖, 1)), which grows ×2 when a step at the
+    boundary has gain ratio > 0.75 and shrinks to ¼ of the step below 0.25;
+    a rejected step retries without a new Jacobian.  maxfev = max_iter·D as
+    in the reference (solver.cpp:108); ten accepted steps in a row that each
+    reduce the objective by less than 0.1 % stop it (status 5).
     """
     max_iter: int = 500
     xtol: float = 1e-7
-    ridge: float = 1e-12
+    tau: float = 1e-3
+    radius0: float = 0.1
 
     def honors_bounds(self):
         return False
@@ -190,6 +202,7 @@ class HybridSolver:
         maxfev = self.max_iter * D
         sess.set_params(x)
         delta = None
+        mu = None
         status = None
         stall = 0
         for it in range(self.max_iter):
@@ -199,12 +212,13 @@ class HybridSolver:
             info["nfev"] += 1
             if it == 0:
                 info["obj"].append(obj)
-            scale = math.sqrt(max(float(np.mean(np.diag(A))), 1.0))
-            p_gn = sess.lm_step(self.ridge * scale * scale, 0)
+            if mu is None:
+                mu = self.tau * max(float(np.max(np.diag(A))), 1e-300)
+            p_gn = sess.lm_step(mu, 0)
             gAg = float(g @ (A @ g))
             p_sd = -(float(g @ g) / gAg) * g if gAg > 0 else -g
             if delta is None:
-                delta = max(float(np.linalg.norm(p_gn)), 1e-12)
+                delta = self.radius0 * max(float(np.linalg.norm(x)), 1.0)
             while True:
                 p = self._dogleg(p_gn, p_sd, delta)
                 pred = -2.0 * float(g @ p) - float(p @ (A @ p))
@@ -217,11 +231,14 @@ class HybridSolver:
                 elif rho > 0.75 and pn >= 0.99 * delta:
                     delta = 2.0 * delta
                 if rho > 0.0 and np.isfinite(o):
+                    mu *= 1.0 / 3.0 if rho > 0.75 else (2.0 if rho < 0.25 else 1.0)
                     x = x + p
                     stall = 0 if (obj - o) > 1e-3 * obj else stall + 1
                     obj = o
                     info["obj"].append(obj)
                     break
+                mu *= 2.0
+                p_gn = sess.lm_step(mu, 0)
                 if delta <= self.xtol * max(float(np.linalg.norm(x)), self.xtol):
                     status = HY_RELATIVE_ERROR_TOO_SMALL
                     break

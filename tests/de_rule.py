@@ -4,7 +4,7 @@ Python integers and IEEE doubles, for bit-exact checks of one generation.
 Random numbers: u(seed, gen, i, draw) = top 53 bits of
 mix(seed ^ mix(gen·0x100000001B3 ^ mix(i·0x9E3779B1 + draw))) · 2⁻⁵³, with
 mix the SplitMix64 finaliser; draws 0,1,… pick r1, r2, r3 (rejecting i and
-repeats), draw 2³³ picks the forced coordinate, draw 2³² + j decides
+repeats; after 64 draws for one parent, the first free index), draw 2³³ picks the forced coordinate, draw 2³² + j decides
 crossover of coordinate j; the initial population uses gen = 2³² − 1 and
 draw j.
 """
@@ -44,12 +44,16 @@ def de_trials(seed, gen, pop, lo, hi, F, CR):
     for i in range(NP):
         r = []
         draw = 0
-        while len(r) < 3:
-            c = int(urand(seed, gen, i, draw) * NP)
-            draw += 1
-            c = min(c, NP - 1)
-            if c == i or c in r:
-                continue
+        for _ in range(3):
+            c = -1
+            for _t in range(64):
+                v = min(int(urand(seed, gen, i, draw) * NP), NP - 1)
+                draw += 1
+                if v != i and v not in r:
+                    c = v
+                    break
+            if c < 0:
+                c = next(v for v in range(NP) if v != i and v not in r)
             r.append(c)
         jr = min(int(urand(seed, gen, i, 1 << 33) * D), D - 1)
         for j in range(D):

@@ -130,8 +130,8 @@ def test_device_solver_vs_oracle_driven(problem, make):
     s = _oracle_step_session(ds, start)
     _, xo, io = make().minimize(s, x)
     oo = s.eval(1.0, 0.0, want=("obj",))["obj"]
-    assert og < 1e-2 * o0
-    floor = 1e-10 * o0  # both runs converge to ~0 on exactly-representable labels
+    assert og < 1e-4 * o0
+    floor = 1e-9 * o0  # both runs converge to ~0 on exactly-representable labels
     assert og <= 1.1 * oo + floor and oo <= 1.1 * og + floor
 
 
