@@ -57,6 +57,12 @@ class fs_gpu_opts(C.Structure):
                 ("lanes_per_atom", C.c_int32), ("reserved", C.c_int32)]
 
 
+class fs_surrogate_opts(C.Structure):
+    _fields_ = [("screen", C.c_int32), ("warm_generations", C.c_int32), ("batch", C.c_int32),
+                ("steps_per_generation", C.c_int32), ("lr", C.c_double), ("gate", C.c_double),
+                ("holdout", C.c_double), ("seed", C.c_uint64), ("archive_rows", C.c_int64)]
+
+
 class fs_de_opts(C.Structure):
     _fields_ = [("NP", C.c_int32), ("reserved", C.c_int32), ("mutation", C.c_double),
                 ("crossover", C.c_double), ("seed", C.c_uint64), ("w_e", C.c_double),

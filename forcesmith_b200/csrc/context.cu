@@ -115,6 +115,8 @@ void free_configs(fs_gpu *h) {
   h->pop_alloc = 0;
   fsg::de_free(h->de);
   h->de = nullptr;
+  fsg::surrogate_free(h->sur);
+  h->sur = nullptr;
   h->rows_alloc = 0;
   h->rcut_built = -1.0;
   h->n_pairs = 0;
@@ -169,6 +171,9 @@ int check_ready(fs_gpu *h) {
 }
 
 } // namespace
+
+int sync_checked(fs_gpu *h) { return sync(h); }
+
 } // namespace fsg
 
 extern "C" {
@@ -221,6 +226,8 @@ int fs_gpu_destroy(fs_gpu *h) {
   dfree(h->d_chol);
   dfree(h->d_dx);
   dfree(h->d_flag);
+  fsg::mlp_free(h->mlp);
+  h->mlp = nullptr;
   dfree(h->d_pop_spl);
   dfree(h->d_pop_vals);
   dfree(h->d_pop_obj);
@@ -385,6 +392,10 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
   free_jacobian(h);
   fsg::de_free(h->de);
   h->de = nullptr;
+  fsg::surrogate_free(h->sur);
+  h->sur = nullptr;
+  fsg::mlp_free(h->mlp);
+  h->mlp = nullptr;
   dfree(h->d_pop_spl);
   h->pop_spl_count = 0;
   FS_TRY(upload_tables(h));

@@ -95,6 +95,10 @@ struct HostTable {
 namespace fsg {
 struct DeState;
 void de_free(DeState *s);
+struct Mlp;
+void mlp_free(Mlp *s);
+struct Surrogate;
+void surrogate_free(Surrogate *s);
 } // namespace fsg
 
 struct fs_gpu {
@@ -189,13 +193,17 @@ struct fs_gpu {
   double *d_pop_vals = nullptr;
   double *d_pop_obj = nullptr;
 
-  // device differential evolution (population.cu)
+  // device differential evolution (population.cu) and its surrogate (mlp.cu)
   fsg::DeState *de = nullptr;
+  fsg::Mlp *mlp = nullptr;
+  fsg::Surrogate *sur = nullptr;
 };
 
 namespace fsg {
 
 int set_error(fs_gpu *h, int code, const std::string &m);
+// stream sync + the device error word of bounded waits
+int sync_checked(fs_gpu *h);
 
 // Phases of one residual + Jacobian evaluation, timed with CUDA events
 // when profiling is on: residual, per-atom Jacobian, force/stress rows,
@@ -229,6 +237,23 @@ int lm_solve(fs_gpu *h, double lambda, int mode, double *dx_host);
 // population.cu / eam.cu
 int eval_population(fs_gpu *h, double w_e, double w_s, const double *xs, int NP, double *obj);
 int eval_population_device(fs_gpu *h, double w_e, double w_s, const double *d_xs, int NP, double *d_obj);
+
+// mlp.cu
+int64_t mlp_param_count(int D);
+int mlp_create(fs_gpu *h, int D, uint64_t seed, float lr, Mlp **out);
+int mlp_set_params(fs_gpu *h, Mlp *s, const float *host_params);
+int mlp_get(fs_gpu *h, Mlp *s, const float *dev_flat, float *host_params);
+float *mlp_param_ptr(Mlp *s);
+float *mlp_grad_ptr(Mlp *s);
+float *mlp_rows_x(Mlp *s); // FP32 features, row-major D, capacity mlp_capacity rows
+float *mlp_rows_t(Mlp *s); // FP32 targets
+float *mlp_rows_y(Mlp *s); // FP32 predictions
+float *mlp_loss_ptr(Mlp *s);
+int mlp_capacity(Mlp *s);
+int mlp_reserve(fs_gpu *h, Mlp *s, int rows);
+int mlp_forward_dev(fs_gpu *h, Mlp *s, int rows);
+int mlp_gradient_dev(fs_gpu *h, Mlp *s, int rows);
+int mlp_adam_dev(fs_gpu *h, Mlp *s);
 
 inline int64_t rows_of(const fs_gpu *h, double w_s) {
   return 3 * h->n_atoms + static_cast<int64_t>(h->n_cfg) * (2 + (w_s > 0.0 ? 6 : 0));

@@ -50,11 +50,16 @@ __global__ void de_init_kernel(double *pop, const double *lo, const double *hi, 
   }
 }
 
-// Member i builds its trial vector (one block per member).
+// Member i builds candidate k of its trial vector (block (i, k)); candidate
+// k draws from the random stream of member i + k·2³², so k = 0 is the plain
+// DE trial.  Optionally writes the candidate's model features
+// 2(x − lo)/(hi − lo) − 1 in FP32.
 __global__ void de_trial_kernel(const double *__restrict__ pop, double *__restrict__ trial,
-                                const double *__restrict__ lo, const double *__restrict__ hi, int NP, int D, double F,
-                                double CR, uint64_t seed, const int64_t *__restrict__ gen_ctr) {
+                                float *__restrict__ feat, const double *__restrict__ lo,
+                                const double *__restrict__ hi, int NP, int D, double F, double CR, uint64_t seed,
+                                const int64_t *__restrict__ gen_ctr) {
   const int i = blockIdx.x;
+  const uint64_t stream = static_cast<uint64_t>(i) + (static_cast<uint64_t>(blockIdx.y) << 32);
   const uint64_t gen = static_cast<uint64_t>(*gen_ctr);
   __shared__ int r[3], jrand;
   if (threadIdx.x == 0) {
@@ -63,7 +68,7 @@ __global__ void de_trial_kernel(const double *__restrict__ pop, double *__restri
       // up to 64 random draws, then the first free index (NP >= 4 leaves one)
       int c = -1;
       for (int t = 0; t < 64 && c < 0; ++t) {
-        int v = static_cast<int>(urand(seed, gen, i, draw++) * NP);
+        int v = static_cast<int>(urand(seed, gen, stream, draw++) * NP);
         if (v >= NP) v = NP - 1;
         if (!(v == i || (q > 0 && v == r[0]) || (q > 1 && v == r[1]))) c = v;
       }
@@ -71,17 +76,81 @@ __global__ void de_trial_kernel(const double *__restrict__ pop, double *__restri
         if (!(v == i || (q > 0 && v == r[0]) || (q > 1 && v == r[1]))) c = v;
       r[q] = c;
     }
-    jrand = static_cast<int>(urand(seed, gen, i, 1ull << 33) * D);
+    jrand = static_cast<int>(urand(seed, gen, stream, 1ull << 33) * D);
     if (jrand >= D) jrand = D - 1;
   }
   __syncthreads();
   const double *x1 = pop + static_cast<int64_t>(r[0]) * D, *x2 = pop + static_cast<int64_t>(r[1]) * D,
                *x3 = pop + static_cast<int64_t>(r[2]) * D, *xi = pop + static_cast<int64_t>(i) * D;
-  double *t = trial + static_cast<int64_t>(i) * D;
+  const int64_t row = static_cast<int64_t>(blockIdx.y) * NP + i;
+  double *t = trial + row * D;
   for (int j = threadIdx.x; j < D; j += blockDim.x) {
-    const bool take = j == jrand || urand(seed, gen, i, (1ull << 32) + j) < CR;
-    t[j] = take ? fmin(fmax(__dadd_rn(x1[j], __dmul_rn(F, __dsub_rn(x2[j], x3[j]))), lo[j]), hi[j]) : xi[j];
+    const bool take = j == jrand || urand(seed, gen, stream, (1ull << 32) + j) < CR;
+    const double v =
+        take ? fmin(fmax(__dadd_rn(x1[j], __dmul_rn(F, __dsub_rn(x2[j], x3[j]))), lo[j]), hi[j]) : xi[j];
+    t[j] = v;
+    if (feat) feat[row * D + j] = hi[j] > lo[j] ? static_cast<float>(2.0 * (v - lo[j]) / (hi[j] - lo[j]) - 1.0) : 0.f;
   }
+}
+
+// Per member: the candidate with the lowest predicted value (NaN last) is
+// copied to the trial buffer and its features to the archive row.
+__global__ void de_pick_kernel(const double *__restrict__ cand, const float *__restrict__ cfeat,
+                               const float *__restrict__ y, int NP, int S, int D, double *__restrict__ trial,
+                               float *__restrict__ feat_out) {
+  const int i = blockIdx.x;
+  __shared__ int best;
+  if (threadIdx.x == 0) {
+    int b = 0;
+    float bv = INFINITY;
+    for (int k = 0; k < S; ++k) {
+      const float v = y[static_cast<int64_t>(k) * NP + i];
+      if (v < bv) {
+        bv = v;
+        b = k;
+      }
+    }
+    best = b;
+  }
+  __syncthreads();
+  const int64_t src = static_cast<int64_t>(best) * NP + i;
+  for (int j = threadIdx.x; j < D; j += blockDim.x) {
+    trial[static_cast<int64_t>(i) * D + j] = cand[src * D + j];
+    feat_out[static_cast<int64_t>(i) * D + j] = cfeat[src * D + j];
+  }
+}
+
+// archive targets: log of the exact objective
+__global__ void arch_target_kernel(const double *__restrict__ tobj, int NP, float *__restrict__ t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < NP) t[i] = static_cast<float>(log(fmax(tobj[i], 1e-300)));
+}
+
+// Training batch: uniform rows of the archive outside the held-out slice
+// (every P-th row, index ≡ P−1 mod P), targets standardised.
+__global__ void arch_batch_kernel(const float *__restrict__ ax, const float *__restrict__ at, int64_t n, int P, int D,
+                                  int rows, uint64_t seed, uint64_t ctr, float mu, float inv_sigma,
+                                  float *__restrict__ xs, float *__restrict__ t) {
+  const int r = blockIdx.x;
+  __shared__ int64_t idx;
+  if (threadIdx.x == 0) {
+    int64_t k = static_cast<int64_t>(urand(seed, ctr, static_cast<uint64_t>(r), 7) * static_cast<double>(n));
+    if (k >= n) k = n - 1;
+    if (P > 1 && k % P == P - 1) k -= 1;
+    idx = k;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < D; j += blockDim.x) xs[static_cast<int64_t>(r) * D + j] = ax[idx * D + j];
+  if (threadIdx.x == 0) t[r] = (at[idx] - mu) * inv_sigma;
+}
+
+// The most recent `rows` held-out archive rows.
+__global__ void arch_holdout_kernel(const float *__restrict__ ax, const float *__restrict__ at, int64_t n_held, int P,
+                                    int D, float *__restrict__ xs, float *__restrict__ t) {
+  const int r = blockIdx.x;
+  const int64_t idx = (n_held - 1 - r) * P + (P - 1);
+  for (int j = threadIdx.x; j < D; j += blockDim.x) xs[static_cast<int64_t>(r) * D + j] = ax[idx * D + j];
+  if (threadIdx.x == 0) t[r] = at[idx];
 }
 
 // Greedy selection + best tracking; the last block advances the generation.
@@ -253,8 +322,8 @@ int de_init(fs_gpu *h, const fs_de_opts *o, const double *lo, const double *hi, 
 }
 
 static int de_generation(fs_gpu *h, DeState *s) {
-  de_trial_kernel<<<s->NP, 128, 0, h->stream>>>(s->pop, s->trial, s->lo, s->hi, s->NP, s->D, s->F, s->CR, s->seed,
-                                                 s->gen);
+  de_trial_kernel<<<s->NP, 128, 0, h->stream>>>(s->pop, s->trial, nullptr, s->lo, s->hi, s->NP, s->D, s->F, s->CR,
+                                                 s->seed, s->gen);
   FS_CUDA(cudaGetLastError());
   FS_TRY(eval_population_device(h, s->w_e, s->w_s, s->trial, s->NP, s->tobj));
   de_select_kernel<<<s->NP, 128, 0, h->stream>>>(s->pop, s->obj, s->trial, s->tobj, s->NP, s->D, s->gen, s->accepted);
@@ -332,6 +401,224 @@ int de_population(fs_gpu *h, double *pop, double *obj) {
   return FS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// surrogate-screened DE
+
+struct Surrogate {
+  fs_surrogate_opts o{};
+  int D = 0;
+  int P = 10;                     // held-out period: every P-th archive row
+  float *ax = nullptr, *at = nullptr;
+  int64_t cap = 0, n = 0;         // archive rows (FP32 features, log objective)
+  double *cand = nullptr;         // S·NP candidate vectors
+  int64_t cand_cap = 0;
+  float mu = 0.f, inv_sigma = 1.f;
+  int64_t generations = 0;
+  bool gate_open = false;
+  double last_rho = 0.0;
+  uint64_t ctr = 0;
+};
+
+void surrogate_free(Surrogate *s) {
+  if (!s) return;
+  cudaFree(s->ax);
+  cudaFree(s->at);
+  cudaFree(s->cand);
+  delete s;
+}
+
+// Spearman rank correlation (average ranks for ties).
+static double spearman(const std::vector<float> &a, const std::vector<float> &b) {
+  const size_t n = a.size();
+  if (n < 3) return 0.0;
+  auto ranks = [n](const std::vector<float> &v) {
+    std::vector<int> ix(n);
+    for (size_t k = 0; k < n; ++k) ix[k] = static_cast<int>(k);
+    std::sort(ix.begin(), ix.end(), [&](int p, int q) { return v[p] < v[q]; });
+    std::vector<double> r(n);
+    for (size_t k = 0; k < n;) {
+      size_t e = k;
+      while (e + 1 < n && v[ix[e + 1]] == v[ix[k]]) ++e;
+      const double avg = 0.5 * static_cast<double>(k + e);
+      for (size_t q = k; q <= e; ++q) r[ix[q]] = avg;
+      k = e + 1;
+    }
+    return r;
+  };
+  const std::vector<double> ra = ranks(a), rb = ranks(b);
+  double ma = 0, mb = 0;
+  for (size_t k = 0; k < n; ++k) {
+    ma += ra[k];
+    mb += rb[k];
+  }
+  ma /= n;
+  mb /= n;
+  double sab = 0, saa = 0, sbb = 0;
+  for (size_t k = 0; k < n; ++k) {
+    sab += (ra[k] - ma) * (rb[k] - mb);
+    saa += (ra[k] - ma) * (ra[k] - ma);
+    sbb += (rb[k] - mb) * (rb[k] - mb);
+  }
+  return (saa > 0 && sbb > 0) ? sab / std::sqrt(saa * sbb) : 0.0;
+}
+
+static int surrogate_train(fs_gpu *h, Surrogate *sv, int steps) {
+  const int B = sv->o.batch;
+  FS_TRY(mlp_reserve(h, h->mlp, B));
+  for (int k = 0; k < steps; ++k) {
+    arch_batch_kernel<<<B, 64, 0, h->stream>>>(sv->ax, sv->at, sv->n, sv->P, sv->D, B, sv->o.seed ^ 0x5EEDull,
+                                               sv->ctr++, sv->mu, sv->inv_sigma, mlp_rows_x(h->mlp),
+                                               mlp_rows_t(h->mlp));
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+    FS_TRY(mlp_gradient_dev(h, h->mlp, B));
+    FS_TRY(mlp_adam_dev(h, h->mlp));
+  }
+  return FS_OK;
+}
+
+// Rank correlation of the model on the newest held-out rows (≤ 2048).
+static int surrogate_gate(fs_gpu *h, Surrogate *sv, double *rho) {
+  const int64_t n_held = sv->P > 1 ? sv->n / sv->P : 0;
+  const int rows = static_cast<int>(std::min<int64_t>(n_held, 2048));
+  *rho = 0.0;
+  if (rows < 8) return FS_OK;
+  FS_TRY(mlp_reserve(h, h->mlp, rows));
+  arch_holdout_kernel<<<rows, 64, 0, h->stream>>>(sv->ax, sv->at, n_held, sv->P, sv->D, mlp_rows_x(h->mlp),
+                                                   mlp_rows_t(h->mlp));
+  FS_CUDA(cudaGetLastError());
+  ++h->launches;
+  FS_TRY(mlp_forward_dev(h, h->mlp, rows));
+  std::vector<float> y(rows), t(rows);
+  FS_CUDA(cudaMemcpyAsync(y.data(), mlp_rows_y(h->mlp), rows * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  FS_CUDA(cudaMemcpyAsync(t.data(), mlp_rows_t(h->mlp), rows * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  FS_CUDA(cudaStreamSynchronize(h->stream));
+  *rho = spearman(y, t);
+  return FS_OK;
+}
+
+int de_run_screened(fs_gpu *h, int generations, double *best_obj, double *best_x, double *history, double *rho_out,
+                    int32_t *screened_out) {
+  DeState *s = h->de;
+  Surrogate *sv = h->sur;
+  if (!s || !sv || !h->mlp) return set_error(h, FS_ERR_STATE, "de_run_screened: fs_gpu_de_init and fs_gpu_surrogate_init first");
+  if (sv->D != s->D) return set_error(h, FS_ERR_STATE, "de_run_screened: surrogate and DE sizes differ");
+  const int NP = s->NP, D = s->D, S = std::max(1, sv->o.screen);
+  // archive: grows in whole generations (ring once the capacity is reached)
+  const int64_t want = sv->n + static_cast<int64_t>(generations) * NP;
+  if (want > sv->cap) {
+    const int64_t cap = std::min<int64_t>(std::max<int64_t>(want, 16 * NP), sv->o.archive_rows > 0 ? sv->o.archive_rows : want);
+    float *ax = nullptr, *at = nullptr;
+    if (cudaMalloc(&ax, cap * D * sizeof(float)) != cudaSuccess || cudaMalloc(&at, cap * sizeof(float)) != cudaSuccess) {
+      cudaFree(ax);
+      return set_error(h, FS_ERR_NOMEM, "de_run_screened: archive");
+    }
+    const int64_t keep = std::min(sv->n, cap);
+    if (keep > 0) {
+      FS_CUDA(cudaMemcpyAsync(ax, sv->ax, keep * D * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+      FS_CUDA(cudaMemcpyAsync(at, sv->at, keep * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    FS_CUDA(cudaStreamSynchronize(h->stream));
+    cudaFree(sv->ax);
+    cudaFree(sv->at);
+    sv->ax = ax;
+    sv->at = at;
+    sv->cap = cap;
+    sv->n = keep;
+  }
+  if (sv->cand_cap < static_cast<int64_t>(S) * NP) {
+    cudaFree(sv->cand);
+    sv->cand = nullptr;
+    FS_CUDA(cudaMalloc(&sv->cand, static_cast<size_t>(S) * NP * D * sizeof(double)));
+    sv->cand_cap = static_cast<int64_t>(S) * NP;
+  }
+  FS_TRY(mlp_reserve(h, h->mlp, std::max(S * NP, sv->o.batch)));
+  for (int g = 0; g < generations; ++g) {
+    if (sv->n + NP > sv->cap) sv->n = 0; // ring: start over at the front
+    float *frow = sv->ax + sv->n * D;
+    const bool screen = sv->generations >= sv->o.warm_generations && sv->gate_open && S > 1;
+    if (screen) {
+      de_trial_kernel<<<dim3(NP, S), 128, 0, h->stream>>>(s->pop, sv->cand, mlp_rows_x(h->mlp), s->lo, s->hi, NP, D,
+                                                           s->F, s->CR, s->seed, s->gen);
+      FS_CUDA(cudaGetLastError());
+      FS_TRY(mlp_forward_dev(h, h->mlp, S * NP));
+      de_pick_kernel<<<NP, 128, 0, h->stream>>>(sv->cand, mlp_rows_x(h->mlp), mlp_rows_y(h->mlp), NP, S, D, s->trial,
+                                                frow);
+      FS_CUDA(cudaGetLastError());
+      h->launches += 2;
+    } else {
+      de_trial_kernel<<<NP, 128, 0, h->stream>>>(s->pop, s->trial, frow, s->lo, s->hi, NP, D, s->F, s->CR, s->seed,
+                                                 s->gen);
+      FS_CUDA(cudaGetLastError());
+      ++h->launches;
+    }
+    FS_TRY(eval_population_device(h, s->w_e, s->w_s, s->trial, NP, s->tobj));
+    arch_target_kernel<<<(NP + 255) / 256, 256, 0, h->stream>>>(s->tobj, NP, sv->at + sv->n);
+    de_select_kernel<<<NP, 128, 0, h->stream>>>(s->pop, s->obj, s->trial, s->tobj, NP, D, s->gen, s->accepted);
+    de_advance_kernel<<<1, 1, 0, h->stream>>>(s->gen);
+    FS_CUDA(cudaGetLastError());
+    h->launches += 3;
+    sv->n += NP;
+    sv->generations += 1;
+    s->generations += 1;
+    if (sv->generations == sv->o.warm_generations) {
+      // fix the target standardisation from the warm-start archive
+      std::vector<float> t(sv->n);
+      FS_CUDA(cudaMemcpyAsync(t.data(), sv->at, sv->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+      FS_CUDA(cudaStreamSynchronize(h->stream));
+      double m = 0, q = 0;
+      for (float v : t) m += v;
+      m /= std::max<size_t>(t.size(), 1);
+      for (float v : t) q += (v - m) * (v - m);
+      const double sd = std::sqrt(q / std::max<size_t>(t.size(), 1));
+      sv->mu = static_cast<float>(m);
+      sv->inv_sigma = static_cast<float>(sd > 0 ? 1.0 / sd : 1.0);
+      FS_TRY(surrogate_train(h, sv, sv->o.steps_per_generation * std::max(1, sv->o.warm_generations)));
+    } else if (sv->generations > sv->o.warm_generations) {
+      FS_TRY(surrogate_train(h, sv, sv->o.steps_per_generation));
+    }
+    double rho = 0.0;
+    if (sv->generations >= sv->o.warm_generations) {
+      FS_TRY(surrogate_gate(h, sv, &rho));
+      sv->gate_open = rho >= sv->o.gate;
+    }
+    sv->last_rho = rho;
+    if (rho_out) rho_out[g] = rho;
+    if (screened_out) screened_out[g] = screen ? 1 : 0;
+    if (history) {
+      argmin_kernel<<<1, 1024, 0, h->stream>>>(s->obj, NP, s->best);
+      int b = 0;
+      FS_CUDA(cudaMemcpyAsync(&b, s->best, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      FS_CUDA(cudaStreamSynchronize(h->stream));
+      FS_CUDA(cudaMemcpy(&history[g], s->obj + b, sizeof(double), cudaMemcpyDeviceToHost));
+    }
+  }
+  argmin_kernel<<<1, 1024, 0, h->stream>>>(s->obj, NP, s->best);
+  FS_CUDA(cudaGetLastError());
+  int b = 0;
+  FS_CUDA(cudaMemcpyAsync(&b, s->best, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  FS_CUDA(cudaStreamSynchronize(h->stream));
+  if (best_obj) FS_CUDA(cudaMemcpy(best_obj, s->obj + b, sizeof(double), cudaMemcpyDeviceToHost));
+  if (best_x)
+    FS_CUDA(cudaMemcpy(best_x, s->pop + static_cast<int64_t>(b) * D, D * sizeof(double), cudaMemcpyDeviceToHost));
+  return FS_OK;
+}
+
+int surrogate_init(fs_gpu *h, const fs_surrogate_opts *o) {
+  surrogate_free(h->sur);
+  h->sur = nullptr;
+  mlp_free(h->mlp);
+  h->mlp = nullptr;
+  FS_TRY(mlp_create(h, h->D, o->seed, static_cast<float>(o->lr), &h->mlp));
+  Surrogate *sv = new Surrogate();
+  sv->o = *o;
+  sv->D = h->D;
+  sv->P = o->holdout > 0.0 ? std::max(2, static_cast<int>(std::lround(1.0 / o->holdout))) : 1;
+  h->sur = sv;
+  FS_CUDA(cudaStreamSynchronize(h->stream));
+  return FS_OK;
+}
+
 } // namespace fsg
 
 extern "C" {
@@ -359,6 +646,91 @@ int fs_gpu_de_population(fs_gpu *h, double *pop, double *obj) {
   if (!h) return FS_ERR_ARG;
   cudaSetDevice(h->device);
   return fsg::de_population(h, pop, obj);
+}
+
+int fs_gpu_surrogate_init(fs_gpu *h, const fs_surrogate_opts *opts) {
+  if (!h || !opts) return FS_ERR_ARG;
+  if (!h->have_model) return fsg::set_error(h, FS_ERR_STATE, "surrogate_init: no model");
+  if (opts->batch < 8 || opts->batch % 8 || opts->screen < 1 || opts->warm_generations < 0 ||
+      opts->steps_per_generation < 0 || !(opts->lr > 0.0) || opts->holdout < 0.0 || opts->holdout >= 1.0)
+    return fsg::set_error(h, FS_ERR_ARG, "surrogate_init: bad options");
+  cudaSetDevice(h->device);
+  return fsg::surrogate_init(h, opts);
+}
+
+int fs_gpu_surrogate_param_count(fs_gpu *h, int64_t *n) {
+  if (!h || !n) return FS_ERR_ARG;
+  if (!h->mlp) return fsg::set_error(h, FS_ERR_STATE, "surrogate: not initialised");
+  *n = fsg::mlp_param_count(h->D);
+  return FS_OK;
+}
+
+int fs_gpu_surrogate_get_params(fs_gpu *h, float *params) {
+  if (!h || !params) return FS_ERR_ARG;
+  if (!h->mlp) return fsg::set_error(h, FS_ERR_STATE, "surrogate: not initialised");
+  cudaSetDevice(h->device);
+  return fsg::mlp_get(h, h->mlp, fsg::mlp_param_ptr(h->mlp), params);
+}
+
+int fs_gpu_surrogate_set_params(fs_gpu *h, const float *params) {
+  if (!h || !params) return FS_ERR_ARG;
+  if (!h->mlp) return fsg::set_error(h, FS_ERR_STATE, "surrogate: not initialised");
+  cudaSetDevice(h->device);
+  return fsg::mlp_set_params(h, h->mlp, params);
+}
+
+static int load_rows(fs_gpu *h, const float *x, const float *t, int32_t rows) {
+  FS_TRY(fsg::mlp_reserve(h, h->mlp, rows));
+  FS_CUDA(cudaMemcpyAsync(fsg::mlp_rows_x(h->mlp), x, static_cast<size_t>(rows) * h->D * sizeof(float),
+                          cudaMemcpyHostToDevice, h->stream));
+  if (t)
+    FS_CUDA(cudaMemcpyAsync(fsg::mlp_rows_t(h->mlp), t, rows * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  return FS_OK;
+}
+
+int fs_gpu_surrogate_predict(fs_gpu *h, const float *x, int32_t rows, float *y) {
+  if (!h || !x || !y || rows < 1) return FS_ERR_ARG;
+  if (!h->mlp) return fsg::set_error(h, FS_ERR_STATE, "surrogate: not initialised");
+  cudaSetDevice(h->device);
+  FS_TRY(load_rows(h, x, nullptr, rows));
+  FS_TRY(fsg::mlp_forward_dev(h, h->mlp, rows));
+  FS_CUDA(cudaMemcpyAsync(y, fsg::mlp_rows_y(h->mlp), rows * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  return fsg::sync_checked(h);
+}
+
+int fs_gpu_surrogate_gradient(fs_gpu *h, const float *x, const float *t, int32_t rows, float *grad, float *loss) {
+  if (!h || !x || !t || rows < 8) return FS_ERR_ARG;
+  if (!h->mlp) return fsg::set_error(h, FS_ERR_STATE, "surrogate: not initialised");
+  cudaSetDevice(h->device);
+  FS_TRY(load_rows(h, x, t, rows));
+  FS_TRY(fsg::mlp_gradient_dev(h, h->mlp, rows));
+  if (loss) FS_CUDA(cudaMemcpyAsync(loss, fsg::mlp_loss_ptr(h->mlp), sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  FS_TRY(fsg::sync_checked(h));
+  if (grad) FS_TRY(fsg::mlp_get(h, h->mlp, fsg::mlp_grad_ptr(h->mlp), grad));
+  if (loss) *loss /= static_cast<float>(rows);
+  return FS_OK;
+}
+
+int fs_gpu_surrogate_train(fs_gpu *h, const float *x, const float *t, int32_t rows, int32_t steps, float *loss) {
+  if (!h || !x || !t || rows < 8 || steps < 0) return FS_ERR_ARG;
+  if (!h->mlp) return fsg::set_error(h, FS_ERR_STATE, "surrogate: not initialised");
+  cudaSetDevice(h->device);
+  FS_TRY(load_rows(h, x, t, rows));
+  for (int k = 0; k < steps; ++k) {
+    FS_TRY(fsg::mlp_gradient_dev(h, h->mlp, rows));
+    FS_TRY(fsg::mlp_adam_dev(h, h->mlp));
+  }
+  if (loss) FS_CUDA(cudaMemcpyAsync(loss, fsg::mlp_loss_ptr(h->mlp), sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  FS_TRY(fsg::sync_checked(h));
+  if (loss) *loss /= static_cast<float>(rows);
+  return FS_OK;
+}
+
+int fs_gpu_de_run_screened(fs_gpu *h, int32_t generations, double *best_obj, double *best_x, double *history,
+                           double *rho, int32_t *screened) {
+  if (!h || generations < 0) return FS_ERR_ARG;
+  cudaSetDevice(h->device);
+  return fsg::de_run_screened(h, generations, best_obj, best_x, history, rho, screened);
 }
 
 } // extern "C"

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import (fs_de_opts, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
+from .abi import (fs_de_opts, fs_surrogate_opts, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
                   fs_model, load_library)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -55,8 +55,21 @@ def lib() -> C.CDLL:
         L.fs_gpu_de_init.argtypes = [vp, C.POINTER(fs_de_opts), pd, pd, pd]
         L.fs_gpu_de_run.argtypes = [vp, i32, i32, pd, pd, pd]
         L.fs_gpu_de_population.argtypes = [vp, pd, pd]
+        pf = C.POINTER(C.c_float)
+        L.fs_gpu_surrogate_init.argtypes = [vp, C.POINTER(fs_surrogate_opts)]
+        L.fs_gpu_de_run_screened.argtypes = [vp, i32, pd, pd, pd, pd, pi]
+        L.fs_gpu_surrogate_param_count.argtypes = [vp, C.POINTER(i64)]
+        L.fs_gpu_surrogate_get_params.argtypes = [vp, pf]
+        L.fs_gpu_surrogate_set_params.argtypes = [vp, pf]
+        L.fs_gpu_surrogate_predict.argtypes = [vp, pf, i32, pf]
+        L.fs_gpu_surrogate_gradient.argtypes = [vp, pf, pf, i32, pf, pf]
+        L.fs_gpu_surrogate_train.argtypes = [vp, pf, pf, i32, i32, pf]
         _LIB = L
     return _LIB
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 def _err(h) -> str:
@@ -169,6 +182,62 @@ class GpuSession(Session):
                                             _dp(best), _dp(x), _dp(hist) if history else None),
                     "de_run")
         return (best[0], x, hist[:generations]) if history else (best[0], x)
+
+    # -- surrogate-screened DE ------------------------------------------------
+    def surrogate_init(self, screen=4, warm_generations=5, batch=512, steps_per_generation=32,
+                       lr=1e-3, gate=0.8, holdout=0.1, seed=1, archive_rows=0):
+        o = fs_surrogate_opts(int(screen), int(warm_generations), int(batch),
+                              int(steps_per_generation), float(lr), float(gate), float(holdout),
+                              int(seed), int(archive_rows))
+        self._check(self._lib.fs_gpu_surrogate_init(self._h, C.byref(o)), "surrogate_init")
+
+    def de_run_screened(self, generations):
+        g = int(generations)
+        best = np.zeros(1)
+        x = np.zeros(self.D)
+        hist = np.zeros(max(g, 1))
+        rho = np.zeros(max(g, 1))
+        scr = np.zeros(max(g, 1), np.int32)
+        self._check(self._lib.fs_gpu_de_run_screened(self._h, g, _dp(best), _dp(x), _dp(hist),
+                                                     _dp(rho), _ip(scr)), "de_run_screened")
+        return best[0], x, dict(history=hist[:g], rho=rho[:g], screened=scr[:g].astype(bool))
+
+    def surrogate_params(self):
+        n = C.c_int64()
+        self._check(self._lib.fs_gpu_surrogate_param_count(self._h, C.byref(n)), "surrogate_param_count")
+        p = np.zeros(n.value, np.float32)
+        self._check(self._lib.fs_gpu_surrogate_get_params(self._h, _fp(p)), "surrogate_get_params")
+        return p
+
+    def surrogate_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self._lib.fs_gpu_surrogate_set_params(self._h, _fp(p)), "surrogate_set_params")
+
+    def surrogate_predict(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        self._check(self._lib.fs_gpu_surrogate_predict(self._h, _fp(X), X.shape[0], _fp(y)),
+                    "surrogate_predict")
+        return y
+
+    def surrogate_gradient(self, X, t):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        n = C.c_int64()
+        self._check(self._lib.fs_gpu_surrogate_param_count(self._h, C.byref(n)), "surrogate_param_count")
+        g = np.zeros(n.value, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self._lib.fs_gpu_surrogate_gradient(self._h, _fp(X), _fp(t), X.shape[0], _fp(g),
+                                                        _fp(loss)), "surrogate_gradient")
+        return float(loss[0]), g
+
+    def surrogate_train(self, X, t, steps):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self._lib.fs_gpu_surrogate_train(self._h, _fp(X), _fp(t), X.shape[0], int(steps),
+                                                     _fp(loss)), "surrogate_train")
+        return float(loss[0])
 
     def de_population(self):
         D = self.D

@@ -10,6 +10,7 @@ dogleg, the D×D JᵀJ), never J.
   LMSolver              EigenLMSolver       solver.cpp:67-85
   HybridSolver          EigenHybridSolver   solver.cpp:87-111
   DESolver              BoostDESolver       solver.cpp:113-155
+  SurrogateDESolver     (none: DE with a learned pre-screen of trial vectors)
   NormalEquationsSolver NormalEquationsSolver solver.cpp:242-266
 
 The reference's LM is MINPACK lmder (QR with column pivoting) and its hybrid
@@ -303,6 +304,40 @@ class DESolver:
         info = dict(obj=best, generations=self.max_generations, lower=lb, upper=ub)
         if history:
             info["history"] = out[2]
+        return 0, xb, info
+
+
+@dataclass
+class SurrogateDESolver(DESolver):
+    """DESolver with learned pre-screening (no reference counterpart).
+
+    A BF16 MLP D → 256 → 256 → 1 trained on the device (Adam, lr 1e-3) on
+    the log objective of every exact evaluation ranks `screen` candidate
+    trials per member; only the best-ranked one is evaluated exactly, and
+    the exact objective alone decides acceptance.  The first
+    `warm_generations` generations are plain DE, and a generation falls back
+    to plain DE while the model's Spearman correlation on the held-out
+    archive slice is below `gate`."""
+    screen: int = 4
+    warm_generations: int = 5
+    batch: int = 512
+    steps_per_generation: int = 32
+    lr: float = 1e-3
+    gate: float = 0.8
+    holdout: float = 0.1
+
+    def minimize(self, sess, x, lower=None, upper=None, w_e=1.0, w_s=0.0, history=False):
+        x = np.array(x, np.float64)
+        lb, ub = de_box(x, lower, upper)
+        sess.de_init(lb, ub, x0=np.clip(x, lb, ub), NP=self.NP_factor * x.size,
+                     mutation=self.mutation_factor, crossover=self.crossover_probability,
+                     seed=self.seed, w_e=w_e, w_s=w_s)
+        sess.surrogate_init(screen=self.screen, warm_generations=self.warm_generations,
+                            batch=self.batch, steps_per_generation=self.steps_per_generation,
+                            lr=self.lr, gate=self.gate, holdout=self.holdout, seed=self.seed)
+        best, xb, info = sess.de_run_screened(self.max_generations)
+        sess.set_params(xb)
+        info.update(obj=best, generations=self.max_generations, lower=lb, upper=ub)
         return 0, xb, info
 
 

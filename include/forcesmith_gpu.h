@@ -270,6 +270,55 @@ int fs_gpu_de_run(fs_gpu *h, int32_t generations, int32_t use_graph,
                   double *best_obj, double *best_x, double *history);
 int fs_gpu_de_population(fs_gpu *h, double *pop, double *obj);
 
+/*
+ * Surrogate-screened DE (no reference counterpart: the reference evaluates
+ * every DE trial exactly).  A BF16 MLP  D → 256 → 256 → 1  (GELU, FP32
+ * accumulation, tcgen05 tensor cores) is trained with Adam on the log of
+ * every exact objective the run computes.  After `warm_generations` plain
+ * generations, each generation draws `screen` candidate trials per member,
+ * the model ranks them, and only each member's best-ranked candidate is
+ * evaluated exactly; the exact objective alone decides acceptance.  Every
+ * round(1/holdout)-th archive row is held out of training; when the model's
+ * Spearman correlation on the newest held-out rows (at most 2048) is below
+ * `gate`, the next generation is plain DE.  D ≤ 256.
+ *
+ * fs_gpu_surrogate_init: (re)creates the model (uniform ±1/√fan-in weights
+ * from `seed`, zero biases) and an empty archive for the current model's D.
+ * fs_gpu_de_run_screened: like fs_gpu_de_run (after fs_gpu_de_init); rho and
+ * screened (nullable, `generations` entries) report the gate's correlation
+ * and whether each generation was screened.
+ *
+ * Model access (tests and tools): parameters are FP32 in the order
+ * W1 [256 × D] row-major, b1 [256], W2 [256 × 256], b2 [256], w3 [256],
+ * b3 [1].  Inputs x are FP32 rows of D features (the DE run uses
+ * 2(x − lo)/(hi − lo) − 1); loss = mean (y − t)²; gradient rows >= 8 and a
+ * multiple of 8.
+ */
+typedef struct fs_surrogate_opts {
+    int32_t screen;               /* candidates per member (4)                  */
+    int32_t warm_generations;     /* plain generations before screening (5)     */
+    int32_t batch;                /* training batch, multiple of 8 (512)        */
+    int32_t steps_per_generation; /* Adam steps after each generation (32)      */
+    double lr;                    /* Adam learning rate (1e-3)                  */
+    double gate;                  /* Spearman threshold (0.8)                   */
+    double holdout;               /* held-out fraction of the archive (0.1)     */
+    uint64_t seed;
+    int64_t archive_rows;         /* archive capacity, 0 = every evaluation     */
+} fs_surrogate_opts;
+
+int fs_gpu_surrogate_init(fs_gpu *h, const fs_surrogate_opts *opts);
+int fs_gpu_de_run_screened(fs_gpu *h, int32_t generations, double *best_obj,
+                           double *best_x, double *history, double *rho,
+                           int32_t *screened);
+int fs_gpu_surrogate_param_count(fs_gpu *h, int64_t *n);
+int fs_gpu_surrogate_get_params(fs_gpu *h, float *params);
+int fs_gpu_surrogate_set_params(fs_gpu *h, const float *params);
+int fs_gpu_surrogate_predict(fs_gpu *h, const float *x, int32_t rows, float *y);
+int fs_gpu_surrogate_gradient(fs_gpu *h, const float *x, const float *t,
+                              int32_t rows, float *grad, float *loss);
+int fs_gpu_surrogate_train(fs_gpu *h, const float *x, const float *t,
+                           int32_t rows, int32_t steps, float *loss);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -99,7 +99,10 @@ def test_de_solver_reduces_objective(problem):
     g.set_model(start)
     x = g.gather_params()
     o0 = g.eval(1.0, 0.0, want=("obj",))["obj"]
-    st, xb, info = solvers.DESolver(NP_factor=2, max_generations=40, seed=3).minimize(g, x, history=True)
+    lo, hi = x - 0.1 * np.abs(x) - 1e-3, x + 0.1 * np.abs(x) + 1e-3  # finite bounds are kept
+    st, xb, info = solvers.DESolver(NP_factor=2, max_generations=40, seed=3).minimize(g, x, lo, hi,
+                                                                                      history=True)
+    np.testing.assert_array_equal(info["lower"], lo)
     assert st == 0
     assert info["obj"] <= o0
     assert info["history"][-1] < info["history"][0]

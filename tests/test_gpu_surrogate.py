@@ -1,0 +1,122 @@
+"""The surrogate MLP's device kernels against the CPU oracle, and the gain of
+surrogate screening over plain DE.
+
+  forward      ‖y_gpu − y_oracle‖ ≤ 2e-3 ‖y_oracle‖ (BF16 rounding points
+               emulated by the oracle; FP32 vs FP64 accumulation)
+  gradient     per tensor ‖g_gpu − g_oracle‖ ≤ 1e-2 ‖g_oracle‖; loss 1e-4 rel
+  Adam         one device step = the oracle's update of the device gradient,
+               1e-5 relative + 1e-9
+  screening    surrogate-screened DE reaches plain DE's final objective
+               (within 1 %) in fewer generations, i.e. fewer exact
+               evaluations (NP per generation either way)
+"""
+import numpy as np
+import pytest
+
+from forcesmith_b200 import solvers
+from oracle import api as O
+from oracle import surrogate as S
+from tests.helpers import label, small_ternary, ternary_models
+
+pytestmark = pytest.mark.gpu
+
+TENSORS = ("W1", "b1", "W2", "b2", "w3", "b3")
+
+
+def _split(g, D):
+    sizes = [S.H * D, S.H, S.H * S.H, S.H, S.H, 1]
+    return dict(zip(TENSORS, np.split(np.asarray(g, np.float64), np.cumsum(sizes)[:-1])))
+
+
+@pytest.fixture(scope="module")
+def sess():
+    from forcesmith_b200.gpu import GpuSession
+    true, start = ternary_models(8)
+    ds = label(small_ternary(3, 32, seed=11), true, O.Oracle, 1.0, 0.0)
+    g = GpuSession(0, "fp32")
+    g.upload(ds)
+    g.set_model(start)
+    g.surrogate_init(seed=9)
+    return g
+
+
+def test_forward_matches_oracle(sess):
+    D = sess.D
+    rng = np.random.default_rng(1)
+    X = rng.uniform(-1, 1, (300, D)).astype(np.float32)
+    p = sess.surrogate_params().astype(np.float64)
+    y = sess.surrogate_predict(X)
+    yo, _ = S.forward(p, X.astype(np.float64), bf=True)
+    assert np.linalg.norm(y - yo) <= 2e-3 * np.linalg.norm(yo)
+
+
+def test_gradient_matches_oracle(sess):
+    D = sess.D
+    rng = np.random.default_rng(2)
+    X = rng.uniform(-1, 1, (256, D)).astype(np.float32)
+    t = rng.normal(0, 1, 256).astype(np.float32)
+    p = sess.surrogate_params().astype(np.float64)
+    loss, g = sess.surrogate_gradient(X, t)
+    lo, go, _ = S.loss_and_grad(p, X.astype(np.float64), t.astype(np.float64), bf=True)
+    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    gs, gos = _split(g, D), _split(go, D)
+    for k in TENSORS:
+        err = np.linalg.norm(gs[k] - gos[k])
+        assert err <= 1e-2 * np.linalg.norm(gos[k]) + 1e-12, (k, err, np.linalg.norm(gos[k]))
+
+
+def test_adam_step_and_training(sess):
+    D = sess.D
+    rng = np.random.default_rng(3)
+    X = rng.uniform(-1, 1, (512, D)).astype(np.float32)
+    t = (np.sin(2 * X[:, :8]).sum(1) + 0.5 * X[:, 8:16].sum(1)).astype(np.float32)
+    t = (t - t.mean()) / t.std()
+    sess.surrogate_init(seed=4)
+    p0 = sess.surrogate_params().astype(np.float64)
+    loss0, g = sess.surrogate_gradient(X, t)
+    sess.surrogate_train(X, t, 1)
+    p1 = sess.surrogate_params().astype(np.float64)
+    want, _, _ = S.adam(p0, g.astype(np.float64), np.zeros_like(p0), np.zeros_like(p0), 1)
+    np.testing.assert_allclose(p1, want, rtol=1e-5, atol=1e-9)
+    loss = sess.surrogate_train(X, t, 300)
+    assert loss < 0.2 * loss0
+
+
+def _de(problem_ds, start, screened, gens, seed, gate=0.8):
+    from forcesmith_b200.gpu import GpuSession
+    g = GpuSession(0, "fp32")
+    g.upload(problem_ds)
+    g.set_model(start)
+    x = g.gather_params()
+    lb, ub = solvers.de_box(x, x - 0.1 * np.abs(x) - 1e-3, x + 0.1 * np.abs(x) + 1e-3)
+    g.de_init(lb, ub, x0=x, NP=256, seed=seed)
+    if screened:
+        g.surrogate_init(screen=4, warm_generations=5, gate=gate, seed=seed)
+        _, _, info = g.de_run_screened(gens)
+        return info
+    _, _, hist = g.de_run(gens, use_graph=True, history=True)
+    return dict(history=hist)
+
+
+def test_screening_gains_over_plain_de():
+    true, start = ternary_models(8)
+    ds = label(small_ternary(3, 32, seed=11), true, O.Oracle, 1.0, 0.0)
+    gens = 80
+    plain = _de(ds, start, False, gens, 21)["history"]
+    scr = _de(ds, start, True, gens, 21)
+    target = 1.01 * plain[-1]
+    reached = np.nonzero(scr["history"] <= target)[0]
+    assert reached.size > 0, (plain[-1], scr["history"][-1], scr["rho"][-5:])
+    assert reached[0] + 1 < gens, (reached[0], plain[-1], scr["history"][-1])
+    assert scr["screened"].sum() > 0
+    # the exact objective decides acceptance: the best objective never increases
+    assert np.all(np.diff(scr["history"]) <= 0)
+
+
+def test_gate_closed_means_plain_de():
+    true, start = ternary_models(8)
+    ds = label(small_ternary(3, 32, seed=11), true, O.Oracle, 1.0, 0.0)
+    plain = _de(ds, start, False, 12, 5)["history"]
+    closed = _de(ds, start, True, 12, 5, gate=2.0)  # unreachable threshold
+    assert not closed["screened"].any()
+    np.testing.assert_array_equal(closed["history"], plain)
