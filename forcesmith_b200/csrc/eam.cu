@@ -287,6 +287,289 @@ __global__ void __launch_bounds__(256) pop_eval_kernel(ResArgs<T> A, const typen
   }
 }
 
+// Population objective, FP32, lanes = trials.  A CTA holds the spline
+// coefficients of 32 trial vectors in shared memory ([segment][trial], so a
+// warp's coefficient load is conflict-free) and walks a size-balanced stride
+// of the configurations, staging each one's geometry in turn.  A warp takes
+// atoms in turn; for a batch of 32 of the atom's pairs its lanes compute the
+// trial-independent geometry once (unit vector, ½dd/r, and per spline role
+// the segment and local coordinate) into a shared record, then every lane
+// walks the batch reading each record as a broadcast and applying its own
+// trial's coefficients.  Per-trial forces, energy and stress accumulate in
+// the lane; the configuration's Σ rows² per trial is summed over warps in a
+// fixed order (deterministic).
+constexpr int kPopLanes = 32;
+constexpr int kPopWarps = 16;
+
+struct PopRec { // 80 B; 16 warps × 32 records also hold the 16 × 32 × 10 FP64 partials
+  float4 a;  // ux, uy, uz, t(φ)
+  float4 b;  // ½·dx·dx/r, ½·dy·dy/r, ½·dz·dz/r, ½·dx·dy/r
+  float4 c;  // ½·dx·dz/r, ½·dy·dz/r, t(ρ_j), t(ρ_i)
+  float4 ih; // 1/h of the φ, ρ_j, ρ_i tables
+  int4 d;    // j, segment of φ, ρ_j, ρ_i (−1: outside the table's gate)
+};
+
+struct PopArgs {
+  Common c;
+  const float4 *pop_seg;              // [trial][n_segs]
+  int NP, n_tiles, n_chunks, nseg_pd; // nseg_pd: segments of the pair + density tables (staged)
+  int max_atoms, max_img;
+  const int32_t *order;               // configurations by decreasing size
+  double *part;                       // [trial][config]
+  double w_e, w_s;
+};
+
+size_t pop_lanes_smem(int n_tables, int nseg_pd, int max_atoms, int max_img, bool eam) {
+  size_t b = 0;
+  b += align16(static_cast<size_t>(nseg_pd) * kPopLanes * sizeof(float4));
+  b += align16(n_tables * sizeof(STab<float>));
+  b += align16(3 * max_atoms * sizeof(double));
+  b += align16(3 * max_img * sizeof(double));
+  b += align16(max_atoms);
+  if (eam) b += align16(static_cast<size_t>(max_atoms) * kPopLanes * sizeof(float));
+  b += align16(kPopWarps * 32 * sizeof(PopRec));
+  b += align16(kPopLanes * 10 * sizeof(double));
+  b += align16((max_atoms + 1) * sizeof(int32_t));
+  return b + 64;
+}
+
+__device__ __forceinline__ float poly_val(const float4 &a, float t) { return a.x + t * (a.y + t * (a.z + t * a.w)); }
+__device__ __forceinline__ float poly_der(const float4 &a, float t) { return a.y + t * (2.f * a.z + 3.f * t * a.w); }
+
+template <bool EAM>
+__global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tile = blockIdx.x % A.n_tiles, chunk = blockIdx.x / A.n_tiles;
+  const int k0 = tile * kPopLanes;
+  const int ntr = min(kPopLanes, A.NP - k0);
+  const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  Smem S(smem_raw);
+  float4 *coef = S.take<float4>(static_cast<size_t>(A.nseg_pd) * kPopLanes);
+  STab<float> *tabs = S.take<STab<float>>(A.c.n_tables);
+  double *wpos = S.take<double>(3 * A.max_atoms);
+  double *shift = S.take<double>(3 * A.max_img);
+  uint8_t *typ = S.take<uint8_t>(A.max_atoms);
+  float *rf = EAM ? S.take<float>(static_cast<size_t>(A.max_atoms) * kPopLanes) : nullptr; // ρ, then F'(ρ)
+  PopRec *stage = S.take<PopRec>(kPopWarps * 32);
+  double *red = S.take<double>(kPopLanes * 10);
+  int32_t *sstart = S.take<int32_t>(A.max_atoms + 1);
+  for (int q = threadIdx.x; q < A.nseg_pd * kPopLanes; q += blockDim.x) {
+    const int k = q / A.nseg_pd, e = q % A.nseg_pd;
+    coef[e * kPopLanes + k] =
+        k < ntr ? A.pop_seg[static_cast<int64_t>(k0 + k) * A.c.n_segs + e] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  const uint32_t *pack = A.c.nb_pack;
+  PopRec *wst = stage + w * 32;
+  // this CTA's configurations: every n_chunks-th of the size-sorted order
+  for (int ci = chunk; ci < A.c.cfg_count; ci += A.n_chunks) {
+    const int c = A.order[ci];
+    const CfgDev &cd = A.c.cfg[c];
+    const int N = cd.natoms;
+    __syncthreads(); // the previous configuration is done with the staged data
+    stage_geometry(cd, A.c, wpos, shift, typ);
+    for (int k = threadIdx.x; k <= N; k += blockDim.x) sstart[k] = A.c.nb_start[cd.atom0 + k];
+    __syncthreads();
+    const int32_t *start = sstart;
+    // the neighbour words of an atom's first batch of 32 pairs (0 past its end)
+    auto first_batch = [&](int ii) -> uint32_t {
+      return (ii < N && start[ii] + l < start[ii + 1]) ? pack[start[ii] + l] : 0u;
+    };
+    double e_emb = 0.0, lim = 0.0, e_pair = 0.0, objf = 0.0;
+    double sg[6] = {0, 0, 0, 0, 0, 0};
+
+    if constexpr (EAM) {
+      // ρ_i per trial (closed gate, eam_force.cpp:59-66)
+      int2 *wst2 = reinterpret_cast<int2 *>(wst);
+      uint32_t pk = first_batch(w);
+      for (int i = w; i < N; i += kPopWarps) {
+        const int p0 = start[i], p1 = start[i + 1];
+        float acc = 0.f;
+        if (p0 == p1) pk = first_batch(i + kPopWarps);
+        for (int pb = p0; pb < p1; pb += 32) {
+          const int p = pb + l;
+          const uint32_t cur = pk;
+          // prefetch the next batch: this atom's, else the warp's next atom's first
+          pk = pb + 32 < p1 ? (pb + 32 + l < p1 ? pack[pb + 32 + l] : 0u) : first_batch(i + kPopWarps);
+          int2 rec = make_int2(-1, 0);
+          if (p < p1) {
+            int j;
+            float dx, dy, dz;
+            pair_vec(wpos, shift, i, cur, j, dx, dy, dz);
+            const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+            const STab<float> &tb = tabs[np + typ[j]];
+            if (in_span(tb, r)) {
+              float t;
+              rec.x = seg_of(tb, r, t);
+              rec.y = __float_as_int(t);
+            }
+          }
+          wst2[l] = rec;
+          __syncwarp();
+          const int cnt = min(32, p1 - pb);
+          for (int q = 0; q < cnt; ++q) {
+            const int2 rr = wst2[q];
+            if (rr.x >= 0) acc += poly_val(coef[rr.x * kPopLanes + l], __int_as_float(rr.y));
+          }
+          __syncwarp();
+        }
+        rf[i * kPopLanes + l] = acc;
+      }
+      __syncthreads();
+      // clamp + F(ρ), F'(ρ) per (atom, trial) (kernels.hpp:19-31; eam_force.cpp:68-73)
+      for (int i = w; i < N; i += kPopWarps) {
+        const STab<float> &tb = tabs[np + nt + typ[i]];
+        float rr = rf[i * kPopLanes + l];
+        if (rr > tb.xmax) {
+          const double d = static_cast<double>(rr) - static_cast<double>(tb.xmax);
+          lim += 100.0 * 10.0 * d * d;
+          rr = tb.xmax;
+        } else if (rr < tb.x0) {
+          const double d = static_cast<double>(tb.x0) - static_cast<double>(rr);
+          lim += 100.0 * 10.0 * d * d;
+          rr = tb.x0;
+        }
+        float t;
+        const int e = seg_of(tb, rr, t);
+        const float4 a =
+            l < ntr ? A.pop_seg[static_cast<int64_t>(k0 + l) * A.c.n_segs + e] : make_float4(0.f, 0.f, 0.f, 0.f);
+        e_emb += static_cast<double>(poly_val(a, t));
+        rf[i * kPopLanes + l] = poly_der(a, t) * tb.inv_h;
+      }
+      __syncthreads();
+    }
+    // forces, ½φ energy, −½ d fᵀ stress (eam_force.cpp:75-100; kernels.hpp:33-38)
+    uint32_t pk = first_batch(w);
+    for (int i = w; i < N; i += kPopWarps) {
+      const int ti = typ[i];
+      const int p0 = start[i], p1 = start[i + 1];
+      const float gFi = EAM ? rf[i * kPopLanes + l] : 0.f;
+      const int64_t ga = static_cast<int64_t>(cd.atom0) + i;
+      const double fr0 = A.c.ref_force[3 * ga], fr1 = A.c.ref_force[3 * ga + 1], fr2 = A.c.ref_force[3 * ga + 2];
+      float f0 = 0.f, f1 = 0.f, f2 = 0.f, ep = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f;
+      if (p0 == p1) pk = first_batch(i + kPopWarps);
+      for (int pb = p0; pb < p1; pb += 32) {
+        const int p = pb + l;
+        const uint32_t cur = pk;
+        pk = pb + 32 < p1 ? (pb + 32 + l < p1 ? pack[pb + 32 + l] : 0u) : first_batch(i + kPopWarps);
+        if (p < p1) {
+          PopRec rec;
+          rec.d = make_int4(0, -1, -1, -1);
+          rec.a = rec.b = rec.c = rec.ih = make_float4(0.f, 0.f, 0.f, 0.f);
+          int j;
+          float dx, dy, dz;
+          pair_vec(wpos, shift, i, cur, j, dx, dy, dz);
+          const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+          if (r >= 1e-14f) {
+            const float inv = 1.f / r, hi = 0.5f * inv;
+            rec.d.x = j;
+            rec.a = make_float4(dx * inv, dy * inv, dz * inv, 0.f);
+            rec.b = make_float4(hi * dx * dx, hi * dy * dy, hi * dz * dz, hi * dx * dy);
+            rec.c = make_float4(hi * dx * dz, hi * dy * dz, 0.f, 0.f);
+            const int tj = typ[j];
+            const STab<float> &tp = tabs[pair_ord(ti, tj, nt)];
+            // EAM: closed gate; pair: [rmin, rmax) (pair_force.cpp:28)
+            const bool gate = EAM ? in_span(tp, r) : (r >= tp.x0 && r < tp.xmax);
+            if (gate) {
+              float t;
+              rec.d.y = seg_of(tp, r, t);
+              rec.a.w = t;
+              rec.ih.x = tp.inv_h;
+            }
+            if constexpr (EAM) {
+              const STab<float> &gj = tabs[np + tj], &gi = tabs[np + ti];
+              if (in_span(gj, r)) {
+                float t;
+                rec.d.z = seg_of(gj, r, t);
+                rec.c.z = t;
+                rec.ih.y = gj.inv_h;
+              }
+              if (in_span(gi, r)) {
+                float t;
+                rec.d.w = seg_of(gi, r, t);
+                rec.c.w = t;
+                rec.ih.z = gi.inv_h;
+              }
+            }
+          }
+          wst[l] = rec;
+        }
+        __syncwarp();
+        const int cnt = min(32, p1 - pb);
+        for (int q = 0; q < cnt; ++q) {
+          // the whole record as five 128-bit broadcast loads
+          const float4 ra = wst[q].a, rb = wst[q].b, rc = wst[q].c, rh = wst[q].ih;
+          const int4 rd = wst[q].d;
+          float g = 0.f;
+          if (rd.y >= 0) {
+            const float4 a = coef[rd.y * kPopLanes + l];
+            ep += poly_val(a, ra.w);
+            g = poly_der(a, ra.w) * rh.x;
+          }
+          if constexpr (EAM) {
+            if (rd.z >= 0) g += gFi * poly_der(coef[rd.z * kPopLanes + l], rc.z) * rh.y;
+            if (rd.w >= 0) g += rf[rd.x * kPopLanes + l] * poly_der(coef[rd.w * kPopLanes + l], rc.w) * rh.z;
+          }
+          f0 += g * ra.x;
+          f1 += g * ra.y;
+          f2 += g * ra.z;
+          s0 -= g * rb.x;
+          s1 -= g * rb.y;
+          s2 -= g * rb.z;
+          s3 -= g * rb.w;
+          s4 -= g * rc.x;
+          s5 -= g * rc.y;
+        }
+        __syncwarp();
+      }
+      const double r0 = static_cast<double>(f0) - fr0;
+      const double r1 = static_cast<double>(f1) - fr1;
+      const double r2 = static_cast<double>(f2) - fr2;
+      objf += r0 * r0 + r1 * r1 + r2 * r2;
+      e_pair += 0.5 * static_cast<double>(ep);
+      sg[0] += s0;
+      sg[1] += s1;
+      sg[2] += s2;
+      sg[3] += s3;
+      sg[4] += s4;
+      sg[5] += s5;
+    }
+    // per-(warp, trial) partials into the staging area (16 × 32 × 10 doubles),
+    // then a fixed-order sum over warps
+    __syncthreads();
+    double *pw = reinterpret_cast<double *>(stage) + (w * kPopLanes + l) * 10;
+    pw[0] = objf;
+    pw[1] = e_emb + e_pair;
+    pw[2] = lim;
+    for (int a = 0; a < 6; ++a) pw[3 + a] = sg[a];
+    __syncthreads();
+    if (threadIdx.x < kPopLanes) {
+      const double *base = reinterpret_cast<const double *>(stage) + threadIdx.x * 10;
+      for (int q = 0; q < 9; ++q) {
+        double acc = 0.0;
+        for (int ww = 0; ww < kPopWarps; ++ww) acc += base[ww * kPopLanes * 10 + q];
+        red[threadIdx.x * 10 + q] = acc;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < ntr) {
+      const double *R = red + threadIdx.x * 10;
+      const double iv = 1.0 / cd.volume;
+      const double re = A.w_e * (R[1] - cd.ref_energy);
+      double o = R[0] + re * re;
+      static constexpr int vi[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+      if (A.w_s > 0.0)
+        for (int v = 0; v < 6; ++v) {
+          const double rs = A.w_s * (R[3 + v] * iv - cd.ref_stress[3 * vi[v][0] + vi[v][1]]);
+          o += rs * rs;
+        }
+      o += R[2] * R[2];
+      A.part[static_cast<int64_t>(k0 + threadIdx.x) * A.c.cfg_count + c] = o;
+    }
+  } // configurations
+}
+
 // Σ over configurations in a fixed order (deterministic objective).
 __global__ void sum_kernel(const double *__restrict__ part, int n, double *__restrict__ out) {
   __shared__ double red[32];
@@ -1174,6 +1457,36 @@ int launch_population_t(fs_gpu *h, double w_e, double w_s, const double *d_xs, i
                                                  h->n_segs, pop_seg);
     FS_CUDA(cudaGetLastError());
     ++h->launches;
+  }
+  if constexpr (std::is_same_v<T, float>) {
+    // one lane per trial when the largest configuration fits in shared memory
+    const int np_ = npair_of(h->ntypes);
+    const int nseg_pd = EAM ? h->desc[np_ + h->ntypes].seg0 : h->n_segs;
+    const size_t sml = pop_lanes_smem(a.c.n_tables, nseg_pd, h->max_natoms, max_images(h), EAM);
+    if (sml <= 227 * 1024) {
+      PopArgs pa;
+      pa.c = a.c;
+      pa.pop_seg = pop_seg;
+      pa.NP = NP;
+      pa.n_tiles = (NP + kPopLanes - 1) / kPopLanes;
+      // about four waves of one CTA per SM
+      pa.n_chunks = std::max(1, std::min(h->n_cfg, (4 * 148 + pa.n_tiles - 1) / pa.n_tiles));
+      pa.nseg_pd = nseg_pd;
+      pa.max_atoms = h->max_natoms;
+      pa.max_img = max_images(h);
+      pa.order = order;
+      pa.part = part;
+      pa.w_e = w_e;
+      pa.w_s = w_s;
+      auto kl = pop_lanes_kernel<EAM>;
+      FS_CUDA(cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sml)));
+      kl<<<static_cast<unsigned>(pa.n_chunks) * pa.n_tiles, kPopWarps * 32, sml, h->stream>>>(pa);
+      FS_CUDA(cudaGetLastError());
+      pop_reduce_kernel<<<(NP + 127) / 128, 128, 0, h->stream>>>(part, h->n_cfg, NP, d_obj);
+      FS_CUDA(cudaGetLastError());
+      h->launches += 2;
+      return FS_OK;
+    }
   }
   const int tile = std::max(1, std::min(16, NP));
   const int n_tiles = (NP + tile - 1) / tile;

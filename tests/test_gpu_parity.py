@@ -207,6 +207,28 @@ def test_population_objective(ternary_small):
     _close(og, oo, 1e-9, "population objective")
 
 
+@pytest.mark.parametrize("family", ["eam", "pair"])
+def test_population_objective_fp32_lanes(ternary_small, family):
+    """FP32 population path (one lane per trial vector): against the FP64
+    oracle (relative 1e-4, the FP32 objective bar) and against the FP32
+    single-vector residual path (relative 1e-5); NP = 37 leaves a partial
+    tile of trials."""
+    ds, _, start = ternary_small
+    model = start if family == "eam" else spline_pair_model(3, 14)
+    g, o = _pair(ds.subset([0, 1, 2, 3]), model, "fp32")
+    x0 = g.gather_params()
+    xs = np.stack([x0 * synth.uniform(x0.size, 0.97, 1.03, 200 + k) for k in range(37)])
+    og = g.eval_population(xs, 1.0, 0.1)
+    oo = o.eval_population(xs, 1.0, 0.1)
+    _close(og, oo, 1e-4, "population objective vs oracle")
+    single = []
+    for x in xs[:5]:
+        g.set_params(x)
+        single.append(g.eval(1.0, 0.1, want=("obj",))["obj"])
+    np.testing.assert_allclose(og[:5], single, rtol=1e-5)
+    assert np.array_equal(og, g.eval_population(xs, 1.0, 0.1)), "deterministic"
+
+
 def test_gradient_directional_full_size():
     """Size-independent property at the full ternary workload (500 × 256):
     d/dε ‖F(x + εv)‖² = 2 vᵀJᵀF, with J from the FP32 analytic path and the
