@@ -21,6 +21,8 @@
 #include "kern_common.cuh"
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 namespace fsg {
 namespace {
@@ -1510,6 +1512,111 @@ template <class T, bool EAM> int launch_population_lpa(fs_gpu *h, double w_e, do
   }
 }
 
+// ---------------------------------------------------------------------------
+// Population objective with caller-owned buffers and no allocation
+// (fs_gpu_eval_population_noalloc).  The same kernels as the allocating
+// path; its scratch — configuration order, spline-table list, per-trial
+// segments and per-(trial, configuration) partial sums — lives in one
+// fixed-size device array, g_noalloc_scratch below.
+
+__global__ void iota_kernel(int32_t *__restrict__ v, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+struct NoAllocLayout {
+  size_t ord, spl, seg, part, total;
+};
+
+template <class T> NoAllocLayout noalloc_layout(const fs_gpu *h, int NP) {
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  NoAllocLayout L;
+  L.ord = 0;
+  L.spl = L.ord + up(h->n_cfg * sizeof(int32_t));
+  L.seg = L.spl + up(h->desc.size() * sizeof(int32_t));
+  L.part = L.seg + up(static_cast<size_t>(NP) * h->n_segs * sizeof(typename Vec4T<T>::type));
+  L.total = L.part + static_cast<size_t>(NP) * h->n_cfg * sizeof(double);
+  return L;
+}
+
+// Launches of launch_population_t with every buffer taken from `scratch`.
+template <class T, int LPA, bool EAM>
+int launch_population_static(fs_gpu *h, double w_e, double w_s, const double *d_xs, int NP, double *d_obj,
+                             unsigned char *scratch) {
+  using T4 = typename Vec4T<T>::type;
+  const NoAllocLayout L = noalloc_layout<T>(h, NP);
+  int32_t *order = reinterpret_cast<int32_t *>(scratch + L.ord);
+  int32_t *spl = reinterpret_cast<int32_t *>(scratch + L.spl);
+  T4 *pop_seg = reinterpret_cast<T4 *>(scratch + L.seg);
+  double *part = reinterpret_cast<double *>(scratch + L.part);
+  const int n_tables = static_cast<int>(h->desc.size());
+  // every table is a spline here, so the table list is 0..n_tables−1; the
+  // configurations go in upload order (the order only balances the work)
+  iota_kernel<<<(h->n_cfg + 255) / 256, 256, 0, h->stream>>>(order, h->n_cfg);
+  iota_kernel<<<1, 256, 0, h->stream>>>(spl, n_tables);
+  FS_CUDA(cudaGetLastError());
+  dim3 g(static_cast<unsigned>(n_tables), static_cast<unsigned>(NP));
+  pop_setup_kernel<T><<<g, 32, 0, h->stream>>>(h->d_desc, spl, h->d_vals, h->d_cmap, d_xs, h->D, h->n_segs, pop_seg);
+  FS_CUDA(cudaGetLastError());
+  h->launches += 3;
+  ResArgs<T> a;
+  a.c = make_common<T>(h);
+  a.seg_a = nullptr;
+  a.w_e = w_e;
+  a.w_s = w_s;
+  a.F = a.forces = a.energy = a.stress9 = a.limit = a.obj_part = nullptr;
+  if constexpr (std::is_same_v<T, float>) {
+    const int np_ = npair_of(h->ntypes);
+    const int nseg_pd = EAM ? h->desc[np_ + h->ntypes].seg0 : h->n_segs;
+    const size_t sml = pop_lanes_smem(a.c.n_tables, nseg_pd, h->max_natoms, max_images(h), EAM);
+    if (sml <= 227 * 1024) {
+      PopArgs pa;
+      pa.c = a.c;
+      pa.pop_seg = pop_seg;
+      pa.NP = NP;
+      pa.n_tiles = (NP + kPopLanes - 1) / kPopLanes;
+      pa.n_chunks = std::max(1, std::min(h->n_cfg, (4 * 148 + pa.n_tiles - 1) / pa.n_tiles));
+      pa.nseg_pd = nseg_pd;
+      pa.max_atoms = h->max_natoms;
+      pa.max_img = max_images(h);
+      pa.order = order;
+      pa.part = part;
+      pa.w_e = w_e;
+      pa.w_s = w_s;
+      auto kl = pop_lanes_kernel<EAM>;
+      FS_CUDA(cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sml)));
+      kl<<<static_cast<unsigned>(pa.n_chunks) * pa.n_tiles, kPopWarps * 32, sml, h->stream>>>(pa);
+      FS_CUDA(cudaGetLastError());
+      pop_reduce_kernel<<<(NP + 127) / 128, 128, 0, h->stream>>>(part, h->n_cfg, NP, d_obj);
+      FS_CUDA(cudaGetLastError());
+      h->launches += 2;
+      return FS_OK;
+    }
+  }
+  const int tile = std::max(1, std::min(16, NP));
+  const int n_tiles = (NP + tile - 1) / tile;
+  const size_t sm = residual_smem<T>(a.c.n_tables, h->n_segs, h->max_natoms, max_images(h));
+  if (sm > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "population: configuration too large for shared memory");
+  auto k = pop_eval_kernel<T, LPA, EAM>;
+  FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+  k<<<static_cast<unsigned>(h->n_cfg) * n_tiles, 256, sm, h->stream>>>(a, pop_seg, NP, tile, n_tiles, order, part);
+  FS_CUDA(cudaGetLastError());
+  pop_reduce_kernel<<<(NP + 127) / 128, 128, 0, h->stream>>>(part, h->n_cfg, NP, d_obj);
+  FS_CUDA(cudaGetLastError());
+  h->launches += 2;
+  return FS_OK;
+}
+
+template <class T, bool EAM>
+int launch_population_static_lpa(fs_gpu *h, double w_e, double w_s, const double *xs, int NP, double *obj,
+                                 unsigned char *scratch) {
+  switch (choose_lpa(h)) {
+  case 4: return launch_population_static<T, 4, EAM>(h, w_e, w_s, xs, NP, obj, scratch);
+  case 8: return launch_population_static<T, 8, EAM>(h, w_e, w_s, xs, NP, obj, scratch);
+  case 16: return launch_population_static<T, 16, EAM>(h, w_e, w_s, xs, NP, obj, scratch);
+  default: return launch_population_static<T, 32, EAM>(h, w_e, w_s, xs, NP, obj, scratch);
+  }
+}
+
 } // namespace
 
 int eval_residual(fs_gpu *h, double w_e, double w_s) {
@@ -1549,3 +1656,83 @@ int eval_population_device(fs_gpu *h, double w_e, double w_s, const double *d_xs
              : launch_population_lpa<float, false>(h, w_e, w_s, d_xs, NP, d_obj);
 }
 } // namespace fsg
+
+// ---------------------------------------------------------------------------
+// fs_gpu_eval_population_noalloc: the scratch array and its device address.
+
+namespace fsg {
+
+// 8 MiB of device memory in the library image: every GPU that loads the
+// library holds it until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// The array's device address on h's device (looked up once per device, with
+// that device current).  The host-side symbol itself is not a device address.
+int noalloc_scratch(fs_gpu *h, unsigned char **out) {
+  if (h->device < 0 || h->device >= kMaxDevices) return set_error(h, FS_ERR_ARG, "eval_population_noalloc: device ordinal");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[h->device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(h, FS_ERR_CUDA, std::string("eval_population_noalloc: cudaGetSymbolAddress: ") +
+                                           cudaGetErrorString(e));
+    g_noalloc_addr[h->device] = p;
+  }
+  *out = static_cast<unsigned char *>(g_noalloc_addr[h->device]);
+  return FS_OK;
+}
+
+bool on_device(const void *p, int device) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device;
+}
+} // namespace
+} // namespace fsg
+
+extern "C" int fs_gpu_eval_population_noalloc(fs_gpu *h, double w_e, double w_s, const double *xs_dev, int32_t NP,
+                                              double *obj_dev) {
+  using namespace fsg;
+  if (!h) return FS_ERR_ARG;
+  if (!xs_dev || !obj_dev || NP < 1) return set_error(h, FS_ERR_ARG, "eval_population_noalloc: bad arguments");
+  if (h->n_cfg == 0 || !h->have_model) return set_error(h, FS_ERR_STATE, "eval_population_noalloc: no configurations or model");
+  if (h->rcut_built < 0 || model_max_cutoff(h) > h->rcut_built)
+    return set_error(h, FS_ERR_STATE, "eval_population_noalloc: neighbour lists not built for the model; call fs_gpu_prepare");
+  if (h->family != FS_FAMILY_EAM && h->family != FS_FAMILY_PAIR)
+    return set_error(h, FS_ERR_UNSUPPORTED, "eval_population_noalloc: EAM and pair families");
+  for (const HostTable &t : h->tables)
+    if (t.kind != FS_TABLE_SPLINE) return set_error(h, FS_ERR_UNSUPPORTED, "eval_population_noalloc: spline tables");
+  if (cudaSetDevice(h->device) != cudaSuccess) return set_error(h, FS_ERR_CUDA, "eval_population_noalloc: cudaSetDevice");
+  if (!on_device(xs_dev, h->device) || !on_device(obj_dev, h->device))
+    return set_error(h, FS_ERR_ARG, "eval_population_noalloc: xs and obj must be device memory of the context's GPU");
+  const bool fp64 = h->precision == FS_PREC_FP64;
+  const size_t need = fp64 ? noalloc_layout<double>(h, NP).total : noalloc_layout<float>(h, NP).total;
+  if (need > kNoAllocScratchBytes) {
+    const size_t per_trial = fp64 ? noalloc_layout<double>(h, 2).total - noalloc_layout<double>(h, 1).total
+                                  : noalloc_layout<float>(h, 2).total - noalloc_layout<float>(h, 1).total;
+    const size_t fixed = (fp64 ? noalloc_layout<double>(h, 1).total : noalloc_layout<float>(h, 1).total) - per_trial;
+    const long long max_np = per_trial ? static_cast<long long>((kNoAllocScratchBytes - fixed) / per_trial) : 0;
+    return set_error(h, FS_ERR_ARG,
+                     "eval_population_noalloc: NP = " + std::to_string(NP) + " needs " + std::to_string(need) +
+                         " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
+                         " bytes (NP <= about " + std::to_string(max_np) + " for these configurations and model)");
+  }
+  unsigned char *scratch = nullptr;
+  FS_TRY(noalloc_scratch(h, &scratch));
+  const bool eam = h->family == FS_FAMILY_EAM;
+  if (fp64)
+    return eam ? launch_population_static_lpa<double, true>(h, w_e, w_s, xs_dev, NP, obj_dev, scratch)
+               : launch_population_static_lpa<double, false>(h, w_e, w_s, xs_dev, NP, obj_dev, scratch);
+  return eam ? launch_population_static_lpa<float, true>(h, w_e, w_s, xs_dev, NP, obj_dev, scratch)
+             : launch_population_static_lpa<float, false>(h, w_e, w_s, xs_dev, NP, obj_dev, scratch);
+}

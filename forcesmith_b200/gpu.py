@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
         L.fs_gpu_de_init.argtypes = [vp, C.POINTER(fs_de_opts), pd, pd, pd]
         L.fs_gpu_de_run.argtypes = [vp, i32, i32, pd, pd, pd]
         L.fs_gpu_de_population.argtypes = [vp, pd, pd]
+        L.fs_gpu_eval_population_noalloc.argtypes = [vp, dbl, dbl, vp, i32, vp]
         pf = C.POINTER(C.c_float)
         L.fs_gpu_surrogate_init.argtypes = [vp, C.POINTER(fs_surrogate_opts)]
         L.fs_gpu_de_run_screened.argtypes = [vp, i32, pd, pd, pd, pd, pi]
@@ -158,6 +159,15 @@ class GpuSession(Session):
         self._check(self._lib.fs_gpu_eval_population(self._h, w_e, w_s, _dp(xs), xs.shape[0],
                                                      _dp(obj)), "eval_population")
         return obj
+
+    def eval_population_noalloc(self, xs_dev_ptr, NP, obj_dev_ptr, w_e=1.0, w_s=0.0):
+        """fs_gpu_eval_population_noalloc: objectives of NP trial vectors
+        already in device memory (xs_dev_ptr: NP × D doubles) into device
+        memory (obj_dev_ptr: NP doubles), with no allocation by the library.
+        Asynchronous on this context's stream."""
+        self._check(self._lib.fs_gpu_eval_population_noalloc(
+            self._h, w_e, w_s, C.c_void_p(xs_dev_ptr), int(NP), C.c_void_p(obj_dev_ptr)),
+            "eval_population_noalloc")
 
     # -- differential evolution on the device ---------------------------------
     def de_init(self, lo, hi, x0=None, NP=None, mutation=0.65, crossover=0.5, seed=42,

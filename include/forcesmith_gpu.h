@@ -238,6 +238,41 @@ int fs_gpu_eval_population(fs_gpu *h, double w_e, double w_s, const double *xs,
                            int32_t NP, double *obj);
 
 /*
+ * fs_gpu_eval_population_noalloc — the batched objective of
+ * fs_gpu_eval_population for callers that cannot allocate device memory.
+ * No counterpart in the reference (its DE evaluates trials one at a time on
+ * the CPU).
+ *
+ * Who needs it: a host that has handed all of the GPU's memory to its own
+ * pool and forbids further cudaMalloc, or a latency-critical loop that must
+ * not call cudaMalloc / cudaFree because they can synchronise the device.
+ * This call allocates nothing and frees nothing: the caller passes device
+ * buffers xs_dev (NP × D doubles, row-major) and obj_dev (NP doubles) on the
+ * context's GPU, and the kernels' scratch (per-trial spline segments and
+ * per-(trial, configuration) partial sums) lives in one fixed 8 MiB device
+ * array inside the library, which every GPU that loads the library holds
+ * until the process exits.  NP whose scratch would exceed 8 MiB is rejected
+ * with FS_ERR_ARG and a message giving the largest NP that fits (about 1000
+ * trials for 500 configurations of a 12-table EAM model in FP32).
+ *
+ * Results equal fs_gpu_eval_population's (same kernels).  The call is
+ * asynchronous on the context's stream (fs_gpu_get_stream): obj_dev is ready
+ * once that stream reaches it.  The context must have been prepared
+ * (fs_gpu_prepare) with its configurations and model; EAM or pair family,
+ * spline tables.
+ *
+ * The first call on each GPU looks up the array's device address (a
+ * runtime query, no allocation); make that first call before any stream
+ * capture.  All calls in the process share the one array and it keeps the
+ * previous call's contents; every byte a call reads it has written first,
+ * so nothing needs clearing, but two calls whose kernels overlap on the
+ * same GPU (two contexts, two streams) race on it — serialise them.
+ */
+int fs_gpu_eval_population_noalloc(fs_gpu *h, double w_e, double w_s,
+                                   const double *xs_dev, int32_t NP,
+                                   double *obj_dev);
+
+/*
  * Differential evolution on the device — replaces BoostDESolver::solve
  * (src/optimization/solver.cpp:113-155; DEParams: NP, mutation F, crossover
  * CR, seed, max_generations).  DE/rand/1/bin with box clamping and greedy
