@@ -68,7 +68,8 @@ def peaks():
 
 def workload(rank=0, small=False):
     from forcesmith_b200 import synth
-    n_cfg, n_at = (20, 256) if small else (N_CFG, N_ATOMS)
+    # the small case (profiler captures): 200 configurations, J = 149 MB > L2
+    n_cfg, n_at = (200, 256) if small else (N_CFG, N_ATOMS)
     ds = synth.packing(np.full(n_cfg, n_at, np.int32), seed=20261204 + 7919 * rank)
     true = synth.ternary_true_model(20)
     start = synth.perturb(true, 0.95, 1.05, seed=7)

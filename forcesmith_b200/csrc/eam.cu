@@ -788,7 +788,7 @@ template <class T> struct V2T;
 template <> struct V2T<float> { using type = float2; };
 template <> struct V2T<double> { using type = double2; };
 
-template <class T, bool EAM>
+template <class T, bool EAM, bool STAGE>
 __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
   using T4 = typename Vec4T<T>::type;
   using T2 = typename V2T<T>::type;
@@ -820,7 +820,9 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
   int dstr = nd;
   const T *gFa = A.gF + cd.atom0, *cFa = A.cF + cd.atom0, *dgda = A.dgd + static_cast<int64_t>(cd.atom0) * kWin;
   const int32_t *wsFa = A.wsF + cd.atom0;
-  if (EAM && A.stage) {
+  // STAGE: the configuration's per-atom data comes from shared memory (the
+  // pointers below then address the shared window only)
+  if constexpr (EAM && STAGE) {
     T *s_dr = S.take<T>(static_cast<size_t>(N) * (nd + 1));
     T *s_gf = S.take<T>(N);
     T *s_cf = S.take<T>(N);
@@ -1323,7 +1325,8 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
       sm2 = k2_smem(wp);
     }
   if (warps < 1) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: configuration too large");
-  auto k2 = eam ? jac_forces_kernel<T, true> : jac_forces_kernel<T, false>;
+  auto k2 = eam ? (a.stage ? jac_forces_kernel<T, true, true> : jac_forces_kernel<T, true, false>)
+                : jac_forces_kernel<T, false, false>;
   FS_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm2)));
   k2<<<h->n_cfg, 32 * warps, sm2, h->stream>>>(a, warps);
   FS_CUDA(cudaGetLastError());

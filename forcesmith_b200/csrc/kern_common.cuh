@@ -7,14 +7,19 @@
 namespace fsg {
 namespace {
 
+// Bump allocator over the dynamic shared-memory block.  Offsets are aligned
+// as integers and added to the block's base pointer, so every carved pointer
+// stays a pointer into the shared window (no round trip through an integer
+// address, which would turn its loads into generic ones).  The block itself
+// is declared 16-byte aligned.
 struct Smem {
-  unsigned char *p;
-  __device__ explicit Smem(unsigned char *base) : p(base) {}
+  unsigned char *base;
+  size_t off = 0;
+  __device__ explicit Smem(unsigned char *b) : base(b) {}
   template <class X> __device__ X *take(size_t n, size_t align = 16) {
-    uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    a = (a + align - 1) & ~(uintptr_t)(align - 1);
-    X *r = reinterpret_cast<X *>(a);
-    p = reinterpret_cast<unsigned char *>(a + n * sizeof(X));
+    off = (off + align - 1) & ~(align - 1);
+    X *r = reinterpret_cast<X *>(base + off);
+    off += n * sizeof(X);
     return r;
   }
 };
