@@ -18,6 +18,11 @@ w_e = 1, w_s = 0.1 — rows = 388,000.  FP32 compute, FP64 sums.
             on a bounded sample of FD columns, extrapolated to one Jacobian
 
 `--impl reference` times that CPU path alone as the reference arm.
+
+Two more legs ride in the same JSON line (one GPU, rank 0): `de`, the
+batched DE population objective on 200 configurations of 32-512 atoms with
+NP = 15 D, and `surrogate`, the wall time surrogate-screened DE needs to reach
+plain device DE's final objective (within 1 %) against plain DE's own time.
 Multi-GPU (torchrun): every rank evaluates its own 500-configuration shard
 (weak scaling) and the normal equations are summed over ranks with one
 NCCL all-reduce per step (the exchange an LM step needs).
@@ -54,6 +59,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-columns", type=int, default=4)
     p.add_argument("--small", action="store_true", help="small case for profiler captures")
+    p.add_argument("--de-generations", type=int, default=200,
+                   help="generations of the DE and surrogate-screened DE legs (0: skip them)")
     return p.parse_args()
 
 
@@ -151,6 +158,101 @@ def algorithmic(g, phase, M, D, P, N, ndens=60):
         return "hbm", P * 4 + N * (ndens * 4 + 40) + 2 * D * 8
     # JᵀJ: 2·m·D² FLOPs (dense contraction), plus Jᵀr
     return "tensor", 2.0 * M * D * D + 2.0 * M * D
+
+
+def traffic_from_profiles(kernel):
+    """DRAM bytes per full-size launch of `kernel`, from the committed ncu
+    summary (a line `traffic_bytes_per_launch[kernel]: N`), else None."""
+    import glob
+    import re
+    pat = re.compile(r"traffic_bytes_per_launch\[" + re.escape(kernel) + r"\]:\s*([0-9.eE+]+)")
+    for f in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(f) as fh:
+            m = pat.search(fh.read())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def de_legs(local, generations):
+    """Batched DE on the 200-configuration set (32-512 atoms, NP = 15 D):
+    throughput of the population objective, then the surrogate comparison -
+    wall time of plain device DE over `generations` generations against the
+    wall time surrogate-screened DE needs to reach plain DE's final best
+    objective within 1 %."""
+    import torch
+    from forcesmith_b200 import gpu as G, solvers, synth
+    ds = synth.de_geometry()
+    true = synth.ternary_true_model(20)
+    start = synth.perturb(true, 0.95, 1.05, seed=7)
+    ds = label_on_gpu(ds, true, local)
+    g = G.GpuSession(local, "fp32")
+    g.upload(ds)
+    g.set_model(start)
+    x = g.gather_params()
+    D, P = x.size, g.num_pairs()
+    NP = 15 * D
+    # finite knot box x0 ± 10 % (the reference keeps finite bounds as given)
+    lb, ub = solvers.de_box(x, x - 0.1 * np.abs(x) - 1e-3, x + 0.1 * np.abs(x) + 1e-3)
+    g.de_init(lb, ub, x0=x, NP=NP, seed=11)
+    g.de_run(3, use_graph=True)  # warm-up (graph capture)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(g.stream)
+    n_t = 10
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    g.de_run(n_t, use_graph=True)
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_gen = ev0.elapsed_time(ev1) / n_t
+    flops = 60.0 * P * NP / (ms_gen * 1e-3)
+    sm_mhz = 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6  # FP32 CUDA-core FMA rate at the max SM clock (nominal)
+    de = {"workload": f"DE population objective, {ds.n_cfg} configs x 32-512 atoms ({ds.n_atoms} atoms, "
+                      f"{P} pairs), NP={NP}, D={D}, F=0.65, CR=0.5, box x0 +/- 10%",
+          "ms_per_generation": ms_gen, "pair_trials_per_s": P * NP / (ms_gen * 1e-3),
+          "roofline": {"bound": "fp32", "achieved": flops / 1e12, "peak": fp32_peak / 1e12,
+                       "unit": "TFLOP/s", "frac": flops / fp32_peak, "peak_source": "nominal",
+                       "algorithmic": "60 FLOP per pair-trial"}}
+    if generations <= 0:
+        g.close()
+        return de, None
+    # plain DE, device-resident, graph replay: wall time of `generations` generations
+    g.de_init(lb, ub, x0=x, NP=NP, seed=11)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    best_plain, _ = g.de_run(generations, use_graph=True)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    target = 1.01 * best_plain
+    # surrogate-screened DE from the same start, in chunks until the target
+    g.de_init(lb, ub, x0=x, NP=NP, seed=11)
+    g.surrogate_init(seed=11)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done, gens, best_s, screened = 0, 0, float("inf"), 0
+    chunk = 5
+    while gens < generations:
+        b, _, info = g.de_run_screened(min(chunk, generations - gens))
+        gens += min(chunk, generations - gens)
+        screened += int(info["screened"].sum())
+        best_s = b
+        if b <= target:
+            done = 1
+            break
+    torch.cuda.synchronize()
+    t_scr = time.perf_counter() - t0
+    g.close()
+    sur = {"plain_generations": generations, "plain_final_objective": best_plain, "plain_wall_s": t_plain,
+           "target": "plain final objective x 1.01", "screened_reached": bool(done),
+           "screened_generations": gens, "screened_generations_screened": screened,
+           "screened_best_objective": best_s, "screened_wall_s": t_scr,
+           "wall_ratio": t_scr / t_plain,
+           "model": "BF16 MLP D->256->256->1 (GELU, Adam lr 1e-3), 4 candidates per member, "
+                    "warm start 5 generations, Spearman gate 0.8 on a 10% held-out slice"}
+    return de, sur
 
 
 def cpu_baseline(ds, start, columns):
@@ -338,8 +440,14 @@ def run_ours(args):
                      "algorithmic": alg},
         "clocks": clk,
     }
+    line["roofline"]["traffic"] = traffic_from_profiles(dom)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ds, start, args.cpu_columns)
+    if rank == 0 and world == 1 and not args.small and args.de_generations >= 0:
+        de, sur = de_legs(local, args.de_generations)
+        line["de"] = de
+        if sur is not None:
+            line["surrogate"] = sur
     if dist is not None:
         dist.barrier()
     g.close()

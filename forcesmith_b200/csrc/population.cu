@@ -504,10 +504,14 @@ int de_run_screened(fs_gpu *h, int generations, double *best_obj, double *best_x
   if (!s || !sv || !h->mlp) return set_error(h, FS_ERR_STATE, "de_run_screened: fs_gpu_de_init and fs_gpu_surrogate_init first");
   if (sv->D != s->D) return set_error(h, FS_ERR_STATE, "de_run_screened: surrogate and DE sizes differ");
   const int NP = s->NP, D = s->D, S = std::max(1, sv->o.screen);
+  if (sv->o.archive_rows > 0 && sv->o.archive_rows < 2 * static_cast<int64_t>(NP))
+    return set_error(h, FS_ERR_ARG, "de_run_screened: archive_rows must hold at least two generations (2 NP)");
   // archive: grows in whole generations (ring once the capacity is reached)
   const int64_t want = sv->n + static_cast<int64_t>(generations) * NP;
   if (want > sv->cap) {
-    const int64_t cap = std::min<int64_t>(std::max<int64_t>(want, 16 * NP), sv->o.archive_rows > 0 ? sv->o.archive_rows : want);
+    // grow geometrically so that runs made of many short calls copy little
+    const int64_t grown = std::max<int64_t>(std::max<int64_t>(want, 2 * sv->cap), 16 * NP);
+    const int64_t cap = sv->o.archive_rows > 0 ? std::min<int64_t>(grown, sv->o.archive_rows) : grown;
     float *ax = nullptr, *at = nullptr;
     if (cudaMalloc(&ax, cap * D * sizeof(float)) != cudaSuccess || cudaMalloc(&at, cap * sizeof(float)) != cudaSuccess) {
       cudaFree(ax);
