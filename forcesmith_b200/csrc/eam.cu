@@ -52,7 +52,7 @@ template <class T> size_t residual_smem(int n_tables, int n_segs, int max_atoms,
 // The residual of one configuration from staged tables and geometry: writes
 // its rows when ROWS, and returns Σ rows² (valid on thread 0) — shared by the
 // residual kernel and the population kernel.
-template <class T, int LPA, bool EAM, bool ROWS>
+template <class T, int LPA, bool EAM, bool ROWS, bool AN = false>
 __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, const STab<T> *tabs,
                               const typename Vec4T<T>::type *seg, const double *wpos, const double *shift,
                               const uint8_t *typ, T *rho, T *gradF, double *red) {
@@ -73,11 +73,7 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
           pair_vec(wpos, shift, i, A.c.nb_pack[p], j, dx, dy, dz);
           const T r = sqrt_t(dx * dx + dy * dy + dz * dz);
           const STab<T> &tb = tabs[np + typ[j]];
-          if (in_span(tb, r)) {
-            T t;
-            const int e = seg_of(tb, r, t);
-            acc += seg_val<T>(seg[e], t);
-          }
+          if (in_span(tb, r)) acc += tab_vd<T, AN>(tb, seg, A.c.vals, r).v;
         }
       }
       acc = warp_sum_group(acc, LPA);
@@ -97,10 +93,9 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
         lim += 100.0 * 10.0 * d * d;
         rr = tb.x0;
       }
-      T t;
-      const int e = seg_of(tb, rr, t);
-      e_emb += static_cast<double>(seg_val<T>(seg[e], t));
-      gradF[i] = seg_der<T>(seg[e], t, tb.inv_h);
+      const VD<T> fv = tab_vd<T, AN>(tb, seg, A.c.vals, rr);
+      e_emb += static_cast<double>(fv.v);
+      gradF[i] = fv.d;
     }
     __syncthreads();
   }
@@ -125,33 +120,23 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
         T phi = T(0), dphi = T(0);
         if constexpr (EAM) {
           if (in_span(tp, r)) {
-            T t;
-            const int e = seg_of(tp, r, t);
-            phi = seg_val<T>(seg[e], t);
-            dphi = seg_der<T>(seg[e], t, tp.inv_h);
+            const VD<T> pv = tab_vd<T, AN>(tp, seg, A.c.vals, r);
+            phi = pv.v;
+            dphi = pv.d;
           }
         } else {
           // make_pair_bond's half-open gate [rmin, rmax) (pair_force.cpp:28)
           if (r < tp.x0 || r >= tp.xmax) continue;
-          T t;
-          const int e = seg_of(tp, r, t);
-          phi = seg_val<T>(seg[e], t);
-          dphi = seg_der<T>(seg[e], t, tp.inv_h);
+          const VD<T> pv = tab_vd<T, AN>(tp, seg, A.c.vals, r);
+          phi = pv.v;
+          dphi = pv.d;
         }
         T fs = dphi;
         if constexpr (EAM) {
           const STab<T> &gj = tabs[np + tj], &gi = tabs[np + ti];
           T drho_j = T(0), drho_i = T(0);
-          if (in_span(gj, r)) {
-            T t;
-            const int e = seg_of(gj, r, t);
-            drho_j = seg_der<T>(seg[e], t, gj.inv_h);
-          }
-          if (in_span(gi, r)) {
-            T t;
-            const int e = seg_of(gi, r, t);
-            drho_i = seg_der<T>(seg[e], t, gi.inv_h);
-          }
+          if (in_span(gj, r)) drho_j = tab_vd<T, AN>(gj, seg, A.c.vals, r).d;
+          if (in_span(gi, r)) drho_i = tab_vd<T, AN>(gi, seg, A.c.vals, r).d;
           fs = dphi + gradF[i] * drho_j + gradF[j] * drho_i;
         }
         fs = fs * (T(1) / r);
@@ -229,7 +214,7 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
   return out;
 }
 
-template <class T, int LPA, bool EAM>
+template <class T, int LPA, bool EAM, bool AN>
 __global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
   using T4 = typename Vec4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -250,7 +235,7 @@ __global__ void __launch_bounds__(256) residual_kernel(ResArgs<T> A) {
   for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) seg[k] = A.seg_a[k];
   stage_geometry(cd, A.c, wpos, shift, typ);
   __syncthreads();
-  const double o = config_pass<T, LPA, EAM, true>(A, c, cd, tabs, seg, wpos, shift, typ, rho, gradF, red);
+  const double o = config_pass<T, LPA, EAM, true, AN>(A, c, cd, tabs, seg, wpos, shift, typ, rho, gradF, red);
   if (threadIdx.x == 0) A.obj_part[c] = o;
 }
 
@@ -1127,6 +1112,7 @@ template <class T> Common make_common(fs_gpu *h) {
   c.type = h->d_type;
   c.ref_force = h->d_ref_force;
   c.nb_start = h->d_nb_start;
+  c.vals = h->d_vals;
   c.nb_pack = h->d_nb_pack;
   c.desc = h->d_desc;
   c.cmap = h->d_cmap;
@@ -1168,7 +1154,9 @@ template <class T, int LPA, bool EAM> int launch_residual_t(fs_gpu *h, double w_
   a.obj_part = h->d_obj_part;
   const size_t sm = residual_smem<T>(a.c.n_tables, h->n_segs, h->max_natoms, max_images(h));
   if (sm > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "residual: configuration too large for shared memory");
-  auto k = residual_kernel<T, LPA, EAM>;
+  bool analytic = false;
+  for (const HostTable &t : h->tables) analytic = analytic || t.kind == FS_TABLE_ANALYTIC;
+  auto k = analytic ? residual_kernel<T, LPA, EAM, true> : residual_kernel<T, LPA, EAM, false>;
   FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
   k<<<h->n_cfg, 256, sm, h->stream>>>(a);
   FS_CUDA(cudaGetLastError());
@@ -1638,6 +1626,13 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s) {
     extern int eval_jacobian_other(fs_gpu * h, double w_e, double w_s);
     return eval_jacobian_other(h, w_e, w_s);
   }
+  for (const HostTable &t : h->tables)
+    if (t.kind == FS_TABLE_ANALYTIC) {
+      // analytic tables: the reference's central differences on the device
+      // (fd_jacobian.hpp:37-49); FP64 contexts only
+      extern int eval_jacobian_fd(fs_gpu * h, double w_e, double w_s);
+      return eval_jacobian_fd(h, w_e, w_s);
+    }
   return h->precision == FS_PREC_FP64 ? launch_jacobian_t<double>(h, w_e, w_s)
                                       : launch_jacobian_t<float>(h, w_e, w_s);
 }

@@ -35,6 +35,7 @@ struct Common {
   const uint32_t *nb_pack;
   const TableDesc *desc;
   const int32_t *cmap;
+  const double *vals; // table values / analytic parameters (FP64, table order)
   int n_tables, n_segs, n_cmap, ntypes;
   int family; // FS_FAMILY_EAM or FS_FAMILY_PAIR
   int cfg_count;

@@ -230,6 +230,11 @@ int upload_tables(fs_gpu *h) {
       d.x0 = ht.rmin + 0.0 * d.h;
       d.xmax = ht.rmin + static_cast<double>(ht.n - 1) * d.h;
       d.inv_h = 1.0 / d.h;
+    } else if (ht.kind == FS_TABLE_ANALYTIC) {
+      // closed form on its gate span [rmin, rmax] (the reference's range gate)
+      d.x0 = ht.rmin;
+      d.xmax = ht.rmax;
+      d.h = d.inv_h = 1.0;
     }
     cmap.insert(cmap.end(), ht.cols.begin(), ht.cols.end());
     vals.insert(vals.end(), ht.v.begin(), ht.v.end());
