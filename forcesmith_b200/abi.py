@@ -57,6 +57,12 @@ class fs_gpu_opts(C.Structure):
                 ("lanes_per_atom", C.c_int32), ("reserved", C.c_int32)]
 
 
+class fs_tune_report(C.Structure):
+    _fields_ = [("lanes_per_atom", C.c_int32), ("k2_warps", C.c_int32), ("pop_waves", C.c_int32),
+                ("reserved", C.c_int32), ("residual_ms", C.c_double * 4), ("jacobian_ms", C.c_double * 5),
+                ("population_ms", C.c_double * 3)]
+
+
 class fs_surrogate_opts(C.Structure):
     _fields_ = [("screen", C.c_int32), ("warm_generations", C.c_int32), ("batch", C.c_int32),
                 ("steps_per_generation", C.c_int32), ("lr", C.c_double), ("gate", C.c_double),

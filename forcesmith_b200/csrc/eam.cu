@@ -1133,6 +1133,7 @@ int max_images(const fs_gpu *h) {
 
 int choose_lpa(const fs_gpu *h) {
   if (h->lanes_per_atom) return h->lanes_per_atom;
+  if (h->tuned_lpa) return h->tuned_lpa;
   const double avg = h->n_atoms ? static_cast<double>(h->n_pairs) / h->n_atoms : 0.0;
   if (avg > 24) return 16;
   if (avg > 10) return 8;
@@ -1300,6 +1301,17 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   const size_t cap = 227 * 1024;
   int warps = 0;
   size_t sm2 = 0;
+  if (h->tuned_k2_warps > 0) {
+    const int wp = h->tuned_k2_warps;
+    if (eam && k2_smem(wp) + stage_b <= cap) {
+      warps = wp;
+      sm2 = k2_smem(wp) + stage_b;
+      a.stage = 1;
+    } else if (k2_smem(wp) <= cap) {
+      warps = wp;
+      sm2 = k2_smem(wp);
+    }
+  }
   if (eam)
     for (int wp = 8; wp >= 4 && !warps; --wp)
       if (k2_smem(wp) + stage_b <= cap) {
@@ -1462,8 +1474,9 @@ int launch_population_t(fs_gpu *h, double w_e, double w_s, const double *d_xs, i
       pa.pop_seg = pop_seg;
       pa.NP = NP;
       pa.n_tiles = (NP + kPopLanes - 1) / kPopLanes;
-      // about four waves of one CTA per SM
-      pa.n_chunks = std::max(1, std::min(h->n_cfg, (4 * 148 + pa.n_tiles - 1) / pa.n_tiles));
+      // about four waves of one CTA per SM (or the tuned number)
+      const int waves = h->tuned_pop_waves > 0 ? h->tuned_pop_waves : 4;
+      pa.n_chunks = std::max(1, std::min(h->n_cfg, (waves * 148 + pa.n_tiles - 1) / pa.n_tiles));
       pa.nseg_pd = nseg_pd;
       pa.max_atoms = h->max_natoms;
       pa.max_img = max_images(h);

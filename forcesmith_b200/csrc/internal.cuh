@@ -193,6 +193,11 @@ struct fs_gpu {
   double *d_pop_vals = nullptr;
   double *d_pop_obj = nullptr;
 
+  // schedules chosen by fs_gpu_autotune (0: built-in choice)
+  int tuned_lpa = 0;       // residual lanes per atom
+  int tuned_k2_warps = 0;  // warps per CTA of the Jacobian force-row kernel
+  int tuned_pop_waves = 0; // CTA waves of the FP32 population kernel
+
   // device differential evolution (population.cu) and its surrogate (mlp.cu)
   fsg::DeState *de = nullptr;
   fsg::Mlp *mlp = nullptr;

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .abi import (fs_de_opts, fs_surrogate_opts, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
+from .abi import (fs_de_opts, fs_surrogate_opts, fs_tune_report, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
                   fs_model, load_library)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
         L.fs_gpu_de_run.argtypes = [vp, i32, i32, pd, pd, pd]
         L.fs_gpu_de_population.argtypes = [vp, pd, pd]
         L.fs_gpu_eval_population_noalloc.argtypes = [vp, dbl, dbl, vp, i32, vp]
+        L.fs_gpu_autotune.argtypes = [vp, dbl, dbl, C.POINTER(fs_tune_report)]
         pf = C.POINTER(C.c_float)
         L.fs_gpu_surrogate_init.argtypes = [vp, C.POINTER(fs_surrogate_opts)]
         L.fs_gpu_de_run_screened.argtypes = [vp, i32, pd, pd, pd, pd, pi]
@@ -159,6 +160,15 @@ class GpuSession(Session):
         self._check(self._lib.fs_gpu_eval_population(self._h, w_e, w_s, _dp(xs), xs.shape[0],
                                                      _dp(obj)), "eval_population")
         return obj
+
+    def autotune(self, w_e=1.0, w_s=0.0):
+        """fs_gpu_autotune: time the kernels' launch shapes on this context's
+        data and keep the fastest; returns the choices and timings."""
+        r = fs_tune_report()
+        self._check(self._lib.fs_gpu_autotune(self._h, w_e, w_s, C.byref(r)), "autotune")
+        return dict(lanes_per_atom=r.lanes_per_atom, k2_warps=r.k2_warps, pop_waves=r.pop_waves,
+                    residual_ms=list(r.residual_ms), jacobian_ms=list(r.jacobian_ms),
+                    population_ms=list(r.population_ms))
 
     def eval_population_noalloc(self, xs_dev_ptr, NP, obj_dev_ptr, w_e=1.0, w_s=0.0):
         """fs_gpu_eval_population_noalloc: objectives of NP trial vectors

@@ -238,6 +238,25 @@ int fs_gpu_eval_population(fs_gpu *h, double w_e, double w_s, const double *xs,
                            int32_t NP, double *obj);
 
 /*
+ * Schedule autotuner (no reference counterpart: the CPU path has no launch
+ * shapes).  Times, on this context's configurations and model, the residual
+ * kernel's lanes per atom (4, 8, 16, 32; skipped when fs_gpu_opts fixed it),
+ * the Jacobian force-row kernel's warps per CTA (8 … 4) and, in FP32, the
+ * population kernel's CTA waves (2, 4, 8), and keeps the fastest for every
+ * later call of this context.  Results differ between schedules only in the
+ * summation order of their sums.  Milliseconds per candidate are reported
+ * (0 where a candidate was not timed).
+ */
+typedef struct fs_tune_report {
+    int32_t lanes_per_atom, k2_warps, pop_waves, reserved;
+    double residual_ms[4];    /* lanes 4, 8, 16, 32 */
+    double jacobian_ms[5];    /* warps 8, 7, 6, 5, 4 */
+    double population_ms[3];  /* waves 2, 4, 8 */
+} fs_tune_report;
+
+int fs_gpu_autotune(fs_gpu *h, double w_e, double w_s, fs_tune_report *report);
+
+/*
  * fs_gpu_eval_population_noalloc — the batched objective of
  * fs_gpu_eval_population for callers that cannot allocate device memory.
  * No counterpart in the reference (its DE evaluates trials one at a time on

@@ -319,3 +319,30 @@ def test_adp_residual_and_fd_jacobian_fp64():
     res = g.jacobian(1.0, 0.1)
     Jf = o.jacobian_fd(1.0, 0.1)
     assert np.max(np.abs(res["J"] - Jf)) <= 1e-6 * (1 + np.abs(Jf).max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_autotune_keeps_results(ternary_small, precision):
+    """fs_gpu_autotune picks schedules from its candidate sets; results after
+    tuning equal the untuned ones up to summation order (FP64 1e-12
+    relative; FP32 at its stated bars)."""
+    ds, _, start = ternary_small
+    g, _ = _pair(ds, start, precision)
+    before = g.eval(1.0, 0.1)
+    jb = g.jacobian(1.0, 0.1, want_J=False)
+    x0 = g.gather_params()
+    xs = np.stack([x0 * synth.uniform(x0.size, 0.98, 1.02, 300 + k) for k in range(5)])
+    pb = g.eval_population(xs, 1.0, 0.1)
+    rep = g.autotune(1.0, 0.1)
+    assert rep["lanes_per_atom"] in (4, 8, 16, 32)
+    assert rep["k2_warps"] in (4, 5, 6, 7, 8)
+    assert rep["pop_waves"] in ((2, 4, 8) if precision == "fp32" else (0,))
+    after = g.eval(1.0, 0.1)
+    ja = g.jacobian(1.0, 0.1, want_J=False)
+    pa = g.eval_population(xs, 1.0, 0.1)
+    tol = 1e-12 if precision == "fp64" else 1e-4
+    _close(after["F"], before["F"], tol if precision == "fp64" else 1e-5, "F")
+    assert abs(after["obj"] - before["obj"]) <= tol * abs(before["obj"])
+    np.testing.assert_allclose(ja["JtJ"], jb["JtJ"], rtol=tol if precision == "fp64" else 1e-3,
+                               atol=(1e-12 if precision == "fp64" else 1e-3) * np.abs(jb["JtJ"]).max())
+    np.testing.assert_allclose(pa, pb, rtol=tol)
