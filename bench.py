@@ -23,6 +23,8 @@ Two more legs ride in the same JSON line (one GPU, rank 0): `de`, the
 batched DE population objective on 200 configurations of 32-512 atoms with
 NP = 15 D, and `surrogate`, the wall time surrogate-screened DE needs to reach
 plain device DE's final objective (within 1 %) against plain DE's own time.
+With the CPU leg on, `sw` (Stillinger-Weber Si, 1000 configurations) and
+`al99_fit` (the Al fcc LM fit, device-driven against oracle-driven) are added.
 Multi-GPU (torchrun): every rank evaluates its own 500-configuration shard
 (weak scaling) and the normal equations are summed over ranks with one
 NCCL all-reduce per step (the exchange an LM step needs).
@@ -257,6 +259,95 @@ def de_legs(local, generations):
     return de, sur
 
 
+def sw_leg(local, steps=20):
+    """Stillinger-Weber Si: 1000 diamond configurations of 64, 216 or 512
+    atoms (sigma = 0.15 A, volumetric strain U[0.95, 1.05]), 7 perturbed SW
+    parameters; FP32 residual + analytic parameter Jacobian + normal
+    equations per second, against the oracle (16 threads, FP64) running the
+    reference's central differences for SW (2 D + 1 residual evaluations),
+    timed on one residual and extrapolated."""
+    import torch
+    from forcesmith_b200 import gpu as G, synth
+    from oracle.api import Oracle, set_threads
+    ds = synth.diamond(1000)
+    true, start = synth.sw_model(), synth.sw_start_model()
+    ds = label_on_gpu(ds, true, local)
+    g = G.GpuSession(local, "fp32")
+    g.upload(ds)
+    g.set_model(start)
+    D = g.D
+    for _ in range(3):
+        g.jacobian_async(W_E, W_S)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(g.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(steps):
+        g.jacobian_async(W_E, W_S)
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    P = g.num_pairs()
+    g.close()
+    threads = set_threads(os.cpu_count() or 1)
+    o = Oracle()
+    o.upload(ds)
+    o.set_model(start)
+    o.eval(W_E, W_S, want=("obj",))
+    t0 = time.perf_counter()
+    o.eval(W_E, W_S, want=("F",))
+    t_res = time.perf_counter() - t0
+    cpu = 1.0 / (t_res * (2 * D + 1))
+    return {"workload": f"Stillinger-Weber Si, {ds.n_cfg} configs x 64/216/512 atoms ({ds.n_atoms} atoms, "
+                        f"{P} pairs), D={D}, w_e=1, w_s=0.1, FP32 residual + analytic Jacobian + JtJ",
+            "value": 1000.0 / ms, "unit": "evals/s", "ms_per_eval": ms,
+            "cpu_baseline": {"value": cpu, "unit": "evals/s", "cores": threads, "kind": "port",
+                             "sample": f"one FP64 residual ({t_res*1e3:.0f} ms) x (2 D + 1) central-difference "
+                                       "evaluations"}}
+
+
+def al99_leg(local):
+    """Al fcc LM fit (20 x 108 atoms, three 15-knot splines, D = 45,
+    max_iter 200, w_e = 1, w_s = 0; labels from the Al99 setfl fixture): wall
+    time of the device-driven LM against the same solver driven by the oracle
+    (16 threads, FP64, analytic Jacobian)."""
+    import numpy as np
+    from forcesmith_b200 import gpu as G, solvers
+    from forcesmith_b200.abi import Dataset, Model, Table, FS_FAMILY_EAM
+    from oracle import api as O
+    z = np.load(os.path.join(ROOT, "tests", "golden", "al99_c1.npz"))
+    ds = Dataset(z["natoms"], z["box9"], z["pos"], z["type"], z["forces"], z["energy"], z["stress9"])
+    start = Model(FS_FAMILY_EAM, 1, [Table.spline(float(lo), float(hi), z["start_knots"][k])
+                                     for k, (lo, hi) in enumerate(z["start_domains"])])
+
+    class OracleSteps(O.Oracle):
+        def jacobian_async(self, w_e=1.0, w_s=0.0):
+            F = self.eval(w_e, w_s, want=("F",))["F"]
+            self._ne = O.normal_equations(self.jacobian_analytic(w_e, w_s), F) + (float(F @ F),)
+
+        def normal_equations(self):
+            return self._ne
+
+        def lm_step(self, lam, mode=0):
+            return O.lm_step(self._ne[0], self._ne[1], lam, mode)
+
+    out = {"workload": "Al fcc, 20 configs x 108 atoms, 3 x 15-knot splines (D=45), LM max_iter 200, "
+                       "labels: Al99 setfl"}
+    for name, make in (("gpu_fp64", lambda: G.GpuSession(local, "fp64")), ("cpu_oracle", O.Oracle)):
+        sess = OracleSteps() if name == "cpu_oracle" else make()
+        sess.upload(ds)
+        sess.set_model(start)
+        x0 = sess.gather_params()
+        t0 = time.perf_counter()
+        _, x, info = solvers.LMSolver(max_iter=200).minimize(sess, x0)
+        out[name] = {"wall_s": time.perf_counter() - t0, "iterations": info["iterations"],
+                     "final_objective": info["obj"][-1], "start_objective": info["obj"][0]}
+    out["speedup"] = out["cpu_oracle"]["wall_s"] / out["gpu_fp64"]["wall_s"]
+    return out
+
+
 def cpu_baseline(ds, start, columns):
     """Reference method on the host: FD Jacobian = 1 + 2·D residual evaluations."""
     from oracle.api import Oracle, set_threads
@@ -456,6 +547,9 @@ def run_ours(args):
     line["roofline"]["traffic"] = traffic_from_profiles(dom)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ds, start, args.cpu_columns)
+    if rank == 0 and world == 1 and not args.small and not args.no_cpu_baseline:
+        line["sw"] = sw_leg(local)
+        line["al99_fit"] = al99_leg(local)
     if rank == 0 and world == 1 and not args.small and args.de_generations >= 0:
         de, sur = de_legs(local, args.de_generations)
         line["de"] = de
