@@ -1,0 +1,319 @@
+"""Forcesmith's data formats on either side of the device path.
+
+  read_configs / write_configs  the configuration JSON of
+      src/io/config_reader.cpp:58-200 — a top-level array of
+      {name?, X, Y, Z, E, W?, S?, atoms: [{element, position, force?}]};
+      the box's lattice vectors are X, Y, Z (its columns), S is the stress
+      in the order xx, yy, zz, xy, yz, xz (config_reader.cpp:78-91), and the
+      species slots are the elements present sorted by atomic number (the
+      species registry, species.hpp).
+  read_model / write_model  the force-model JSON of
+      src/io/force_model_reader.cpp:134-440 for the families this path
+      evaluates: a bare pair file (no "model" key; the pair count fixes
+      ntypes), and "pair", "eam", "adp" (table sections "pair", "density",
+      "embedding", "dipole", "quadrupole"), "stiweb" ("potentials": SWParams
+      objects, "lambda").  A table section is {"format", "potentials": [...]}
+      with tabulated {rmin, rmax, knots, fixed?} or analytic {type, rmin,
+      rmax, <parameter>: number | {value, min?, max?, fixed?}} entries
+      (src/io/potential_reader.cpp:60-200).  Global parameters ("globals")
+      are not supported here.
+  read_setfl  a single-element LAMMPS setfl file as three makima tables on
+      the file's own grids (φ = r·φ / r from the second r point on).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+
+from .abi import (FS_FAMILY_ADP, FS_FAMILY_EAM, FS_FAMILY_PAIR, FS_FAMILY_SW, FS_TABLE_ANALYTIC,
+                  FS_TABLE_LAMBDA, FS_TABLE_SPLINE, FS_TABLE_SW, FORMS, Dataset, Model, Table)
+
+SYMBOLS = (
+    "H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
+    "Rb Sr Y Zr Nb Mo Tc Ru Rh Pd Ag Cd In Sn Sb Te I Xe Cs Ba La Ce Pr Nd Pm Sm Eu Gd Tb Dy Ho Er Tm "
+    "Yb Lu Hf Ta W Re Os Ir Pt Au Hg Tl Pb Bi Po At Rn Fr Ra Ac Th Pa U Np Pu Am Cm Bk Cf Es Fm Md No "
+    "Lr Rf Db Sg Bh Hs Mt Ds Rg Cn Nh Fl Mc Lv Ts Og").split()
+Z_OF = {s: z + 1 for z, s in enumerate(SYMBOLS)}
+
+# analytic form names (and aliases) and parameter names, as the reference spells them
+FORM_SPEC = {
+    "lj": ("lj", ("epsilon", "sigma")), "pair_lj": ("lj", ("epsilon", "sigma")),
+    "morse": ("morse", ("De", "a", "re")),
+    "exp_decay": ("exp_decay", ("A", "B")), "exp": ("exp_decay", ("A", "B")),
+    "sqrt": ("sqrt", ("A", "B")),
+    "power_decay": ("power_decay", ("A", "n")), "power": ("power_decay", ("A", "n")),
+    "mexp_decay": ("mexp_decay", ("A", "B", "r0")), "mexp": ("mexp_decay", ("A", "B", "r0")),
+    "harmonic": ("harmonic", ("k", "r0")),
+    "exp_plus": ("exp_plus", ("A", "B", "C")), "expplus": ("exp_plus", ("A", "B", "C")),
+    "parabola": ("parabola", ("A", "B", "C")),
+    "const": ("const", ("C",)),
+    "buckingham": ("buckingham", ("A", "rho", "C")), "buck": ("buckingham", ("A", "rho", "C")),
+    "born": ("born", ("A", "B", "C", "D", "E")),
+}
+FORM_NAME = {FORMS[canon][0]: canon for canon, _ in FORM_SPEC.values()}
+PARAM_NAMES = {FORMS[canon][0]: names for canon, names in FORM_SPEC.values()}
+SW_FIELDS = ("A", "B", "p", "q", "delta", "a1", "gamma", "a2")
+TABLE_KEYS = {FS_FAMILY_PAIR: ("pair",), FS_FAMILY_EAM: ("pair", "density", "embedding"),
+              FS_FAMILY_ADP: ("pair", "density", "embedding", "dipole", "quadrupole")}
+PER_PAIR = {"pair": True, "density": False, "embedding": False, "dipole": True, "quadrupole": True}
+FAMILY_OF = {"pair": FS_FAMILY_PAIR, "eam": FS_FAMILY_EAM, "adp": FS_FAMILY_ADP, "stiweb": FS_FAMILY_SW}
+NAME_OF = {v: k for k, v in FAMILY_OF.items()}
+
+
+class FormatError(ValueError):
+    pass
+
+
+def _text(src):
+    if isinstance(src, (str, os.PathLike)) and os.path.exists(src):
+        with open(src) as f:
+            return f.read()
+    return src
+
+
+# ---------------------------------------------------------------------------
+# configurations
+
+def species_slots(symbols):
+    """The species registry: the distinct elements sorted by atomic number."""
+    unknown = [s for s in symbols if s not in Z_OF]
+    if unknown:
+        raise FormatError(f"unknown element symbol(s): {unknown}")
+    return sorted(set(symbols), key=lambda s: Z_OF[s])
+
+
+def read_configs(src):
+    """Configuration JSON → (Dataset, species symbols by slot, names, weights)."""
+    j = json.loads(_text(src))
+    if not isinstance(j, list):
+        raise FormatError("top-level JSON must be an array of configurations")
+    syms = [a["element"] for c in j if isinstance(c, dict) for a in c.get("atoms", [])
+            if isinstance(a, dict) and isinstance(a.get("element"), str)]
+    slots = species_slots(syms)
+    slot_of = {s: k for k, s in enumerate(slots)}
+    natoms, box9, pos, typ, frc, ene, st9, names, weights = [], [], [], [], [], [], [], [], []
+    for ci, c in enumerate(j):
+        ctx = f"config[{ci}]"
+        if not isinstance(c, dict):
+            raise FormatError(f"{ctx}: each configuration must be a JSON object")
+        for k in ("X", "Y", "Z", "E", "atoms"):
+            if k not in c:
+                raise FormatError(f"{ctx}: missing key '{k}'")
+        cols = [np.asarray(c[k], np.float64) for k in ("X", "Y", "Z")]
+        if any(v.shape != (3,) for v in cols):
+            raise FormatError(f"{ctx}: X, Y, Z must be arrays of 3 doubles")
+        box9.append(np.stack(cols, axis=1).ravel())  # lattice vectors as columns, row-major
+        ene.append(float(c["E"]))
+        weights.append(float(c.get("W", 1.0)))
+        names.append(c.get("name", ""))
+        s = np.zeros((3, 3))
+        if "S" in c:
+            v = np.asarray(c["S"], np.float64)
+            if v.shape != (6,):
+                raise FormatError(f"{ctx} 'S': must be an array of 6 doubles")
+            s[0, 0], s[1, 1], s[2, 2] = v[0], v[1], v[2]
+            s[0, 1] = s[1, 0] = v[3]
+            s[1, 2] = s[2, 1] = v[4]
+            s[0, 2] = s[2, 0] = v[5]
+        st9.append(s.ravel())
+        atoms = c["atoms"]
+        if not isinstance(atoms, list):
+            raise FormatError(f"{ctx}: 'atoms' must be an array")
+        natoms.append(len(atoms))
+        for ai, a in enumerate(atoms):
+            if "element" not in a or "position" not in a:
+                raise FormatError(f"{ctx} atom[{ai}]: needs 'element' and 'position'")
+            typ.append(slot_of[a["element"]])
+            pos.append(np.asarray(a["position"], np.float64))
+            frc.append(np.asarray(a.get("force", (0.0, 0.0, 0.0)), np.float64))
+    ds = Dataset(np.asarray(natoms, np.int32), np.asarray(box9).reshape(-1, 9),
+                 np.asarray(pos).reshape(-1, 3), np.asarray(typ, np.int32), np.asarray(frc).reshape(-1, 3),
+                 np.asarray(ene), np.asarray(st9).reshape(-1, 9))
+    return ds, slots, names, np.asarray(weights)
+
+
+def write_configs(ds, slots, names=None, weights=None):
+    """Dataset → configuration JSON text (the inverse of read_configs)."""
+    out, a0 = [], 0
+    for c in range(ds.n_cfg):
+        b = np.asarray(ds.box9[c]).reshape(3, 3)
+        s = np.asarray(ds.ref_stress9[c]).reshape(3, 3)
+        n = int(ds.natoms[c])
+        atoms = [{"element": slots[int(ds.type[a0 + k])], "position": [float(v) for v in ds.pos[a0 + k]],
+                  "force": [float(v) for v in ds.ref_force[a0 + k]]} for k in range(n)]
+        cfg = {"X": b[:, 0].tolist(), "Y": b[:, 1].tolist(), "Z": b[:, 2].tolist(),
+               "E": float(ds.ref_energy[c]),
+               "S": [s[0, 0], s[1, 1], s[2, 2], s[0, 1], s[1, 2], s[0, 2]], "atoms": atoms}
+        if names is not None:
+            cfg["name"] = names[c]
+        if weights is not None:
+            cfg["W"] = float(weights[c])
+        out.append(cfg)
+        a0 += n
+    return json.dumps(out, indent=1)
+
+
+# ---------------------------------------------------------------------------
+# models
+
+def _param(v):
+    if isinstance(v, dict):
+        if "value" not in v:
+            raise FormatError("parameter object missing 'value'")
+        lo, hi = float(v.get("min", -math.inf)), float(v.get("max", math.inf))
+        if lo > hi:
+            raise FormatError("parameter has min > max")
+        return float(v["value"]), lo, hi, bool(v.get("fixed", False))
+    return float(v), -math.inf, math.inf, False
+
+
+def _potential(p):
+    if not isinstance(p, dict):
+        raise FormatError("potential spec must be a JSON object")
+    if "type" in p:
+        if p["type"] not in FORM_SPEC:
+            raise FormatError(f"unknown analytic function: {p['type']}")
+        canon, names = FORM_SPEC[p["type"]]
+        vals = []
+        for nm in names:
+            if nm not in p:
+                raise FormatError(f"missing parameter '{nm}' for type {p['type']}")
+            vals.append(_param(p[nm]))
+        v = np.array([x[0] for x in vals])
+        return Table.analytic(canon, v, float(p["rmin"]), float(p["rmax"]),
+                              fixed=np.array([x[3] for x in vals], np.uint8),
+                              lower=np.array([x[1] for x in vals]), upper=np.array([x[2] for x in vals]))
+    if "knots" in p:
+        y = np.asarray(p["knots"], np.float64)
+        if y.size < 2:
+            raise FormatError("tabulated potential needs at least 2 knots")
+        rmin, rmax = float(p["rmin"]), float(p["rmax"])
+        if not rmax > rmin:
+            raise FormatError(f"tabulated potential requires rmax > rmin (got rmin={rmin}, rmax={rmax})")
+        fixed = np.ones(y.size, np.uint8) if p.get("fixed", False) else None
+        return Table.spline(rmin, rmax, y, fixed=fixed)
+    raise FormatError("potential spec has neither 'type' (analytic) nor 'knots' (tabulated)")
+
+
+def _section(sub, want, label):
+    if "format" not in sub:
+        raise FormatError(f"{label}: missing 'format' key")
+    if sub["format"] not in ("analytic", "tabulated"):
+        raise FormatError(f"{label}: unsupported potential format '{sub['format']}'")
+    pots = sub.get("potentials")
+    if not isinstance(pots, list):
+        raise FormatError(f"{label}: missing or invalid 'potentials' array")
+    if len(pots) != want:
+        raise FormatError(f"{label}: expected {want} potentials, got {len(pots)}")
+    return [_potential(p) for p in pots]
+
+
+def read_model(src):
+    """Force-model JSON → Model (families pair, eam, adp, stiweb)."""
+    j = json.loads(_text(src))
+    if "globals" in j:
+        raise FormatError("global parameters are not supported by this reader")
+    if "model" not in j:
+        count = len(j.get("potentials", [])) if isinstance(j.get("potentials"), list) else 0
+        nt = 1
+        while nt * (nt + 1) // 2 < count:
+            nt += 1
+        if nt * (nt + 1) // 2 != count:
+            raise FormatError(f"bare pair file: {count} potentials is not a valid pair count for any ntypes")
+        return Model(FS_FAMILY_PAIR, nt, _section(j, count, "pair"))
+    name = j["model"]
+    if name not in FAMILY_OF:
+        raise FormatError(f"unsupported model '{name}'")
+    fam, nt = FAMILY_OF[name], int(j.get("ntypes", 1))
+    npair = nt * (nt + 1) // 2
+    if fam == FS_FAMILY_SW:
+        pots = j.get("potentials")
+        if not isinstance(pots, list) or len(pots) != npair:
+            raise FormatError(f"stiweb: expected {npair} entries for ntypes={nt}")
+        tabs = []
+        for p in pots:
+            vals = [_param(p[k]) for k in SW_FIELDS]
+            tabs.append(Table(FS_TABLE_SW, np.array([v[0] for v in vals]), 0.0, 0.0, 0,
+                              np.array([v[3] for v in vals], np.uint8), np.array([v[1] for v in vals]),
+                              np.array([v[2] for v in vals])))
+        lam = j.get("lambda")
+        if not isinstance(lam, list) or len(lam) != nt * npair:
+            raise FormatError(f"stiweb: expected {nt * npair} lambda entries for ntypes={nt}")
+        vals = [_param(v) for v in lam]
+        tabs.append(Table(FS_TABLE_LAMBDA, np.array([v[0] for v in vals]), 0.0, 0.0, 0,
+                          np.array([v[3] for v in vals], np.uint8), np.array([v[1] for v in vals]),
+                          np.array([v[2] for v in vals])))
+        return Model(fam, nt, tabs)
+    tabs = []
+    for key in TABLE_KEYS[fam]:
+        sub = j if (name == "pair" and key == "pair" and "pair" not in j) else j.get(key)
+        if sub is None:
+            raise FormatError(f"{name}: missing section '{key}'")
+        tabs += _section(sub, npair if PER_PAIR[key] else nt, f"{name}.{key}")
+    return Model(fam, nt, tabs)
+
+
+def _pot_json(t):
+    if t.kind == FS_TABLE_SPLINE:
+        d = {"rmin": t.rmin, "rmax": t.rmax, "knots": [float(v) for v in t.values]}
+        if t.fixed is not None and np.all(t.fixed):
+            d["fixed"] = True
+        return d
+    name = FORM_NAME[t.form]
+    d = {"type": name, "rmin": t.rmin, "rmax": t.rmax}
+    for k, nm in enumerate(PARAM_NAMES[t.form]):
+        lo = -math.inf if t.lower is None else float(t.lower[k])
+        hi = math.inf if t.upper is None else float(t.upper[k])
+        fx = False if t.fixed is None else bool(t.fixed[k])
+        if math.isinf(lo) and math.isinf(hi) and not fx:
+            d[nm] = float(t.values[k])
+        else:
+            d[nm] = {"value": float(t.values[k]), "fixed": fx,
+                     **({} if math.isinf(lo) else {"min": lo}), **({} if math.isinf(hi) else {"max": hi})}
+    return d
+
+
+def write_model(model):
+    """Model → force-model JSON text (families pair, eam, adp)."""
+    nt, fam = model.ntypes, model.family
+    if fam not in TABLE_KEYS:
+        raise FormatError("write_model: pair, eam and adp families")
+    npair = nt * (nt + 1) // 2
+    out = {"model": NAME_OF[fam], "ntypes": nt}
+    k = 0
+    for key in TABLE_KEYS[fam]:
+        n = npair if PER_PAIR[key] else nt
+        tabs = model.tables[k:k + n]
+        k += n
+        fmt = "analytic" if all(t.kind == FS_TABLE_ANALYTIC for t in tabs) else "tabulated"
+        out[key] = {"format": fmt, "potentials": [_pot_json(t) for t in tabs]}
+    return json.dumps(out, indent=1)
+
+
+# ---------------------------------------------------------------------------
+# LAMMPS setfl
+
+def read_setfl(path):
+    """Single-element setfl → (Model, header) with makima tables on the file's
+    grids: φ = (r·φ)/r on r_k = k·dr (k = 1…Nr−1), ρ on r_k (k = 0…Nr−1),
+    F on ρ_k = k·dρ (k = 0…Nρ−1).  Layout: three comment lines, "1 El",
+    "Nrho drho Nr dr rc", "Z mass a0 lattice", then F, ρ, r·φ."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    if int(lines[3].split()[0]) != 1:
+        raise FormatError("read_setfl: single-element files only")
+    nrho, drho, nr, dr, rc = lines[4].split()
+    nrho, nr, drho, dr, rc = int(nrho), int(nr), float(drho), float(dr), float(rc)
+    vals = np.array([float(v) for ln in lines[6:] for v in ln.split()])
+    if vals.size < nrho + 2 * nr:
+        raise FormatError("read_setfl: file ends early")
+    F, rho, rphi = vals[:nrho], vals[nrho:nrho + nr], vals[nrho + nr:nrho + 2 * nr]
+    r = dr * np.arange(1, nr)
+    model = Model(FS_FAMILY_EAM, 1, [Table.spline(dr, dr * (nr - 1), rphi[1:] / r),
+                                     Table.spline(0.0, dr * (nr - 1), rho),
+                                     Table.spline(0.0, drho * (nrho - 1), F)])
+    header = dict(element=lines[3].split()[1], nrho=nrho, drho=drho, nr=nr, dr=dr, rc=rc)
+    return model, header

@@ -27,34 +27,16 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from forcesmith_b200 import synth  # noqa: E402
-from forcesmith_b200.abi import FS_FAMILY_EAM, Model, Table  # noqa: E402
+from forcesmith_b200.io import read_setfl  # noqa: E402
 from oracle import api as O  # noqa: E402
 
 SETFL = os.environ.get("AL99_SETFL", "/root/reference/data/Al99.eam.alloy")
 
 
-def read_setfl(path):
-    with open(path) as f:
-        lines = f.read().split("\n")
-    nrho, drho, nr, dr, rc = lines[4].split()
-    nrho, nr, drho, dr, rc = int(nrho), int(nr), float(drho), float(dr), float(rc)
-    vals = np.array([float(v) for ln in lines[6:] for v in ln.split()])
-    F = vals[:nrho]
-    rho = vals[nrho:nrho + nr]
-    rphi = vals[nrho + nr:nrho + 2 * nr]
-    return dict(nrho=nrho, drho=drho, nr=nr, dr=dr, rc=rc, F=F, rho=rho, rphi=rphi)
-
-
 def main():
-    t = read_setfl(SETFL)
+    label, t = read_setfl(SETFL)
     nr, dr, nrho, drho = t["nr"], t["dr"], t["nrho"], t["drho"]
-    r = dr * np.arange(1, nr)
-    phi = t["rphi"][1:] / r
-    label = Model(FS_FAMILY_EAM, 1, [
-        Table.spline(dr, dr * (nr - 1), phi),
-        Table.spline(0.0, dr * (nr - 1), t["rho"]),
-        Table.spline(0.0, drho * (nrho - 1), t["F"]),
-    ])
+    phi, rho, F = (tb.values for tb in label.tables)
     ds = synth.fcc(20, 3, 4.05, 0.10, 0.97, 1.03, seed=20261203)
     o = O.Oracle()
     o.upload(ds.with_labels(np.zeros((ds.n_atoms, 3)), np.zeros(ds.n_cfg), np.zeros((ds.n_cfg, 9))))
@@ -69,7 +51,7 @@ def main():
     e_ideal = float(oi.eval(1.0, 0.0, want=("energy",))["energy"][0]) / ideal.n_atoms
     # start model: 15 knots per table, read off the label splines, perturbed
     doms = [(dr, t["rc"]), (0.0, t["rc"]), (0.0, drho * (nrho - 1))]
-    grids = [(dr * np.arange(1, nr), phi), (dr * np.arange(nr), t["rho"]), (drho * np.arange(nrho), t["F"])]
+    grids = [(dr * np.arange(1, nr), phi), (dr * np.arange(nr), rho), (drho * np.arange(nrho), F)]
     rng = synth.uniform(45, 0.95, 1.05, 7)
     knots = []
     for k, ((lo, hi), (x, y)) in enumerate(zip(doms, grids)):
