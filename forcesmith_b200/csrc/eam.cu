@@ -758,20 +758,24 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
 // is staged in shared memory when it fits, so the inner loops never wait on
 // global memory.
 // ---------------------------------------------------------------------------
-template <class T> struct PairRec {
-  // per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window)
-  int e[4];        // extended segment (−1: no contribution)
-  int cbase[4];    // column-map index of the window's first knot
-  int nv[4];       // valid knots in the window
-  T t[4], w[4], ih[4];
-  T u[3], v[6];
-  T dgi, cFj;      // ρ'_{ti}(r), F''_j
-  int j;
-};
-
 template <class T> struct V2T;
 template <> struct V2T<float> { using type = float2; };
 template <> struct V2T<double> { using type = double2; };
+
+// One pair, laid out for vector loads: a scatter lane reads its slot's
+// integers with one 128-bit load and (t, weight) with one 64/128-bit load.
+template <class T> struct PairRec {
+  // per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window):
+  // extended segment (−1: no contribution; −2: F window), column-map index
+  // of the window's first knot, valid knots in the window
+  int4 si[4];
+  typename V2T<T>::type sf[4]; // local coordinate t; weight × the table's 1/h (F window: ρ'_{ti}(r))
+  typename Vec4T<T>::type uv;  // u_x, u_y, u_z, v_xx
+  typename Vec4T<T>::type vv;  // v_yy, v_zz, v_xy, v_xz
+  typename V2T<T>::type vd;    // v_yz, ρ'_{ti}(r)
+  T cFj;                       // F''_j
+  int j;
+};
 
 template <class T, bool EAM, bool STAGE>
 __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
@@ -875,98 +879,100 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         const int tj = typ[j];
         R.j = j;
         for (int s = 0; s < 4; ++s) {
-          R.e[s] = -1;
-          R.cbase[s] = 0;
-          R.nv[s] = 0;
-          R.t[s] = R.w[s] = R.ih[s] = T(0);
+          R.si[s] = make_int4(-1, 0, 0, 0);
+          R.sf[s].x = R.sf[s].y = T(0);
         }
-        R.dgi = R.cFj = T(0);
+        T dgi = T(0), cFj = T(0), u[3] = {0, 0, 0}, v[6] = {0, 0, 0, 0, 0, 0};
         T dgj = T(0);
         if (r >= T(1e-14)) {
           const T ir = T(1) / r;
-          for (int a = 0; a < 3; ++a) R.u[a] = d[a] * ir;
-          R.v[0] = d[0] * d[0] * ir;
-          R.v[1] = d[1] * d[1] * ir;
-          R.v[2] = d[2] * d[2] * ir;
-          R.v[3] = d[0] * d[1] * ir;
-          R.v[4] = d[0] * d[2] * ir;
-          R.v[5] = d[1] * d[2] * ir;
-          auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt) {
+          for (int a = 0; a < 3; ++a) u[a] = d[a] * ir;
+          v[0] = d[0] * d[0] * ir;
+          v[1] = d[1] * d[1] * ir;
+          v[2] = d[2] * d[2] * ir;
+          v[3] = d[0] * d[1] * ir;
+          v[4] = d[0] * d[2] * ir;
+          v[5] = d[1] * d[2] * ir;
+          auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt, T &tout) {
             T t;
             const int e = seg_of(tb, rr, t);
-            R.e[s] = e;
-            R.t[s] = t;
-            R.w[s] = wgt;
-            R.ih[s] = tb.inv_h;
-            R.cbase[s] = tb.cmap0 + segws[e];
-            R.nv[s] = tb.n - segws[e];
+            R.si[s] = make_int4(e, tb.cmap0 + segws[e], tb.n - segws[e], 0);
+            R.sf[s].x = t;
+            R.sf[s].y = wgt * tb.inv_h;
+            tout = t;
             return e;
           };
+          T t_;
           const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
           const bool phi_in = EAM ? in_span(tp, r) : (r >= tp.x0 && r < tp.xmax);
-          if (phi_in) set_slot(0, tp, r, T(1));
+          if (phi_in) set_slot(0, tp, r, T(1), t_);
           if constexpr (EAM) {
             const STab<T> &gj = tabs[np + tj], &gi_ = tabs[np + ti];
             const T gFj = gFa[j];
-            R.cFj = cFa[j];
+            cFj = cFa[j];
             if (in_span(gj, r)) {
-              const int e = set_slot(1, gj, r, tj == ti ? gFi + gFj : gFi);
-              dgj = seg_der<T>(seg[e], R.t[1], gj.inv_h);
+              const int e = set_slot(1, gj, r, tj == ti ? gFi + gFj : gFi, t_);
+              dgj = seg_der<T>(seg[e], t_, gj.inv_h);
             }
             if (in_span(gi_, r)) {
               T t;
               const int e = seg_of(gi_, r, t);
-              R.dgi = seg_der<T>(seg[e], t, gi_.inv_h);
-              if (tj != ti) set_slot(2, gi_, r, gFj);
+              dgi = seg_der<T>(seg[e], t, gi_.inv_h);
+              if (tj != ti) set_slot(2, gi_, r, gFj, t_);
             }
             // F_j window: coefficient dgd_j[q]·ρ'_{ti}(r)
             const STab<T> &te = tabs[np + nt + tj];
             const int wsj = wsFa[j];
-            R.e[3] = -2;
-            R.w[3] = R.dgi;
-            R.cbase[3] = te.cmap0 + wsj;
-            R.nv[3] = te.n - wsj;
+            R.si[3] = make_int4(-2, te.cmap0 + wsj, te.n - wsj, 0);
+            R.sf[3].y = dgi;
           }
-        } else {
-          for (int a = 0; a < 3; ++a) R.u[a] = T(0);
-          for (int a = 0; a < 6; ++a) R.v[a] = T(0);
         }
+        R.uv = {u[0], u[1], u[2], v[0]};
+        R.vv = {v[1], v[2], v[3], v[4]};
+        R.vd.x = v[5];
+        R.vd.y = dgi;
+        R.cFj = cFj;
         rec[lane] = R;
-        for (int a = 0; a < 3; ++a) V[a] += dgj * R.u[a];
-        for (int a = 0; a < 6; ++a) P[a] += dgj * R.v[a];
+        for (int a = 0; a < 3; ++a) V[a] += dgj * u[a];
+        for (int a = 0; a < 6; ++a) P[a] += dgj * v[a];
       }
       __syncwarp();
       // sparse knot-window scatter, one pair at a time, 24 lanes = 4 slots × 6 knots
       for (int k = 0; k < cnt; ++k) {
         const PairRec<T> &R = rec[k];
         if (lane < 4 * kWin) {
-          const int e = R.e[slot];
-          const int col = (e != -1 && q < R.nv[slot]) ? cmap[R.cbase[slot] + q] : -1;
+          const int4 si = R.si[slot];
+          const int e = si.x;
+          const int col = (e != -1 && q < si.z) ? cmap[si.y + q] : -1;
           if (col >= 0) {
-            const T tt = R.t[slot];
+            const T2 sf = R.sf[slot];
+            const T tt = sf.x;
             T cf, dv = T(0);
             if (e >= 0) {
               const T *G = segg + e * 4 * kWin;
               const T g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
-              cf = R.w[slot] * ((g1 + tt * (T(2) * g2 + T(3) * tt * g3)) * R.ih[slot]);
+              cf = sf.y * (g1 + tt * (T(2) * g2 + T(3) * tt * g3));
               if (slot == 0) dv = half_we * (G[q] + tt * (g1 + tt * (g2 + tt * g3)));
             } else {
-              cf = R.w[slot] * dgda[R.j * kWin + q];
+              cf = sf.y * dgda[R.j * kWin + q];
             }
+            const T4 uv = R.uv;
             T4 fr = frow[col];
-            fr.x += cf * R.u[0];
-            fr.y += cf * R.u[1];
-            fr.z += cf * R.u[2];
+            fr.x += cf * uv.x;
+            fr.y += cf * uv.y;
+            fr.z += cf * uv.z;
             fr.w += dv;
             frow[col] = fr;
             if (want_stress && e >= 0) {
+              const T4 vv = R.vv;
+              const T v5 = R.vd.x;
               T2 s0 = srow[3 * col], s1 = srow[3 * col + 1], s2 = srow[3 * col + 2];
-              s0.x += cf * R.v[0];
-              s0.y += cf * R.v[1];
-              s1.x += cf * R.v[2];
-              s1.y += cf * R.v[3];
-              s2.x += cf * R.v[4];
-              s2.y += cf * R.v[5];
+              s0.x += cf * uv.w;
+              s0.y += cf * vv.x;
+              s1.x += cf * vv.y;
+              s1.y += cf * vv.z;
+              s2.x += cf * vv.w;
+              s2.y += cf * v5;
               srow[3 * col] = s0;
               srow[3 * col + 1] = s1;
               srow[3 * col + 2] = s2;
@@ -979,10 +985,11 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         // dense ρ-chain: Σ_j F''_j ρ'_{ti}(r) u drho_j[m]
         for (int k = 0; k < cnt; ++k) {
           const PairRec<T> &R = rec[k];
-          const T wgt = R.cFj * R.dgi;
+          const T wgt = R.cFj * R.vd.y;
           if (wgt == T(0)) continue;
           const T *drj = drho + R.j * dstr;
-          const T u0 = R.u[0], u1 = R.u[1], u2 = R.u[2];
+          const T4 uv = R.uv;
+          const T u0 = uv.x, u1 = uv.y, u2 = uv.z;
           for (int s2 = 0; s2 < 2; ++s2) {
             const int m = lane + 32 * s2;
             if (m < nd) {
