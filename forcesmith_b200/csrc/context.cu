@@ -104,6 +104,8 @@ void free_configs(fs_gpu *h) {
   dfree(h->d_nb_start);
   dfree(h->d_nb_pack);
   dfree(h->d_nb_count);
+  dfree(h->d_cfg_by_work);
+  h->max_cfg_work = 0;
   dfree(h->d_F);
   dfree(h->d_forces);
   dfree(h->d_energy);

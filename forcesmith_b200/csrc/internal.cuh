@@ -128,6 +128,11 @@ struct fs_gpu {
   int32_t *d_nb_start = nullptr; // n_atoms + 1 (global pair offsets)
   uint32_t *d_nb_pack = nullptr; // j_local (20 bits) | image index (12 bits)
   int32_t *d_nb_count = nullptr; // per atom
+  // 3-body work: the largest count of directed pairs + neighbour pairs (j < k)
+  // of one configuration, and the configurations ordered by that count,
+  // heaviest first (launch order of the per-configuration 3-body kernels)
+  int64_t max_cfg_work = 0;
+  int32_t *d_cfg_by_work = nullptr;
 
   // model
   bool have_model = false;

@@ -14,6 +14,7 @@
 // warp exclusive scan places every lane's pairs behind those of lower j.
 #include "internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 namespace fsg {
@@ -176,6 +177,24 @@ int build_neighbors(fs_gpu *h, double rcut) {
   start[h->n_atoms] = static_cast<int32_t>(total);
   for (int c = 0; c < n_cfg; ++c) h->cfg_host[c].pair0 = start[h->atom0[c]];
   h->n_pairs = total;
+  std::vector<int32_t> order(n_cfg); // outlives the asynchronous upload below (synchronised at the end)
+  {
+    std::vector<int64_t> work(n_cfg, 0);
+    h->max_cfg_work = 0;
+    for (int c = 0; c < n_cfg; ++c) {
+      const int64_t a0 = h->atom0[c];
+      for (int64_t i = a0; i < a0 + h->cfg_host[c].natoms; ++i)
+        work[c] += cnt[i] + static_cast<int64_t>(cnt[i]) * (cnt[i] - 1) / 2;
+      h->max_cfg_work = std::max(h->max_cfg_work, work[c]);
+    }
+    for (int c = 0; c < n_cfg; ++c) order[c] = c;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return work[x] > work[y]; });
+    if (h->d_cfg_by_work) cudaFree(h->d_cfg_by_work);
+    h->d_cfg_by_work = nullptr;
+    FS_CUDA(cudaMalloc(&h->d_cfg_by_work, std::max(n_cfg, 1) * sizeof(int32_t)));
+    FS_CUDA(cudaMemcpyAsync(h->d_cfg_by_work, order.data(), n_cfg * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            h->stream));
+  }
   FS_CUDA(cudaMemcpyAsync(h->d_nb_start, start.data(), (h->n_atoms + 1) * sizeof(int32_t),
                           cudaMemcpyHostToDevice, h->stream));
   FS_CUDA(cudaMemcpyAsync(h->d_cfg, h->cfg_host.data(), n_cfg * sizeof(CfgDev), cudaMemcpyHostToDevice,

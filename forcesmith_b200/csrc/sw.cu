@@ -11,16 +11,28 @@
 //   differences); here every partial ∂/∂{A,B,p,q,δ,a1,γ,a2,λ} is carried
 //   exactly by forward-mode dual numbers through the same expressions.
 //
-// One CTA per configuration, one thread per central atom.  Forces on the end
-// atoms j, k of a triplet and the Jacobian block of the configuration
-// ((3N + rows) × D, D = the few free SW parameters) accumulate in shared
-// memory with atomics, then stream out.
+// One CTA per configuration.  A block scan lays out the configuration's work
+// items, and threads take them flat: first one directed pair each (2-body),
+// then one neighbour pair (j < k) of a central atom each (3-body), so atoms
+// with few or many neighbours cost the same lanes.  Forces and the Jacobian
+// block of the configuration ((3N + rows) × D, D = the few free SW parameters)
+// accumulate in shared memory with atomics, then stream out; the energy and
+// stress rows, which every item hits, are summed in registers first.
 #include "kern_common.cuh"
 
 #include <algorithm>
 
 namespace fsg {
 namespace {
+
+// Reciprocal, exp and log: the hardware approximations in FP32 (a few ulp,
+// inside the FP32 path's stated tolerances), IEEE in FP64.
+__device__ __forceinline__ float rcp_t(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double rcp_t(double x) { return 1.0 / x; }
+__device__ __forceinline__ float exp_t(float x) { return __expf(x); }
+__device__ __forceinline__ double exp_t(double x) { return exp(x); }
+__device__ __forceinline__ float log_t(float x) { return __logf(x); }
+__device__ __forceinline__ double log_t(double x) { return log(x); }
 
 template <class T, int N> struct Dual {
   T v;
@@ -64,14 +76,14 @@ template <class T, int N> __device__ Dual<T, N> operator*(T s, const Dual<T, N> 
   return r;
 }
 template <class T, int N> __device__ Dual<T, N> operator/(const Dual<T, N> &a, const Dual<T, N> &b) {
-  const T ib = T(1) / b.v;
+  const T ib = rcp_t(b.v);
   Dual<T, N> r(a.v * ib);
 #pragma unroll
   for (int k = 0; k < N; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
   return r;
 }
 template <class T, int N> __device__ Dual<T, N> dexp(const Dual<T, N> &a) {
-  Dual<T, N> r(exp(a.v));
+  Dual<T, N> r(exp_t(a.v));
 #pragma unroll
   for (int k = 0; k < N; ++k) r.d[k] = r.v * a.d[k];
   return r;
@@ -91,7 +103,7 @@ __device__ void v2_dual(T r, const T *P, Dual<T, 6> &v2, Dual<T, 6> &dv2) {
   const D6 d = rr - a1;
   const D6 e = dexp(delta / d);
   if (e.v == T(0)) return;
-  const T lr = log(r);
+  const T lr = log_t(r);
   const D6 rp = dexp(T(-1) * (p * D6(lr)));
   const D6 rq = dexp(T(-1) * (q * D6(lr)));
   const D6 rp1 = rp / rr, rq1 = rq / rr; // r^{-p-1}, r^{-q-1}
@@ -142,17 +154,130 @@ template <class T> struct SwArgs {
   int64_t ld;
   int D;
   double *jtr_part;
+  const int32_t *order; // configurations by work, heaviest first (CTA b runs order[b])
+  int use_own;          // work-item owner table in shared memory (else binary search)
 };
+
+constexpr int kSwThreads = 256;
+
+// Block sums of K values at once (one pair of barriers); valid on thread 0.
+// red holds K × 32 doubles.
+template <int K> __device__ void block_sum_k(double (&v)[K], double *red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k * 32 + w] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double t = 0.0;
+      for (int q = 0; q < nw; ++q) t += red[k * 32 + q];
+      v[k] = t;
+    }
+}
 
 template <class T>
 __device__ __forceinline__ void add_row(T *Jb, int D, int row, int col, T v) {
-  if (col >= 0 && v != T(0)) atomicAdd(&Jb[static_cast<int64_t>(row) * D + col], v);
+  if (col >= 0 && v != T(0)) atomicAdd(&Jb[row * D + col], v); // the block is < 227 KB: int offsets
+}
+
+// The energy and six stress rows of the Jacobian block for NQ dual slots,
+// summed in registers while a thread's consecutive work items map their slots
+// to the same columns, and added to shared memory when the columns change
+// (with one species: once, at the end of the phase).
+template <class T, int NQ> struct RowAcc {
+  T a[NQ][7];
+  int col[NQ];
+  __device__ RowAcc() {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      col[q] = -1;
+#pragma unroll
+      for (int r = 0; r < 7; ++r) a[q][r] = T(0);
+    }
+  }
+  __device__ __forceinline__ void flush(T *Jb, int D, int rowE) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int r = 0; r < 7; ++r) {
+        add_row(Jb, D, rowE + r, col[q], a[q][r]);
+        a[q][r] = T(0);
+      }
+  }
+  __device__ __forceinline__ void use(const int (&cols)[NQ], T *Jb, int D, int rowE) {
+    bool same = true;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) same &= cols[q] == col[q];
+    if (!same) {
+      flush(Jb, D, rowE);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) col[q] = cols[q];
+    }
+  }
+};
+
+// Largest i in [0, N) with first[i] <= w, for non-decreasing first[] with
+// first[0] = 0 <= w < first[N]: the atom that owns work item w.
+__device__ __forceinline__ int owner_of(const int *first, int N, int w) {
+  int lo = 0, hi = N;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Work-item offsets of one configuration: pfirst[i] = first directed pair of
+// atom i (relative to atom 0's), tfirst[i] = first neighbour pair (j < k) of
+// atom i, n_i (n_i − 1)/2 per atom; both with the totals at [N].  One block
+// scan; blockDim.x a multiple of 32, at most 1024.
+__device__ void stage_work(const int32_t *nb, int N, int *pfirst, int *tfirst, int *wsum) {
+  for (int k = threadIdx.x; k <= N; k += blockDim.x) pfirst[k] = nb[k] - nb[0];
+  const int per = (N + blockDim.x - 1) / blockDim.x;
+  const int b = min(N, static_cast<int>(threadIdx.x) * per), e = min(N, b + per);
+  int s = 0;
+  for (int k = b; k < e; ++k) {
+    const int n = nb[k + 1] - nb[k];
+    s += n * (n - 1) / 2;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < nw ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    __syncwarp();
+    if (lane < nw) wsum[lane] = v;
+  }
+  __syncthreads();
+  int base = x - s + (w > 0 ? wsum[w - 1] : 0);
+  for (int k = b; k < e; ++k) {
+    tfirst[k] = base;
+    const int n = nb[k + 1] - nb[k];
+    base += n * (n - 1) / 2;
+  }
+  if (threadIdx.x == blockDim.x - 1) tfirst[N] = base;
 }
 
 template <class T, bool JAC>
-__global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
+__global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(SwArgs<T> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int c = blockIdx.x;
+  const int c = A.order ? A.order[blockIdx.x] : blockIdx.x;
   const CfgDev &cd = A.c.cfg[c];
   const int N = cd.natoms;
   const int nt = A.c.ntypes, np = nt * (nt + 1) / 2;
@@ -167,8 +292,12 @@ __global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
   T *lam = S.take<T>(nt * np);
   int *pcol = S.take<int>(8 * np);
   int *lcol = S.take<int>(nt * np);
-  double *red = S.take<double>(64);
+  double *red = S.take<double>(8 * 32);
+  int *pfirst = S.take<int>(N + 1);
+  int *tfirst = S.take<int>(N + 1);
+  int *wsum = S.take<int>(32);
   T *Jb = JAC ? S.take<T>(static_cast<size_t>(3 * N + 7) * D) : nullptr; // force rows, E, 6 stress
+  double *jpart = JAC ? S.take<double>(static_cast<size_t>(D) * (blockDim.x >> 5)) : nullptr;
   for (int k = threadIdx.x; k < 8 * np; k += blockDim.x) {
     const TableDesc &td = A.c.desc[k / 8];
     par[k] = static_cast<T>(A.vals[td.pv0 + k % 8]);
@@ -183,70 +312,112 @@ __global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
   if constexpr (JAC)
     for (int k = threadIdx.x; k < (3 * N + 7) * D; k += blockDim.x) Jb[k] = T(0);
   stage_geometry(cd, A.c, wpos, shift, typ);
-  __syncthreads();
   const int32_t *start = A.c.nb_start + cd.atom0;
+  stage_work(start, N, pfirst, tfirst, wsum);
+  __syncthreads();
+  const uint32_t *nbp = A.c.nb_pack + start[0];
+  const int npair = pfirst[N], ntri = tfirst[N];
+  // owner of each work item: pair p → i; neighbour pair t → (row a << 16) | i,
+  // row a = index of j in i's list (N and the row below 2^16, checked at launch)
+  uint32_t *own = nullptr;
+  if (A.use_own) {
+    own = S.take<uint32_t>(npair + ntri);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const int p0 = pfirst[i], n = pfirst[i + 1] - p0;
+      for (int q = 0; q < n; ++q) own[p0 + q] = static_cast<uint32_t>(i);
+      uint32_t *ot = own + npair + tfirst[i];
+      for (int a = 0; a + 1 < n; ++a)
+        for (int b = a + 1; b < n; ++b) *ot++ = (static_cast<uint32_t>(a) << 16) | static_cast<uint32_t>(i);
+    }
+    __syncthreads();
+  }
   double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0};
   const int rowE = 3 * N; // local rows of the block: 3N force, E, 6 stress
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const int ti = typ[i];
-    T fi[3] = {0, 0, 0};
-    // ---- 2-body (½ v₂ per directed pair, force on i)
-    for (int p = start[i]; p < start[i + 1]; ++p) {
+  // ---- 2-body: one thread per directed pair (½ v₂ each, force on i)
+  {
+    RowAcc<T, JAC ? 6 : 1> ra;
+    for (int w = threadIdx.x; w < npair; w += blockDim.x) {
+      const int i = own ? static_cast<int>(own[w]) : owner_of(pfirst, N, w);
       int j;
       T d[3];
-      pair_vec(wpos, shift, i, A.c.nb_pack[p], j, d[0], d[1], d[2]);
+      pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
       const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (r < T(1e-14)) continue;
-      const int sl = pair_ord(ti, typ[j], nt);
+      const int sl = pair_ord(typ[i], typ[j], nt);
       const T *P = par + 8 * sl;
+      T v2v, s;
+      Dual<T, 6> v2, dv2;
       if constexpr (JAC) {
-        Dual<T, 6> v2, dv2;
         v2_dual(r, P, v2, dv2);
-        const T s = dv2.v / r;
-        for (int a = 0; a < 3; ++a) fi[a] += s * d[a];
-        e_acc += 0.5 * static_cast<double>(v2.v);
-        const T f[3] = {s * d[0], s * d[1], s * d[2]};
-        sg[0] -= 0.5 * d[0] * f[0];
-        sg[1] -= 0.5 * d[1] * f[1];
-        sg[2] -= 0.5 * d[2] * f[2];
-        sg[3] -= 0.5 * d[0] * f[1];
-        sg[4] -= 0.5 * d[0] * f[2];
-        sg[5] -= 0.5 * d[1] * f[2];
-        for (int k = 0; k < 6; ++k) {
-          const int col = pcol[8 * sl + k];
-          if (col < 0) continue;
-          const T ds = dv2.d[k] / r;
-          for (int a = 0; a < 3; ++a) add_row(Jb, D, 3 * i + a, col, ds * d[a]);
-          add_row(Jb, D, rowE, col, static_cast<T>(0.5 * A.w_e) * v2.d[k]);
-          const T df[3] = {ds * d[0], ds * d[1], ds * d[2]};
-          add_row(Jb, D, rowE + 1, col, T(-0.5) * d[0] * df[0]);
-          add_row(Jb, D, rowE + 2, col, T(-0.5) * d[1] * df[1]);
-          add_row(Jb, D, rowE + 3, col, T(-0.5) * d[2] * df[2]);
-          add_row(Jb, D, rowE + 4, col, T(-0.5) * d[0] * df[1]);
-          add_row(Jb, D, rowE + 5, col, T(-0.5) * d[0] * df[2]);
-          add_row(Jb, D, rowE + 6, col, T(-0.5) * d[1] * df[2]);
-        }
+        v2v = v2.v;
+        s = dv2.v / r;
       } else {
-        T v2, dv2;
-        v2_plain(r, P, v2, dv2);
-        const T s = dv2 / r;
-        const T f[3] = {s * d[0], s * d[1], s * d[2]};
-        for (int a = 0; a < 3; ++a) fi[a] += f[a];
-        e_acc += 0.5 * static_cast<double>(v2);
-        const T hx = T(0.5) * d[0], hy = T(0.5) * d[1], hz = T(0.5) * d[2];
-        sg[0] -= hx * f[0];
-        sg[1] -= hy * f[1];
-        sg[2] -= hz * f[2];
-        sg[3] -= hx * f[1];
-        sg[4] -= hx * f[2];
-        sg[5] -= hy * f[2];
+        T dv2p;
+        v2_plain(r, P, v2v, dv2p);
+        s = dv2p / r;
+      }
+      const T f[3] = {s * d[0], s * d[1], s * d[2]};
+      atomicAdd(&Fs[3 * i], f[0]);
+      atomicAdd(&Fs[3 * i + 1], f[1]);
+      atomicAdd(&Fs[3 * i + 2], f[2]);
+      e_acc += 0.5 * static_cast<double>(v2v);
+      const T hx = T(0.5) * d[0], hy = T(0.5) * d[1], hz = T(0.5) * d[2];
+      sg[0] -= hx * f[0];
+      sg[1] -= hy * f[1];
+      sg[2] -= hz * f[2];
+      sg[3] -= hx * f[1];
+      sg[4] -= hx * f[2];
+      sg[5] -= hy * f[2];
+      if constexpr (JAC) {
+        int cols[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) cols[k] = pcol[8 * sl + k];
+        ra.use(cols, Jb, D, rowE);
+        const T we = static_cast<T>(0.5 * A.w_e), ir = rcp_t(r);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const T ds = dv2.d[k] * ir;
+          const T df[3] = {ds * d[0], ds * d[1], ds * d[2]};
+#pragma unroll
+          for (int a = 0; a < 3; ++a) add_row(Jb, D, 3 * i + a, cols[k], df[a]);
+          ra.a[k][0] += we * v2.d[k];
+          ra.a[k][1] -= hx * df[0];
+          ra.a[k][2] -= hy * df[1];
+          ra.a[k][3] -= hz * df[2];
+          ra.a[k][4] -= hx * df[1];
+          ra.a[k][5] -= hx * df[2];
+          ra.a[k][6] -= hy * df[2];
+        }
       }
     }
-    // ---- 3-body, neighbour pairs jj < kk of central atom i
-    for (int pj = start[i]; pj < start[i + 1]; ++pj) {
+    if constexpr (JAC) ra.flush(Jb, D, rowE);
+  }
+  // ---- 3-body: one thread per neighbour pair (j < k) of a central atom i
+  {
+    RowAcc<T, JAC ? 5 : 1> rb;
+    for (int w = threadIdx.x; w < ntri; w += blockDim.x) {
+      int i, a0, u;
+      if (own) {
+        const uint32_t v = own[npair + w];
+        i = static_cast<int>(v & 0xFFFFu);
+        a0 = static_cast<int>(v >> 16);
+        const int n = pfirst[i + 1] - pfirst[i];
+        u = w - tfirst[i] - a0 * (2 * n - a0 - 1) / 2; // row a0 starts after Σ_{a<a0} (n − 1 − a)
+      } else {
+        i = owner_of(tfirst, N, w);
+        const int n = pfirst[i + 1] - pfirst[i];
+        u = w - tfirst[i];
+        a0 = 0;
+        while (u >= n - 1 - a0) {
+          u -= n - 1 - a0;
+          ++a0;
+        }
+      }
+      const int pj = pfirst[i] + a0, pk = pj + 1 + u;
+      const int ti = typ[i];
       int j;
       T d1[3];
-      pair_vec(wpos, shift, i, A.c.nb_pack[pj], j, d1[0], d1[1], d1[2]);
+      pair_vec(wpos, shift, i, nbp[pj], j, d1[0], d1[1], d1[2]);
       const T r1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
       if (r1 < T(1e-14)) continue;
       const int tj = typ[j];
@@ -254,79 +425,81 @@ __global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
       Dual<T, 5> h1, dh1;
       h_dual<T, 5>(r1, par[8 * s1 + 6], par[8 * s1 + 7], 0, 1, h1, dh1);
       if (h1.v == T(0) && dh1.v == T(0)) continue; // make_jbond (stiweb_force.cpp:107-121)
-      const T ir1 = T(1) / r1;
-      for (int pk = pj + 1; pk < start[i + 1]; ++pk) {
-        int k;
-        T d2[3];
-        pair_vec(wpos, shift, i, A.c.nb_pack[pk], k, d2[0], d2[1], d2[2]);
-        const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
-        if (r2 < T(1e-14)) continue;
-        const int tk = typ[k];
-        const int s2 = pair_ord(ti, tk, nt);
-        Dual<T, 5> h2, dh2;
-        h_dual<T, 5>(r2, par[8 * s2 + 6], par[8 * s2 + 7], 2, 3, h2, dh2);
-        if (h2.v == T(0) && dh2.v == T(0)) continue;
-        const T ir2 = T(1) / r2;
-        const int lt = ti * np + pair_ord(tj, tk, nt);
-        const Dual<T, 5> L = Dual<T, 5>::var(lam[lt], 4);
-        const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;
-        const T cp = cth + T(1) / T(3);
-        const Dual<T, 5> w = (cp * cp) * L, dw = (T(2) * cp) * L;
-        // three_body_forces (kernels.hpp:44-58)
-        const T irr = ir1 * ir2;
-        const T Aa = cth * ir1 * ir1 - irr, Bb = cth * ir2 * ir2 - irr;
-        const Dual<T, 5> c1 = (ir1 * dh1) * h2 * w;   // df1·inv_r1·f2·g
-        const Dual<T, 5> c2 = h1 * (ir2 * dh2) * w;   // f1·df2·inv_r2·g
-        const Dual<T, 5> c3 = h1 * h2 * dw;           // f1·f2·dg
-        const Dual<T, 5> e3 = h1 * h2 * w;
-        T Fi[3], Fj[3], Fk[3];
-        for (int a = 0; a < 3; ++a) {
-          Fi[a] = c1.v * d1[a] + c2.v * d2[a] - c3.v * (Aa * d1[a] + Bb * d2[a]);
-          Fj[a] = -(c1.v * d1[a]) - c3.v * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
-          Fk[a] = -(c2.v * d2[a]) - c3.v * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
-          fi[a] += Fi[a];
-        }
-        atomicAdd(&Fs[3 * j], Fj[0]);
-        atomicAdd(&Fs[3 * j + 1], Fj[1]);
-        atomicAdd(&Fs[3 * j + 2], Fj[2]);
-        atomicAdd(&Fs[3 * k], Fk[0]);
-        atomicAdd(&Fs[3 * k + 1], Fk[1]);
-        atomicAdd(&Fs[3 * k + 2], Fk[2]);
-        e_acc += static_cast<double>(e3.v);
-        sg[0] += d1[0] * Fj[0] + d2[0] * Fk[0];
-        sg[1] += d1[1] * Fj[1] + d2[1] * Fk[1];
-        sg[2] += d1[2] * Fj[2] + d2[2] * Fk[2];
-        sg[3] += d1[0] * Fj[1] + d2[0] * Fk[1];
-        sg[4] += d1[0] * Fj[2] + d2[0] * Fk[2];
-        sg[5] += d1[1] * Fj[2] + d2[1] * Fk[2];
-        if constexpr (JAC) {
-          const int cols[5] = {pcol[8 * s1 + 6], pcol[8 * s1 + 7], pcol[8 * s2 + 6], pcol[8 * s2 + 7], lcol[lt]};
-          for (int q = 0; q < 5; ++q) {
-            const int col = cols[q];
-            if (col < 0) continue;
-            T gi[3], gj[3], gk[3];
-            for (int a = 0; a < 3; ++a) {
-              gi[a] = c1.d[q] * d1[a] + c2.d[q] * d2[a] - c3.d[q] * (Aa * d1[a] + Bb * d2[a]);
-              gj[a] = -(c1.d[q] * d1[a]) - c3.d[q] * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
-              gk[a] = -(c2.d[q] * d2[a]) - c3.d[q] * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
-              add_row(Jb, D, 3 * i + a, col, gi[a]);
-              add_row(Jb, D, 3 * j + a, col, gj[a]);
-              add_row(Jb, D, 3 * k + a, col, gk[a]);
-            }
-            add_row(Jb, D, rowE, col, static_cast<T>(A.w_e) * e3.d[q]);
-            add_row(Jb, D, rowE + 1, col, d1[0] * gj[0] + d2[0] * gk[0]);
-            add_row(Jb, D, rowE + 2, col, d1[1] * gj[1] + d2[1] * gk[1]);
-            add_row(Jb, D, rowE + 3, col, d1[2] * gj[2] + d2[2] * gk[2]);
-            add_row(Jb, D, rowE + 4, col, d1[0] * gj[1] + d2[0] * gk[1]);
-            add_row(Jb, D, rowE + 5, col, d1[0] * gj[2] + d2[0] * gk[2]);
-            add_row(Jb, D, rowE + 6, col, d1[1] * gj[2] + d2[1] * gk[2]);
+      int k;
+      T d2[3];
+      pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
+      const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
+      if (r2 < T(1e-14)) continue;
+      const int tk = typ[k];
+      const int s2 = pair_ord(ti, tk, nt);
+      Dual<T, 5> h2, dh2;
+      h_dual<T, 5>(r2, par[8 * s2 + 6], par[8 * s2 + 7], 2, 3, h2, dh2);
+      if (h2.v == T(0) && dh2.v == T(0)) continue;
+      const T ir1 = rcp_t(r1), ir2 = rcp_t(r2);
+      const int lt = ti * np + pair_ord(tj, tk, nt);
+      const Dual<T, 5> L = Dual<T, 5>::var(lam[lt], 4);
+      const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;
+      const T cp = cth + T(1) / T(3);
+      const Dual<T, 5> wg = (cp * cp) * L, dw = (T(2) * cp) * L;
+      // three_body_forces (kernels.hpp:44-58)
+      const T irr = ir1 * ir2;
+      Dual<T, 5> c1 = (ir1 * dh1) * h2 * wg; // df1·inv_r1·f2·g
+      Dual<T, 5> c2 = h1 * (ir2 * dh2) * wg; // f1·df2·inv_r2·g
+      Dual<T, 5> c3 = h1 * h2 * dw;          // f1·f2·dg
+      Dual<T, 5> e3 = h1 * h2 * wg;
+      T Fi[3], Fj[3], Fk[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        Fj[a] = -(c1.v * d1[a]) - c3.v * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
+        Fk[a] = -(c2.v * d2[a]) - c3.v * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
+        Fi[a] = -(Fj[a] + Fk[a]); // the three forces sum to zero
+        atomicAdd(&Fs[3 * i + a], Fi[a]);
+        atomicAdd(&Fs[3 * j + a], Fj[a]);
+        atomicAdd(&Fs[3 * k + a], Fk[a]);
+      }
+      e_acc += static_cast<double>(e3.v);
+      sg[0] += d1[0] * Fj[0] + d2[0] * Fk[0];
+      sg[1] += d1[1] * Fj[1] + d2[1] * Fk[1];
+      sg[2] += d1[2] * Fj[2] + d2[2] * Fk[2];
+      sg[3] += d1[0] * Fj[1] + d2[0] * Fk[1];
+      sg[4] += d1[0] * Fj[2] + d2[0] * Fk[2];
+      sg[5] += d1[1] * Fj[2] + d2[1] * Fk[2];
+      if constexpr (JAC) {
+        int cols[5] = {pcol[8 * s1 + 6], pcol[8 * s1 + 7], pcol[8 * s2 + 6], pcol[8 * s2 + 7], lcol[lt]};
+        // both ends in the same pair slot: one column each for γ and a2
+#pragma unroll
+        for (int q = 2; q < 4; ++q)
+          if (cols[q] == cols[q - 2]) {
+            c1.d[q - 2] += c1.d[q];
+            c2.d[q - 2] += c2.d[q];
+            c3.d[q - 2] += c3.d[q];
+            e3.d[q - 2] += e3.d[q];
+            cols[q] = -1;
           }
+        rb.use(cols, Jb, D, rowE);
+        const T we = static_cast<T>(A.w_e);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          T gj[3], gk[3];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            gj[a] = -(c1.d[q] * d1[a]) - c3.d[q] * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
+            gk[a] = -(c2.d[q] * d2[a]) - c3.d[q] * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
+            add_row(Jb, D, 3 * i + a, cols[q], -(gj[a] + gk[a]));
+            add_row(Jb, D, 3 * j + a, cols[q], gj[a]);
+            add_row(Jb, D, 3 * k + a, cols[q], gk[a]);
+          }
+          rb.a[q][0] += we * e3.d[q];
+          rb.a[q][1] += d1[0] * gj[0] + d2[0] * gk[0];
+          rb.a[q][2] += d1[1] * gj[1] + d2[1] * gk[1];
+          rb.a[q][3] += d1[2] * gj[2] + d2[2] * gk[2];
+          rb.a[q][4] += d1[0] * gj[1] + d2[0] * gk[1];
+          rb.a[q][5] += d1[0] * gj[2] + d2[0] * gk[2];
+          rb.a[q][6] += d1[1] * gj[2] + d2[1] * gk[2];
         }
       }
     }
-    atomicAdd(&Fs[3 * i], fi[0]);
-    atomicAdd(&Fs[3 * i + 1], fi[1]);
-    atomicAdd(&Fs[3 * i + 2], fi[2]);
+    if constexpr (JAC) rb.flush(Jb, D, rowE);
   }
   __syncthreads();
   const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
@@ -340,26 +513,23 @@ __global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
     if (A.forces) A.forces[ga] = f;
     objp += res * res;
   }
-  const double E = block_sum(e_acc, red);
-  double st[6];
-  for (int a = 0; a < 6; ++a) st[a] = block_sum(sg[a], red);
-  const double op = block_sum(objp, red);
-  __shared__ double s_rows[8];
+  double sums[8] = {e_acc, sg[0], sg[1], sg[2], sg[3], sg[4], sg[5], objp};
+  block_sum_k(sums, red);
   if (threadIdx.x == 0) {
+    const double E = sums[0];
+    double st[6];
     const double iv = 1.0 / cd.volume;
-    for (int a = 0; a < 6; ++a) st[a] *= iv;
+    for (int a = 0; a < 6; ++a) st[a] = sums[1 + a] * iv;
     int64_t row = row0 + 3 * N;
-    double o = op;
+    double o = sums[7];
     const double re = A.w_e * (E - cd.ref_energy);
     A.F[row++] = re;
-    s_rows[0] = re;
     o += re * re;
     static constexpr int vi[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
     if (A.w_s > 0.0)
       for (int v = 0; v < 6; ++v) {
         const double rs = A.w_s * (st[v] - cd.ref_stress[3 * vi[v][0] + vi[v][1]]);
         A.F[row++] = rs;
-        s_rows[1 + v] = rs;
         o += rs * rs;
       }
     A.F[row++] = 0.0; // no embedding: limit row is zero
@@ -380,6 +550,7 @@ __global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
     __syncthreads();
     const double sc = A.w_s / cd.volume;
     const int nrow = 3 * N + 2 + (A.w_s > 0.0 ? 6 : 0);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int col = 0; col < D; ++col) {
       double jr = 0.0;
       for (int r = threadIdx.x; r < nrow; r += blockDim.x) {
@@ -395,8 +566,14 @@ __global__ void __launch_bounds__(256) sw_kernel(SwArgs<T> A) {
         A.J[static_cast<int64_t>(col) * A.ld + row0 + r] = static_cast<T>(v);
         jr += v * A.F[row0 + r];
       }
-      jr = block_sum(jr, red);
-      if (threadIdx.x == 0) A.jtr_part[static_cast<int64_t>(c) * D + col] = jr;
+      for (int o = 16; o > 0; o >>= 1) jr += __shfl_xor_sync(0xffffffffu, jr, o);
+      if (lane == 0) jpart[col * nw + w] = jr;
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < D; col += blockDim.x) {
+      double jr = 0.0;
+      for (int k = 0; k < nw; ++k) jr += jpart[col * nw + k];
+      A.jtr_part[static_cast<int64_t>(c) * D + col] = jr;
     }
   }
 }
@@ -405,8 +582,11 @@ template <class T> size_t sw_smem(fs_gpu *h, int max_img, bool jac) {
   const int nt = h->ntypes, np = npair_of(nt), N = h->max_natoms;
   size_t b = align16(3 * N * sizeof(double)) + align16(3 * max_img * sizeof(double)) + align16(N) +
              align16(3 * N * sizeof(T)) + align16(8 * np * sizeof(T)) + align16(nt * np * sizeof(T)) +
-             align16(8 * np * sizeof(int)) + align16(nt * np * sizeof(int)) + align16(64 * sizeof(double));
-  if (jac) b += align16(static_cast<size_t>(3 * N + 7) * h->D * sizeof(T));
+             align16(8 * np * sizeof(int)) + align16(nt * np * sizeof(int)) + align16(8 * 32 * sizeof(double)) +
+             2 * align16((N + 1) * sizeof(int)) + align16(32 * sizeof(int));
+  if (jac)
+    b += align16(static_cast<size_t>(3 * N + 7) * h->D * sizeof(T)) +
+         align16(static_cast<size_t>(h->D) * (kSwThreads / 32) * sizeof(double));
   return b + 128;
 }
 
@@ -487,11 +667,16 @@ template <class T> int launch_sw(fs_gpu *h, double w_e, double w_s, bool jac) {
     a.ld = ldj;
     a.jtr_part = h->d_jtr_part;
   }
-  const size_t sm = sw_smem<T>(h, max_images_of(h), jac);
+  size_t sm = sw_smem<T>(h, max_images_of(h), jac);
   if (sm > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "SW: configuration too large for shared memory");
+  // the owner table when it fits (else each work item finds its atom by binary search)
+  const size_t own_bytes = align16(static_cast<size_t>(h->max_cfg_work) * sizeof(uint32_t));
+  a.use_own = (sm + own_bytes <= 227 * 1024 && h->max_natoms < 65536) ? 1 : 0;
+  if (a.use_own) sm += own_bytes;
+  a.order = h->d_cfg_by_work;
   auto k = jac ? sw_kernel<T, true> : sw_kernel<T, false>;
   FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-  k<<<h->n_cfg, 256, sm, h->stream>>>(a);
+  k<<<h->n_cfg, kSwThreads, sm, h->stream>>>(a);
   FS_CUDA(cudaGetLastError());
   sum_parts<<<1, 1024, 0, h->stream>>>(h->d_obj_part, h->n_cfg, h->d_obj);
   FS_CUDA(cudaGetLastError());

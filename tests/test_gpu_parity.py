@@ -303,6 +303,41 @@ def test_sw_jacobian_vs_central_differences(sw_case, precision, tol):
     assert np.max(np.abs(res["Jtr"] - Jtr)) <= 10 * tol * np.max(np.abs(Jtr))
 
 
+def binary_sw_model():
+    """Two species: three pair slots with their own (A, B, δ, a1, γ, a2)
+    (p, q fixed) and six λ_{i;jk}, one of them fixed — triplets whose ends sit
+    in different slots, and columns that change from one triplet to the next."""
+    from forcesmith_b200.abi import Model, Table, FS_FAMILY_SW
+    base = synth.sw_model().tables[0].values
+    tabs = []
+    for s, f in enumerate((1.0, 0.93, 1.06)):
+        v = base * np.array([f, 2.0 - f, 1, 1, f, 1.0 + 0.02 * s, 1.0 - 0.03 * s, 1.0 + 0.01 * s])
+        tabs.append(Table.sw(*v, fixed=np.array([0, 0, 1, 1, 0, 0, 0, 0], np.uint8)))
+    lam = 45.5 * np.array([1.0, 0.8, 1.2, 0.9, 1.1, 0.7])
+    tabs.append(Table.lam(lam, fixed=np.array([0, 0, 1, 0, 0, 0], np.uint8)))
+    return Model(FS_FAMILY_SW, 2, tabs)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-5), ("fp32", 2e-3)])
+def test_sw_binary_residual_and_jacobian(precision, tol):
+    from tests.helpers import small_diamond
+    ds = small_diamond(3, (2, 3), seed=37)
+    ds.type[:] = np.random.default_rng(5).integers(0, 2, ds.type.size)
+    model = binary_sw_model()
+    ds = label(ds, model.with_values(model.free_values() * 1.03), O.Oracle, 1.0, 0.2)
+    g, o = _pair(ds, model, precision)
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    ftol = 1e-9 if precision == "fp64" else 2e-5
+    assert np.max(np.abs(rg["forces"] - ro["forces"])) <= ftol * np.max(np.abs(ro["forces"]))
+    assert abs(rg["obj"] - ro["obj"]) <= (1e-9 if precision == "fp64" else 1e-4) * ro["obj"]
+    res = g.jacobian(1.0, 0.2)
+    Jf = o.jacobian_fd(1.0, 0.2)
+    assert res["J"].shape == Jf.shape and Jf.shape[1] == 3 * 6 + 5
+    colmax = np.abs(Jf).max(axis=0)
+    err = np.abs(res["J"] - Jf) / (tol * np.abs(Jf) + 1e-8 + 1e-7 * colmax)
+    assert err.max() <= 1.0, err.max()
+
+
 # --------------------------------------------------------------- ADP ---
 
 def test_adp_residual_and_fd_jacobian_fp64():
