@@ -751,9 +751,17 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
 //   F'_j     (embedding window of j)             weight ρ'_{t_i}(r)
 // into the warp's row buffer (distinct columns per pair, no atomics), and
 // every lane adds the dense ρ-chain term Σ_j F''_j ρ'_{t_i}(r) u drho_j for
-// the density columns it owns.  The stress rows use the pair symmetry of the
-// full list for the chain terms: Σ_pairs v (F''_i drho_i ρ'_{tj} + F''_j
-// drho_j ρ'_{ti}) = 2 Σ_i P_i F''_i drho_i with P_i = Σ_j v_ij ρ'_{tj}(r_ij).
+// the density columns it owns.
+//
+// Stress rows, W = Σ_pairs d ⊗ ∂f/∂y over the full list.  The pair force is
+// antisymmetric under (i, j, s) → (j, i, −s) (its scalar is symmetric in i, j
+// and u flips), and d = x_j + s − x_i, so
+//   W = −2 Σ_i (x_i − c) ⊗ ∂F_i/∂y + Σ_{pairs with s ≠ 0} s ⊗ ∂f/∂y
+// for any origin c (Σ_i ∂F_i/∂y = 0); c is the cell centre.  The first term is
+// added when atom i's rows are written; only pairs that leave the cell (about
+// a third here) scatter stress.  Their chain terms use the same symmetry:
+// Σ (s ⊗ u)(F''_i drho_i ρ'_{tj} + F''_j drho_j ρ'_{ti}) = 2 Σ_i P_i F''_i drho_i
+// with P_i = Σ_{j, s≠0} (s ⊗ u) ρ'_{tj}(r_ij).
 // The configuration's per-atom data (∂ρ/∂y rows, F', F'', embedding windows)
 // is staged in shared memory when it fits, so the inner loops never wait on
 // global memory.
@@ -767,11 +775,12 @@ template <> struct V2T<double> { using type = double2; };
 template <class T> struct PairRec {
   // per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window):
   // extended segment (−1: no contribution; −2: F window), column-map index
-  // of the window's first knot, valid knots in the window
+  // of the window's first knot, valid knots in the window, 1 if the pair
+  // leaves the cell and stress is wanted
   int4 si[4];
   typename V2T<T>::type sf[4]; // local coordinate t; weight × the table's 1/h (F window: ρ'_{ti}(r))
-  typename Vec4T<T>::type uv;  // u_x, u_y, u_z, v_xx
-  typename Vec4T<T>::type vv;  // v_yy, v_zz, v_xy, v_xz
+  typename Vec4T<T>::type uv;  // u_x, u_y, u_z, v_xx     (v = s ⊗ u for pairs that leave the
+  typename Vec4T<T>::type vv;  // v_yy, v_zz, v_xy, v_xz  cell, image shift s; zero otherwise)
   typename V2T<T>::type vd;    // v_yz, ρ'_{ti}(r)
   T cFj;                       // F''_j
   int j;
@@ -854,6 +863,9 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
   const T half_we = static_cast<T>(0.5 * A.w_e);
   const bool want_stress = A.w_s > 0.0;
   const int slot = lane / kWin, q = lane % kWin;
+  const int home = (cd.sx * (2 * cd.sy + 1) + cd.sy) * (2 * cd.sz + 1) + cd.sz; // image (0, 0, 0)
+  double ctr[3];                                                                   // cell centre
+  for (int a = 0; a < 3; ++a) ctr[a] = 0.5 * (cd.box[3 * a] + cd.box[3 * a + 1] + cd.box[3 * a + 2]);
 
   for (int i = w; i < N; i += warps) {
     for (int k = lane; k < D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
@@ -874,9 +886,12 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         PairRec<T> R;
         int j;
         T d[3];
-        pair_vec(wpos, shift, i, A.c.nb_pack[p0 + lane], j, d[0], d[1], d[2]);
+        const uint32_t pk = A.c.nb_pack[p0 + lane];
+        pair_vec(wpos, shift, i, pk, j, d[0], d[1], d[2]);
         const T r = sqrt_t(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         const int tj = typ[j];
+        const int img = static_cast<int>(pk >> 20);
+        const int cross = want_stress && img != home; // the pair leaves the cell: image shift s ≠ 0
         R.j = j;
         for (int s = 0; s < 4; ++s) {
           R.si[s] = make_int4(-1, 0, 0, 0);
@@ -887,16 +902,20 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         if (r >= T(1e-14)) {
           const T ir = T(1) / r;
           for (int a = 0; a < 3; ++a) u[a] = d[a] * ir;
-          v[0] = d[0] * d[0] * ir;
-          v[1] = d[1] * d[1] * ir;
-          v[2] = d[2] * d[2] * ir;
-          v[3] = d[0] * d[1] * ir;
-          v[4] = d[0] * d[2] * ir;
-          v[5] = d[1] * d[2] * ir;
+          if (cross) { // v = s ⊗ u in the order xx, yy, zz, xy, xz, yz
+            const T s0 = static_cast<T>(shift[3 * img]), s1 = static_cast<T>(shift[3 * img + 1]),
+                    s2 = static_cast<T>(shift[3 * img + 2]);
+            v[0] = s0 * u[0];
+            v[1] = s1 * u[1];
+            v[2] = s2 * u[2];
+            v[3] = s0 * u[1];
+            v[4] = s0 * u[2];
+            v[5] = s1 * u[2];
+          }
           auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt, T &tout) {
             T t;
             const int e = seg_of(tb, rr, t);
-            R.si[s] = make_int4(e, tb.cmap0 + segws[e], tb.n - segws[e], 0);
+            R.si[s] = make_int4(e, tb.cmap0 + segws[e], tb.n - segws[e], cross);
             R.sf[s].x = t;
             R.sf[s].y = wgt * tb.inv_h;
             tout = t;
@@ -963,7 +982,7 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
             fr.z += cf * uv.z;
             fr.w += dv;
             frow[col] = fr;
-            if (want_stress && e >= 0) {
+            if (si.w) { // stress scatter: pairs that leave the cell only
               const T4 vv = R.vv;
               const T v5 = R.vd.x;
               T2 s0 = srow[3 * col], s1 = srow[3 * col + 1], s2 = srow[3 * col + 2];
@@ -1054,6 +1073,8 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
     }
     __syncwarp();
     const double F0 = A.F[row0 + 3 * i], F1 = A.F[row0 + 3 * i + 1], F2 = A.F[row0 + 3 * i + 2];
+    const T x0 = static_cast<T>(-2.0 * (wpos[3 * i] - ctr[0])), x1 = static_cast<T>(-2.0 * (wpos[3 * i + 1] - ctr[1])),
+            x2 = static_cast<T>(-2.0 * (wpos[3 * i + 2] - ctr[2]));
     for (int col = lane; col < D; col += 32) {
       const T4 fr = frow[col];
       T *Jc = A.J + static_cast<int64_t>(col) * A.ld + row0 + 3 * i;
@@ -1062,6 +1083,18 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
       Jc[2] = fr.z;
       erow[col] += fr.w;
       jtr[col] += static_cast<double>(fr.x) * F0 + static_cast<double>(fr.y) * F1 + static_cast<double>(fr.z) * F2;
+      if (want_stress) { // −2 (x_i − c) ⊗ ∂F_i/∂y: the in-cell part of Σ_pairs d ⊗ ∂f/∂y
+        T2 s0 = srow[3 * col], s1 = srow[3 * col + 1], s2 = srow[3 * col + 2];
+        s0.x += x0 * fr.x;
+        s0.y += x1 * fr.y;
+        s1.x += x2 * fr.z;
+        s1.y += x0 * fr.y;
+        s2.x += x0 * fr.z;
+        s2.y += x1 * fr.z;
+        srow[3 * col] = s0;
+        srow[3 * col + 1] = s1;
+        srow[3 * col + 2] = s2;
+      }
     }
     __syncwarp();
   }
