@@ -786,6 +786,8 @@ template <class T> struct PairRec {
   int j;
 };
 
+constexpr int kPairStep = 4; // pairs whose scatter terms are formed together
+
 template <class T, bool EAM, bool STAGE>
 __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
   using T4 = typename Vec4T<T>::type;
@@ -809,7 +811,7 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
   uint8_t *typ = S.take<uint8_t>(N);
   // per warp: force rows + φ energy as [col] × (x, y, z, e); stress as
   // [col] × 3 pairs (xx,yy)(zz,xy)(xz,yz); energy row; pair records
-  T4 *frow_all = S.take<T4>(static_cast<size_t>(warps) * D);
+  T4 *frow_all = S.take<T4>(static_cast<size_t>(warps) * (D + 1)); // + a spare column
   T2 *srow_all = S.take<T2>(static_cast<size_t>(warps) * 3 * D);
   T *erow_all = S.take<T>(static_cast<size_t>(warps) * D);
   PairRec<T> *recs = S.take<PairRec<T>>(static_cast<size_t>(warps) * 32);
@@ -852,7 +854,7 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
   __syncthreads();
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  T4 *frow = frow_all + static_cast<size_t>(w) * D;
+  T4 *frow = frow_all + static_cast<size_t>(w) * (D + 1);
   T2 *srow = srow_all + static_cast<size_t>(w) * 3 * D;
   T *erow = erow_all + static_cast<size_t>(w) * D;
   double *jtr = jtr_all + static_cast<size_t>(w) * D;
@@ -863,12 +865,14 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
   const T half_we = static_cast<T>(0.5 * A.w_e);
   const bool want_stress = A.w_s > 0.0;
   const int slot = lane / kWin, q = lane % kWin;
+  const int slot_c = slot < 4 ? slot : 3; // lanes 24..31 read slot 3's record and add nothing
+  const bool lane_ok = lane < 4 * kWin;
   const int home = (cd.sx * (2 * cd.sy + 1) + cd.sy) * (2 * cd.sz + 1) + cd.sz; // image (0, 0, 0)
   double ctr[3];                                                                   // cell centre
   for (int a = 0; a < 3; ++a) ctr[a] = 0.5 * (cd.box[3 * a] + cd.box[3 * a + 1] + cd.box[3 * a + 2]);
 
   for (int i = w; i < N; i += warps) {
-    for (int k = lane; k < D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
+    for (int k = lane; k <= D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
     const int ti = typ[i];
     T gFi = T(0), cFi = T(0);
     int wsFi = 0;
@@ -956,68 +960,82 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         for (int a = 0; a < 6; ++a) P[a] += dgj * v[a];
       }
       __syncwarp();
-      // sparse knot-window scatter, one pair at a time, 24 lanes = 4 slots × 6 knots
-      for (int k = 0; k < cnt; ++k) {
-        const PairRec<T> &R = rec[k];
-        if (lane < 4 * kWin) {
-          const int4 si = R.si[slot];
+      // sparse knot-window scatter, 24 lanes = 4 slots × 6 knots per pair.
+      // kPairStep pairs per step: their columns, coefficients and the dense
+      // ρ-chain terms are computed together (independent work), then the
+      // read-modify-writes of the row buffer go one pair at a time (windows
+      // of different pairs may share columns across lanes).  Unused slots add
+      // zero to the spare column D.
+#pragma unroll 1
+      for (int k0 = 0; k0 < cnt; k0 += kPairStep) {
+        int col[kPairStep];
+        T cf[kPairStep], dv[kPairStep];
+        bool st[kPairStep];
+        T4 uvs[kPairStep];
+#pragma unroll
+        for (int u = 0; u < kPairStep; ++u) {
+          const bool live = k0 + u < cnt;
+          const PairRec<T> &R = rec[live ? k0 + u : k0];
+          const int4 si = R.si[slot_c];
           const int e = si.x;
-          const int col = (e != -1 && q < si.z) ? cmap[si.y + q] : -1;
-          if (col >= 0) {
-            const T2 sf = R.sf[slot];
-            const T tt = sf.x;
-            T cf, dv = T(0);
-            if (e >= 0) {
-              const T *G = segg + e * 4 * kWin;
-              const T g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
-              cf = sf.y * (g1 + tt * (T(2) * g2 + T(3) * tt * g3));
-              if (slot == 0) dv = half_we * (G[q] + tt * (g1 + tt * (g2 + tt * g3)));
-            } else {
-              cf = sf.y * dgda[R.j * kWin + q];
-            }
-            const T4 uv = R.uv;
-            T4 fr = frow[col];
-            fr.x += cf * uv.x;
-            fr.y += cf * uv.y;
-            fr.z += cf * uv.z;
-            fr.w += dv;
-            frow[col] = fr;
-            if (si.w) { // stress scatter: pairs that leave the cell only
-              const T4 vv = R.vv;
-              const T v5 = R.vd.x;
-              T2 s0 = srow[3 * col], s1 = srow[3 * col + 1], s2 = srow[3 * col + 2];
-              s0.x += cf * uv.w;
-              s0.y += cf * vv.x;
-              s1.x += cf * vv.y;
-              s1.y += cf * vv.z;
-              s2.x += cf * vv.w;
-              s2.y += cf * v5;
-              srow[3 * col] = s0;
-              srow[3 * col + 1] = s1;
-              srow[3 * col + 2] = s2;
+          const bool ok = live && lane_ok && e != -1 && q < si.z;
+          const int c0 = cmap[ok ? si.y + q : 0];
+          const T2 sf = R.sf[slot_c];
+          const T tt = sf.x;
+          const T *G = segg + (e >= 0 ? e : 0) * 4 * kWin;
+          const T g0 = G[q], g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
+          T base = g1 + tt * (T(2) * g2 + T(3) * tt * g3);
+          if constexpr (EAM)
+            if (e == -2) base = dgda[R.j * kWin + q]; // F window of j: ∂F'_j/∂y_q
+          const bool use = ok && c0 >= 0;
+          col[u] = use ? c0 : D;
+          cf[u] = use ? sf.y * base : T(0);
+          dv[u] = (use && slot == 0) ? half_we * (g0 + tt * (g1 + tt * (g2 + tt * g3))) : T(0);
+          st[u] = use && si.w != 0 && e >= 0;
+          uvs[u] = R.uv;
+          if constexpr (EAM) {
+            // dense ρ-chain: Σ_j F''_j ρ'_{ti}(r) u drho_j[m]
+            const T wgt = live ? R.cFj * R.vd.y : T(0);
+            if (wgt != T(0)) {
+              const T *drj = drho + R.j * dstr;
+#pragma unroll
+              for (int s2 = 0; s2 < 2; ++s2) {
+                const int m = lane + 32 * s2;
+                if (m < nd) {
+                  const T dd = wgt * drj[m];
+                  dacc[s2][0] += dd * uvs[u].x;
+                  dacc[s2][1] += dd * uvs[u].y;
+                  dacc[s2][2] += dd * uvs[u].z;
+                }
+              }
             }
           }
         }
-        __syncwarp();
-      }
-      if constexpr (EAM) {
-        // dense ρ-chain: Σ_j F''_j ρ'_{ti}(r) u drho_j[m]
-        for (int k = 0; k < cnt; ++k) {
-          const PairRec<T> &R = rec[k];
-          const T wgt = R.cFj * R.vd.y;
-          if (wgt == T(0)) continue;
-          const T *drj = drho + R.j * dstr;
-          const T4 uv = R.uv;
-          const T u0 = uv.x, u1 = uv.y, u2 = uv.z;
-          for (int s2 = 0; s2 < 2; ++s2) {
-            const int m = lane + 32 * s2;
-            if (m < nd) {
-              const T dv = wgt * drj[m];
-              dacc[s2][0] += dv * u0;
-              dacc[s2][1] += dv * u1;
-              dacc[s2][2] += dv * u2;
-            }
+#pragma unroll
+        for (int u = 0; u < kPairStep; ++u) {
+          const int cu = col[u];
+          T4 fr = frow[cu];
+          fr.x += cf[u] * uvs[u].x;
+          fr.y += cf[u] * uvs[u].y;
+          fr.z += cf[u] * uvs[u].z;
+          fr.w += dv[u];
+          frow[cu] = fr;
+          if (st[u]) { // stress scatter: pairs that leave the cell only
+            const PairRec<T> &R = rec[k0 + u];
+            const T4 vv = R.vv;
+            const T v5 = R.vd.x, c = cf[u];
+            T2 s0 = srow[3 * cu], s1 = srow[3 * cu + 1], s2 = srow[3 * cu + 2];
+            s0.x += c * uvs[u].w;
+            s0.y += c * vv.x;
+            s1.x += c * vv.y;
+            s1.y += c * vv.z;
+            s2.x += c * vv.w;
+            s2.y += c * v5;
+            srow[3 * cu] = s0;
+            srow[3 * cu + 1] = s1;
+            srow[3 * cu + 2] = s2;
           }
+          __syncwarp();
         }
       }
       __syncwarp();
@@ -1332,7 +1350,7 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   // per-warp buffers + (optionally) the configuration's staged per-atom data;
   // prefer the most warps that fit with staging, else the most without
   auto k2_smem = [&](int wp) {
-    return common + align16(static_cast<size_t>(wp) * D * 4 * sizeof(T)) +
+    return common + align16(static_cast<size_t>(wp) * (D + 1) * 4 * sizeof(T)) +
            align16(static_cast<size_t>(wp) * 3 * D * 2 * sizeof(T)) + align16(static_cast<size_t>(wp) * D * sizeof(T)) +
            align16(static_cast<size_t>(wp) * 32 * sizeof(PairRec<T>)) +
            align16(static_cast<size_t>(wp) * D * sizeof(double)) + 112;
