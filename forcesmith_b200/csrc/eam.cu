@@ -972,6 +972,23 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         T cf[kPairStep], dv[kPairStep];
         bool st[kPairStep];
         T4 uvs[kPairStep];
+        T dval[kPairStep][2], dwgt[kPairStep];
+        if constexpr (EAM) {
+          // the dense ρ-chain's ∂ρ_j/∂y loads go out first; they are used
+          // after the row updates below, which hide their latency
+#pragma unroll
+          for (int u = 0; u < kPairStep; ++u) {
+            const bool live = k0 + u < cnt;
+            const PairRec<T> &R = rec[live ? k0 + u : k0];
+            dwgt[u] = live ? R.cFj * R.vd.y : T(0);
+            const T *drj = drho + R.j * dstr;
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+              const int m = lane + 32 * s2;
+              dval[u][s2] = (m < nd && dwgt[u] != T(0)) ? drj[m] : T(0);
+            }
+          }
+        }
 #pragma unroll
         for (int u = 0; u < kPairStep; ++u) {
           const bool live = k0 + u < cnt;
@@ -993,23 +1010,6 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
           dv[u] = (use && slot == 0) ? half_we * (g0 + tt * (g1 + tt * (g2 + tt * g3))) : T(0);
           st[u] = use && si.w != 0 && e >= 0;
           uvs[u] = R.uv;
-          if constexpr (EAM) {
-            // dense ρ-chain: Σ_j F''_j ρ'_{ti}(r) u drho_j[m]
-            const T wgt = live ? R.cFj * R.vd.y : T(0);
-            if (wgt != T(0)) {
-              const T *drj = drho + R.j * dstr;
-#pragma unroll
-              for (int s2 = 0; s2 < 2; ++s2) {
-                const int m = lane + 32 * s2;
-                if (m < nd) {
-                  const T dd = wgt * drj[m];
-                  dacc[s2][0] += dd * uvs[u].x;
-                  dacc[s2][1] += dd * uvs[u].y;
-                  dacc[s2][2] += dd * uvs[u].z;
-                }
-              }
-            }
-          }
         }
 #pragma unroll
         for (int u = 0; u < kPairStep; ++u) {
@@ -1036,6 +1036,18 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
             srow[3 * cu + 2] = s2;
           }
           __syncwarp();
+        }
+        if constexpr (EAM) {
+          // dense ρ-chain: Σ_j F''_j ρ'_{ti}(r) u drho_j[m]
+#pragma unroll
+          for (int u = 0; u < kPairStep; ++u)
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+              const T dd = dwgt[u] * dval[u][s2];
+              dacc[s2][0] += dd * uvs[u].x;
+              dacc[s2][1] += dd * uvs[u].y;
+              dacc[s2][2] += dd * uvs[u].z;
+            }
         }
       }
       __syncwarp();
