@@ -2,7 +2,8 @@
 // context's own configurations and model, with CUDA events on the context's
 // stream, and keeps the fastest for later calls.
 //   residual          lanes per atom 4, 8, 16, 32
-//   Jacobian          warps per CTA of the force-row kernel 8 … 4 (those that fit)
+//   Jacobian          warps per CTA of the force-row kernel 11, 10, 8, 6, 4 (FP64:
+//                     at most 8; those that fit)
 //   population (FP32) CTA waves 2, 4, 8 of the lanes-per-trial kernel
 // Every candidate computes the same quantities; only summation order (and
 // so the last bits of FP32/FP64 sums) differs between them.
@@ -60,14 +61,18 @@ extern "C" int fs_gpu_autotune(fs_gpu *h, double w_e, double w_s, fs_tune_report
   }
   r.lanes_per_atom = h->lanes_per_atom ? h->lanes_per_atom : h->tuned_lpa;
   if (ep && splines) {
+    static const int k2w[5] = {11, 10, 8, 6, 4};
+    const int max_wp = h->precision == FS_PREC_FP64 ? 8 : 11;
     int best = -1;
     for (int k = 0; k < 5; ++k) {
-      h->tuned_k2_warps = 8 - k;
+      r.jacobian_ms[k] = INFINITY;
+      if (k2w[k] > max_wp) continue;
+      h->tuned_k2_warps = k2w[k];
       r.jacobian_ms[k] = time_ms(h, [&] { return eval_jacobian(h, w_e, w_s); }, 2, &rc);
       FS_TRY(rc);
       if (best < 0 || r.jacobian_ms[k] < r.jacobian_ms[best]) best = k;
     }
-    h->tuned_k2_warps = 8 - best;
+    h->tuned_k2_warps = k2w[best];
     r.k2_warps = h->tuned_k2_warps;
     h->jac_valid = false;
   }

@@ -787,9 +787,12 @@ template <class T> struct PairRec {
 };
 
 constexpr int kPairStep = 4; // pairs whose scatter terms are formed together
+// warps per CTA of the force-row kernel: at most 11 in FP32 (the per-warp row
+// buffers of 11 warps fill the shared memory), 8 in FP64 (registers)
+template <class T> constexpr int kMaxK2Warps = sizeof(T) == 4 ? 11 : 8;
 
 template <class T, bool EAM, bool STAGE>
-__global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
+__global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
   using T4 = typename Vec4T<T>::type;
   using T2 = typename V2T<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -972,14 +975,15 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
         T cf[kPairStep], dv[kPairStep];
         bool st[kPairStep];
         T4 uvs[kPairStep];
-        T dval[kPairStep][2], dwgt[kPairStep];
+        T dval[kPairStep][2], dwgt[kPairStep], fwin[kPairStep];
         if constexpr (EAM) {
-          // the dense ρ-chain's ∂ρ_j/∂y loads go out first; they are used
-          // after the row updates below, which hide their latency
+          // per-atom loads go out first: the F-window terms ∂F'_j/∂y_q (slot 3
+          // lanes) and the dense ρ-chain's ∂ρ_j/∂y, used after the row updates
 #pragma unroll
           for (int u = 0; u < kPairStep; ++u) {
             const bool live = k0 + u < cnt;
             const PairRec<T> &R = rec[live ? k0 + u : k0];
+            fwin[u] = slot_c == 3 ? dgda[R.j * kWin + q] : T(0);
             dwgt[u] = live ? R.cFj * R.vd.y : T(0);
             const T *drj = drho + R.j * dstr;
 #pragma unroll
@@ -1003,7 +1007,7 @@ __global__ void __launch_bounds__(256, 1) jac_forces_kernel(JacArgs<T> A, int wa
           const T g0 = G[q], g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
           T base = g1 + tt * (T(2) * g2 + T(3) * tt * g3);
           if constexpr (EAM)
-            if (e == -2) base = dgda[R.j * kWin + q]; // F window of j: ∂F'_j/∂y_q
+            if (e == -2) base = fwin[u]; // F window of j: ∂F'_j/∂y_q
           const bool use = ok && c0 >= 0;
           col[u] = use ? c0 : D;
           cf[u] = use ? sf.y * base : T(0);
@@ -1371,8 +1375,9 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   const size_t cap = 227 * 1024;
   int warps = 0;
   size_t sm2 = 0;
+  const int max_wp = kMaxK2Warps<T>;
   if (h->tuned_k2_warps > 0) {
-    const int wp = h->tuned_k2_warps;
+    const int wp = std::min(h->tuned_k2_warps, max_wp);
     if (eam && k2_smem(wp) + stage_b <= cap) {
       warps = wp;
       sm2 = k2_smem(wp) + stage_b;
@@ -1383,13 +1388,13 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
     }
   }
   if (eam)
-    for (int wp = 8; wp >= 4 && !warps; --wp)
+    for (int wp = max_wp; wp >= 4 && !warps; --wp)
       if (k2_smem(wp) + stage_b <= cap) {
         warps = wp;
         sm2 = k2_smem(wp) + stage_b;
         a.stage = 1;
       }
-  for (int wp = 8; wp >= 1 && !warps; --wp)
+  for (int wp = max_wp; wp >= 1 && !warps; --wp)
     if (k2_smem(wp) <= cap) {
       warps = wp;
       sm2 = k2_smem(wp);

@@ -250,7 +250,7 @@ int fs_gpu_eval_population(fs_gpu *h, double w_e, double w_s, const double *xs,
 typedef struct fs_tune_report {
     int32_t lanes_per_atom, k2_warps, pop_waves, reserved;
     double residual_ms[4];    /* lanes 4, 8, 16, 32 */
-    double jacobian_ms[5];    /* warps 8, 7, 6, 5, 4 */
+    double jacobian_ms[5];    /* warps 11, 10, 8, 6, 4 (infinite: not tried) */
     double population_ms[3];  /* waves 2, 4, 8 */
 } fs_tune_report;
 

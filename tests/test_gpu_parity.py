@@ -370,7 +370,7 @@ def test_autotune_keeps_results(ternary_small, precision):
     pb = g.eval_population(xs, 1.0, 0.1)
     rep = g.autotune(1.0, 0.1)
     assert rep["lanes_per_atom"] in (4, 8, 16, 32)
-    assert rep["k2_warps"] in (4, 5, 6, 7, 8)
+    assert rep["k2_warps"] in ((4, 6, 8) if precision == "fp64" else (4, 6, 8, 10, 11))
     assert rep["pop_waves"] in ((2, 4, 8) if precision == "fp32" else (0,))
     after = g.eval(1.0, 0.1)
     ja = g.jacobian(1.0, 0.1, want_J=False)
