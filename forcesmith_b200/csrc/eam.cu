@@ -670,11 +670,20 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
       rho += seg_val<T>(seg[e], t);
       const int ws = segws[e];
       const T *G = segg + e * 4 * kWin;
-      for (int q = 0; q < kWin && ws + q < tb.n; ++q) {
-        const int col = cmap[tb.cmap0 + ws + q];
-        if (col < 0) continue;
-        dr[col - A.dens_c0] += G[q] + t * (G[kWin + q] + t * (G[2 * kWin + q] + t * G[3 * kWin + q]));
+      // the window's knots are distinct columns: load all, add, store all
+      // (knots past the table's end and fixed knots add zero to the pad column nd)
+      int m[kWin];
+      T add[kWin], cur[kWin];
+#pragma unroll
+      for (int q = 0; q < kWin; ++q) {
+        const int col = ws + q < tb.n ? cmap[tb.cmap0 + ws + q] : -1;
+        m[q] = col >= 0 ? col - A.dens_c0 : nd;
+        add[q] = col >= 0 ? G[q] + t * (G[kWin + q] + t * (G[2 * kWin + q] + t * G[3 * kWin + q])) : T(0);
       }
+#pragma unroll
+      for (int q = 0; q < kWin; ++q) cur[q] = dr[m[q]];
+#pragma unroll
+      for (int q = 0; q < kWin; ++q) dr[m[q]] = cur[q] + add[q];
     }
     const int ti = typ[i];
     const STab<T> &te = tabs[np + nt + ti];
