@@ -1118,12 +1118,19 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     const double F0 = A.F[row0 + 3 * i], F1 = A.F[row0 + 3 * i + 1], F2 = A.F[row0 + 3 * i + 2];
     const T x0 = static_cast<T>(-2.0 * (wpos[3 * i] - ctr[0])), x1 = static_cast<T>(-2.0 * (wpos[3 * i + 1] - ctr[1])),
             x2 = static_cast<T>(-2.0 * (wpos[3 * i + 2] - ctr[2]));
+    // the atom's 3 rows of a column in two stores: a pair on its even row
+    // (ld is a multiple of 32, so the row parity is the address parity)
+    const bool even = ((row0 + 3 * i) & 1) == 0;
     for (int col = lane; col < D; col += 32) {
       const T4 fr = frow[col];
       T *Jc = A.J + static_cast<int64_t>(col) * A.ld + row0 + 3 * i;
-      Jc[0] = fr.x;
-      Jc[1] = fr.y;
-      Jc[2] = fr.z;
+      if (even) {
+        *reinterpret_cast<T2 *>(Jc) = T2{fr.x, fr.y};
+        Jc[2] = fr.z;
+      } else {
+        Jc[0] = fr.x;
+        *reinterpret_cast<T2 *>(Jc + 1) = T2{fr.y, fr.z};
+      }
       erow[col] += fr.w;
       jtr[col] += static_cast<double>(fr.x) * F0 + static_cast<double>(fr.y) * F1 + static_cast<double>(fr.z) * F2;
       if (want_stress) { // −2 (x_i − c) ⊗ ∂F_i/∂y: the in-cell part of Σ_pairs d ⊗ ∂f/∂y
