@@ -606,6 +606,12 @@ template <class T> size_t jac_common_smem(int n_tables, int n_segs, int n_cmap, 
 
 // Shared-memory copy of the per-atom Jacobian data of one configuration
 // (row stride ndens + 1 keeps a warp's column reads on distinct banks).
+// The per-atom scalars alone (F', F'', embedding window start, ∂F'/∂y window).
+template <class T> size_t atom_scalar_stage_smem(int max_atoms) {
+  return 3 * align16(max_atoms * sizeof(T)) + align16(max_atoms * sizeof(int32_t)) +
+         align16(static_cast<size_t>(max_atoms) * kWin * sizeof(T)) + 80;
+}
+
 template <class T> size_t atom_stage_smem(int max_atoms, int ndens) {
   return align16(static_cast<size_t>(max_atoms) * (ndens + 1) * sizeof(T)) +
          3 * align16(max_atoms * sizeof(T)) + align16(max_atoms * sizeof(int32_t)) +
@@ -800,7 +806,7 @@ constexpr int kPairStep = 4; // pairs whose scatter terms are formed together
 // buffers of 11 warps fill the shared memory), 8 in FP64 (registers)
 template <class T> constexpr int kMaxK2Warps = sizeof(T) == 4 ? 11 : 8;
 
-template <class T, bool EAM, bool STAGE>
+template <class T, bool EAM, int STAGE>
 __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
   using T4 = typename Vec4T<T>::type;
   using T2 = typename V2T<T>::type;
@@ -832,25 +838,28 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   int dstr = nd;
   const T *gFa = A.gF + cd.atom0, *cFa = A.cF + cd.atom0, *dgda = A.dgd + static_cast<int64_t>(cd.atom0) * kWin;
   const int32_t *wsFa = A.wsF + cd.atom0;
-  // STAGE: the configuration's per-atom data comes from shared memory (the
-  // pointers below then address the shared window only)
-  if constexpr (EAM && STAGE) {
+  // STAGE 1: the configuration's per-atom scalars and ∂F'/∂y windows come
+  // from shared memory; STAGE 2: also the ∂ρ/∂y rows (the pointers below then
+  // address the shared window only)
+  if constexpr (EAM && STAGE == 2) {
     T *s_dr = S.take<T>(static_cast<size_t>(N) * (nd + 1));
+    for (int k = threadIdx.x; k < N * nd; k += blockDim.x) s_dr[(k / nd) * (nd + 1) + k % nd] = drho[k];
+    drho = s_dr;
+    dstr = nd + 1;
+  }
+  if constexpr (EAM && STAGE >= 1) {
     T *s_gf = S.take<T>(N);
     T *s_cf = S.take<T>(N);
     T *s_pad = S.take<T>(N);
     int32_t *s_ws = S.take<int32_t>(N);
     T *s_dgd = S.take<T>(static_cast<size_t>(N) * kWin);
     (void)s_pad;
-    for (int k = threadIdx.x; k < N * nd; k += blockDim.x) s_dr[(k / nd) * (nd + 1) + k % nd] = drho[k];
     for (int k = threadIdx.x; k < N; k += blockDim.x) {
       s_gf[k] = gFa[k];
       s_cf[k] = cFa[k];
       s_ws[k] = wsFa[k];
     }
     for (int k = threadIdx.x; k < N * kWin; k += blockDim.x) s_dgd[k] = dgda[k];
-    drho = s_dr;
-    dstr = nd + 1;
     gFa = s_gf;
     cFa = s_cf;
     wsFa = s_ws;
@@ -1387,37 +1396,36 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
            align16(static_cast<size_t>(wp) * 32 * sizeof(PairRec<T>)) +
            align16(static_cast<size_t>(wp) * D * sizeof(double)) + 112;
   };
-  const size_t stage_b = eam ? atom_stage_smem<T>(h->max_natoms, ndens) : 0;
+  // staging levels (EAM): 2 = per-atom scalars + ∂ρ/∂y rows, 1 = scalars only
+  const size_t stage_sz[3] = {0, eam ? atom_scalar_stage_smem<T>(h->max_natoms) : 0,
+                              eam ? atom_scalar_stage_smem<T>(h->max_natoms) +
+                                        align16(static_cast<size_t>(h->max_natoms) * (ndens + 1) * sizeof(T)) + 16
+                                  : 0};
   const size_t cap = 227 * 1024;
   int warps = 0;
   size_t sm2 = 0;
   const int max_wp = kMaxK2Warps<T>;
-  if (h->tuned_k2_warps > 0) {
-    const int wp = std::min(h->tuned_k2_warps, max_wp);
-    if (eam && k2_smem(wp) + stage_b <= cap) {
-      warps = wp;
-      sm2 = k2_smem(wp) + stage_b;
-      a.stage = 1;
-    } else if (k2_smem(wp) <= cap) {
-      warps = wp;
-      sm2 = k2_smem(wp);
-    }
-  }
-  if (eam)
-    for (int wp = max_wp; wp >= 4 && !warps; --wp)
-      if (k2_smem(wp) + stage_b <= cap) {
+  // the given warp count with the most staging that fits
+  auto fit = [&](int wp) {
+    for (int lv = eam ? 2 : 0; lv >= 0; --lv)
+      if (k2_smem(wp) + stage_sz[lv] <= cap) {
         warps = wp;
-        sm2 = k2_smem(wp) + stage_b;
-        a.stage = 1;
+        sm2 = k2_smem(wp) + stage_sz[lv];
+        a.stage = lv;
+        return true;
       }
-  for (int wp = max_wp; wp >= 1 && !warps; --wp)
-    if (k2_smem(wp) <= cap) {
-      warps = wp;
-      sm2 = k2_smem(wp);
-    }
+    return false;
+  };
+  if (h->tuned_k2_warps > 0) fit(std::min(h->tuned_k2_warps, max_wp));
+  if (eam) // untuned: the most warps with full staging, else the most warps
+    for (int wp = max_wp; wp >= 4 && !warps; --wp)
+      if (k2_smem(wp) + stage_sz[2] <= cap) fit(wp);
+  for (int wp = max_wp; wp >= 1 && !warps; --wp) fit(wp);
   if (warps < 1) return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: configuration too large");
-  auto k2 = eam ? (a.stage ? jac_forces_kernel<T, true, true> : jac_forces_kernel<T, true, false>)
-                : jac_forces_kernel<T, false, false>;
+  auto k2 = eam ? (a.stage == 2   ? jac_forces_kernel<T, true, 2>
+                   : a.stage == 1 ? jac_forces_kernel<T, true, 1>
+                                  : jac_forces_kernel<T, true, 0>)
+                : jac_forces_kernel<T, false, 0>;
   FS_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm2)));
   k2<<<h->n_cfg, 32 * warps, sm2, h->stream>>>(a, warps);
   FS_CUDA(cudaGetLastError());
