@@ -834,6 +834,8 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   T *erow_all = S.take<T>(static_cast<size_t>(warps) * D);
   PairRec<T> *recs = S.take<PairRec<T>>(static_cast<size_t>(warps) * 32);
   double *jtr_all = S.take<double>(static_cast<size_t>(warps) * D);
+  int32_t *s_start = S.take<int32_t>(N + 1); // the configuration's neighbour offsets
+  for (int k = threadIdx.x; k <= N; k += blockDim.x) s_start[k] = A.c.nb_start[cd.atom0 + k];
   const T *drho = A.drho + static_cast<int64_t>(cd.atom0) * nd;
   int dstr = nd;
   const T *gFa = A.gF + cd.atom0, *cFa = A.cF + cd.atom0, *dgda = A.dgd + static_cast<int64_t>(cd.atom0) * kWin;
@@ -880,7 +882,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   T *erow = erow_all + static_cast<size_t>(w) * D;
   double *jtr = jtr_all + static_cast<size_t>(w) * D;
   PairRec<T> *rec = recs + w * 32;
-  const int32_t *start = A.c.nb_start + cd.atom0;
+  const int32_t *start = s_start;
   const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
   const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
   const T half_we = static_cast<T>(0.5 * A.w_e);
@@ -892,6 +894,14 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   double ctr[3];                                                                   // cell centre
   for (int a = 0; a < 3; ++a) ctr[a] = 0.5 * (cd.box[3 * a] + cd.box[3 * a + 1] + cd.box[3 * a + 2]);
 
+  // each chunk's packed neighbour entries are loaded one chunk ahead
+  int pre_p0 = -1;
+  uint32_t pk_next = 0;
+  auto prefetch = [&](int p, int end) {
+    pre_p0 = p;
+    pk_next = lane < end - p ? A.c.nb_pack[p + lane] : 0u;
+  };
+  if (w < N) prefetch(start[w], start[w + 1]);
   for (int i = w; i < N; i += warps) {
     for (int k = lane; k <= D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
     const int ti = typ[i];
@@ -907,11 +917,22 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     __syncwarp();
     for (int p0 = start[i]; p0 < start[i + 1]; p0 += 32) {
       const int cnt = min(32, start[i + 1] - p0);
+      uint32_t pk_cur = pk_next;
+      if (pre_p0 != p0) pk_cur = lane < cnt ? A.c.nb_pack[p0 + lane] : 0u; // (after an atom without pairs)
+      {
+        int np0 = p0 + 32, nend = start[i + 1];
+        if (np0 >= nend) {
+          const int in = i + warps;
+          np0 = in < N ? start[in] : 0;
+          nend = in < N ? start[in + 1] : 0;
+        }
+        prefetch(np0, nend);
+      }
       if (lane < cnt) {
         PairRec<T> R;
         int j;
         T d[3];
-        const uint32_t pk = A.c.nb_pack[p0 + lane];
+        const uint32_t pk = pk_cur;
         pair_vec(wpos, shift, i, pk, j, d[0], d[1], d[2]);
         const T r = sqrt_t(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         const int tj = typ[j];
@@ -1394,7 +1415,8 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
     return common + align16(static_cast<size_t>(wp) * (D + 1) * 4 * sizeof(T)) +
            align16(static_cast<size_t>(wp) * 3 * D * 2 * sizeof(T)) + align16(static_cast<size_t>(wp) * D * sizeof(T)) +
            align16(static_cast<size_t>(wp) * 32 * sizeof(PairRec<T>)) +
-           align16(static_cast<size_t>(wp) * D * sizeof(double)) + 112;
+           align16(static_cast<size_t>(wp) * D * sizeof(double)) +
+           align16(static_cast<size_t>(h->max_natoms + 1) * sizeof(int32_t)) + 112;
   };
   // staging levels (EAM): 2 = per-atom scalars + ∂ρ/∂y rows, 1 = scalars only
   const size_t stage_sz[3] = {0, eam ? atom_scalar_stage_smem<T>(h->max_natoms) : 0,
