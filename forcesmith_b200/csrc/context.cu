@@ -224,6 +224,10 @@ int fs_gpu_destroy(fs_gpu *h) {
   dfree(h->d_seg_a);
   dfree(h->d_seg_g);
   dfree(h->d_seg_ws);
+  dfree(h->d_spl);
+  if (h->h_vals_pin) cudaFreeHost(h->h_vals_pin);
+  if (h->h_ne_pin) cudaFreeHost(h->h_ne_pin);
+  if (h->vals_ev) cudaEventDestroy(h->vals_ev);
   dfree(h->d_x);
   dfree(h->d_chol);
   dfree(h->d_dx);
@@ -501,7 +505,7 @@ int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D) {
   for (HostTable &t : h->tables)
     for (int k = 0; k < t.n; ++k)
       if (t.cols[k] >= 0) t.v[k] = x[t.cols[k]];
-  FS_TRY(upload_tables(h));
+  FS_TRY(upload_values(h));
   h->params_dirty = true;
   h->jac_valid = false;
   // A larger cutoff (SW a1/a2) needs longer lists; a smaller one does not:
@@ -565,11 +569,24 @@ int fs_gpu_fetch_normal_equations(fs_gpu *h, double *JtJ, double *Jtr, double *o
   if (!h) return FS_ERR_ARG;
   if (!h->jac_valid) return set_error(h, FS_ERR_STATE, "no Jacobian evaluated");
   cudaSetDevice(h->device);
-  const size_t D = h->D;
-  if (JtJ) FS_CUDA(cudaMemcpyAsync(JtJ, h->d_JtJ, D * D * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (Jtr) FS_CUDA(cudaMemcpyAsync(Jtr, h->d_Jtr, D * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (obj) FS_CUDA(cudaMemcpyAsync(obj, h->d_obj, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  return sync(h);
+  const size_t D = h->D, n = D * D + D + 1;
+  // one DMA per part into a pinned buffer, one wait, then host copies
+  if (h->h_ne_pin_n < n) {
+    if (h->h_ne_pin) cudaFreeHost(h->h_ne_pin);
+    h->h_ne_pin = nullptr;
+    h->h_ne_pin_n = 0;
+    FS_CUDA(cudaMallocHost(&h->h_ne_pin, n * sizeof(double)));
+    h->h_ne_pin_n = n;
+  }
+  double *pin = h->h_ne_pin;
+  if (JtJ) FS_CUDA(cudaMemcpyAsync(pin, h->d_JtJ, D * D * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (Jtr) FS_CUDA(cudaMemcpyAsync(pin + D * D, h->d_Jtr, D * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (obj) FS_CUDA(cudaMemcpyAsync(pin + D * D + D, h->d_obj, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  FS_TRY(sync(h));
+  if (JtJ) std::memcpy(JtJ, pin, D * D * sizeof(double));
+  if (Jtr) std::memcpy(Jtr, pin + D * D, D * sizeof(double));
+  if (obj) *obj = pin[D * D + D];
+  return FS_OK;
 }
 
 int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F, double *J, double *JtJ,

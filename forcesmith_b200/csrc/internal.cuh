@@ -150,6 +150,13 @@ struct fs_gpu {
   int32_t *d_seg_ws = nullptr;   // [n_segs]
   double *d_x = nullptr;         // current parameter vector (D)
   bool params_dirty = true;
+  int32_t *d_spl = nullptr;      // indices of the spline tables (segment setup)
+  int n_spl = 0;
+  // pinned host staging: parameter values going up, normal equations coming
+  // back (one DMA each, no pageable staging); vals_ev marks the last upload
+  double *h_vals_pin = nullptr, *h_ne_pin = nullptr;
+  size_t h_vals_pin_n = 0, h_ne_pin_n = 0;
+  cudaEvent_t vals_ev = nullptr;
 
   // evaluation buffers
   int64_t rows_alloc = 0;
@@ -230,6 +237,7 @@ int build_neighbors(fs_gpu *h, double rcut);
 
 // tables.cu
 int upload_tables(fs_gpu *h);          // structure + values (after set_model)
+int upload_values(fs_gpu *h);          // values only (after set_params), asynchronous
 int refresh_segments(fs_gpu *h);       // recompute segment data from d_vals
 double model_max_cutoff(const fs_gpu *h);
 

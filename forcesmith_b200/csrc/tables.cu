@@ -265,29 +265,57 @@ int upload_tables(fs_gpu *h) {
                           h->stream));
   FS_CUDA(cudaMemcpyAsync(h->d_vals, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice,
                           h->stream));
+  std::vector<int32_t> spl;
+  for (int t = 0; t < nt; ++t)
+    if (desc[t].kind == FS_TABLE_SPLINE) spl.push_back(t);
+  if (h->d_spl) cudaFree(h->d_spl);
+  h->d_spl = nullptr;
+  h->n_spl = static_cast<int>(spl.size());
+  if (!spl.empty()) {
+    FS_CUDA(cudaMalloc(&h->d_spl, spl.size() * sizeof(int32_t)));
+    FS_CUDA(cudaMemcpyAsync(h->d_spl, spl.data(), spl.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            h->stream));
+  }
   FS_CUDA(cudaStreamSynchronize(h->stream));
   return FS_OK;
 }
 
+// New values of an unchanged model: one copy from a pinned buffer, ordered on
+// the context's stream, no host wait (unless the previous upload from the
+// buffer is still in flight).
+int upload_values(fs_gpu *h) {
+  size_t n = 0;
+  for (const HostTable &ht : h->tables) n += ht.v.size();
+  if (!h->d_vals || static_cast<int>(n) != h->n_vals) return upload_tables(h);
+  if (h->h_vals_pin_n < n) {
+    if (h->h_vals_pin) cudaFreeHost(h->h_vals_pin);
+    h->h_vals_pin = nullptr;
+    h->h_vals_pin_n = 0;
+    FS_CUDA(cudaMallocHost(&h->h_vals_pin, std::max<size_t>(n, 1) * sizeof(double)));
+    h->h_vals_pin_n = n;
+  }
+  if (!h->vals_ev) FS_CUDA(cudaEventCreateWithFlags(&h->vals_ev, cudaEventDisableTiming));
+  FS_CUDA(cudaEventSynchronize(h->vals_ev));
+  size_t k = 0;
+  for (const HostTable &ht : h->tables)
+    for (double v : ht.v) h->h_vals_pin[k++] = v;
+  FS_CUDA(cudaMemcpyAsync(h->d_vals, h->h_vals_pin, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  FS_CUDA(cudaEventRecord(h->vals_ev, h->stream));
+  return FS_OK;
+}
+
 int refresh_segments(fs_gpu *h) {
-  std::vector<int> spl;
-  for (int t = 0; t < static_cast<int>(h->desc.size()); ++t)
-    if (h->desc[t].kind == FS_TABLE_SPLINE) spl.push_back(t);
-  if (spl.empty()) return FS_OK;
-  int *d_spl = nullptr;
-  FS_CUDA(cudaMallocAsync(&d_spl, spl.size() * sizeof(int), h->stream));
-  FS_CUDA(cudaMemcpyAsync(d_spl, spl.data(), spl.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if (h->n_spl == 0) return FS_OK;
   if (h->precision == FS_PREC_FP64)
-    spline_setup_kernel<double><<<static_cast<int>(spl.size()), 128, 0, h->stream>>>(
-        h->d_desc, d_spl, h->d_vals, static_cast<double *>(h->d_seg_a), static_cast<double *>(h->d_seg_g),
+    spline_setup_kernel<double><<<h->n_spl, 128, 0, h->stream>>>(
+        h->d_desc, h->d_spl, h->d_vals, static_cast<double *>(h->d_seg_a), static_cast<double *>(h->d_seg_g),
         h->d_seg_ws);
   else
-    spline_setup_kernel<float><<<static_cast<int>(spl.size()), 128, 0, h->stream>>>(
-        h->d_desc, d_spl, h->d_vals, static_cast<float *>(h->d_seg_a), static_cast<float *>(h->d_seg_g),
+    spline_setup_kernel<float><<<h->n_spl, 128, 0, h->stream>>>(
+        h->d_desc, h->d_spl, h->d_vals, static_cast<float *>(h->d_seg_a), static_cast<float *>(h->d_seg_g),
         h->d_seg_ws);
   FS_CUDA(cudaGetLastError());
   ++h->launches;
-  FS_CUDA(cudaFreeAsync(d_spl, h->stream));
   return FS_OK;
 }
 
