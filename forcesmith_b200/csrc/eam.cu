@@ -887,9 +887,12 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
   const T half_we = static_cast<T>(0.5 * A.w_e);
   const bool want_stress = A.w_s > 0.0;
-  const int slot = lane / kWin, q = lane % kWin;
-  const int slot_c = slot < 4 ? slot : 3; // lanes 24..31 read slot 3's record and add nothing
-  const bool lane_ok = lane < 4 * kWin;
+  // scatter lanes: lane = slot × 8 + knot, knots 6, 7 idle, so each 8-lane
+  // phase of a 128-bit row-buffer access covers one window's consecutive
+  // columns (distinct banks); idle lanes address knot 0 and add nothing
+  const int slot = lane >> 3, q = (lane & 7) < kWin ? (lane & 7) : 0;
+  const int slot_c = slot;
+  const bool lane_ok = (lane & 7) < kWin;
   const int home = (cd.sx * (2 * cd.sy + 1) + cd.sy) * (2 * cd.sz + 1) + cd.sz; // image (0, 0, 0)
   double ctr[3];                                                                   // cell centre
   for (int a = 0; a < 3; ++a) ctr[a] = 0.5 * (cd.box[3 * a] + cd.box[3 * a + 1] + cd.box[3 * a + 2]);
