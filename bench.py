@@ -539,6 +539,8 @@ def run_ours(args):
                         "(JtJ, Jtr, objective to host)"},
         "gpu_launches": int(launches),
         "phases_ms": {k: round(v, 5) for k, v in per.items()},
+        "phases_note": "stream-ordered phase boundaries of one step; the residual runs on a side stream "
+                       "beside jac_atoms, so its time falls inside jac_atoms / jac_forces",
         "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                      "frac": achieved / peak, "peak_source": src, "traffic": None,
                      "algorithmic": alg},

@@ -239,6 +239,12 @@ int fs_gpu_destroy(fs_gpu *h) {
   dfree(h->d_pop_obj);
   dfree(h->d_err);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
+  if (h->side) {
+    cudaStreamSynchronize(h->side);
+    cudaStreamDestroy(h->side);
+    cudaEventDestroy(h->ev_fork);
+    cudaEventDestroy(h->ev_join);
+  }
   cudaStreamDestroy(h->stream);
   delete h;
   return FS_OK;
@@ -553,9 +559,35 @@ int fs_gpu_eval_jacobian_async(fs_gpu *h, double w_e, double w_s) {
   FS_TRY(ensure_eval_buffers(h, w_s));
   FS_TRY(ensure_params(h));
   mark(h, 0);
-  FS_TRY(eval_residual(h, w_e, w_s));
+  // spline EAM / pair: the residual and the per-atom Jacobian pass read the
+  // same inputs and write disjoint buffers, so the residual runs on a side
+  // stream beside it; the force-row pass waits for it (it reads F)
+  bool side = h->family == FS_FAMILY_EAM || h->family == FS_FAMILY_PAIR;
+  for (const HostTable &t : h->tables) side = side && t.kind == FS_TABLE_SPLINE;
+  if (side) {
+    if (!h->side) {
+      FS_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+      FS_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+      FS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
+    FS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+    FS_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    std::swap(h->stream, h->side); // the residual's launches go to the side stream
+    const int rc = eval_residual(h, w_e, w_s);
+    std::swap(h->stream, h->side);
+    FS_TRY(rc);
+    FS_CUDA(cudaEventRecord(h->ev_join, h->side));
+    h->join_pending = true;
+  } else {
+    FS_TRY(eval_residual(h, w_e, w_s));
+  }
   mark(h, 1);
-  FS_TRY(eval_jacobian(h, w_e, w_s));
+  const int rcj = eval_jacobian(h, w_e, w_s);
+  if (h->join_pending) { // not consumed (an error path): keep the stream order
+    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+    h->join_pending = false;
+  }
+  FS_TRY(rcj);
   FS_TRY(gram(h, rows_of(h, w_s), h->d_JtJ, h->d_Jtr));
   mark(h, 4);
   if (h->prof_slots > 0 && h->prof_used < h->prof_slots) ++h->prof_used;

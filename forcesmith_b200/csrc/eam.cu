@@ -1412,6 +1412,10 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
     ++h->launches;
   }
   mark(h, 2);
+  if (h->join_pending) { // the residual (side stream) must be done: F feeds Jᵀr here
+    FS_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    h->join_pending = false;
+  }
   // per-warp buffers + (optionally) the configuration's staged per-atom data;
   // prefer the most warps that fit with staging, else the most without
   auto k2_smem = [&](int wp) {

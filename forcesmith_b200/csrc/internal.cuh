@@ -106,6 +106,11 @@ struct fs_gpu {
   int precision = FS_PREC_FP32;
   int lanes_per_atom = 0;
   cudaStream_t stream = nullptr;
+  // side stream of a Jacobian step: the residual runs there beside the
+  // per-atom Jacobian pass; the force-row pass waits for ev_join
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool join_pending = false;
   std::string err;
 
   // configs (host)
