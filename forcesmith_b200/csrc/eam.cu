@@ -789,9 +789,11 @@ template <> struct V2T<double> { using type = double2; };
 // integers with one 128-bit load and (t, weight) with one 64/128-bit load.
 template <class T> struct PairRec {
   // per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window):
-  // extended segment (−1: no contribution; −2: F window), column-map index
-  // of the window's first knot, valid knots in the window, 1 if the pair
-  // leaves the cell and stress is wanted
+  // offset of the segment's knot-derivative block (4 × kWin coefficients),
+  // column-map index of the window's first knot (0, the map's leading block
+  // of −1, when the slot adds nothing; knots past the table's end read the
+  // −1 padding after it), unused, 1 if the pair leaves the cell and stress
+  // is wanted
   int4 si[4];
   typename V2T<T>::type sf[4]; // local coordinate t; weight × the table's 1/h (F window: ρ'_{ti}(r))
   typename Vec4T<T>::type uv;  // u_x, u_y, u_z, v_xx     (v = s ⊗ u for pairs that leave the
@@ -943,7 +945,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
         const int cross = want_stress && img != home; // the pair leaves the cell: image shift s ≠ 0
         R.j = j;
         for (int s = 0; s < 4; ++s) {
-          R.si[s] = make_int4(-1, 0, 0, 0);
+          R.si[s] = make_int4(0, 0, 0, 0);
           R.sf[s].x = R.sf[s].y = T(0);
         }
         T dgi = T(0), cFj = T(0), u[3] = {0, 0, 0}, v[6] = {0, 0, 0, 0, 0, 0};
@@ -964,7 +966,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt, T &tout) {
             T t;
             const int e = seg_of(tb, rr, t);
-            R.si[s] = make_int4(e, tb.cmap0 + segws[e], tb.n - segws[e], cross);
+            R.si[s] = make_int4(e * 4 * kWin, tb.cmap0 + segws[e], 0, cross);
             R.sf[s].x = t;
             R.sf[s].y = wgt * tb.inv_h;
             tout = t;
@@ -991,7 +993,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
             // F_j window: coefficient dgd_j[q]·ρ'_{ti}(r)
             const STab<T> &te = tabs[np + nt + tj];
             const int wsj = wsFa[j];
-            R.si[3] = make_int4(-2, te.cmap0 + wsj, te.n - wsj, 0);
+            R.si[3] = make_int4(0, te.cmap0 + wsj, 0, 0);
             R.sf[3].y = dgi;
           }
         }
@@ -1040,21 +1042,19 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           const bool live = k0 + u < cnt;
           const PairRec<T> &R = rec[live ? k0 + u : k0];
           const int4 si = R.si[slot_c];
-          const int e = si.x;
-          const bool ok = live && lane_ok && e != -1 && q < si.z;
-          const int c0 = cmap[ok ? si.y + q : 0];
+          const int c0 = cmap[si.y + q]; // −1: no term (padding, fixed knot, unused slot)
           const T2 sf = R.sf[slot_c];
           const T tt = sf.x;
-          const T *G = segg + (e >= 0 ? e : 0) * 4 * kWin;
+          const T *G = segg + si.x;
           const T g0 = G[q], g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
           T base = g1 + tt * (T(2) * g2 + T(3) * tt * g3);
           if constexpr (EAM)
-            if (e == -2) base = fwin[u]; // F window of j: ∂F'_j/∂y_q
-          const bool use = ok && c0 >= 0;
+            if (slot_c == 3) base = fwin[u]; // F window of j: ∂F'_j/∂y_q
+          const bool use = live && lane_ok && c0 >= 0;
           col[u] = use ? c0 : D;
           cf[u] = use ? sf.y * base : T(0);
           dv[u] = (use && slot == 0) ? half_we * (g0 + tt * (g1 + tt * (g2 + tt * g3))) : T(0);
-          st[u] = use && si.w != 0 && e >= 0;
+          st[u] = use && si.w != 0;
           uvs[u] = R.uv;
         }
 #pragma unroll

@@ -206,7 +206,10 @@ __global__ void spline_setup_kernel(const TableDesc *__restrict__ desc, const in
 int upload_tables(fs_gpu *h) {
   const int nt = static_cast<int>(h->tables.size());
   std::vector<TableDesc> desc(nt);
-  std::vector<int32_t> cmap;
+  // column map: a leading block of kWin entries −1 (a window that adds
+  // nothing reads there), then each table's knots followed by kWin entries −1
+  // (a window that runs past the table's last knot reads −1 there)
+  std::vector<int32_t> cmap(kWin, -1);
   std::vector<double> vals;
   int segs = 0;
   for (int t = 0; t < nt; ++t) {
@@ -237,6 +240,7 @@ int upload_tables(fs_gpu *h) {
       d.h = d.inv_h = 1.0;
     }
     cmap.insert(cmap.end(), ht.cols.begin(), ht.cols.end());
+    cmap.insert(cmap.end(), kWin, -1);
     vals.insert(vals.end(), ht.v.begin(), ht.v.end());
   }
   if (segs > kMaxSegs) return set_error(h, FS_ERR_UNSUPPORTED, "model has too many spline segments");
