@@ -204,7 +204,16 @@ int fs_gpu_create(const fs_gpu_opts *opts, fs_gpu **out) {
     return FS_ERR_CUDA;
   }
   if (cudaSetDevice(h->device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->vals_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->vals_ev) cudaEventDestroy(h->vals_ev);
     delete h;
     return FS_ERR_CUDA;
   }
@@ -565,11 +574,6 @@ int fs_gpu_eval_jacobian_async(fs_gpu *h, double w_e, double w_s) {
   bool side = h->family == FS_FAMILY_EAM || h->family == FS_FAMILY_PAIR;
   for (const HostTable &t : h->tables) side = side && t.kind == FS_TABLE_SPLINE;
   if (side) {
-    if (!h->side) {
-      FS_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
-      FS_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
-      FS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-    }
     FS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
     FS_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
     std::swap(h->stream, h->side); // the residual's launches go to the side stream
@@ -603,13 +607,7 @@ int fs_gpu_fetch_normal_equations(fs_gpu *h, double *JtJ, double *Jtr, double *o
   cudaSetDevice(h->device);
   const size_t D = h->D, n = D * D + D + 1;
   // one DMA per part into a pinned buffer, one wait, then host copies
-  if (h->h_ne_pin_n < n) {
-    if (h->h_ne_pin) cudaFreeHost(h->h_ne_pin);
-    h->h_ne_pin = nullptr;
-    h->h_ne_pin_n = 0;
-    FS_CUDA(cudaMallocHost(&h->h_ne_pin, n * sizeof(double)));
-    h->h_ne_pin_n = n;
-  }
+  FS_TRY(ensure_pinned(h, &h->h_ne_pin, &h->h_ne_pin_n, n));
   double *pin = h->h_ne_pin;
   if (JtJ) FS_CUDA(cudaMemcpyAsync(pin, h->d_JtJ, D * D * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (Jtr) FS_CUDA(cudaMemcpyAsync(pin + D * D, h->d_Jtr, D * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -243,6 +243,7 @@ int build_neighbors(fs_gpu *h, double rcut);
 // tables.cu
 int upload_tables(fs_gpu *h);          // structure + values (after set_model)
 int upload_values(fs_gpu *h);          // values only (after set_params), asynchronous
+int ensure_pinned(fs_gpu *h, double **buf, size_t *cap, size_t n);
 int refresh_segments(fs_gpu *h);       // recompute segment data from d_vals
 double model_max_cutoff(const fs_gpu *h);
 

@@ -203,6 +203,17 @@ __global__ void spline_setup_kernel(const TableDesc *__restrict__ desc, const in
 
 } // namespace
 
+// A pinned host buffer of at least n doubles (kept between calls).
+int ensure_pinned(fs_gpu *h, double **buf, size_t *cap, size_t n) {
+  if (*cap >= n && *buf) return FS_OK;
+  if (*buf) cudaFreeHost(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  FS_CUDA(cudaMallocHost(buf, std::max<size_t>(n, 1) * sizeof(double)));
+  *cap = std::max<size_t>(n, 1);
+  return FS_OK;
+}
+
 int upload_tables(fs_gpu *h) {
   const int nt = static_cast<int>(h->tables.size());
   std::vector<TableDesc> desc(nt);
@@ -269,6 +280,11 @@ int upload_tables(fs_gpu *h) {
                           h->stream));
   FS_CUDA(cudaMemcpyAsync(h->d_vals, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice,
                           h->stream));
+  // pinned staging for the parameter values and the normal equations, sized
+  // here (model set-up) rather than on a fit's first step
+  FS_TRY(ensure_pinned(h, &h->h_vals_pin, &h->h_vals_pin_n, vals.size()));
+  FS_TRY(ensure_pinned(h, &h->h_ne_pin, &h->h_ne_pin_n,
+                       static_cast<size_t>(h->D) * h->D + h->D + 1));
   std::vector<int32_t> spl;
   for (int t = 0; t < nt; ++t)
     if (desc[t].kind == FS_TABLE_SPLINE) spl.push_back(t);
@@ -291,15 +307,8 @@ int upload_values(fs_gpu *h) {
   size_t n = 0;
   for (const HostTable &ht : h->tables) n += ht.v.size();
   if (!h->d_vals || static_cast<int>(n) != h->n_vals) return upload_tables(h);
-  if (h->h_vals_pin_n < n) {
-    if (h->h_vals_pin) cudaFreeHost(h->h_vals_pin);
-    h->h_vals_pin = nullptr;
-    h->h_vals_pin_n = 0;
-    FS_CUDA(cudaMallocHost(&h->h_vals_pin, std::max<size_t>(n, 1) * sizeof(double)));
-    h->h_vals_pin_n = n;
-  }
-  if (!h->vals_ev) FS_CUDA(cudaEventCreateWithFlags(&h->vals_ev, cudaEventDisableTiming));
-  FS_CUDA(cudaEventSynchronize(h->vals_ev));
+  FS_CUDA(cudaEventSynchronize(h->vals_ev)); // the previous upload from the buffer is done
+  FS_TRY(ensure_pinned(h, &h->h_vals_pin, &h->h_vals_pin_n, n));
   size_t k = 0;
   for (const HostTable &ht : h->tables)
     for (double v : ht.v) h->h_vals_pin[k++] = v;
