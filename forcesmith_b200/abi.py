@@ -22,8 +22,9 @@ FS_ERR_NOMEM = -5
 FS_ERR_DEVICE = -6
 FS_ERR_NUMERIC = -7
 
-FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW = 0, 1, 2, 3
-FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA = 0, 1, 2, 3
+FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW, FS_FAMILY_TERSOFF = 0, 1, 2, 3, 4
+FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA, FS_TABLE_TERSOFF = 0, 1, 2, 3, 4
+TERSOFF_FIELDS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S", "omega")
 FS_PREC_FP32, FS_PREC_FP64 = 0, 1
 
 FORMS = {
@@ -115,6 +116,17 @@ class Table:
         v = np.array([A, B, p, q, delta, a1, gamma, a2], dtype=np.float64)
         return Table(FS_TABLE_SW, v, 0.0, 0.0, 0,
                      None if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8))
+
+    @staticmethod
+    def tersoff(A, B, lam, mu, beta, n, c, d, h, R, S, omega=1.0, fixed=None):
+        """TersoffParams of one pair slot, in the reference's field order
+        (tersoff_force.hpp:17-31); omega is fixed unless `fixed` says
+        otherwise, as the reference declares it."""
+        v = np.array([A, B, lam, mu, beta, n, c, d, h, R, S, omega], dtype=np.float64)
+        fx = np.zeros(12, np.uint8) if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8)
+        if fixed is None:
+            fx[11] = 1
+        return Table(FS_TABLE_TERSOFF, v, 0.0, 0.0, 0, fx)
 
     @staticmethod
     def lam(values, fixed=None):

@@ -73,6 +73,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_EAM: return np + 2 * nt;
   case FS_FAMILY_ADP: return 3 * np + 2 * nt;
   case FS_FAMILY_SW: return np + 1;
+  case FS_FAMILY_TERSOFF: return np;
   }
   return -1;
 }
@@ -374,7 +375,12 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
     ht.rmin = ft.rmin;
     ht.rmax = ft.rmax;
     const bool sw_fam = m->family == FS_FAMILY_SW;
-    if (sw_fam) {
+    if (m->family == FS_FAMILY_TERSOFF) {
+      if (ft.kind != FS_TABLE_TERSOFF || ft.n != 12)
+        return set_error(h, FS_ERR_ARG, "set_model: Tersoff tables are tersoff[npair] with 12 params");
+    } else if (ft.kind == FS_TABLE_TERSOFF) {
+      return set_error(h, FS_ERR_ARG, "set_model: Tersoff tables belong to the Tersoff family");
+    } else if (sw_fam) {
       const int want = t < np ? FS_TABLE_SW : FS_TABLE_LAMBDA;
       if (ft.kind != want) return set_error(h, FS_ERR_ARG, "set_model: SW tables are sw[npair], lambda");
       if (t < np && ft.n != 8) return set_error(h, FS_ERR_ARG, "set_model: SW table needs 8 params");

@@ -67,5 +67,78 @@ __device__ __forceinline__ void pair_vec(const double *wpos, const double *shift
 template <class T> __device__ __forceinline__ T sqrt_t(T x) { return sqrt(x); }
 
 
+// Block sums of K values at once (one pair of barriers); valid on thread 0.
+// red holds K × 32 doubles.
+template <int K> __device__ void block_sum_k(double (&v)[K], double *red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k * 32 + w] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double t = 0.0;
+      for (int q = 0; q < nw; ++q) t += red[k * 32 + q];
+      v[k] = t;
+    }
+}
+
+// Largest i in [0, N) with first[i] <= w, for non-decreasing first[] with
+// first[0] = 0 <= w < first[N]: the atom that owns work item w.
+__device__ __forceinline__ int owner_of(const int *first, int N, int w) {
+  int lo = 0, hi = N;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Work-item offsets of one configuration: pfirst[i] = first directed pair of
+// atom i (relative to atom 0's), tfirst[i] = first neighbour pair (j < k) of
+// atom i, n_i (n_i − 1)/2 per atom; both with the totals at [N].  One block
+// scan; blockDim.x a multiple of 32, at most 1024.
+__device__ void stage_work(const int32_t *nb, int N, int *pfirst, int *tfirst, int *wsum) {
+  for (int k = threadIdx.x; k <= N; k += blockDim.x) pfirst[k] = nb[k] - nb[0];
+  const int per = (N + blockDim.x - 1) / blockDim.x;
+  const int b = min(N, static_cast<int>(threadIdx.x) * per), e = min(N, b + per);
+  int s = 0;
+  for (int k = b; k < e; ++k) {
+    const int n = nb[k + 1] - nb[k];
+    s += n * (n - 1) / 2;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < nw ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    __syncwarp();
+    if (lane < nw) wsum[lane] = v;
+  }
+  __syncthreads();
+  int base = x - s + (w > 0 ? wsum[w - 1] : 0);
+  for (int k = b; k < e; ++k) {
+    tfirst[k] = base;
+    const int n = nb[k + 1] - nb[k];
+    base += n * (n - 1) / 2;
+  }
+  if (threadIdx.x == blockDim.x - 1) tfirst[N] = base;
+}
+
 } // namespace
 } // namespace fsg

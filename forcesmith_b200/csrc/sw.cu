@@ -160,26 +160,6 @@ template <class T> struct SwArgs {
 
 constexpr int kSwThreads = 256;
 
-// Block sums of K values at once (one pair of barriers); valid on thread 0.
-// red holds K × 32 doubles.
-template <int K> __device__ void block_sum_k(double (&v)[K], double *red) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-  __syncthreads();
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; ++k) red[k * 32 + w] = v[k];
-  __syncthreads();
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double t = 0.0;
-      for (int q = 0; q < nw; ++q) t += red[k * 32 + q];
-      v[k] = t;
-    }
-}
 
 template <class T>
 __device__ __forceinline__ void add_row(T *Jb, int D, int row, int col, T v) {
@@ -222,57 +202,6 @@ template <class T, int NQ> struct RowAcc {
   }
 };
 
-// Largest i in [0, N) with first[i] <= w, for non-decreasing first[] with
-// first[0] = 0 <= w < first[N]: the atom that owns work item w.
-__device__ __forceinline__ int owner_of(const int *first, int N, int w) {
-  int lo = 0, hi = N;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (first[mid] <= w) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// Work-item offsets of one configuration: pfirst[i] = first directed pair of
-// atom i (relative to atom 0's), tfirst[i] = first neighbour pair (j < k) of
-// atom i, n_i (n_i − 1)/2 per atom; both with the totals at [N].  One block
-// scan; blockDim.x a multiple of 32, at most 1024.
-__device__ void stage_work(const int32_t *nb, int N, int *pfirst, int *tfirst, int *wsum) {
-  for (int k = threadIdx.x; k <= N; k += blockDim.x) pfirst[k] = nb[k] - nb[0];
-  const int per = (N + blockDim.x - 1) / blockDim.x;
-  const int b = min(N, static_cast<int>(threadIdx.x) * per), e = min(N, b + per);
-  int s = 0;
-  for (int k = b; k < e; ++k) {
-    const int n = nb[k + 1] - nb[k];
-    s += n * (n - 1) / 2;
-  }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  int x = s;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsum[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    int v = lane < nw ? wsum[lane] : 0;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += y;
-    }
-    __syncwarp();
-    if (lane < nw) wsum[lane] = v;
-  }
-  __syncthreads();
-  int base = x - s + (w > 0 ? wsum[w - 1] : 0);
-  for (int k = b; k < e; ++k) {
-    tfirst[k] = base;
-    const int n = nb[k + 1] - nb[k];
-    base += n * (n - 1) / 2;
-  }
-  if (threadIdx.x == blockDim.x - 1) tfirst[N] = base;
-}
 
 template <class T, bool JAC>
 __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(SwArgs<T> A) {
@@ -692,12 +621,14 @@ template <class T> int launch_sw(fs_gpu *h, double w_e, double w_s, bool jac) {
 } // namespace
 
 int eval_residual_adp(fs_gpu *h, double w_e, double w_s);
+int eval_residual_tersoff(fs_gpu *h, double w_e, double w_s);
 int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s);
 
 int eval_residual_other(fs_gpu *h, double w_e, double w_s) {
   if (h->family == FS_FAMILY_SW)
     return h->precision == FS_PREC_FP64 ? launch_sw<double>(h, w_e, w_s, false) : launch_sw<float>(h, w_e, w_s, false);
   if (h->family == FS_FAMILY_ADP) return eval_residual_adp(h, w_e, w_s);
+  if (h->family == FS_FAMILY_TERSOFF) return eval_residual_tersoff(h, w_e, w_s);
   return set_error(h, FS_ERR_UNSUPPORTED, "residual: family not handled by this build");
 }
 
@@ -709,7 +640,8 @@ int eval_jacobian_other(fs_gpu *h, double w_e, double w_s) {
     mark(h, 3);
     return rc;
   }
-  if (h->family == FS_FAMILY_ADP) return eval_jacobian_fd(h, w_e, w_s);
+  // ADP and Tersoff: the reference's own central differences (FP64 contexts)
+  if (h->family == FS_FAMILY_ADP || h->family == FS_FAMILY_TERSOFF) return eval_jacobian_fd(h, w_e, w_s);
   return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: family not handled by this build");
 }
 

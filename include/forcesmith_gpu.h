@@ -81,14 +81,18 @@ enum fs_family {
   FS_FAMILY_PAIR = 0, /* tables: pair[npair]                                */
   FS_FAMILY_EAM = 1,  /* tables: pair[npair], density[nt], embedding[nt]    */
   FS_FAMILY_ADP = 2,  /* tables: EAM + dipole[npair], quadrupole[npair]     */
-  FS_FAMILY_SW = 3    /* tables: sw[npair] (8 params each), lambda[1]       */
+  FS_FAMILY_SW = 3,   /* tables: sw[npair] (8 params each), lambda[1]       */
+  FS_FAMILY_TERSOFF = 4 /* tables: tersoff[npair] (12 params each)         */
 };
 
 enum fs_table_kind {
   FS_TABLE_SPLINE = 0,   /* uniform-grid makima spline: n knot values       */
   FS_TABLE_ANALYTIC = 1, /* closed form `form` with n parameters            */
   FS_TABLE_SW = 2,       /* SWParams {A,B,p,q,delta,a1,gamma,a2}, n == 8    */
-  FS_TABLE_LAMBDA = 3    /* SW triplet strengths, n == nt * npair           */
+  FS_TABLE_LAMBDA = 3,   /* SW triplet strengths, n == nt * npair           */
+  FS_TABLE_TERSOFF = 4   /* TersoffParams {A,B,lambda,mu,beta,n,c,d,h,R,S,omega},
+                            n == 12 (include/forcesmith/force/tersoff_force.hpp:17-31;
+                            gather order tersoff_force.cpp:14-25)          */
 };
 
 /* Analytic radial forms (include/forcesmith/potentials/analytic_potential.hpp). */

@@ -156,6 +156,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_EAM: return np + 2 * nt;
   case FS_FAMILY_ADP: return 3 * np + 2 * nt;
   case FS_FAMILY_SW: return np + 1;
+  case FS_FAMILY_TERSOFF: return np;
   }
   return -1;
 }
@@ -169,6 +170,10 @@ double max_cutoff(const State &S) {
   if (S.family == FS_FAMILY_SW) {
     for (int p = 0; p < np; ++p)
       m = std::max(m, std::max(S.tables[p].v[5], S.tables[p].v[7]));
+    return m;
+  }
+  if (S.family == FS_FAMILY_TERSOFF) { // max S over pair slots (tersoff_force.cpp:259-265)
+    for (int p = 0; p < np; ++p) m = std::max(m, S.tables[p].v[10]);
     return m;
   }
   for (int t = 0; t < static_cast<int>(S.tables.size()); ++t) {
@@ -259,7 +264,7 @@ void prime_sites(State &S) {
   const int64_t P = S.nb_j.size();
   for (auto &v : S.site) v.assign(P, Site{});
   for (auto &v : S.site_ok) v.assign(P, 0);
-  if (S.family == FS_FAMILY_SW) return;
+  if (S.family == FS_FAMILY_SW || S.family == FS_FAMILY_TERSOFF) return;
   const Roles R{npair_of(S.ntypes), S.ntypes};
 #pragma omp parallel for schedule(dynamic)
   for (int c = 0; c < static_cast<int>(S.cfgs.size()); ++c) {
@@ -598,6 +603,124 @@ void eval_sw(const State &S, int c, Out &o) {
   }
 }
 
+// Tersoff (src/force/tersoff_force.cpp).  Per directed bond i→j with the
+// (t_i, t_j) parameters p: f_c, V_R = A e^{−λr}, V_A = B e^{−μr} (make_bond
+// :85-101); ζ_ij = Σ_{k≠j} ω_ik f_c(r_ik) g_ij(cos θ_ijk) with the (t_i, t_k)
+// cutoff and ω (add_zeta :103-128); b = (1 + (βζ)^n)^{−1/2n} (bond_order
+// :63-70); E += ½ f_c (V_R − b V_A) and the radial pair force on i, −on j
+// (accumulate_pair :135-151); then the ζ-gradient forces on i, j, k with
+// P = ½ f_c V_A ∂b/∂ζ (accumulate_three_body :153-206).
+constexpr double kPi = 3.14159265358979323846; // std::numbers::pi
+struct TsP {
+  double A, B, lam, mu, beta, n, c, d, h, R, S, omega;
+};
+inline TsP tsp(const Table &t) {
+  return {t.v[0], t.v[1], t.v[2], t.v[3], t.v[4], t.v[5], t.v[6], t.v[7], t.v[8], t.v[9], t.v[10], t.v[11]};
+}
+// fc_val / dfc_val (:26-43)
+inline double ts_fc(double r, double R, double S) {
+  if (r <= R) return 1.0;
+  if (r >= S) return 0.0;
+  return 0.5 + 0.5 * std::cos(kPi * (r - R) / (S - R));
+}
+inline double ts_dfc(double r, double R, double S) {
+  if (r <= R || r >= S) return 0.0;
+  return -0.5 * kPi / (S - R) * std::sin(kPi * (r - R) / (S - R));
+}
+// g_val / dg_val (:45-61)
+inline double ts_g(double c, const TsP &p) {
+  const double c2 = p.c * p.c, d2 = p.d * p.d, hc = p.h - c;
+  return 1.0 + c2 / d2 - c2 / (d2 + hc * hc);
+}
+inline double ts_dg(double c, const TsP &p) {
+  const double c2 = p.c * p.c, d2 = p.d * p.d, hc = p.h - c;
+  const double den = d2 + hc * hc;
+  return -2.0 * c2 * hc / (den * den);
+}
+// bond_order / dbond_dzeta (:63-83)
+inline double ts_b(double zeta, const TsP &p) {
+  if (zeta == 0.0) return 1.0;
+  return std::pow(1.0 + std::pow(p.beta * zeta, p.n), -0.5 / p.n);
+}
+inline double ts_db(double zeta, const TsP &p) {
+  if (zeta == 0.0) return 0.0;
+  const double bzn = std::pow(p.beta * zeta, p.n);
+  const double b = std::pow(1.0 + bzn, -0.5 / p.n);
+  return -0.5 * b * bzn / (zeta * (1.0 + bzn));
+}
+
+void eval_tersoff(const State &S, int c, Out &o) {
+  const Config &cf = S.cfgs[c];
+  const int nt = S.ntypes, np = npair_of(nt);
+  std::vector<TsP> P(np);
+  for (int s = 0; s < np; ++s) P[s] = tsp(S.tables[s]);
+  for (int i = 0; i < cf.natoms; ++i) {
+    const int64_t gi = cf.atom0 + i;
+    const int ti = S.type[gi];
+    const int64_t s0 = S.nb_start[gi], s1 = S.nb_start[gi + 1];
+    for (int64_t pj = s0; pj < s1; ++pj) {
+      const Vec3 &d1 = S.nb_d[pj];
+      const double r1 = norm(d1);
+      const int j = S.nb_j[pj];
+      const TsP &p = P[pair_ordinal(ti, S.type[cf.atom0 + j], nt)];
+      if (r1 < 1e-14) continue;
+      const double fc = ts_fc(r1, p.R, p.S), dfc = ts_dfc(r1, p.R, p.S);
+      if (fc == 0.0 && dfc == 0.0) continue;
+      const double VR = p.A * std::exp(-p.lam * r1), VA = p.B * std::exp(-p.mu * r1);
+      const double VRp = -p.lam * VR, VAp = -p.mu * VA;
+      double zeta = 0.0;
+      for (int64_t pk = s0; pk < s1; ++pk) {
+        if (pk == pj) continue;
+        const Vec3 &d2 = S.nb_d[pk];
+        const double r2 = norm(d2);
+        if (r2 < 1e-14) continue;
+        const TsP &q = P[pair_ordinal(ti, S.type[cf.atom0 + S.nb_j[pk]], nt)];
+        const double fck = ts_fc(r2, q.R, q.S);
+        if (fck == 0.0) continue;
+        const double cth = dot(d1, d2) / (r1 * r2);
+        zeta += q.omega * fck * ts_g(cth, p);
+      }
+      const double b = ts_b(zeta, p);
+      o.energy += 0.5 * fc * (VR - b * VA);
+      const double pc = 0.5 * (dfc * (VR - b * VA) + fc * (VRp - b * VAp)) / r1;
+      const Vec3 Fp = pc * d1;
+      o.force[i] = o.force[i] + Fp;
+      o.force[j] = o.force[j] - Fp;
+      for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb) o.stress[a][bb] += 0.5 * d1[a] * (-Fp[bb]);
+      if (zeta == 0.0) continue;
+      const double Pz = 0.5 * fc * VA * ts_db(zeta, p);
+      const double inv_r1 = 1.0 / r1;
+      for (int64_t pk = s0; pk < s1; ++pk) {
+        if (pk == pj) continue;
+        const Vec3 &d2 = S.nb_d[pk];
+        const double r2 = norm(d2);
+        if (r2 < 1e-14) continue;
+        const int k = S.nb_j[pk];
+        const TsP &q = P[pair_ordinal(ti, S.type[cf.atom0 + k], nt)];
+        const double fck = ts_fc(r2, q.R, q.S), dfck = ts_dfc(r2, q.R, q.S);
+        if (fck == 0.0 && dfck == 0.0) continue;
+        const double inv_r2 = 1.0 / r2;
+        const double cth = dot(d1, d2) * inv_r1 * inv_r2;
+        const double gv = ts_g(cth, p), dgv = ts_dg(cth, p);
+        const double Ac = cth * inv_r1 * inv_r1 - inv_r1 * inv_r2;
+        const double Bc = cth * inv_r2 * inv_r2 - inv_r1 * inv_r2;
+        const double w = q.omega;
+        const Vec3 dzi = w * ((-dfck * inv_r2 * gv) * d2 + (fck * dgv) * (Ac * d1 + Bc * d2));
+        const Vec3 dzj = (w * fck * dgv) * ((inv_r1 * inv_r2) * d2 - (cth * inv_r1 * inv_r1) * d1);
+        const Vec3 dzk =
+            w * ((dfck * inv_r2 * gv) * d2 + (fck * dgv) * ((inv_r1 * inv_r2) * d1 - (cth * inv_r2 * inv_r2) * d2));
+        const Vec3 Fi = Pz * dzi, Fj = Pz * dzj, Fk = Pz * dzk;
+        o.force[i] = o.force[i] + Fi;
+        o.force[j] = o.force[j] + Fj;
+        o.force[k] = o.force[k] + Fk;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) o.stress[a][bb] += d1[a] * Fj[bb] + d2[a] * Fk[bb];
+      }
+    }
+  }
+}
+
 // with_eval_scope (include/forcesmith/force/eval_scope.hpp:13-31): zero,
 // run the kernel, σ /= V.
 void eval_config(const State &S, int c, Out &o) {
@@ -610,6 +733,7 @@ void eval_config(const State &S, int c, Out &o) {
   case FS_FAMILY_PAIR: eval_pair(S, c, o); break;
   case FS_FAMILY_ADP: eval_adp(S, c, o); break;
   case FS_FAMILY_SW: eval_sw(S, c, o); break;
+  case FS_FAMILY_TERSOFF: eval_tersoff(S, c, o); break;
   }
   const double V = cf.pbc.volume;
   for (auto &row : o.stress)
@@ -965,6 +1089,8 @@ int orc_set_model(orc_state *h, const fs_model *m) {
     if (ft.n < 1 || !ft.values) return FS_ERR_ARG;
     if (ft.kind == FS_TABLE_SPLINE && (ft.n < 2 || !(ft.rmax > ft.rmin))) return FS_ERR_ARG;
     if (ft.kind == FS_TABLE_ANALYTIC && form_nparams(ft.form) != ft.n) return FS_ERR_ARG;
+    if ((m->family == FS_FAMILY_TERSOFF) != (ft.kind == FS_TABLE_TERSOFF)) return FS_ERR_ARG;
+    if (ft.kind == FS_TABLE_TERSOFF && ft.n != 12) return FS_ERR_ARG;
     S.tables[t].init(ft);
   }
   S.have_model = true;
