@@ -22,7 +22,7 @@ FS_ERR_NOMEM = -5
 FS_ERR_DEVICE = -6
 FS_ERR_NUMERIC = -7
 
-FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW, FS_FAMILY_TERSOFF = 0, 1, 2, 3, 4
+FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_FAMILY_ANGULAR = 0, 1, 2, 3, 4, 5
 FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA, FS_TABLE_TERSOFF = 0, 1, 2, 3, 4
 TERSOFF_FIELDS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S", "omega")
 FS_PREC_FP32, FS_PREC_FP64 = 0, 1

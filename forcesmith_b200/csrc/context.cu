@@ -74,6 +74,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_ADP: return 3 * np + 2 * nt;
   case FS_FAMILY_SW: return np + 1;
   case FS_FAMILY_TERSOFF: return np;
+  case FS_FAMILY_ANGULAR: return 2 * np + nt;
   }
   return -1;
 }
@@ -389,8 +390,8 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
     } else if (ft.kind == FS_TABLE_SPLINE) {
       if (ft.n < 2 || !(ft.rmax > ft.rmin)) return set_error(h, FS_ERR_ARG, "set_model: bad spline");
     } else if (ft.kind == FS_TABLE_ANALYTIC) {
-      if (m->family != FS_FAMILY_EAM && m->family != FS_FAMILY_PAIR)
-        return set_error(h, FS_ERR_UNSUPPORTED, "set_model: analytic tables in EAM and pair models only");
+      if (m->family != FS_FAMILY_EAM && m->family != FS_FAMILY_PAIR && m->family != FS_FAMILY_ANGULAR)
+        return set_error(h, FS_ERR_UNSUPPORTED, "set_model: analytic tables in EAM, pair and angular models only");
       static const int nparams[FS_FORM_COUNT] = {2, 3, 2, 2, 2, 3, 2, 3, 3, 1, 3, 5};
       if (ft.form < 0 || ft.form >= FS_FORM_COUNT || ft.n != nparams[ft.form])
         return set_error(h, FS_ERR_ARG, "set_model: analytic form and parameter count do not match");

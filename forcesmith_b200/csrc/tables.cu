@@ -26,7 +26,8 @@ double model_max_cutoff(const fs_gpu *h) {
   for (int t = 0; t < static_cast<int>(h->desc.size()); ++t) {
     const bool emb = (h->family == FS_FAMILY_EAM || h->family == FS_FAMILY_ADP) && t >= np + nt &&
                      t < np + 2 * nt;
-    if (!emb) m = std::max(m, h->desc[t].xmax);
+    const bool ang = h->family == FS_FAMILY_ANGULAR && t >= 2 * np; // cos θ tables are not radial
+    if (!emb && !ang) m = std::max(m, h->desc[t].xmax);
   }
   return m;
 }

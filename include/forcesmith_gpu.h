@@ -82,7 +82,9 @@ enum fs_family {
   FS_FAMILY_EAM = 1,  /* tables: pair[npair], density[nt], embedding[nt]    */
   FS_FAMILY_ADP = 2,  /* tables: EAM + dipole[npair], quadrupole[npair]     */
   FS_FAMILY_SW = 3,   /* tables: sw[npair] (8 params each), lambda[1]       */
-  FS_FAMILY_TERSOFF = 4 /* tables: tersoff[npair] (12 params each)         */
+  FS_FAMILY_TERSOFF = 4, /* tables: tersoff[npair] (12 params each)        */
+  FS_FAMILY_ANGULAR = 5  /* tables: pair[npair], radial[npair], angular[nt]:
+                            spline or analytic (angular_force.hpp:15-33)   */
 };
 
 enum fs_table_kind {

@@ -157,6 +157,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_ADP: return 3 * np + 2 * nt;
   case FS_FAMILY_SW: return np + 1;
   case FS_FAMILY_TERSOFF: return np;
+  case FS_FAMILY_ANGULAR: return 2 * np + nt;
   }
   return -1;
 }
@@ -179,7 +180,8 @@ double max_cutoff(const State &S) {
   for (int t = 0; t < static_cast<int>(S.tables.size()); ++t) {
     const bool embedding = (S.family == FS_FAMILY_EAM || S.family == FS_FAMILY_ADP) &&
                            t >= np + nt && t < np + 2 * nt;
-    if (!embedding) m = std::max(m, S.tables[t].span().second);
+    const bool angular = S.family == FS_FAMILY_ANGULAR && t >= 2 * np; // cos θ, not radial
+    if (!embedding && !angular) m = std::max(m, S.tables[t].span().second);
   }
   return m;
 }
@@ -264,7 +266,7 @@ void prime_sites(State &S) {
   const int64_t P = S.nb_j.size();
   for (auto &v : S.site) v.assign(P, Site{});
   for (auto &v : S.site_ok) v.assign(P, 0);
-  if (S.family == FS_FAMILY_SW || S.family == FS_FAMILY_TERSOFF) return;
+  if (S.family == FS_FAMILY_SW || S.family == FS_FAMILY_TERSOFF || S.family == FS_FAMILY_ANGULAR) return;
   const Roles R{npair_of(S.ntypes), S.ntypes};
 #pragma omp parallel for schedule(dynamic)
   for (int c = 0; c < static_cast<int>(S.cfgs.size()); ++c) {
@@ -721,6 +723,73 @@ void eval_tersoff(const State &S, int c, Out &o) {
   }
 }
 
+// Angular (src/force/angular_force.cpp:13-88): the pair term φ_{t_i t_j}
+// (½ per directed pair, accumulate_pair kernels.hpp:33-38) plus, per central
+// atom i and neighbour pair j < k, f_{t_i t_j}(r_ij) f_{t_i t_k}(r_ik)
+// g_{t_i}(cos θ) with three_body_forces / accumulate_triplet
+// (kernels.hpp:44-68).  φ and f are gated to their closed spans
+// (force_calculator_concept.hpp:94-98); g is evaluated ungated.
+void eval_angular(const State &S, int c, Out &o) {
+  const Config &cf = S.cfgs[c];
+  const int nt = S.ntypes, np = npair_of(nt);
+  for (int i = 0; i < cf.natoms; ++i) {
+    const int64_t gi = cf.atom0 + i;
+    const int ti = S.type[gi];
+    for (int64_t p = S.nb_start[gi]; p < S.nb_start[gi + 1]; ++p) {
+      const Vec3 &d = S.nb_d[p];
+      const double r = norm(d);
+      if (r < 1e-14) continue;
+      const Table &T = S.tables[pair_ordinal(ti, S.type[cf.atom0 + S.nb_j[p]], nt)];
+      if (!T.in_range(r)) continue;
+      const double phi = T.eval(r), dphi = T.deriv(r);
+      acc_pair(o, o.force[i], d, (dphi / r) * d, phi);
+    }
+  }
+  for (int i = 0; i < cf.natoms; ++i) {
+    const int64_t gi = cf.atom0 + i;
+    const int ti = S.type[gi];
+    const Table &G = S.tables[2 * np + ti];
+    const int64_t s0 = S.nb_start[gi], s1 = S.nb_start[gi + 1];
+    for (int64_t pj = s0; pj < s1; ++pj) {
+      const Vec3 &d1 = S.nb_d[pj];
+      const double r1 = norm(d1);
+      if (r1 < 1e-14) continue;
+      const double inv_r1 = 1.0 / r1;
+      const int j = S.nb_j[pj];
+      const Table &Rj = S.tables[np + pair_ordinal(ti, S.type[cf.atom0 + j], nt)];
+      if (!Rj.in_range(r1)) continue;
+      const double f1 = Rj.eval(r1), df1 = Rj.deriv(r1);
+      for (int64_t pk = pj + 1; pk < s1; ++pk) {
+        const Vec3 &d2 = S.nb_d[pk];
+        const double r2 = norm(d2);
+        if (r2 < 1e-14) continue;
+        const double inv_r2 = 1.0 / r2;
+        const int k = S.nb_j[pk];
+        const Table &Rk = S.tables[np + pair_ordinal(ti, S.type[cf.atom0 + k], nt)];
+        if (!Rk.in_range(r2)) continue;
+        const double f2 = Rk.eval(r2), df2 = Rk.deriv(r2);
+        const double cth = dot(d1, d2) * inv_r1 * inv_r2;
+        const double g = G.eval(cth), dg = G.deriv(cth);
+        o.energy += f1 * f2 * g;
+        const double inv_r1r2 = inv_r1 * inv_r2;
+        const double Aa = cth * inv_r1 * inv_r1 - inv_r1r2;
+        const double Bb = cth * inv_r2 * inv_r2 - inv_r1r2;
+        const Vec3 fi = (df1 * inv_r1 * f2 * g) * d1 + (f1 * df2 * inv_r2 * g) * d2 -
+                        (f1 * f2 * dg) * (Aa * d1 + Bb * d2);
+        const Vec3 fj = -1.0 * ((df1 * inv_r1 * f2 * g) * d1) -
+                        (f1 * f2 * dg) * (inv_r1r2 * d2 - (cth * inv_r1 * inv_r1) * d1);
+        const Vec3 fk = -1.0 * ((f1 * df2 * inv_r2 * g) * d2) -
+                        (f1 * f2 * dg) * (inv_r1r2 * d1 - (cth * inv_r2 * inv_r2) * d2);
+        o.force[i] = o.force[i] + fi;
+        o.force[j] = o.force[j] + fj;
+        o.force[k] = o.force[k] + fk;
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) o.stress[a][b] += d1[a] * fj[b] + d2[a] * fk[b];
+      }
+    }
+  }
+}
+
 // with_eval_scope (include/forcesmith/force/eval_scope.hpp:13-31): zero,
 // run the kernel, σ /= V.
 void eval_config(const State &S, int c, Out &o) {
@@ -734,6 +803,7 @@ void eval_config(const State &S, int c, Out &o) {
   case FS_FAMILY_ADP: eval_adp(S, c, o); break;
   case FS_FAMILY_SW: eval_sw(S, c, o); break;
   case FS_FAMILY_TERSOFF: eval_tersoff(S, c, o); break;
+  case FS_FAMILY_ANGULAR: eval_angular(S, c, o); break;
   }
   const double V = cf.pbc.volume;
   for (auto &row : o.stress)
