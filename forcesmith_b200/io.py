@@ -28,8 +28,9 @@ import os
 
 import numpy as np
 
-from .abi import (FS_FAMILY_ADP, FS_FAMILY_EAM, FS_FAMILY_PAIR, FS_FAMILY_SW, FS_TABLE_ANALYTIC,
-                  FS_TABLE_LAMBDA, FS_TABLE_SPLINE, FS_TABLE_SW, FORMS, Dataset, Model, Table)
+from .abi import (FS_FAMILY_ADP, FS_FAMILY_ANGULAR, FS_FAMILY_EAM, FS_FAMILY_PAIR, FS_FAMILY_SW,
+                  FS_FAMILY_TERSOFF, FS_TABLE_ANALYTIC, FS_TABLE_LAMBDA, FS_TABLE_SPLINE, FS_TABLE_SW,
+                  FS_TABLE_TERSOFF, FORMS, TERSOFF_FIELDS, Dataset, Model, Table)
 
 SYMBOLS = (
     "H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
@@ -56,10 +57,15 @@ FORM_SPEC = {
 FORM_NAME = {FORMS[canon][0]: canon for canon, _ in FORM_SPEC.values()}
 PARAM_NAMES = {FORMS[canon][0]: names for canon, names in FORM_SPEC.values()}
 SW_FIELDS = ("A", "B", "p", "q", "delta", "a1", "gamma", "a2")
+# table sections per family (family_name, include/forcesmith/core/families.hpp:28-43;
+# the TableField lists of the calculators, e.g. angular_force.hpp:21-30)
 TABLE_KEYS = {FS_FAMILY_PAIR: ("pair",), FS_FAMILY_EAM: ("pair", "density", "embedding"),
-              FS_FAMILY_ADP: ("pair", "density", "embedding", "dipole", "quadrupole")}
-PER_PAIR = {"pair": True, "density": False, "embedding": False, "dipole": True, "quadrupole": True}
-FAMILY_OF = {"pair": FS_FAMILY_PAIR, "eam": FS_FAMILY_EAM, "adp": FS_FAMILY_ADP, "stiweb": FS_FAMILY_SW}
+              FS_FAMILY_ADP: ("pair", "density", "embedding", "dipole", "quadrupole"),
+              FS_FAMILY_ANGULAR: ("pair", "radial", "angular")}
+PER_PAIR = {"pair": True, "density": False, "embedding": False, "dipole": True, "quadrupole": True,
+            "radial": True, "angular": False}
+FAMILY_OF = {"pair": FS_FAMILY_PAIR, "eam": FS_FAMILY_EAM, "adp": FS_FAMILY_ADP, "stiweb": FS_FAMILY_SW,
+             "angular": FS_FAMILY_ANGULAR, "tersoff": FS_FAMILY_TERSOFF}
 NAME_OF = {v: k for k, v in FAMILY_OF.items()}
 
 
@@ -212,7 +218,8 @@ def _section(sub, want, label):
 
 
 def read_model(src):
-    """Force-model JSON → Model (families pair, eam, adp, stiweb)."""
+    """Force-model JSON → Model (families pair, eam, adp, angular, stiweb,
+    tersoff)."""
     j = json.loads(_text(src))
     if "globals" in j:
         raise FormatError("global parameters are not supported by this reader")
@@ -229,6 +236,28 @@ def read_model(src):
         raise FormatError(f"unsupported model '{name}'")
     fam, nt = FAMILY_OF[name], int(j.get("ntypes", 1))
     npair = nt * (nt + 1) // 2
+    if fam == FS_FAMILY_TERSOFF:
+        # build_tersoff (src/io/force_model_reader.cpp:166-196): one parameter
+        # block per pair slot; ω is free only when the block gives it
+        pots = j.get("potentials")
+        if not isinstance(pots, list) or len(pots) != npair:
+            raise FormatError(f"tersoff: expected {npair} entries for ntypes={nt}")
+        tabs = []
+        for p in pots:
+            if not isinstance(p, dict):
+                raise FormatError("tersoff: parameter block must be a JSON object")
+            vals = []
+            for k in TERSOFF_FIELDS:
+                if k in p:
+                    vals.append(_param(p[k]))
+                elif k == "omega":
+                    vals.append((1.0, -math.inf, math.inf, True))
+                else:
+                    raise FormatError(f"tersoff: missing parameter '{k}'")
+            tabs.append(Table(FS_TABLE_TERSOFF, np.array([v[0] for v in vals]), 0.0, 0.0, 0,
+                              np.array([v[3] for v in vals], np.uint8), np.array([v[1] for v in vals]),
+                              np.array([v[2] for v in vals])))
+        return Model(fam, nt, tabs)
     if fam == FS_FAMILY_SW:
         pots = j.get("potentials")
         if not isinstance(pots, list) or len(pots) != npair:
@@ -276,12 +305,31 @@ def _pot_json(t):
     return d
 
 
+def _tersoff_json(t):
+    d = {}
+    for k, nm in enumerate(TERSOFF_FIELDS):
+        lo = -math.inf if t.lower is None else float(t.lower[k])
+        hi = math.inf if t.upper is None else float(t.upper[k])
+        fx = False if t.fixed is None else bool(t.fixed[k])
+        if nm == "omega" and fx and math.isinf(lo) and math.isinf(hi) and float(t.values[k]) == 1.0:
+            continue  # the reader's default: ω = 1, fixed
+        if math.isinf(lo) and math.isinf(hi) and not fx:
+            d[nm] = float(t.values[k])
+        else:
+            d[nm] = {"value": float(t.values[k]), "fixed": fx,
+                     **({} if math.isinf(lo) else {"min": lo}), **({} if math.isinf(hi) else {"max": hi})}
+    return d
+
+
 def write_model(model):
-    """Model → force-model JSON text (families pair, eam, adp)."""
+    """Model → force-model JSON text (families pair, eam, adp, angular, tersoff)."""
     nt, fam = model.ntypes, model.family
-    if fam not in TABLE_KEYS:
-        raise FormatError("write_model: pair, eam and adp families")
     npair = nt * (nt + 1) // 2
+    if fam == FS_FAMILY_TERSOFF:
+        return json.dumps({"model": "tersoff", "ntypes": nt,
+                           "potentials": [_tersoff_json(t) for t in model.tables]}, indent=1)
+    if fam not in TABLE_KEYS:
+        raise FormatError("write_model: pair, eam, adp, angular and tersoff families")
     out = {"model": NAME_OF[fam], "ntypes": nt}
     k = 0
     for key in TABLE_KEYS[fam]:

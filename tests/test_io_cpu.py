@@ -73,6 +73,29 @@ def test_model_roundtrip():
     np.testing.assert_array_equal(back.tables[2].fixed, [0, 1, 0, 0, 1])
 
 
+def test_tersoff_and_angular_models():
+    """tersoff: one parameter block per pair slot, ω free only when given
+    (force_model_reader.cpp:166-196); angular: pair, radial, angular sections."""
+    from forcesmith_b200.abi import FS_FAMILY_ANGULAR, FS_FAMILY_TERSOFF
+    blk = dict(A=1830.8, B=471.18, **{"lambda": 2.4799}, mu=1.7322, beta=1.1e-6, n=0.78734,
+               c=1.0039e5, d=16.217, h=-0.59825, R={"value": 2.7, "min": 2.5, "max": 2.9}, S=3.0)
+    m = io.read_model(json.dumps({"model": "tersoff", "ntypes": 2,
+                                  "potentials": [blk, dict(blk, omega=0.9), blk]}))
+    assert m.family == FS_FAMILY_TERSOFF and len(m.tables) == 3
+    assert m.tables[0].fixed[11] == 1 and m.tables[0].values[11] == 1.0
+    assert m.tables[1].fixed[11] == 0 and m.tables[1].values[11] == 0.9
+    assert m.tables[0].lower[9] == 2.5 and m.tables[0].values[2] == 2.4799
+    _tables_equal(io.read_model(io.write_model(m)), m)
+    with pytest.raises(io.FormatError):
+        io.read_model(json.dumps({"model": "tersoff", "ntypes": 1, "potentials": [dict(blk, A=None) | {"A": 1.0}] * 2}))
+    ang = Model(FS_FAMILY_ANGULAR, 1, [Table.analytic("lj", [1.0, 1.0], 0.1, 20.0),
+                                       Table.spline(0.0, 5.0, [1.0, 0.6, 0.3, 0.1, 0.0]),
+                                       Table.analytic("harmonic", [1.0, -0.5], -1.0, 1.0)])
+    back = io.read_model(io.write_model(ang))
+    assert back.family == FS_FAMILY_ANGULAR
+    _tables_equal(back, ang)
+
+
 def test_model_json_forms_and_errors():
     eam = {"model": "eam", "ntypes": 1,
            "pair": {"format": "analytic", "potentials": [{"type": "buck", "rmin": 0.5, "rmax": 6.0, "A": 900.0,
