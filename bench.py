@@ -259,6 +259,84 @@ def de_legs(local, generations):
     return de, sur
 
 
+def three_body_leg(local, which, steps=20):
+    """Tersoff or Angular on diamond Si: 1000 configurations of 64, 216 or 512
+    atoms (sigma = 0.15 A, volumetric strain U[0.95, 1.05]).  Device: FP32
+    residuals per second (CUDA events, 20 evaluations), and the FP64
+    central-difference Jacobian (the reference's method for these families:
+    2 D + 1 residuals) per second.  CPU: the oracle (16 threads, FP64), one
+    residual timed, the Jacobian extrapolated as (2 D + 1) residuals."""
+    import numpy as np
+    import torch
+    from forcesmith_b200 import gpu as G, synth
+    from forcesmith_b200.abi import FS_FAMILY_ANGULAR, FS_FAMILY_TERSOFF, Model, Table
+    from oracle.api import Oracle, set_threads
+    ds = synth.diamond(1000)
+    if which == "tersoff":
+        def model(s):
+            return Model(FS_FAMILY_TERSOFF, 1, [Table.tersoff(
+                3264.7 * s, 95.373, 3.2394, 1.3258, 0.33675, 22.956, 4.8381, 2.0417, 0.0, 3.0, 3.2)])
+        name = "Tersoff Si (1988 parameter set, R = 3.0, S = 3.2 A), D = 11"
+    else:
+        r = np.linspace(2.0, 3.8, 12)
+        c = np.linspace(-1.0, 1.0, 9)
+        def model(s):
+            return Model(FS_FAMILY_ANGULAR, 1, [
+                Table.spline(2.0, 3.8, s * 2.0 * (np.exp(-3 * (r - 2.35)) - 2 * np.exp(-1.5 * (r - 2.35))) * (1 - (r / 3.8) ** 4)),
+                Table.spline(2.0, 3.8, s * np.exp(-1.2 * (r - 2.35)) * (1 - (r / 3.8) ** 3)),
+                Table.spline(-1.0, 1.0, s * 1.5 * (c + 1.0 / 3.0) ** 2)])
+        name = "Angular Si (12-knot pair and radial splines, 9-knot angular spline), D = 33"
+    ds = label_on_gpu(ds, model(1.0), local)
+    start = model(1.05)
+    out = {"workload": f"{name}, {ds.n_cfg} configs x 64/216/512 atoms ({ds.n_atoms} atoms), w_e=1, w_s=0.1"}
+    g = G.GpuSession(local, "fp32")
+    g.upload(ds)
+    g.set_model(start)
+    for _ in range(3):
+        g.eval(W_E, W_S, want=("obj",))
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(g.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(steps):
+        g._lib.fs_gpu_eval(g._h, W_E, W_S, None, None, None, None, None, None)
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    res_ms = ev0.elapsed_time(ev1) / steps
+    P = g.num_pairs()
+    g.close()
+    g = G.GpuSession(local, "fp64")
+    g.upload(ds)
+    g.set_model(start)
+    D = g.D
+    g.jacobian_async(W_E, W_S)
+    g.normal_equations()
+    t0 = time.perf_counter()
+    g.jacobian_async(W_E, W_S)
+    g.normal_equations()
+    jac_s = time.perf_counter() - t0
+    g.close()
+    threads = set_threads(os.cpu_count() or 1)
+    o = Oracle()
+    o.upload(ds)
+    o.set_model(start)
+    o.eval(W_E, W_S, want=("obj",))
+    t0 = time.perf_counter()
+    o.eval(W_E, W_S, want=("F",))
+    t_res = time.perf_counter() - t0
+    out.update({"pairs": P, "D": D,
+                "residual_fp32": {"value": 1000.0 / res_ms, "unit": "evals/s", "ms_per_eval": res_ms},
+                "jacobian_fp64_fd": {"value": 1.0 / jac_s, "unit": "evals/s", "s_per_eval": jac_s,
+                                     "method": "central differences, 2 D + 1 device residuals"},
+                "cpu_baseline": {"residual": {"value": 1.0 / t_res, "unit": "evals/s"},
+                                 "jacobian_fd": {"value": 1.0 / (t_res * (2 * D + 1)), "unit": "evals/s"},
+                                 "cores": threads, "kind": "port",
+                                 "sample": f"one FP64 residual ({t_res * 1e3:.0f} ms); the Jacobian as 2 D + 1 of them"}})
+    return out
+
+
 def sw_leg(local, steps=20):
     """Stillinger-Weber Si: 1000 diamond configurations of 64, 216 or 512
     atoms (sigma = 0.15 A, volumetric strain U[0.95, 1.05]), 7 perturbed SW
@@ -557,6 +635,8 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_baseline(ds, start, args.cpu_columns)
     if rank == 0 and world == 1 and not args.small and not args.no_cpu_baseline:
         line["sw"] = sw_leg(local)
+        line["tersoff"] = three_body_leg(local, "tersoff")
+        line["angular"] = three_body_leg(local, "angular")
         line["al99_fit"] = al99_leg(local)
     if rank == 0 and world == 1 and not args.small and args.de_generations >= 0:
         de, sur = de_legs(local, args.de_generations)
