@@ -23,7 +23,9 @@ FS_ERR_DEVICE = -6
 FS_ERR_NUMERIC = -7
 
 FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_FAMILY_ANGULAR = 0, 1, 2, 3, 4, 5
+FS_FAMILY_ACSF = 6
 FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA, FS_TABLE_TERSOFF = 0, 1, 2, 3, 4
+FS_TABLE_ACSF, FS_TABLE_LINEAR_HEAD = 5, 6
 TERSOFF_FIELDS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S", "omega")
 FS_PREC_FP32, FS_PREC_FP64 = 0, 1
 
@@ -33,6 +35,13 @@ FORMS = {
     "exp_plus": (7, 3), "parabola": (8, 3), "const": (9, 1),
     "buckingham": (10, 3), "born": (11, 5),
 }
+
+
+def acsf_size(spec, nt):
+    """Descriptor length of an ACSF table for nt species (AcsfLayout,
+    acsf.hpp:23-33): nt(nG1 + nG2 + nG3) + npair(nG4 + nG5)."""
+    g1, n2, n3, n4, n5 = (int(x) for x in spec.values[1:6])
+    return nt * (g1 + n2 + n3) + nt * (nt + 1) // 2 * (n4 + n5)
 
 
 class FsError(RuntimeError):
@@ -127,6 +136,28 @@ class Table:
         if fixed is None:
             fx[11] = 1
         return Table(FS_TABLE_TERSOFF, v, 0.0, 0.0, 0, fx)
+
+    @staticmethod
+    def acsf(rcut, g1=0, g2=(), g3=(), g4=(), g5=()):
+        """ACSF symmetry functions (the reference's ACSF fields, acsf.hpp:48-71):
+        g1 parameterless channels, g2 (eta, rs), g3 kappa, g4 and g5
+        (eta, zeta, lambda).  Descriptor hyperparameters are not fitted."""
+        v = [rcut, g1, len(g2), len(g3), len(g4), len(g5)]
+        for seq in (g2, g3, g4, g5):
+            for x in seq:
+                v += list(np.atleast_1d(np.asarray(x, np.float64)))
+        v = np.array(v, np.float64)
+        return Table(FS_TABLE_ACSF, v, 0.0, 0.0, 0, np.ones(v.size, np.uint8))
+
+    @staticmethod
+    def linear_head(coeffs, bias=0.0, bias_fixed=True, fixed=None):
+        """LinearHead E_i = w·D_i + b (ml_force.hpp); the bias is fixed unless
+        bias_fixed is False, as the reference declares it."""
+        v = np.append(np.asarray(coeffs, np.float64), float(bias))
+        fx = np.zeros(v.size, np.uint8) if fixed is None else np.ascontiguousarray(fixed, np.uint8)
+        if fixed is None:
+            fx[-1] = 1 if bias_fixed else 0
+        return Table(FS_TABLE_LINEAR_HEAD, v, 0.0, 0.0, 0, fx)
 
     @staticmethod
     def lam(values, fixed=None):

@@ -1,0 +1,458 @@
+// ACSF descriptors with a linear energy head per species, on the device.
+//
+//   ACSF::get_descriptor (src/force/acsf.cpp:84-196): per central atom i and
+//   neighbour j with 1e-14 ≤ r < rcut, f_c = ½(1 + cos(πr/rcut)):
+//     G1 = f_c, G2 = e^{−η(r − rs)²} f_c, G3 = cos(κr) f_c   (per species of j),
+//   per neighbour pair j < k (per species pair):
+//     G4/G5 = 2^{1−ζ}(1 + λ cos θ)^ζ e^{−η(r_ij² + r_ik² [+ r_jk²])}
+//             f_c(r_ij) f_c(r_ik) [f_c(r_jk)],   skipped when 1 + λ cos θ ≤ 1e-12,
+//   laid out as AcsfLayout (acsf.hpp:23-46).
+//   LinearHead (src/force/ml_force.cpp:11-47): E_i = w_{t_i}·D_i + b_{t_i}.
+//   MLBase::eval_forces (include/forcesmith/force/ml_force.hpp): F −= (∂D/∂r)ᵀ w
+//   on i and its neighbours, σ += d_ij ⊗ (force on j).
+//   The Jacobian with respect to the head coefficients is exact and does not
+//   depend on them: ∂F/∂w = −∂D/∂r, ∂E/∂w = Σ_i D_i, ∂E/∂b = atom count
+//   (eval_cached_jacobian, ml_force.hpp).
+//
+// One CTA per configuration; threads take work items flat from a block scan:
+// one directed pair each (G1–G3), then one neighbour pair (j < k) of a central
+// atom each (G4, G5).  Residual: forces in shared memory with atomics; energy
+// and stress as per-thread FP64 sums.  Jacobian: each term adds its rows into
+// J (global memory, zeroed first) with atomics; a column kernel forms Jᵀr.
+#include "kern_common.cuh"
+
+#include <algorithm>
+
+namespace fsg {
+namespace {
+
+constexpr int kAcThreads = 256;
+
+template <class T> __device__ __forceinline__ void ac_fc(T r, T rc, T &fc, T &fcp) {
+  if (r >= rc) {
+    fc = fcp = T(0);
+    return;
+  }
+  const T x = T(3.14159265358979323846) * r / rc;
+  fc = T(0.5) * (T(1) + cos(x));
+  fcp = T(-0.5) * T(3.14159265358979323846) / rc * sin(x);
+}
+
+// The descriptor hyperparameters and layout (acsf.hpp:23-46), from the ACSF
+// table's values {rcut, nG1..nG5, parameters}.
+struct AcLayout {
+  int g1, n2, n3, n4, n5, nt, S;
+  int base[5];
+  __device__ __host__ void init(const double *v, int ntypes) {
+    g1 = static_cast<int>(v[1]);
+    n2 = static_cast<int>(v[2]);
+    n3 = static_cast<int>(v[3]);
+    n4 = static_cast<int>(v[4]);
+    n5 = static_cast<int>(v[5]);
+    nt = ntypes;
+    const int P = nt * (nt + 1) / 2;
+    base[0] = 0;
+    base[1] = base[0] + g1 * nt;
+    base[2] = base[1] + n2 * nt;
+    base[3] = base[2] + n3 * nt;
+    base[4] = base[3] + n4 * P;
+    S = base[4] + n5 * P;
+  }
+};
+
+template <class T> struct AcArgs {
+  Common c;
+  const double *vals; // all model values (FP64)
+  double w_e, w_s;
+  double *F, *forces, *energy, *stress9, *limit, *obj_part;
+  const int32_t *order;
+  // Jacobian
+  T *J;
+  int64_t ld;
+};
+
+// One CTA per configuration.  JAC = false: residual; JAC = true: J rows.
+template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_kernel(AcArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = A.order ? A.order[blockIdx.x] : blockIdx.x;
+  const CfgDev &cd = A.c.cfg[c];
+  const int N = cd.natoms;
+  const int nt = A.c.ntypes;
+  const int nimg = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+  const double *spec = A.vals + A.c.desc[0].pv0;
+  AcLayout L;
+  L.init(spec, nt);
+  const int nspec = A.c.desc[0].n;
+  Smem S(smem_raw);
+  T *par = S.take<T>(nspec);           // rcut, counts, function parameters
+  T *W = S.take<T>(nt * (L.S + 1));    // heads: w[S], b per species
+  int *col = S.take<int>(nt * (L.S + 1)); // head value → J column (−1 fixed)
+  double *wpos = S.take<double>(3 * N);
+  double *shift = S.take<double>(3 * nimg);
+  uint8_t *typ = S.take<uint8_t>(N);
+  T *Fs = S.take<T>(3 * N);
+  double *red = S.take<double>(8 * 32);
+  int *pfirst = S.take<int>(N + 1);
+  int *tfirst = S.take<int>(N + 1);
+  int *wsum = S.take<int>(32);
+  for (int k = threadIdx.x; k < nspec; k += blockDim.x) par[k] = static_cast<T>(spec[k]);
+  for (int k = threadIdx.x; k < nt * (L.S + 1); k += blockDim.x) {
+    const TableDesc &td = A.c.desc[1 + k / (L.S + 1)];
+    W[k] = static_cast<T>(A.vals[td.pv0 + k % (L.S + 1)]);
+    col[k] = A.c.cmap[td.cmap0 + k % (L.S + 1)];
+  }
+  for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) Fs[k] = T(0);
+  stage_geometry(cd, A.c, wpos, shift, typ);
+  const int32_t *start = A.c.nb_start + cd.atom0;
+  stage_work(start, N, pfirst, tfirst, wsum);
+  __syncthreads();
+  const T rc = par[0];
+  const T *p2 = par + 6, *p3 = p2 + 2 * L.n2, *p4 = p3 + L.n3, *p5 = p4 + 3 * L.n4;
+  const uint32_t *nbp = A.c.nb_pack + start[0];
+  const int npair = pfirst[N], ntri = tfirst[N];
+  const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
+  const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
+  const int64_t rowE = row0 + 3 * N;
+  const T sw = static_cast<T>(A.w_s / cd.volume), we = static_cast<T>(A.w_e);
+  double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0}; // xx, yy, zz, xy, xz, yz
+  // J rows of one term: force rows of i (+g), of n (−g), energy, stress (d ⊗ −g)
+  auto jac_add = [&](int cl, int i, int n, const T (&g)[3], const T (&d)[3], T e) {
+    if (cl < 0) return;
+    T *Jc = A.J + static_cast<int64_t>(cl) * A.ld;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      atomicAdd(&Jc[row0 + 3 * i + a], g[a]);
+      atomicAdd(&Jc[row0 + 3 * n + a], -g[a]);
+    }
+    atomicAdd(&Jc[rowE], we * e);
+    if (A.w_s > 0.0) {
+      atomicAdd(&Jc[rowE + 1], -sw * d[0] * g[0]);
+      atomicAdd(&Jc[rowE + 2], -sw * d[1] * g[1]);
+      atomicAdd(&Jc[rowE + 3], -sw * d[2] * g[2]);
+      atomicAdd(&Jc[rowE + 4], -sw * d[0] * g[1]);
+      atomicAdd(&Jc[rowE + 5], -sw * d[0] * g[2]);
+      atomicAdd(&Jc[rowE + 6], -sw * d[1] * g[2]);
+    }
+  };
+  // ---- G1–G3: one thread per directed pair
+  for (int w = threadIdx.x; w < npair; w += blockDim.x) {
+    const int i = owner_of(pfirst, N, w);
+    int j;
+    T d[3];
+    pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
+    const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (r < T(1e-14) || r >= rc) continue;
+    const T rh[3] = {d[0] / r, d[1] / r, d[2] / r};
+    T fc, fcp;
+    ac_fc(r, rc, fc, fcp);
+    const int s = typ[j], ti = typ[i];
+    const T *w_ = W + ti * (L.S + 1);
+    const int *cl = col + ti * (L.S + 1);
+    T cw = T(0), ew = T(0);
+    auto term = [&](int idx, T g, T dg) {
+      if constexpr (JAC) {
+        const T gv[3] = {dg * rh[0], dg * rh[1], dg * rh[2]};
+        jac_add(cl[idx], i, j, gv, d, g);
+      } else {
+        cw += w_[idx] * dg;
+        ew += w_[idx] * g;
+      }
+    };
+    for (int t = 0; t < L.g1; ++t) term(L.base[0] + s * L.g1 + t, fc, fcp);
+    for (int t = 0; t < L.n2; ++t) {
+      const T eta = p2[2 * t], dr = r - p2[2 * t + 1];
+      const T gs = exp(-eta * dr * dr);
+      term(L.base[1] + s * L.n2 + t, gs * fc, gs * (T(-2) * eta * dr * fc + fcp));
+    }
+    for (int t = 0; t < L.n3; ++t) {
+      const T k = p3[t], cc = cos(k * r), ss = sin(k * r);
+      term(L.base[2] + s * L.n3 + t, cc * fc, -k * ss * fc + cc * fcp);
+    }
+    if constexpr (!JAC) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        atomicAdd(&Fs[3 * i + a], cw * rh[a]);
+        atomicAdd(&Fs[3 * j + a], -cw * rh[a]);
+      }
+      e_acc += static_cast<double>(ew);
+      sg[0] -= static_cast<double>(cw * d[0] * rh[0]);
+      sg[1] -= static_cast<double>(cw * d[1] * rh[1]);
+      sg[2] -= static_cast<double>(cw * d[2] * rh[2]);
+      sg[3] -= static_cast<double>(cw * d[0] * rh[1]);
+      sg[4] -= static_cast<double>(cw * d[0] * rh[2]);
+      sg[5] -= static_cast<double>(cw * d[1] * rh[2]);
+    }
+  }
+  // ---- G4, G5: one thread per neighbour pair (j < k) of a central atom i
+  if (L.n4 + L.n5 > 0)
+    for (int w = threadIdx.x; w < ntri; w += blockDim.x) {
+      const int i = owner_of(tfirst, N, w);
+      const int n = pfirst[i + 1] - pfirst[i];
+      int u = w - tfirst[i], a0 = 0;
+      while (u >= n - 1 - a0) {
+        u -= n - 1 - a0;
+        ++a0;
+      }
+      const int pj = pfirst[i] + a0, pk = pj + 1 + u;
+      int j, k;
+      T d1[3], d2[3];
+      pair_vec(wpos, shift, i, nbp[pj], j, d1[0], d1[1], d1[2]);
+      const T r1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+      if (r1 < T(1e-14) || r1 >= rc) continue;
+      pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
+      const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
+      if (r2 < T(1e-14) || r2 >= rc) continue;
+      const int ti = typ[i];
+      const T *w_ = W + ti * (L.S + 1);
+      const int *cl = col + ti * (L.S + 1);
+      const T h1[3] = {d1[0] / r1, d1[1] / r1, d1[2] / r1}, h2[3] = {d2[0] / r2, d2[1] / r2, d2[2] / r2};
+      T costh = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) / (r1 * r2);
+      costh = min(max(costh, T(-1)), T(1));
+      const T djk[3] = {d2[0] - d1[0], d2[1] - d1[1], d2[2] - d1[2]};
+      const T rjk = sqrt(djk[0] * djk[0] + djk[1] * djk[1] + djk[2] * djk[2]);
+      T hjk[3] = {T(0), T(0), T(0)};
+      if (rjk > T(1e-14))
+        for (int a = 0; a < 3; ++a) hjk[a] = djk[a] / rjk;
+      T f1, fp1, f2, fp2, fjk, fpjk;
+      ac_fc(r1, rc, f1, fp1);
+      ac_fc(r2, rc, f2, fp2);
+      ac_fc(rjk, rc, fjk, fpjk);
+      T dcj[3], dck[3];
+      for (int a = 0; a < 3; ++a) {
+        dcj[a] = (h2[a] - costh * h1[a]) / r1;
+        dck[a] = (h1[a] - costh * h2[a]) / r2;
+      }
+      const int po = pair_ord(typ[j], typ[k], nt);
+      T GJ[3] = {0, 0, 0}, GK[3] = {0, 0, 0}, ew = T(0);
+      auto term = [&](int idx, T eta, T zeta, T lambda, bool with_jk) {
+        const T Aa = T(1) + lambda * costh;
+        if (Aa <= T(1e-12)) return;
+        const T C = pow(T(2), T(1) - zeta), ang = pow(Aa, zeta), dang = zeta * pow(Aa, zeta - T(1)) * lambda;
+        const T rsum = r1 * r1 + r2 * r2 + (with_jk ? rjk * rjk : T(0));
+        const T rad = exp(-eta * rsum);
+        const T fj = with_jk ? fjk : T(1);
+        const T fcs = f1 * f2 * fj;
+        const T g = C * ang * rad * fcs;
+        const T cij = C * ang * (rad * (T(-2) * eta * r1) * fcs + rad * fp1 * f2 * fj);
+        const T cik = C * ang * (rad * (T(-2) * eta * r2) * fcs + rad * f1 * fp2 * fj);
+        const T cjk = with_jk ? C * ang * (rad * (T(-2) * eta * rjk) * fcs + rad * f1 * f2 * fpjk) : T(0);
+        const T ccos = C * rad * fcs * dang;
+        T gj[3], gk[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          gj[a] = cij * h1[a] - cjk * hjk[a] + ccos * dcj[a];
+          gk[a] = cik * h2[a] + cjk * hjk[a] + ccos * dck[a];
+        }
+        if constexpr (JAC) {
+          const int cc = cl[idx];
+          if (cc >= 0) {
+            // rows: j gets −gj, k gets −gk, i gets gj + gk; stress d1 ⊗ −gj + d2 ⊗ −gk
+            T *Jc = A.J + static_cast<int64_t>(cc) * A.ld;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              atomicAdd(&Jc[row0 + 3 * i + a], gj[a] + gk[a]);
+              atomicAdd(&Jc[row0 + 3 * j + a], -gj[a]);
+              atomicAdd(&Jc[row0 + 3 * k + a], -gk[a]);
+            }
+            atomicAdd(&Jc[rowE], we * g);
+            if (A.w_s > 0.0) {
+              atomicAdd(&Jc[rowE + 1], -sw * (d1[0] * gj[0] + d2[0] * gk[0]));
+              atomicAdd(&Jc[rowE + 2], -sw * (d1[1] * gj[1] + d2[1] * gk[1]));
+              atomicAdd(&Jc[rowE + 3], -sw * (d1[2] * gj[2] + d2[2] * gk[2]));
+              atomicAdd(&Jc[rowE + 4], -sw * (d1[0] * gj[1] + d2[0] * gk[1]));
+              atomicAdd(&Jc[rowE + 5], -sw * (d1[0] * gj[2] + d2[0] * gk[2]));
+              atomicAdd(&Jc[rowE + 6], -sw * (d1[1] * gj[2] + d2[1] * gk[2]));
+            }
+          }
+        } else {
+          ew += w_[idx] * g;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            GJ[a] += w_[idx] * gj[a];
+            GK[a] += w_[idx] * gk[a];
+          }
+        }
+      };
+      for (int t = 0; t < L.n4; ++t) term(L.base[3] + po * L.n4 + t, p4[3 * t], p4[3 * t + 1], p4[3 * t + 2], true);
+      for (int t = 0; t < L.n5; ++t) term(L.base[4] + po * L.n5 + t, p5[3 * t], p5[3 * t + 1], p5[3 * t + 2], false);
+      if constexpr (!JAC) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          atomicAdd(&Fs[3 * i + a], GJ[a] + GK[a]);
+          atomicAdd(&Fs[3 * j + a], -GJ[a]);
+          atomicAdd(&Fs[3 * k + a], -GK[a]);
+        }
+        e_acc += static_cast<double>(ew);
+        sg[0] -= static_cast<double>(d1[0] * GJ[0] + d2[0] * GK[0]);
+        sg[1] -= static_cast<double>(d1[1] * GJ[1] + d2[1] * GK[1]);
+        sg[2] -= static_cast<double>(d1[2] * GJ[2] + d2[2] * GK[2]);
+        sg[3] -= static_cast<double>(d1[0] * GJ[1] + d2[0] * GK[1]);
+        sg[4] -= static_cast<double>(d1[0] * GJ[2] + d2[0] * GK[2]);
+        sg[5] -= static_cast<double>(d1[1] * GJ[2] + d2[1] * GK[2]);
+      }
+    }
+  // biases: one per atom
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int ti = typ[i];
+    if constexpr (JAC) {
+      const int cb = col[ti * (L.S + 1) + L.S];
+      if (cb >= 0) atomicAdd(&A.J[static_cast<int64_t>(cb) * A.ld + rowE], we);
+    } else {
+      e_acc += static_cast<double>(W[ti * (L.S + 1) + L.S]);
+    }
+  }
+  if constexpr (JAC) return;
+  __syncthreads();
+  // residual rows of the configuration (residual_layout.hpp:37-54)
+  double objp = 0.0;
+  for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) {
+    const int64_t ga = static_cast<int64_t>(cd.atom0) * 3 + k;
+    const double f = static_cast<double>(Fs[k]);
+    const double res = f - A.c.ref_force[ga];
+    A.F[row0 + k] = res;
+    if (A.forces) A.forces[ga] = f;
+    objp += res * res;
+  }
+  double sums[8] = {e_acc, sg[0], sg[1], sg[2], sg[3], sg[4], sg[5], objp};
+  block_sum_k(sums, red);
+  if (threadIdx.x == 0) {
+    const double E = sums[0], iv = 1.0 / cd.volume;
+    double st[6];
+    for (int a = 0; a < 6; ++a) st[a] = sums[1 + a] * iv;
+    int64_t row = rowE;
+    double o = sums[7];
+    const double re = A.w_e * (E - cd.ref_energy);
+    A.F[row++] = re;
+    o += re * re;
+    static constexpr int vi[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    if (A.w_s > 0.0)
+      for (int v = 0; v < 6; ++v) {
+        const double rs = A.w_s * (st[v] - cd.ref_stress[3 * vi[v][0] + vi[v][1]]);
+        A.F[row++] = rs;
+        o += rs * rs;
+      }
+    A.F[row++] = 0.0; // ML models have no embedding range penalty
+    A.obj_part[c] = o;
+    if (A.energy) A.energy[c] = E;
+    if (A.limit) A.limit[c] = 0.0;
+    if (A.stress9) { // the configuration's virial is symmetric: upper triangle mirrored
+      double *s9 = A.stress9 + 9 * static_cast<int64_t>(c);
+      s9[0] = st[0];
+      s9[4] = st[1];
+      s9[8] = st[2];
+      s9[1] = s9[3] = st[3];
+      s9[2] = s9[6] = st[4];
+      s9[5] = s9[7] = st[5];
+    }
+  }
+}
+
+__global__ void ac_sum_parts(const double *__restrict__ part, int n, double *__restrict__ out) {
+  __shared__ double r[32];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) s += part[k];
+  s = block_sum(s, r);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// Jᵀr: one CTA per column, FP64 sums over the rows.
+template <class T>
+__global__ void ac_jtr_kernel(const T *__restrict__ J, int64_t ld, int64_t M, const double *__restrict__ F,
+                              double *__restrict__ Jtr) {
+  __shared__ double r[32];
+  const T *Jc = J + static_cast<int64_t>(blockIdx.x) * ld;
+  double s = 0.0;
+  for (int64_t k = threadIdx.x; k < M; k += blockDim.x) s += static_cast<double>(Jc[k]) * F[k];
+  s = block_sum(s, r);
+  if (threadIdx.x == 0) Jtr[blockIdx.x] = s;
+}
+
+template <class T> size_t ac_smem(const fs_gpu *h, int mi) {
+  AcLayout L;
+  L.init(h->tables[0].v.data(), h->ntypes);
+  const int N = h->max_natoms, nt = h->ntypes, nspec = h->tables[0].n;
+  return align16(nspec * sizeof(T)) + align16(nt * (L.S + 1) * sizeof(T)) + align16(nt * (L.S + 1) * sizeof(int)) +
+         align16(3 * N * sizeof(double)) + align16(3 * mi * sizeof(double)) + align16(N) + align16(3 * N * sizeof(T)) +
+         align16(8 * 32 * sizeof(double)) + 2 * align16((N + 1) * sizeof(int)) + align16(32 * sizeof(int)) + 160;
+}
+
+template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) {
+  AcArgs<T> a;
+  a.c.cfg = h->d_cfg;
+  a.c.wpos = h->d_wpos;
+  a.c.type = h->d_type;
+  a.c.ref_force = h->d_ref_force;
+  a.c.nb_start = h->d_nb_start;
+  a.c.nb_pack = h->d_nb_pack;
+  a.c.desc = h->d_desc;
+  a.c.cmap = h->d_cmap;
+  a.c.n_tables = static_cast<int>(h->desc.size());
+  a.c.n_segs = h->n_segs;
+  a.c.n_cmap = h->n_cmap;
+  a.c.ntypes = h->ntypes;
+  a.c.family = h->family;
+  a.vals = h->d_vals;
+  a.w_e = w_e;
+  a.w_s = w_s;
+  a.F = h->d_F;
+  a.forces = h->d_forces;
+  a.energy = h->d_energy;
+  a.stress9 = h->d_stress9;
+  a.limit = h->d_limit;
+  a.obj_part = h->d_obj_part;
+  a.order = h->d_cfg_by_work;
+  a.J = nullptr;
+  a.ld = 0;
+  int mi = 1;
+  for (const CfgDev &cd : h->cfg_host) mi = std::max(mi, (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1));
+  const size_t sm = ac_smem<T>(h, mi);
+  if (sm > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "ACSF: configuration too large for shared memory");
+  const int64_t M = rows_of(h, w_s);
+  const int D = h->D;
+  if (jac) {
+    const int64_t ldj = (M + 31) / 32 * 32;
+    const size_t jn = static_cast<size_t>(ldj) * D;
+    if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J) {
+      if (h->d_J) cudaFree(h->d_J);
+      h->d_J = nullptr;
+      FS_CUDA(cudaMalloc(&h->d_J, std::max<size_t>(jn, 1) * sizeof(T)));
+      h->jac_alloc = static_cast<int64_t>(jn);
+      h->ldj = ldj;
+    }
+    if (!h->d_JtJ) {
+      FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
+      FS_CUDA(cudaMalloc(&h->d_Jtr, std::max(D, 1) * sizeof(double)));
+    }
+    FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
+    a.J = static_cast<T *>(h->d_J);
+    a.ld = ldj;
+  }
+  auto k = jac ? acsf_kernel<T, true> : acsf_kernel<T, false>;
+  FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+  k<<<h->n_cfg, kAcThreads, sm, h->stream>>>(a);
+  FS_CUDA(cudaGetLastError());
+  ++h->launches;
+  if (jac) {
+    if (D > 0) {
+      ac_jtr_kernel<T><<<D, 256, 0, h->stream>>>(static_cast<const T *>(h->d_J), h->ldj, M, h->d_F, h->d_Jtr);
+      FS_CUDA(cudaGetLastError());
+      ++h->launches;
+    }
+  } else {
+    ac_sum_parts<<<1, 1024, 0, h->stream>>>(h->d_obj_part, h->n_cfg, h->d_obj);
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+  }
+  return FS_OK;
+}
+
+} // namespace
+
+int eval_residual_acsf(fs_gpu *h, double w_e, double w_s) {
+  return h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, w_e, w_s, false) : launch_acsf<float>(h, w_e, w_s, false);
+}
+int eval_jacobian_acsf(fs_gpu *h, double w_e, double w_s) {
+  return h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, w_e, w_s, true) : launch_acsf<float>(h, w_e, w_s, true);
+}
+
+} // namespace fsg

@@ -75,6 +75,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_SW: return np + 1;
   case FS_FAMILY_TERSOFF: return np;
   case FS_FAMILY_ANGULAR: return 2 * np + nt;
+  case FS_FAMILY_ACSF: return 1 + nt;
   }
   return -1;
 }
@@ -376,7 +377,29 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
     ht.rmin = ft.rmin;
     ht.rmax = ft.rmax;
     const bool sw_fam = m->family == FS_FAMILY_SW;
-    if (m->family == FS_FAMILY_TERSOFF) {
+    if (m->family == FS_FAMILY_ACSF) {
+      // the descriptor table {rcut, nG1..nG5, parameters}, then one linear head
+      // {w[S], b} per species
+      const fs_table &spec = m->tables[0];
+      bool ok = spec.kind == FS_TABLE_ACSF && spec.n >= 6 && spec.values[0] > 0.0;
+      int need = 6;
+      for (int k = 1; ok && k < 6; ++k) ok = spec.values[k] >= 0 && spec.values[k] == std::floor(spec.values[k]);
+      if (ok) {
+        need += 2 * static_cast<int>(spec.values[2]) + static_cast<int>(spec.values[3]) +
+                3 * static_cast<int>(spec.values[4]) + 3 * static_cast<int>(spec.values[5]);
+        ok = spec.n == need;
+      }
+      if (!ok) return set_error(h, FS_ERR_ARG, "set_model: ACSF table {rcut, nG1..nG5, parameters} is malformed");
+      if (t > 0) {
+        const int nt = m->ntypes, P = nt * (nt + 1) / 2;
+        const int S = nt * static_cast<int>(spec.values[1] + spec.values[2] + spec.values[3]) +
+                      P * static_cast<int>(spec.values[4] + spec.values[5]);
+        if (ft.kind != FS_TABLE_LINEAR_HEAD || ft.n != S + 1)
+          return set_error(h, FS_ERR_ARG, "set_model: ACSF heads are linear_head[nt] with S + 1 values");
+      }
+    } else if (ft.kind == FS_TABLE_ACSF || ft.kind == FS_TABLE_LINEAR_HEAD) {
+      return set_error(h, FS_ERR_ARG, "set_model: ACSF tables belong to the ACSF family");
+    } else if (m->family == FS_FAMILY_TERSOFF) {
       if (ft.kind != FS_TABLE_TERSOFF || ft.n != 12)
         return set_error(h, FS_ERR_ARG, "set_model: Tersoff tables are tersoff[npair] with 12 params");
     } else if (ft.kind == FS_TABLE_TERSOFF) {

@@ -623,6 +623,8 @@ template <class T> int launch_sw(fs_gpu *h, double w_e, double w_s, bool jac) {
 int eval_residual_adp(fs_gpu *h, double w_e, double w_s);
 int eval_residual_tersoff(fs_gpu *h, double w_e, double w_s);
 int eval_residual_angular(fs_gpu *h, double w_e, double w_s);
+int eval_residual_acsf(fs_gpu *h, double w_e, double w_s);
+int eval_jacobian_acsf(fs_gpu *h, double w_e, double w_s);
 int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s);
 
 int eval_residual_other(fs_gpu *h, double w_e, double w_s) {
@@ -631,6 +633,7 @@ int eval_residual_other(fs_gpu *h, double w_e, double w_s) {
   if (h->family == FS_FAMILY_ADP) return eval_residual_adp(h, w_e, w_s);
   if (h->family == FS_FAMILY_TERSOFF) return eval_residual_tersoff(h, w_e, w_s);
   if (h->family == FS_FAMILY_ANGULAR) return eval_residual_angular(h, w_e, w_s);
+  if (h->family == FS_FAMILY_ACSF) return eval_residual_acsf(h, w_e, w_s);
   return set_error(h, FS_ERR_UNSUPPORTED, "residual: family not handled by this build");
 }
 
@@ -642,6 +645,8 @@ int eval_jacobian_other(fs_gpu *h, double w_e, double w_s) {
     mark(h, 3);
     return rc;
   }
+  // ACSF with linear heads: exact (the model is linear in its coefficients)
+  if (h->family == FS_FAMILY_ACSF) return eval_jacobian_acsf(h, w_e, w_s);
   // ADP, Tersoff, Angular: the reference's own central differences (FP64 contexts)
   if (h->family == FS_FAMILY_ADP || h->family == FS_FAMILY_TERSOFF || h->family == FS_FAMILY_ANGULAR)
     return eval_jacobian_fd(h, w_e, w_s);

@@ -83,8 +83,11 @@ enum fs_family {
   FS_FAMILY_ADP = 2,  /* tables: EAM + dipole[npair], quadrupole[npair]     */
   FS_FAMILY_SW = 3,   /* tables: sw[npair] (8 params each), lambda[1]       */
   FS_FAMILY_TERSOFF = 4, /* tables: tersoff[npair] (12 params each)        */
-  FS_FAMILY_ANGULAR = 5  /* tables: pair[npair], radial[npair], angular[nt]:
+  FS_FAMILY_ANGULAR = 5, /* tables: pair[npair], radial[npair], angular[nt]:
                             spline or analytic (angular_force.hpp:15-33)   */
+  FS_FAMILY_ACSF = 6     /* tables: acsf[1] (descriptor), head[nt] (linear
+                            energy head per species) (acsf.hpp:48-86,
+                            ml_force.hpp LinearHead)                       */
 };
 
 enum fs_table_kind {
@@ -92,9 +95,17 @@ enum fs_table_kind {
   FS_TABLE_ANALYTIC = 1, /* closed form `form` with n parameters            */
   FS_TABLE_SW = 2,       /* SWParams {A,B,p,q,delta,a1,gamma,a2}, n == 8    */
   FS_TABLE_LAMBDA = 3,   /* SW triplet strengths, n == nt * npair           */
-  FS_TABLE_TERSOFF = 4   /* TersoffParams {A,B,lambda,mu,beta,n,c,d,h,R,S,omega},
+  FS_TABLE_TERSOFF = 4,  /* TersoffParams {A,B,lambda,mu,beta,n,c,d,h,R,S,omega},
                             n == 12 (include/forcesmith/force/tersoff_force.hpp:17-31;
                             gather order tersoff_force.cpp:14-25)          */
+  FS_TABLE_ACSF = 5,     /* ACSF symmetry functions, all values fixed:
+                            {rcut, nG1, nG2, nG3, nG4, nG5,
+                             (eta, rs) × nG2, kappa × nG3,
+                             (eta, zeta, lambda) × nG4, (eta, zeta, lambda) × nG5};
+                            descriptor size S = nt(nG1 + nG2 + nG3)
+                            + npair(nG4 + nG5) (AcsfLayout, acsf.hpp:23-33) */
+  FS_TABLE_LINEAR_HEAD = 6 /* E_i = w·D_i + b: {w[S], b}, n == S + 1; the
+                            bias is fixed unless `fixed` says otherwise    */
 };
 
 /* Analytic radial forms (include/forcesmith/potentials/analytic_potential.hpp). */

@@ -158,6 +158,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_SW: return np + 1;
   case FS_FAMILY_TERSOFF: return np;
   case FS_FAMILY_ANGULAR: return 2 * np + nt;
+  case FS_FAMILY_ACSF: return 1 + nt;
   }
   return -1;
 }
@@ -173,6 +174,7 @@ double max_cutoff(const State &S) {
       m = std::max(m, std::max(S.tables[p].v[5], S.tables[p].v[7]));
     return m;
   }
+  if (S.family == FS_FAMILY_ACSF) return S.tables[0].v[0]; // descriptor_cutoff (acsf.hpp:73)
   if (S.family == FS_FAMILY_TERSOFF) { // max S over pair slots (tersoff_force.cpp:259-265)
     for (int p = 0; p < np; ++p) m = std::max(m, S.tables[p].v[10]);
     return m;
@@ -266,7 +268,9 @@ void prime_sites(State &S) {
   const int64_t P = S.nb_j.size();
   for (auto &v : S.site) v.assign(P, Site{});
   for (auto &v : S.site_ok) v.assign(P, 0);
-  if (S.family == FS_FAMILY_SW || S.family == FS_FAMILY_TERSOFF || S.family == FS_FAMILY_ANGULAR) return;
+  if (S.family == FS_FAMILY_SW || S.family == FS_FAMILY_TERSOFF || S.family == FS_FAMILY_ANGULAR ||
+      S.family == FS_FAMILY_ACSF)
+    return;
   const Roles R{npair_of(S.ntypes), S.ntypes};
 #pragma omp parallel for schedule(dynamic)
   for (int c = 0; c < static_cast<int>(S.cfgs.size()); ++c) {
@@ -790,6 +794,154 @@ void eval_angular(const State &S, int c, Out &o) {
   }
 }
 
+// ACSF descriptors (src/force/acsf.cpp) with a linear energy head per
+// species (LinearHead, src/force/ml_force.cpp:11-47), evaluated as
+// MLBase::eval_forces (include/forcesmith/force/ml_force.hpp): E_i = b + w·D_i;
+// F_i −= (∂D_i/∂r_i)ᵀ w, F_j −= (∂D_i/∂r_j)ᵀ w, σ += d_ij ⊗ F_j part
+// (accumulate_atom_forces).  The head gradient w is constant, so each term's
+// descriptor gradient is weighted by its coefficient as it is formed.
+struct AcsfSpec {
+  double rcut;
+  int g1, n2, n3, n4, n5;
+  const double *p2, *p3, *p4, *p5; // (eta, rs), kappa, (eta, zeta, lambda) ×2
+  explicit AcsfSpec(const double *v)
+      : rcut(v[0]), g1(static_cast<int>(v[1])), n2(static_cast<int>(v[2])), n3(static_cast<int>(v[3])),
+        n4(static_cast<int>(v[4])), n5(static_cast<int>(v[5])) {
+    p2 = v + 6;
+    p3 = p2 + 2 * n2;
+    p4 = p3 + n3;
+    p5 = p4 + 3 * n4;
+  }
+  // AcsfLayout (acsf.hpp:23-46): blocks G1..G3 per species, G4, G5 per pair
+  int index(int block, int chan, int t, int nt) const {
+    const int P = nt * (nt + 1) / 2;
+    const int cnt[5] = {g1, n2, n3, n4, n5}, nch[5] = {nt, nt, nt, P, P};
+    int base = 0;
+    for (int b = 0; b < block; ++b) base += cnt[b] * nch[b];
+    return base + chan * cnt[block] + t;
+  }
+};
+// number of values an ACSF table must have (−1 if the counts are invalid)
+int acsf_values(const double *v, int n) {
+  if (n < 6) return -1;
+  for (int k = 1; k < 6; ++k)
+    if (v[k] < 0 || v[k] != std::floor(v[k])) return -1;
+  return 6 + 2 * static_cast<int>(v[2]) + static_cast<int>(v[3]) + 3 * static_cast<int>(v[4]) +
+         3 * static_cast<int>(v[5]);
+}
+int acsf_size(const AcsfSpec &A, int nt) {
+  return nt * (A.g1 + A.n2 + A.n3) + nt * (nt + 1) / 2 * (A.n4 + A.n5);
+}
+// cutoff (acsf.cpp:15-23)
+inline void acsf_fc(double r, double rc, double &fc, double &fcp) {
+  if (r >= rc) {
+    fc = fcp = 0.0;
+    return;
+  }
+  const double x = kPi * r / rc;
+  fc = 0.5 * (1.0 + std::cos(x));
+  fcp = -0.5 * kPi / rc * std::sin(x);
+}
+
+void eval_acsf(const State &S, int c, Out &o) {
+  const Config &cf = S.cfgs[c];
+  const int nt = S.ntypes;
+  const AcsfSpec A(S.tables[0].v.data());
+  const int Sz = acsf_size(A, nt);
+  struct Nb {
+    int64_t p; // the entry in the atom's neighbour list
+    Vec3 d, rh;
+    double r, fc, fcp;
+    int s;
+  };
+  for (int i = 0; i < cf.natoms; ++i) {
+    const int64_t gi = cf.atom0 + i;
+    const int ti = S.type[gi];
+    const double *w = S.tables[1 + ti].v.data();
+    const int64_t s0 = S.nb_start[gi], s1 = S.nb_start[gi + 1];
+    std::vector<Nb> nb; // collect_neighbors (acsf.cpp:84-99): 1e-14 ≤ r < rcut
+    for (int64_t p = s0; p < s1; ++p) {
+      const Vec3 &d = S.nb_d[p];
+      const double r = norm(d);
+      if (r < 1e-14 || r >= A.rcut) continue;
+      Nb n{p, d, (1.0 / r) * d, r, 0.0, 0.0, S.type[cf.atom0 + S.nb_j[p]]};
+      acsf_fc(r, A.rcut, n.fc, n.fcp);
+      nb.push_back(n);
+    }
+    std::vector<Vec3> gw(s1 - s0, Vec3{0, 0, 0}); // (∂D_i/∂r_j)ᵀ w per neighbour entry
+    Vec3 gself{0, 0, 0};
+    double e = w[Sz];
+    // accumulate_radial (acsf.cpp:101-131) with scatter_radial (:25-30)
+    auto radial = [&](const Nb &n, int idx, double g, double dg) {
+      e += w[idx] * g;
+      gw[n.p - s0] = gw[n.p - s0] + (w[idx] * dg) * n.rh;
+      gself = gself - (w[idx] * dg) * n.rh;
+    };
+    for (const Nb &n : nb) {
+      for (int t = 0; t < A.g1; ++t) radial(n, A.index(0, n.s, t, nt), n.fc, n.fcp);
+      for (int t = 0; t < A.n2; ++t) {
+        const double eta = A.p2[2 * t], rs = A.p2[2 * t + 1], dr = n.r - rs;
+        const double gauss = std::exp(-eta * dr * dr);
+        radial(n, A.index(1, n.s, t, nt), gauss * n.fc, gauss * (-2.0 * eta * dr * n.fc + n.fcp));
+      }
+      for (int t = 0; t < A.n3; ++t) {
+        const double k = A.p3[t], cc = std::cos(k * n.r), ss = std::sin(k * n.r);
+        radial(n, A.index(2, n.s, t, nt), cc * n.fc, -k * ss * n.fc + cc * n.fcp);
+      }
+    }
+    // accumulate_angular (acsf.cpp:133-183) with scatter_angular (:43-79)
+    if (A.n4 + A.n5 > 0)
+      for (size_t a = 0; a < nb.size(); ++a)
+        for (size_t b = a + 1; b < nb.size(); ++b) {
+          const Nb &J = nb[a], &K = nb[b];
+          const double costh = std::clamp(dot(J.d, K.d) / (J.r * K.r), -1.0, 1.0);
+          const Vec3 djk = K.d - J.d;
+          const double rjk = norm(djk);
+          const Vec3 rjk_h = rjk > 1e-14 ? (1.0 / rjk) * djk : Vec3{0, 0, 0};
+          double fcjk, fcpjk;
+          acsf_fc(rjk, A.rcut, fcjk, fcpjk);
+          const Vec3 dcj = (1.0 / J.r) * (K.rh - costh * J.rh), dck = (1.0 / K.r) * (J.rh - costh * K.rh);
+          const int po = pair_ordinal(J.s, K.s, nt);
+          auto angular = [&](int idx, double eta, double zeta, double lambda, bool with_jk) {
+            const double Aa = 1.0 + lambda * costh;
+            if (Aa <= 1e-12) return;
+            const double C = std::pow(2.0, 1.0 - zeta), ang = std::pow(Aa, zeta);
+            const double dang = zeta * std::pow(Aa, zeta - 1.0) * lambda;
+            const double rsum = J.r * J.r + K.r * K.r + (with_jk ? rjk * rjk : 0.0);
+            const double rad = std::exp(-eta * rsum);
+            const double fjk = with_jk ? fcjk : 1.0;
+            const double fcs = J.fc * K.fc * fjk;
+            e += w[idx] * (C * ang * rad * fcs);
+            const double drij = rad * (-2.0 * eta * J.r), drik = rad * (-2.0 * eta * K.r);
+            const double drjk = with_jk ? rad * (-2.0 * eta * rjk) : 0.0;
+            const double dfij = J.fcp * K.fc * fjk, dfik = J.fc * K.fcp * fjk;
+            const double dfjk = with_jk ? J.fc * K.fc * fcpjk : 0.0;
+            const double cij = C * ang * (drij * fcs + rad * dfij), cik = C * ang * (drik * fcs + rad * dfik);
+            const double cjk = C * ang * (drjk * fcs + rad * dfjk), ccos = C * rad * fcs * dang;
+            const Vec3 gj = cij * J.rh - cjk * rjk_h + ccos * dcj;
+            const Vec3 gk = cik * K.rh + cjk * rjk_h + ccos * dck;
+            gw[J.p - s0] = gw[J.p - s0] + w[idx] * gj;
+            gw[K.p - s0] = gw[K.p - s0] + w[idx] * gk;
+            gself = gself - w[idx] * (gj + gk);
+          };
+          for (int t = 0; t < A.n4; ++t)
+            angular(A.index(3, po, t, nt), A.p4[3 * t], A.p4[3 * t + 1], A.p4[3 * t + 2], true);
+          for (int t = 0; t < A.n5; ++t)
+            angular(A.index(4, po, t, nt), A.p5[3 * t], A.p5[3 * t + 1], A.p5[3 * t + 2], false);
+        }
+    // energy and accumulate_atom_forces
+    o.energy += e;
+    o.force[i] = o.force[i] - gself;
+    for (int64_t p = s0; p < s1; ++p) {
+      const Vec3 fj = -1.0 * gw[p - s0];
+      const int j = S.nb_j[p];
+      o.force[j] = o.force[j] + fj;
+      for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb) o.stress[a][bb] += S.nb_d[p][a] * fj[bb];
+    }
+  }
+}
+
 // with_eval_scope (include/forcesmith/force/eval_scope.hpp:13-31): zero,
 // run the kernel, σ /= V.
 void eval_config(const State &S, int c, Out &o) {
@@ -804,6 +956,7 @@ void eval_config(const State &S, int c, Out &o) {
   case FS_FAMILY_SW: eval_sw(S, c, o); break;
   case FS_FAMILY_TERSOFF: eval_tersoff(S, c, o); break;
   case FS_FAMILY_ANGULAR: eval_angular(S, c, o); break;
+  case FS_FAMILY_ACSF: eval_acsf(S, c, o); break;
   }
   const double V = cf.pbc.volume;
   for (auto &row : o.stress)
@@ -1160,6 +1313,12 @@ int orc_set_model(orc_state *h, const fs_model *m) {
     if (ft.kind == FS_TABLE_SPLINE && (ft.n < 2 || !(ft.rmax > ft.rmin))) return FS_ERR_ARG;
     if (ft.kind == FS_TABLE_ANALYTIC && form_nparams(ft.form) != ft.n) return FS_ERR_ARG;
     if ((m->family == FS_FAMILY_TERSOFF) != (ft.kind == FS_TABLE_TERSOFF)) return FS_ERR_ARG;
+    if (m->family == FS_FAMILY_ACSF) {
+      const int want = t == 0 ? FS_TABLE_ACSF : FS_TABLE_LINEAR_HEAD;
+      if (ft.kind != want) return FS_ERR_ARG;
+      if (t == 0 && acsf_values(ft.values, ft.n) != ft.n) return FS_ERR_ARG;
+      if (t > 0 && ft.n != acsf_size(AcsfSpec(m->tables[0].values), m->ntypes) + 1) return FS_ERR_ARG;
+    }
     if (ft.kind == FS_TABLE_TERSOFF && ft.n != 12) return FS_ERR_ARG;
     S.tables[t].init(ft);
   }

@@ -1,0 +1,106 @@
+"""ACSF descriptors with linear heads on the device against the oracle
+(through the C ABI).
+
+Tolerances:
+  FP64  forces, energy, stress, F rows   |Δ| ≤ 1e-9·(1 + |x|); objective 1e-9 relative
+  FP32  forces                           |Δ| ≤ 2e-5·max|F|;    objective 1e-4 relative
+  Jacobian (exact on the device; the oracle's central differences are exact
+  up to rounding, the model being linear in its coefficients: noise
+  ≈ 1e-16·|F| / 2h with h = 1e-5)
+        FP64 |ΔJ| ≤ 1e-6·max|J column| + 1e-9;  FP32 |ΔJ| ≤ 1e-4·max|J column|
+  lsq   one normal-equations step from a perturbed head recovers the labels:
+        objective after ≤ 1e-8 × objective before (FP64)
+"""
+import numpy as np
+import pytest
+
+from forcesmith_b200 import synth
+from forcesmith_b200.abi import FS_FAMILY_ACSF, Model, Table, acsf_size
+from oracle import api as O
+from tests.helpers import label
+
+pytestmark = pytest.mark.gpu
+
+SPEC = Table.acsf(4.2, g1=1, g2=[(0.5, 2.3), (1.0, 3.0), (2.0, 3.8), (0.3, 0.0)], g3=[1.1],
+                  g4=[(0.05, 1.0, 1.0), (0.05, 2.0, -1.0)], g5=[(0.08, 1.5, 1.0)])
+
+
+def model(nt, seed):
+    S = acsf_size(SPEC, nt)
+    rng = np.random.default_rng(seed)
+    return Model(FS_FAMILY_ACSF, nt, [SPEC] + [Table.linear_head(rng.normal(0, 0.3, S), bias=-3.0 + t)
+                                               for t in range(nt)])
+
+
+def _pair(ds, m, precision):
+    from forcesmith_b200.gpu import GpuSession
+    g = GpuSession(0, precision)
+    g.upload(ds)
+    g.set_model(m)
+    o = O.Oracle()
+    o.upload(ds)
+    o.set_model(m)
+    return g, o
+
+
+def _close(a, b, rel, what):
+    err = np.max(np.abs(np.asarray(a) - np.asarray(b)) / (1.0 + np.abs(np.asarray(b))))
+    assert err <= rel, f"{what}: {err:.3e}"
+
+
+@pytest.fixture(scope="module", params=[1, 2], ids=["one", "two"])
+def case(request):
+    nt = request.param
+    ds = synth.diamond(4, cells=(2, 3), seed=71)
+    if nt == 2:
+        ds.type[:] = np.random.default_rng(9).integers(0, 2, ds.type.size)
+    ds = label(ds, model(nt, 1), O.Oracle, 1.0, 0.2)
+    return ds, model(nt, 2)
+
+
+def test_acsf_residual_fp64(case):
+    ds, start = case
+    g, o = _pair(ds, start, "fp64")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    _close(rg["forces"], ro["forces"], 1e-9, "forces")
+    _close(rg["energy"], ro["energy"], 1e-9, "energy")
+    _close(rg["stress"], ro["stress"], 1e-9, "stress")
+    _close(rg["F"], ro["F"], 1e-9, "F")
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-9 * ro["obj"]
+
+
+def test_acsf_residual_fp32(case):
+    ds, start = case
+    g, o = _pair(ds, start, "fp32")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    assert np.max(np.abs(rg["forces"] - ro["forces"])) <= 2e-5 * np.max(np.abs(ro["forces"]))
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-4 * ro["obj"]
+
+
+@pytest.mark.parametrize("precision,rel,floor", [("fp64", 1e-6, 1e-9), ("fp32", 1e-4, 0.0)])
+def test_acsf_jacobian(case, precision, rel, floor):
+    ds, start = case
+    g, o = _pair(ds, start, precision)
+    res = g.jacobian(1.0, 0.2)
+    Jf = o.jacobian_fd(1.0, 0.2)
+    assert res["J"].shape == Jf.shape
+    colmax = np.abs(Jf).max(axis=0)
+    bar = rel * colmax + floor + 1e-30
+    ratio = np.abs(res["J"] - Jf) / bar
+    r, c = np.unravel_index(np.argmax(ratio), ratio.shape)
+    assert ratio.max() <= 1.0, (ratio.max(), r, c, res["J"][r, c], Jf[r, c])
+    F = o.eval(1.0, 0.2)["F"]
+    _, Jtr = O.normal_equations(Jf, F)
+    assert np.max(np.abs(res["Jtr"] - Jtr)) <= 10 * rel * np.max(np.abs(Jtr))
+
+
+def test_acsf_lsq_step_recovers_labels(case):
+    """NormalEquationsSolver on the device (the reference's lsq for linear
+    heads): one step from the perturbed head to the labelling head."""
+    ds, start = case
+    g, _ = _pair(ds, start, "fp64")
+    before = g.jacobian(1.0, 0.2)["obj"]
+    dx = g.lsq_step(0.0)
+    g.set_params(g.gather_params() + dx)
+    after = g.eval(1.0, 0.2, want=("obj",))["obj"]
+    assert after <= 1e-8 * before, (before, after)

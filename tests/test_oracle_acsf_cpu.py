@@ -1,0 +1,90 @@
+"""The oracle's ACSF + linear-head restatement, pinned against the
+reference's unit tests (tests/unit/test_acsf.cpp, tests/unit/test_ml_force.cpp):
+the 4-atom environment (origin plus three neighbours) and the dimer in a
+100 Å box, rcut = 6.
+
+  DescriptorSizeFormula    S = nt(1 + 2 + 1) + npair(2 + 1)
+  G1HandValue / G3HandValue / DimerDescriptorMatchesHand
+                           energies of a unit head = Σ_i D_i, by hand       1e-12
+  AnalyticForceMatchesEnergyFD, NewtonThirdLaw, BeyondCutoffZero
+"""
+import numpy as np
+import pytest
+
+from forcesmith_b200.abi import FS_FAMILY_ACSF, Model, Table, acsf_size
+from oracle import api as O
+from tests.helpers import cluster
+
+ENV = [[0.0, 0.0, 0.0], [2.1, 0.3, -0.2], [0.4, 2.0, 0.5], [-1.3, 0.7, 1.9]]
+
+
+def fc(r, rc=6.0):
+    return np.where(r < rc, 0.5 * (1 + np.cos(np.pi * r / rc)), 0.0)
+
+
+def run(pos, spec, coeffs, bias=0.0, types=None, nt=1):
+    heads = [Table.linear_head(coeffs, bias) for _ in range(nt)]
+    o = O.Oracle()
+    o.upload(cluster(pos, 100.0, types=types))
+    o.set_model(Model(FS_FAMILY_ACSF, nt, [spec] + heads))
+    return o.eval(1.0, 0.0)
+
+
+def pair_dists(pos):
+    p = np.asarray(pos)
+    d = np.linalg.norm(p[:, None] - p[None], axis=-1)
+    return d[~np.eye(len(p), dtype=bool)]
+
+
+def test_descriptor_size_formula():
+    spec = Table.acsf(6.0, g1=1, g2=[(1.0, 0.0), (0.5, 1.0)], g3=[1.0], g4=[(1.0, 1.0, 1.0), (0.5, 2.0, -1.0)],
+                      g5=[(1.0, 1.0, 1.0)])
+    for S in (1, 2, 3):
+        assert acsf_size(spec, S) == S * (1 + 2 + 1) + S * (S + 1) // 2 * (2 + 1)
+
+
+def test_g1_g3_hand_values():
+    r = pair_dists(ENV)
+    out = run(ENV, Table.acsf(6.0, g1=1), [1.0])
+    assert abs(out["energy"][0] - fc(r).sum()) <= 1e-12
+    out = run(ENV, Table.acsf(6.0, g3=[1.3]), [1.0])
+    assert abs(out["energy"][0] - (np.cos(1.3 * r) * fc(r)).sum()) <= 1e-12
+
+
+def test_dimer_g2_hand_value_and_bias():
+    r, eta, rs = 2.5, 0.8, 1.0
+    out = run([[0, 0, 0], [r, 0, 0]], Table.acsf(6.0, g2=[(eta, rs)]), [1.0], bias=0.25)
+    e = np.exp(-eta * (r - rs) ** 2) * fc(np.array(r))
+    assert abs(out["energy"][0] - 2 * (e + 0.25)) <= 1e-12
+
+
+@pytest.mark.parametrize("angular", [False, True])
+def test_forces_match_energy_fd_and_newton(angular):
+    spec = Table.acsf(6.0, g1=1, g2=[(0.5, 0.0), (1.2, 1.5)], g3=[0.9],
+                      g4=[(0.3, 1.0, 1.0), (0.2, 2.0, -1.0)] if angular else (),
+                      g5=[(0.4, 1.5, 1.0)] if angular else ())
+    w = np.linspace(0.3, -0.2, acsf_size(spec, 1))
+    out = run(ENV, spec, w)
+    assert np.linalg.norm(out["forces"].sum(axis=0)) <= 1e-12
+    h = 1e-6
+    for atom in (0, 2):
+        for a in range(3):
+            pp = np.array(ENV, float)
+            pp[atom, a] += h
+            pm = np.array(ENV, float)
+            pm[atom, a] -= h
+            fd = -(run(pp, spec, w)["energy"][0] - run(pm, spec, w)["energy"][0]) / (2 * h)
+            assert abs(out["forces"][atom, a] - fd) <= 1e-6 * abs(fd) + 1e-9, (atom, a)
+    s = out["stress"][0].reshape(3, 3)
+    assert np.max(np.abs(s - s.T)) <= 1e-12
+
+
+def test_beyond_cutoff_zero_and_species_channels():
+    out = run([[0, 0, 0], [6.5, 0, 0]], Table.acsf(6.0, g2=[(0.5, 0.0)]), [1.0])
+    assert abs(out["energy"][0]) <= 1e-14 and np.max(np.abs(out["forces"])) <= 1e-14
+    # two species, every atom of species 0: the species-1 channel stays empty,
+    # so its coefficient changes nothing
+    spec = Table.acsf(6.0, g2=[(0.5, 0.0)])
+    a = run(ENV, spec, [1.0, 0.0], nt=2, types=[0, 0, 0, 0])
+    b = run(ENV, spec, [1.0, 5.0], nt=2, types=[0, 0, 0, 0])
+    assert abs(a["energy"][0] - b["energy"][0]) <= 1e-14
