@@ -28,9 +28,9 @@ import os
 
 import numpy as np
 
-from .abi import (FS_FAMILY_ADP, FS_FAMILY_ANGULAR, FS_FAMILY_EAM, FS_FAMILY_PAIR, FS_FAMILY_SW,
-                  FS_FAMILY_TERSOFF, FS_TABLE_ANALYTIC, FS_TABLE_LAMBDA, FS_TABLE_SPLINE, FS_TABLE_SW,
-                  FS_TABLE_TERSOFF, FORMS, TERSOFF_FIELDS, Dataset, Model, Table)
+from .abi import (FS_FAMILY_ACSF, FS_FAMILY_ADP, FS_FAMILY_ANGULAR, FS_FAMILY_EAM, FS_FAMILY_PAIR,
+                  FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_TABLE_ANALYTIC, FS_TABLE_LAMBDA, FS_TABLE_SPLINE,
+                  FS_TABLE_SW, FS_TABLE_TERSOFF, FORMS, TERSOFF_FIELDS, Dataset, Model, Table, acsf_size)
 
 SYMBOLS = (
     "H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
@@ -219,7 +219,7 @@ def _section(sub, want, label):
 
 def read_model(src):
     """Force-model JSON → Model (families pair, eam, adp, angular, stiweb,
-    tersoff)."""
+    tersoff, and ml with an ACSF descriptor and linear heads)."""
     j = json.loads(_text(src))
     if "globals" in j:
         raise FormatError("global parameters are not supported by this reader")
@@ -232,6 +232,8 @@ def read_model(src):
             raise FormatError(f"bare pair file: {count} potentials is not a valid pair count for any ntypes")
         return Model(FS_FAMILY_PAIR, nt, _section(j, count, "pair"))
     name = j["model"]
+    if name == "ml":
+        return _read_ml(j)
     if name not in FAMILY_OF:
         raise FormatError(f"unsupported model '{name}'")
     fam, nt = FAMILY_OF[name], int(j.get("ntypes", 1))
@@ -305,6 +307,63 @@ def _pot_json(t):
     return d
 
 
+def _read_ml(j):
+    """build_ml / finish_ml / parse_linear_head (src/io/force_model_reader.cpp:
+    217-333): an ACSF ("acsf" or "symmetry_functions") descriptor and one
+    linear head per species."""
+    nt = int(j.get("ntypes", 1))
+    desc = j.get("descriptor")
+    if not isinstance(desc, dict) or not isinstance(desc.get("type"), str):
+        raise FormatError("ml: missing 'descriptor' object with a string 'type'")
+    if desc["type"] not in ("acsf", "symmetry_functions"):
+        raise FormatError(f"ml: descriptor '{desc['type']}' is not supported by this build (acsf only)")
+    if "standardization" in j:
+        raise FormatError("ml: feature standardization is not supported by this build")
+    g1 = desc.get("g1", 0)
+    g1 = len(g1) if isinstance(g1, list) else int(g1) if isinstance(g1, (int, float)) else 0
+    g2 = [(float(g["eta"]), float(g.get("rs", 0.0))) for g in desc.get("g2", [])]
+    g3 = [float(g.get("kappa", 1.0)) for g in desc.get("g3", [])]
+    g4 = [(float(g.get("eta", 1.0)), float(g.get("zeta", 1.0)), float(g.get("lambda", 1.0))) for g in desc.get("g4", [])]
+    g5 = [(float(g.get("eta", 1.0)), float(g.get("zeta", 1.0)), float(g.get("lambda", 1.0))) for g in desc.get("g5", [])]
+    spec = Table.acsf(float(desc.get("rcut", 6.0)), g1, g2, g3, g4, g5)
+    S = acsf_size(spec, nt)
+    if S == 0:
+        raise FormatError("ml: acsf descriptor needs at least one of g1/g2/g3/g4/g5")
+    heads = j.get("heads")
+    if not isinstance(heads, list) or len(heads) != nt:
+        raise FormatError(f"ml: expected {nt} heads")
+    tabs = [spec]
+    for h in heads:
+        if h.get("type", "linear") != "linear":
+            raise FormatError(f"ml: unknown head type '{h.get('type')}'")
+        co = h.get("coeffs")
+        if not isinstance(co, list) or len(co) != S:
+            raise FormatError(f"ml: head coeffs length != descriptor size {S}")
+        fixed = np.zeros(S + 1, np.uint8)
+        fixed[:S] = 1 if h.get("fixed", False) else 0
+        fixed[S] = 1 if h.get("bias_fixed", True) else 0
+        tabs.append(Table.linear_head(co, float(h.get("bias", 0.0)), fixed=fixed))
+    return Model(FS_FAMILY_ACSF, nt, tabs)
+
+
+def _write_ml(model):
+    v = model.tables[0].values
+    g1, n2, n3, n4, n5 = (int(x) for x in v[1:6])
+    p = list(v[6:])
+    g2 = [{"eta": p.pop(0), "rs": p.pop(0)} for _ in range(n2)]
+    g3 = [{"kappa": p.pop(0)} for _ in range(n3)]
+    g4 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n4)]
+    g5 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n5)]
+    desc = {"type": "acsf", "rcut": float(v[0]), "g1": g1, "g2": g2, "g3": g3, "g4": g4, "g5": g5}
+    heads = []
+    for t in model.tables[1:]:
+        fx = np.zeros(t.values.size, np.uint8) if t.fixed is None else t.fixed
+        heads.append({"type": "linear", "coeffs": [float(x) for x in t.values[:-1]],
+                      "fixed": bool(np.all(fx[:-1])) if t.values.size > 1 else False,
+                      "bias": float(t.values[-1]), "bias_fixed": bool(fx[-1])})
+    return json.dumps({"model": "ml", "ntypes": model.ntypes, "descriptor": desc, "heads": heads}, indent=1)
+
+
 def _tersoff_json(t):
     d = {}
     for k, nm in enumerate(TERSOFF_FIELDS):
@@ -322,9 +381,12 @@ def _tersoff_json(t):
 
 
 def write_model(model):
-    """Model → force-model JSON text (families pair, eam, adp, angular, tersoff)."""
+    """Model → force-model JSON text (families pair, eam, adp, angular,
+    tersoff, and ml with an ACSF descriptor)."""
     nt, fam = model.ntypes, model.family
     npair = nt * (nt + 1) // 2
+    if fam == FS_FAMILY_ACSF:
+        return _write_ml(model)
     if fam == FS_FAMILY_TERSOFF:
         return json.dumps({"model": "tersoff", "ntypes": nt,
                            "potentials": [_tersoff_json(t) for t in model.tables]}, indent=1)

@@ -96,6 +96,25 @@ def test_tersoff_and_angular_models():
     _tables_equal(back, ang)
 
 
+def test_ml_acsf_model():
+    """build_ml / parse_linear_head (force_model_reader.cpp:217-333)."""
+    from forcesmith_b200.abi import FS_FAMILY_ACSF, acsf_size
+    j = {"model": "ml", "ntypes": 2,
+         "descriptor": {"type": "symmetry_functions", "rcut": 5.0, "g1": 1, "g2": [{"eta": 0.5, "rs": 1.0}, {"eta": 1.0}],
+                        "g4": [{"eta": 0.1, "zeta": 2.0, "lambda": -1.0}]},
+         "heads": [{"type": "linear", "coeffs": [0.1] * 9, "bias": -3.0},
+                   {"coeffs": [0.2] * 9, "bias": -2.0, "bias_fixed": False, "fixed": True}]}
+    m = io.read_model(json.dumps(j))
+    assert m.family == FS_FAMILY_ACSF and acsf_size(m.tables[0], 2) == 9
+    assert m.tables[0].values[0] == 5.0 and list(m.tables[0].values[1:6]) == [1, 2, 0, 1, 0]
+    assert m.tables[1].fixed[-1] == 1 and m.tables[2].fixed[-1] == 0 and np.all(m.tables[2].fixed[:-1] == 1)
+    _tables_equal(io.read_model(io.write_model(m)), m)
+    with pytest.raises(io.FormatError):
+        io.read_model(json.dumps(dict(j, heads=j["heads"][:1])))
+    with pytest.raises(io.FormatError):
+        io.read_model(json.dumps(dict(j, descriptor={"type": "soap"})))
+
+
 def test_model_json_forms_and_errors():
     eam = {"model": "eam", "ntypes": 1,
            "pair": {"format": "analytic", "potentials": [{"type": "buck", "rmin": 0.5, "rmax": 6.0, "A": 900.0,
