@@ -337,6 +337,67 @@ def three_body_leg(local, which, steps=20):
     return out
 
 
+def acsf_leg(local, steps=20):
+    """ACSF descriptors (G1, 4 G2, G3, 2 G4, G5; rcut 4.2 A) with a linear head
+    on diamond Si, 1000 configurations.  Device FP32: residuals per second,
+    and residual + exact Jacobian + JtJ per second.  CPU: the oracle's
+    residual (16 threads, FP64); the reference forms this Jacobian from
+    cached descriptor gradients, which the oracle does not restate, so no CPU
+    Jacobian rate is given."""
+    import numpy as np
+    import torch
+    from forcesmith_b200 import gpu as G, synth
+    from forcesmith_b200.abi import FS_FAMILY_ACSF, Model, Table, acsf_size
+    from oracle.api import Oracle, set_threads
+    spec = Table.acsf(4.2, g1=1, g2=[(0.5, 2.3), (1.0, 3.0), (2.0, 3.8), (0.3, 0.0)], g3=[1.1],
+                      g4=[(0.05, 1.0, 1.0), (0.05, 2.0, -1.0)], g5=[(0.08, 1.5, 1.0)])
+    S = acsf_size(spec, 1)
+    rng = np.random.default_rng(4)
+
+    def model(w):
+        return Model(FS_FAMILY_ACSF, 1, [spec, Table.linear_head(w, -4.0)])
+    w_true = rng.normal(0, 0.3, S)
+    ds = label_on_gpu(synth.diamond(1000), model(w_true), local)
+    start = model(w_true * (1 + 0.1 * rng.normal(size=S)))
+    g = G.GpuSession(local, "fp32")
+    g.upload(ds)
+    g.set_model(start)
+    for _ in range(3):
+        g.jacobian_async(W_E, W_S)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(g.stream)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+        for _ in range(steps):
+            fn()
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+    res_ms = timed(lambda: g._lib.fs_gpu_eval(g._h, W_E, W_S, None, None, None, None, None, None))
+    jac_ms = timed(lambda: g.jacobian_async(W_E, W_S))
+    P = g.num_pairs()
+    g.close()
+    threads = set_threads(os.cpu_count() or 1)
+    o = Oracle()
+    o.upload(ds)
+    o.set_model(start)
+    o.eval(W_E, W_S, want=("obj",))
+    t0 = time.perf_counter()
+    o.eval(W_E, W_S, want=("F",))
+    t_res = time.perf_counter() - t0
+    return {"workload": f"ACSF + linear head (S = {S}), Si, {ds.n_cfg} configs x 64/216/512 atoms "
+                        f"({ds.n_atoms} atoms, {P} pairs), w_e=1, w_s=0.1",
+            "residual_fp32": {"value": 1000.0 / res_ms, "unit": "evals/s", "ms_per_eval": res_ms},
+            "jacobian_fp32": {"value": 1000.0 / jac_ms, "unit": "evals/s", "ms_per_eval": jac_ms,
+                              "method": "exact (linear head): residual + J + JtJ + Jtr"},
+            "cpu_baseline": {"residual": {"value": 1.0 / t_res, "unit": "evals/s"}, "cores": threads,
+                             "kind": "port", "sample": f"one FP64 residual ({t_res * 1e3:.0f} ms)"}}
+
+
 def sw_leg(local, steps=20):
     """Stillinger-Weber Si: 1000 diamond configurations of 64, 216 or 512
     atoms (sigma = 0.15 A, volumetric strain U[0.95, 1.05]), 7 perturbed SW
@@ -637,6 +698,7 @@ def run_ours(args):
         line["sw"] = sw_leg(local)
         line["tersoff"] = three_body_leg(local, "tersoff")
         line["angular"] = three_body_leg(local, "angular")
+        line["acsf"] = acsf_leg(local)
         line["al99_fit"] = al99_leg(local)
     if rank == 0 and world == 1 and not args.small and args.de_generations >= 0:
         de, sur = de_legs(local, args.de_generations)

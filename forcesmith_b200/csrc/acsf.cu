@@ -17,8 +17,10 @@
 // One CTA per configuration; threads take work items flat from a block scan:
 // one directed pair each (G1–G3), then one neighbour pair (j < k) of a central
 // atom each (G4, G5).  Residual: forces in shared memory with atomics; energy
-// and stress as per-thread FP64 sums.  Jacobian: each term adds its rows into
-// J (global memory, zeroed first) with atomics; a column kernel forms Jᵀr.
+// and stress as per-thread FP64 sums.  Jacobian: each term adds its force rows
+// with atomics into the configuration's force-row block in shared memory,
+// written out once (or, when the block does not fit, straight into J, zeroed
+// first), and its energy and stress rows into J; a column kernel forms Jᵀr.
 #include "kern_common.cuh"
 
 #include <algorithm>
@@ -69,6 +71,8 @@ template <class T> struct AcArgs {
   // Jacobian
   T *J;
   int64_t ld;
+  int D;   // columns (free head values)
+  int smj; // 1: the configuration's J block is summed in shared memory first
 };
 
 // One CTA per configuration.  JAC = false: residual; JAC = true: J rows.
@@ -95,6 +99,10 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   int *pfirst = S.take<int>(N + 1);
   int *tfirst = S.take<int>(N + 1);
   int *wsum = S.take<int>(32);
+  // JAC with smj: the 3N force rows (local) × D columns
+  T *Jb = (JAC && A.smj) ? S.take<T>(static_cast<size_t>(3 * N) * A.D) : nullptr;
+  if (Jb)
+    for (int k = threadIdx.x; k < 3 * N * A.D; k += blockDim.x) Jb[k] = T(0);
   for (int k = threadIdx.x; k < nspec; k += blockDim.x) par[k] = static_cast<T>(spec[k]);
   for (int k = threadIdx.x; k < nt * (L.S + 1); k += blockDim.x) {
     const TableDesc &td = A.c.desc[1 + k / (L.S + 1)];
@@ -115,23 +123,31 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   const int64_t rowE = row0 + 3 * N;
   const T sw = static_cast<T>(A.w_s / cd.volume), we = static_cast<T>(A.w_e);
   double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0}; // xx, yy, zz, xy, xz, yz
+  // J entry (local row r of this configuration: 3N force rows, then E, 6
+  // stress) in column cl: force rows to the shared block when there is one;
+  // the energy and stress rows, which every term hits, to J itself (a
+  // shared-memory atomic on one address serialises across a warp)
+  auto jadd = [&](int cl, int r, T v) {
+    if (Jb && r < 3 * N) atomicAdd(&Jb[r * A.D + cl], v);
+    else atomicAdd(&A.J[static_cast<int64_t>(cl) * A.ld + row0 + r], v);
+  };
+  const int rE = 3 * N;
   // J rows of one term: force rows of i (+g), of n (−g), energy, stress (d ⊗ −g)
   auto jac_add = [&](int cl, int i, int n, const T (&g)[3], const T (&d)[3], T e) {
     if (cl < 0) return;
-    T *Jc = A.J + static_cast<int64_t>(cl) * A.ld;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      atomicAdd(&Jc[row0 + 3 * i + a], g[a]);
-      atomicAdd(&Jc[row0 + 3 * n + a], -g[a]);
+      jadd(cl, 3 * i + a, g[a]);
+      jadd(cl, 3 * n + a, -g[a]);
     }
-    atomicAdd(&Jc[rowE], we * e);
+    jadd(cl, rE, we * e);
     if (A.w_s > 0.0) {
-      atomicAdd(&Jc[rowE + 1], -sw * d[0] * g[0]);
-      atomicAdd(&Jc[rowE + 2], -sw * d[1] * g[1]);
-      atomicAdd(&Jc[rowE + 3], -sw * d[2] * g[2]);
-      atomicAdd(&Jc[rowE + 4], -sw * d[0] * g[1]);
-      atomicAdd(&Jc[rowE + 5], -sw * d[0] * g[2]);
-      atomicAdd(&Jc[rowE + 6], -sw * d[1] * g[2]);
+      jadd(cl, rE + 1, -sw * d[0] * g[0]);
+      jadd(cl, rE + 2, -sw * d[1] * g[1]);
+      jadd(cl, rE + 3, -sw * d[2] * g[2]);
+      jadd(cl, rE + 4, -sw * d[0] * g[1]);
+      jadd(cl, rE + 5, -sw * d[0] * g[2]);
+      jadd(cl, rE + 6, -sw * d[1] * g[2]);
     }
   };
   // ---- G1–G3: one thread per directed pair
@@ -247,21 +263,20 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
           const int cc = cl[idx];
           if (cc >= 0) {
             // rows: j gets −gj, k gets −gk, i gets gj + gk; stress d1 ⊗ −gj + d2 ⊗ −gk
-            T *Jc = A.J + static_cast<int64_t>(cc) * A.ld;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              atomicAdd(&Jc[row0 + 3 * i + a], gj[a] + gk[a]);
-              atomicAdd(&Jc[row0 + 3 * j + a], -gj[a]);
-              atomicAdd(&Jc[row0 + 3 * k + a], -gk[a]);
+              jadd(cc, 3 * i + a, gj[a] + gk[a]);
+              jadd(cc, 3 * j + a, -gj[a]);
+              jadd(cc, 3 * k + a, -gk[a]);
             }
-            atomicAdd(&Jc[rowE], we * g);
+            jadd(cc, rE, we * g);
             if (A.w_s > 0.0) {
-              atomicAdd(&Jc[rowE + 1], -sw * (d1[0] * gj[0] + d2[0] * gk[0]));
-              atomicAdd(&Jc[rowE + 2], -sw * (d1[1] * gj[1] + d2[1] * gk[1]));
-              atomicAdd(&Jc[rowE + 3], -sw * (d1[2] * gj[2] + d2[2] * gk[2]));
-              atomicAdd(&Jc[rowE + 4], -sw * (d1[0] * gj[1] + d2[0] * gk[1]));
-              atomicAdd(&Jc[rowE + 5], -sw * (d1[0] * gj[2] + d2[0] * gk[2]));
-              atomicAdd(&Jc[rowE + 6], -sw * (d1[1] * gj[2] + d2[1] * gk[2]));
+              jadd(cc, rE + 1, -sw * (d1[0] * gj[0] + d2[0] * gk[0]));
+              jadd(cc, rE + 2, -sw * (d1[1] * gj[1] + d2[1] * gk[1]));
+              jadd(cc, rE + 3, -sw * (d1[2] * gj[2] + d2[2] * gk[2]));
+              jadd(cc, rE + 4, -sw * (d1[0] * gj[1] + d2[0] * gk[1]));
+              jadd(cc, rE + 5, -sw * (d1[0] * gj[2] + d2[0] * gk[2]));
+              jadd(cc, rE + 6, -sw * (d1[1] * gj[2] + d2[1] * gk[2]));
             }
           }
         } else {
@@ -296,12 +311,21 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
     const int ti = typ[i];
     if constexpr (JAC) {
       const int cb = col[ti * (L.S + 1) + L.S];
-      if (cb >= 0) atomicAdd(&A.J[static_cast<int64_t>(cb) * A.ld + rowE], we);
+      if (cb >= 0) jadd(cb, rE, we);
     } else {
       e_acc += static_cast<double>(W[ti * (L.S + 1) + L.S]);
     }
   }
-  if constexpr (JAC) return;
+  if constexpr (JAC) {
+    if (!Jb) return;
+    __syncthreads();
+    // the force rows to J (the energy, stress and limit rows are in J already)
+    for (int k = threadIdx.x; k < 3 * N * A.D; k += blockDim.x) {
+      const int cl = k / (3 * N), r = k % (3 * N);
+      A.J[static_cast<int64_t>(cl) * A.ld + row0 + r] = Jb[r * A.D + cl];
+    }
+    return;
+  }
   __syncthreads();
   // residual rows of the configuration (residual_layout.hpp:37-54)
   double objp = 0.0;
@@ -403,9 +427,11 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
   a.order = h->d_cfg_by_work;
   a.J = nullptr;
   a.ld = 0;
+  a.D = h->D;
+  a.smj = 0;
   int mi = 1;
   for (const CfgDev &cd : h->cfg_host) mi = std::max(mi, (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1));
-  const size_t sm = ac_smem<T>(h, mi);
+  size_t sm = ac_smem<T>(h, mi);
   if (sm > 227 * 1024) return set_error(h, FS_ERR_UNSUPPORTED, "ACSF: configuration too large for shared memory");
   const int64_t M = rows_of(h, w_s);
   const int D = h->D;
@@ -426,6 +452,12 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
     FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     a.J = static_cast<T *>(h->d_J);
     a.ld = ldj;
+    // the configuration's J block in shared memory when it fits
+    const size_t jb = align16(static_cast<size_t>(3 * h->max_natoms) * D * sizeof(T));
+    if (D > 0 && sm + jb <= 200 * 1024) {
+      a.smj = 1;
+      sm += jb;
+    }
   }
   auto k = jac ? acsf_kernel<T, true> : acsf_kernel<T, false>;
   FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));

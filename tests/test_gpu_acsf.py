@@ -48,10 +48,12 @@ def _close(a, b, rel, what):
     assert err <= rel, f"{what}: {err:.3e}"
 
 
-@pytest.fixture(scope="module", params=[1, 2], ids=["one", "two"])
+@pytest.fixture(scope="module", params=[(1, (2, 3)), (2, (2, 3)), (2, (4,))], ids=["one", "two", "two-512"])
 def case(request):
-    nt = request.param
-    ds = synth.diamond(4, cells=(2, 3), seed=71)
+    """two-512: a 512-atom configuration whose J block (1543 × 42) does not
+    fit in shared memory, so its terms go straight to J in global memory."""
+    nt, cells = request.param
+    ds = synth.diamond(4 if cells != (4,) else 1, cells=cells, seed=71)
     if nt == 2:
         ds.type[:] = np.random.default_rng(9).integers(0, 2, ds.type.size)
     ds = label(ds, model(nt, 1), O.Oracle, 1.0, 0.2)
