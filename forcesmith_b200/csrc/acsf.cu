@@ -30,6 +30,13 @@ namespace {
 
 constexpr int kAcThreads = 256;
 
+// exp and x^y: the hardware approximations in FP32 (a few ulp, inside the
+// FP32 path's stated tolerances), IEEE in FP64
+__device__ __forceinline__ float ac_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double ac_exp(double x) { return exp(x); }
+__device__ __forceinline__ float ac_pow(float a, float z) { return __expf(z * __logf(a)); }
+__device__ __forceinline__ double ac_pow(double a, double z) { return pow(a, z); }
+
 template <class T> __device__ __forceinline__ void ac_fc(T r, T rc, T &fc, T &fcp) {
   if (r >= rc) {
     fc = fcp = T(0);
@@ -99,11 +106,16 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   int *pfirst = S.take<int>(N + 1);
   int *tfirst = S.take<int>(N + 1);
   int *wsum = S.take<int>(32);
+  T *cz = S.take<T>(L.n4 + L.n5); // 2^{1−ζ} of each G4, G5 function
   // JAC with smj: the 3N force rows (local) × D columns
   T *Jb = (JAC && A.smj) ? S.take<T>(static_cast<size_t>(3 * N) * A.D) : nullptr;
   if (Jb)
     for (int k = threadIdx.x; k < 3 * N * A.D; k += blockDim.x) Jb[k] = T(0);
   for (int k = threadIdx.x; k < nspec; k += blockDim.x) par[k] = static_cast<T>(spec[k]);
+  for (int k = threadIdx.x; k < L.n4 + L.n5; k += blockDim.x) {
+    const double zeta = k < L.n4 ? spec[6 + 2 * L.n2 + L.n3 + 3 * k + 1] : spec[6 + 2 * L.n2 + L.n3 + 3 * L.n4 + 3 * (k - L.n4) + 1];
+    cz[k] = static_cast<T>(pow(2.0, 1.0 - zeta));
+  }
   for (int k = threadIdx.x; k < nt * (L.S + 1); k += blockDim.x) {
     const TableDesc &td = A.c.desc[1 + k / (L.S + 1)];
     W[k] = static_cast<T>(A.vals[td.pv0 + k % (L.S + 1)]);
@@ -116,6 +128,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   __syncthreads();
   const T rc = par[0];
   const T *p2 = par + 6, *p3 = p2 + 2 * L.n2, *p4 = p3 + L.n3, *p5 = p4 + 3 * L.n4;
+  const T *c4 = cz, *c5 = cz + L.n4;
   const uint32_t *nbp = A.c.nb_pack + start[0];
   const int npair = pfirst[N], ntri = tfirst[N];
   const int64_t rows_per_extra = 2 + (A.w_s > 0.0 ? 6 : 0);
@@ -177,7 +190,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
     for (int t = 0; t < L.g1; ++t) term(L.base[0] + s * L.g1 + t, fc, fcp);
     for (int t = 0; t < L.n2; ++t) {
       const T eta = p2[2 * t], dr = r - p2[2 * t + 1];
-      const T gs = exp(-eta * dr * dr);
+      const T gs = ac_exp(-eta * dr * dr);
       term(L.base[1] + s * L.n2 + t, gs * fc, gs * (T(-2) * eta * dr * fc + fcp));
     }
     for (int t = 0; t < L.n3; ++t) {
@@ -240,12 +253,13 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       }
       const int po = pair_ord(typ[j], typ[k], nt);
       T GJ[3] = {0, 0, 0}, GK[3] = {0, 0, 0}, ew = T(0);
-      auto term = [&](int idx, T eta, T zeta, T lambda, bool with_jk) {
+      auto term = [&](int idx, T eta, T zeta, T lambda, T Cz, bool with_jk) {
         const T Aa = T(1) + lambda * costh;
         if (Aa <= T(1e-12)) return;
-        const T C = pow(T(2), T(1) - zeta), ang = pow(Aa, zeta), dang = zeta * pow(Aa, zeta - T(1)) * lambda;
+        // 2^{1−ζ} per function (precomputed); ζ λ A^{ζ−1} = ζ λ A^ζ / A (A > 1e-12)
+        const T C = Cz, ang = ac_pow(Aa, zeta), dang = zeta * lambda * ang / Aa;
         const T rsum = r1 * r1 + r2 * r2 + (with_jk ? rjk * rjk : T(0));
-        const T rad = exp(-eta * rsum);
+        const T rad = ac_exp(-eta * rsum);
         const T fj = with_jk ? fjk : T(1);
         const T fcs = f1 * f2 * fj;
         const T g = C * ang * rad * fcs;
@@ -288,8 +302,10 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
           }
         }
       };
-      for (int t = 0; t < L.n4; ++t) term(L.base[3] + po * L.n4 + t, p4[3 * t], p4[3 * t + 1], p4[3 * t + 2], true);
-      for (int t = 0; t < L.n5; ++t) term(L.base[4] + po * L.n5 + t, p5[3 * t], p5[3 * t + 1], p5[3 * t + 2], false);
+      for (int t = 0; t < L.n4; ++t)
+        term(L.base[3] + po * L.n4 + t, p4[3 * t], p4[3 * t + 1], p4[3 * t + 2], c4[t], true);
+      for (int t = 0; t < L.n5; ++t)
+        term(L.base[4] + po * L.n5 + t, p5[3 * t], p5[3 * t + 1], p5[3 * t + 2], c5[t], false);
       if constexpr (!JAC) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -396,6 +412,7 @@ template <class T> size_t ac_smem(const fs_gpu *h, int mi) {
   L.init(h->tables[0].v.data(), h->ntypes);
   const int N = h->max_natoms, nt = h->ntypes, nspec = h->tables[0].n;
   return align16(nspec * sizeof(T)) + align16(nt * (L.S + 1) * sizeof(T)) + align16(nt * (L.S + 1) * sizeof(int)) +
+         align16((L.n4 + L.n5) * sizeof(T)) +
          align16(3 * N * sizeof(double)) + align16(3 * mi * sizeof(double)) + align16(N) + align16(3 * N * sizeof(T)) +
          align16(8 * 32 * sizeof(double)) + 2 * align16((N + 1) * sizeof(int)) + align16(32 * sizeof(int)) + 160;
 }
