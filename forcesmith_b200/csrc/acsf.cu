@@ -218,10 +218,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       const int i = owner_of(tfirst, N, w);
       const int n = pfirst[i + 1] - pfirst[i];
       int u = w - tfirst[i], a0 = 0;
-      while (u >= n - 1 - a0) {
-        u -= n - 1 - a0;
-        ++a0;
-      }
+      pair_row(n, u, a0);
       const int pj = pfirst[i] + a0, pk = pj + 1 + u;
       int j, k;
       T d1[3], d2[3];

@@ -90,10 +90,7 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     const int i = owner_of(tfirst, N, w);
     const int n = pfirst[i + 1] - pfirst[i];
     int u = w - tfirst[i], a0 = 0;
-    while (u >= n - 1 - a0) {
-      u -= n - 1 - a0;
-      ++a0;
-    }
+    pair_row(n, u, a0);
     const int pj = pfirst[i] + a0, pk = pj + 1 + u;
     const int ti = typ[i];
     int j, k;

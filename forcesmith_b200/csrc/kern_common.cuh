@@ -88,6 +88,20 @@ template <int K> __device__ void block_sum_k(double (&v)[K], double *red) {
     }
 }
 
+// An atom with n neighbours has n(n − 1)/2 neighbour pairs (j < k) in rows
+// a = 0 .. n − 2 of n − 1 − a pairs each, row a starting at a(2n − a − 1)/2.
+// For pair offset u: the row a (from the quadratic's root, then a one-step
+// integer correction either way) and u's offset within that row.
+__device__ __forceinline__ void pair_row(int n, int &u, int &a) {
+  const float b = 2.f * static_cast<float>(n) - 1.f;
+  int r = static_cast<int>((b - sqrtf(fmaxf(b * b - 8.f * static_cast<float>(u), 0.f))) * 0.5f);
+  r = max(0, min(r, n - 2));
+  while (r > 0 && r * (2 * n - r - 1) / 2 > u) --r;
+  while (r + 1 <= n - 2 && (r + 1) * (2 * n - r - 2) / 2 <= u) ++r;
+  u -= r * (2 * n - r - 1) / 2;
+  a = r;
+}
+
 // Largest i in [0, N) with first[i] <= w, for non-decreasing first[] with
 // first[0] = 0 <= w < first[N]: the atom that owns work item w.
 __device__ __forceinline__ int owner_of(const int *first, int N, int w) {

@@ -336,11 +336,7 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
         i = owner_of(tfirst, N, w);
         const int n = pfirst[i + 1] - pfirst[i];
         u = w - tfirst[i];
-        a0 = 0;
-        while (u >= n - 1 - a0) {
-          u -= n - 1 - a0;
-          ++a0;
-        }
+        pair_row(n, u, a0);
       }
       const int pj = pfirst[i] + a0, pk = pj + 1 + u;
       const int ti = typ[i];
