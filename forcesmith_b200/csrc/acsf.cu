@@ -14,13 +14,16 @@
 //   depend on them: ∂F/∂w = −∂D/∂r, ∂E/∂w = Σ_i D_i, ∂E/∂b = atom count
 //   (eval_cached_jacobian, ml_force.hpp).
 //
-// One CTA per configuration; threads take work items flat from a block scan:
-// one directed pair each (G1–G3), then one neighbour pair (j < k) of a central
-// atom each (G4, G5).  Residual: forces in shared memory with atomics; energy
-// and stress as per-thread FP64 sums.  Jacobian: each term adds its force rows
-// with atomics into the configuration's force-row block in shared memory,
-// written out once (or, when the block does not fit, straight into J, zeroed
-// first), and its energy and stress rows into J; a column kernel forms Jᵀr.
+// One CTA per configuration; each warp takes 32 consecutive work items from a
+// block scan: directed pairs (G1–G3), then neighbour pairs (j < k) of a
+// central atom (G4, G5).  Items are ordered by central atom, so runs of lanes
+// share atom i (and, for neighbour pairs, atom j): their force updates are
+// summed over each run with shuffles and added once.  Residual: forces in
+// shared memory; energy and stress as per-thread FP64 sums.  Jacobian: force
+// rows into the configuration's force-row block in shared memory, written out
+// once (or, when the block does not fit, straight into J, zeroed first); the
+// energy and stress rows, which every term hits, summed over the warp into J;
+// a column kernel forms Jᵀr.
 #include "kern_common.cuh"
 
 #include <algorithm>
@@ -68,6 +71,31 @@ struct AcLayout {
     S = base[4] + n5 * P;
   }
 };
+
+// Runs of lanes with the same key, for keys that do not decrease across the
+// warp (work items are ordered by central atom, then by neighbour): bit s of
+// the links is set when lane + 2^s has this lane's key; head: the run's first
+// lane.  All 32 lanes call these together.
+__device__ __forceinline__ unsigned run_links(int key, int lane, bool &head) {
+  unsigned nx = 0;
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int kk = __shfl_down_sync(0xffffffffu, key, 1 << s);
+    if (lane + (1 << s) < 32 && kk == key) nx |= 1u << s;
+  }
+  const int kp = __shfl_up_sync(0xffffffffu, key, 1);
+  head = lane == 0 || kp != key;
+  return nx;
+}
+// Sum of v over this lane and the later lanes of its run (the whole run at its head).
+template <class T> __device__ __forceinline__ T run_sum(T v, unsigned nx) {
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const T t = __shfl_down_sync(0xffffffffu, v, 1 << s);
+    if (nx >> s & 1) v += t;
+  }
+  return v;
+}
 
 template <class T> struct AcArgs {
   Common c;
@@ -137,51 +165,87 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   const T sw = static_cast<T>(A.w_s / cd.volume), we = static_cast<T>(A.w_e);
   double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0}; // xx, yy, zz, xy, xz, yz
   // J entry (local row r of this configuration: 3N force rows, then E, 6
-  // stress) in column cl: force rows to the shared block when there is one;
-  // the energy and stress rows, which every term hits, to J itself (a
-  // shared-memory atomic on one address serialises across a warp)
+  // stress) in column cl: force rows to the shared block when there is one,
+  // else to J
   auto jadd = [&](int cl, int r, T v) {
     if (Jb && r < 3 * N) atomicAdd(&Jb[r * A.D + cl], v);
     else atomicAdd(&A.J[static_cast<int64_t>(cl) * A.ld + row0 + r], v);
   };
   const int rE = 3 * N;
-  // J rows of one term: force rows of i (+g), of n (−g), energy, stress (d ⊗ −g)
-  auto jac_add = [&](int cl, int i, int n, const T (&g)[3], const T (&d)[3], T e) {
-    if (cl < 0) return;
+  const int lane = threadIdx.x & 31;
+  const int nrow = A.w_s > 0.0 ? 7 : 1;
+  // The energy and stress rows of one term in column c0, which every term of
+  // the configuration hits: summed over the warp and added once per row.
+  // Lanes without a term pass zeros; all 32 lanes call this together.
+  auto erows_warp = [&](int c0, T e, const T (&st)[6]) {
+    T v[7] = {we * e};
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      jadd(cl, 3 * i + a, g[a]);
-      jadd(cl, 3 * n + a, -g[a]);
-    }
-    jadd(cl, rE, we * e);
-    if (A.w_s > 0.0) {
-      jadd(cl, rE + 1, -sw * d[0] * g[0]);
-      jadd(cl, rE + 2, -sw * d[1] * g[1]);
-      jadd(cl, rE + 3, -sw * d[2] * g[2]);
-      jadd(cl, rE + 4, -sw * d[0] * g[1]);
-      jadd(cl, rE + 5, -sw * d[0] * g[2]);
-      jadd(cl, rE + 6, -sw * d[1] * g[2]);
-    }
+    for (int m = 0; m < 6; ++m) v[1 + m] = st[m];
+    T *Jc = A.J + static_cast<int64_t>(c0) * A.ld + row0 + rE;
+#pragma unroll
+    for (int m = 0; m < 7; ++m)
+      if (m < nrow) {
+        v[m] = warp_sum_group(v[m], 32);
+        if (lane == 0) atomicAdd(&Jc[m], v[m]);
+      }
   };
-  // ---- G1–G3: one thread per directed pair
-  for (int w = threadIdx.x; w < npair; w += blockDim.x) {
+  // the same rows from one lane
+  auto erows_lane = [&](int cl, T e, const T (&st)[6]) {
+    T *Jc = A.J + static_cast<int64_t>(cl) * A.ld + row0 + rE;
+    atomicAdd(&Jc[0], we * e);
+    for (int m = 1; m < nrow; ++m) atomicAdd(&Jc[m], st[m - 1]);
+  };
+  // ---- G1–G3: one thread per directed pair; each warp takes 32 consecutive
+  // items (the Jacobian's warp sums need every lane; spare lanes repeat the
+  // last item with ok false)
+  for (int w0 = threadIdx.x - lane; w0 < npair; w0 += blockDim.x) {
+    const int w = min(w0 + lane, npair - 1);
     const int i = owner_of(pfirst, N, w);
     int j;
     T d[3];
     pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
     const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    if (r < T(1e-14) || r >= rc) continue;
-    const T rh[3] = {d[0] / r, d[1] / r, d[2] / r};
+    const bool ok = w0 + lane < npair && r >= T(1e-14) && r < rc;
+    if (!__any_sync(0xffffffffu, ok)) continue;
+    const T ir = ok ? T(1) / r : T(0);
+    const T rh[3] = {d[0] * ir, d[1] * ir, d[2] * ir};
     T fc, fcp;
     ac_fc(r, rc, fc, fcp);
     const int s = typ[j], ti = typ[i];
     const T *w_ = W + ti * (L.S + 1);
     const int *cl = col + ti * (L.S + 1);
     T cw = T(0), ew = T(0);
+    bool hi = false;
+    const unsigned xi = run_links(i, lane, hi);
     auto term = [&](int idx, T g, T dg) {
       if constexpr (JAC) {
-        const T gv[3] = {dg * rh[0], dg * rh[1], dg * rh[2]};
-        jac_add(cl[idx], i, j, gv, d, g);
+        // force rows: +g on i, −g on j; stress −sw d ⊗ g
+        T gv[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) gv[a] = ok ? dg * rh[a] : T(0);
+        const T st[6] = {-sw * d[0] * gv[0], -sw * d[1] * gv[1], -sw * d[2] * gv[2],
+                         -sw * d[0] * gv[1], -sw * d[0] * gv[2], -sw * d[1] * gv[2]};
+        const int cc = cl[idx];
+        const int c0 = __shfl_sync(0xffffffffu, cc, 0);
+        if (__all_sync(0xffffffffu, cc == c0)) {
+          // one column for the warp (always, with one species): atom i's rows
+          // summed over its run of lanes, energy and stress over the warp
+          if (c0 < 0) return;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const T t = run_sum(gv[a], xi);
+            if (hi) jadd(c0, 3 * i + a, t);
+            if (ok) jadd(c0, 3 * j + a, -gv[a]);
+          }
+          erows_warp(c0, ok ? g : T(0), st);
+        } else if (ok && cc >= 0) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            jadd(cc, 3 * i + a, gv[a]);
+            jadd(cc, 3 * j + a, -gv[a]);
+          }
+          erows_lane(cc, g, st);
+        }
       } else {
         cw += w_[idx] * dg;
         ew += w_[idx] * g;
@@ -198,12 +262,15 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       term(L.base[2] + s * L.n3 + t, cc * fc, -k * ss * fc + cc * fcp);
     }
     if constexpr (!JAC) {
+      // atom i's force summed over its run of lanes (rh is zero without a term)
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        atomicAdd(&Fs[3 * i + a], cw * rh[a]);
-        atomicAdd(&Fs[3 * j + a], -cw * rh[a]);
+        const T f = cw * rh[a];
+        const T t = run_sum(f, xi);
+        if (hi) atomicAdd(&Fs[3 * i + a], t);
+        if (ok) atomicAdd(&Fs[3 * j + a], -f);
       }
-      e_acc += static_cast<double>(ew);
+      if (ok) e_acc += static_cast<double>(ew);
       sg[0] -= static_cast<double>(cw * d[0] * rh[0]);
       sg[1] -= static_cast<double>(cw * d[1] * rh[1]);
       sg[2] -= static_cast<double>(cw * d[2] * rh[2]);
@@ -212,9 +279,11 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       sg[5] -= static_cast<double>(cw * d[1] * rh[2]);
     }
   }
-  // ---- G4, G5: one thread per neighbour pair (j < k) of a central atom i
+  // ---- G4, G5: one thread per neighbour pair (j < k) of a central atom i,
+  // in warp-sized runs as above
   if (L.n4 + L.n5 > 0)
-    for (int w = threadIdx.x; w < ntri; w += blockDim.x) {
+    for (int w0 = threadIdx.x - lane; w0 < ntri; w0 += blockDim.x) {
+      const int w = min(w0 + lane, ntri - 1);
       const int i = owner_of(tfirst, N, w);
       const int n = pfirst[i + 1] - pfirst[i];
       int u = w - tfirst[i], a0 = 0;
@@ -224,15 +293,17 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       T d1[3], d2[3];
       pair_vec(wpos, shift, i, nbp[pj], j, d1[0], d1[1], d1[2]);
       const T r1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
-      if (r1 < T(1e-14) || r1 >= rc) continue;
+      bool ok = w0 + lane < ntri && r1 >= T(1e-14) && r1 < rc;
       pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
       const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
-      if (r2 < T(1e-14) || r2 >= rc) continue;
+      ok = ok && r2 >= T(1e-14) && r2 < rc;
+      if (!__any_sync(0xffffffffu, ok)) continue;
       const int ti = typ[i];
       const T *w_ = W + ti * (L.S + 1);
       const int *cl = col + ti * (L.S + 1);
-      const T h1[3] = {d1[0] / r1, d1[1] / r1, d1[2] / r1}, h2[3] = {d2[0] / r2, d2[1] / r2, d2[2] / r2};
-      T costh = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) / (r1 * r2);
+      const T ir1 = ok ? T(1) / r1 : T(0), ir2 = ok ? T(1) / r2 : T(0);
+      const T h1[3] = {d1[0] * ir1, d1[1] * ir1, d1[2] * ir1}, h2[3] = {d2[0] * ir2, d2[1] * ir2, d2[2] * ir2};
+      T costh = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * (ir1 * ir2);
       costh = min(max(costh, T(-1)), T(1));
       const T djk[3] = {d2[0] - d1[0], d2[1] - d1[1], d2[2] - d1[2]};
       const T rjk = sqrt(djk[0] * djk[0] + djk[1] * djk[1] + djk[2] * djk[2]);
@@ -245,16 +316,20 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       ac_fc(rjk, rc, fjk, fpjk);
       T dcj[3], dck[3];
       for (int a = 0; a < 3; ++a) {
-        dcj[a] = (h2[a] - costh * h1[a]) / r1;
-        dck[a] = (h1[a] - costh * h2[a]) / r2;
+        dcj[a] = (h2[a] - costh * h1[a]) * ir1;
+        dck[a] = (h1[a] - costh * h2[a]) * ir2;
       }
       const int po = pair_ord(typ[j], typ[k], nt);
+      bool hi = false, hj = false;
+      const unsigned xi = run_links(i, lane, hi);
+      const unsigned xj = run_links(pj, lane, hj); // atom j: runs of the same neighbour slot
       T GJ[3] = {0, 0, 0}, GK[3] = {0, 0, 0}, ew = T(0);
       auto term = [&](int idx, T eta, T zeta, T lambda, T Cz, bool with_jk) {
         const T Aa = T(1) + lambda * costh;
-        if (Aa <= T(1e-12)) return;
+        const bool on = ok && Aa > T(1e-12);
         // 2^{1−ζ} per function (precomputed); ζ λ A^{ζ−1} = ζ λ A^ζ / A (A > 1e-12)
-        const T C = Cz, ang = ac_pow(Aa, zeta), dang = zeta * lambda * ang / Aa;
+        const T Ab = on ? Aa : T(1);
+        const T C = Cz, ang = ac_pow(Ab, zeta), dang = zeta * lambda * ang / Ab;
         const T rsum = r1 * r1 + r2 * r2 + (with_jk ? rjk * rjk : T(0));
         const T rad = ac_exp(-eta * rsum);
         const T fj = with_jk ? fjk : T(1);
@@ -271,26 +346,38 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
           gk[a] = cik * h2[a] + cjk * hjk[a] + ccos * dck[a];
         }
         if constexpr (JAC) {
+          // rows: j gets −gj, k gets −gk, i gets gj + gk; stress d1 ⊗ −gj + d2 ⊗ −gk
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            gj[a] = on ? gj[a] : T(0);
+            gk[a] = on ? gk[a] : T(0);
+          }
+          const T st[6] = {-sw * (d1[0] * gj[0] + d2[0] * gk[0]), -sw * (d1[1] * gj[1] + d2[1] * gk[1]),
+                           -sw * (d1[2] * gj[2] + d2[2] * gk[2]), -sw * (d1[0] * gj[1] + d2[0] * gk[1]),
+                           -sw * (d1[0] * gj[2] + d2[0] * gk[2]), -sw * (d1[1] * gj[2] + d2[1] * gk[2])};
           const int cc = cl[idx];
-          if (cc >= 0) {
-            // rows: j gets −gj, k gets −gk, i gets gj + gk; stress d1 ⊗ −gj + d2 ⊗ −gk
+          const int c0 = __shfl_sync(0xffffffffu, cc, 0);
+          if (__all_sync(0xffffffffu, cc == c0)) {
+            if (c0 < 0) return;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const T ti_ = run_sum(gj[a] + gk[a], xi);
+              const T tj = run_sum(gj[a], xj);
+              if (hi) jadd(c0, 3 * i + a, ti_);
+              if (hj) jadd(c0, 3 * j + a, -tj);
+              if (on) jadd(c0, 3 * k + a, -gk[a]);
+            }
+            erows_warp(c0, on ? g : T(0), st);
+          } else if (on && cc >= 0) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
               jadd(cc, 3 * i + a, gj[a] + gk[a]);
               jadd(cc, 3 * j + a, -gj[a]);
               jadd(cc, 3 * k + a, -gk[a]);
             }
-            jadd(cc, rE, we * g);
-            if (A.w_s > 0.0) {
-              jadd(cc, rE + 1, -sw * (d1[0] * gj[0] + d2[0] * gk[0]));
-              jadd(cc, rE + 2, -sw * (d1[1] * gj[1] + d2[1] * gk[1]));
-              jadd(cc, rE + 3, -sw * (d1[2] * gj[2] + d2[2] * gk[2]));
-              jadd(cc, rE + 4, -sw * (d1[0] * gj[1] + d2[0] * gk[1]));
-              jadd(cc, rE + 5, -sw * (d1[0] * gj[2] + d2[0] * gk[2]));
-              jadd(cc, rE + 6, -sw * (d1[1] * gj[2] + d2[1] * gk[2]));
-            }
+            erows_lane(cc, g, st);
           }
-        } else {
+        } else if (on) {
           ew += w_[idx] * g;
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
@@ -304,11 +391,13 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       for (int t = 0; t < L.n5; ++t)
         term(L.base[4] + po * L.n5 + t, p5[3 * t], p5[3 * t + 1], p5[3 * t + 2], c5[t], false);
       if constexpr (!JAC) {
+        // atoms i and j summed over their runs of lanes (zeros without a term)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          atomicAdd(&Fs[3 * i + a], GJ[a] + GK[a]);
-          atomicAdd(&Fs[3 * j + a], -GJ[a]);
-          atomicAdd(&Fs[3 * k + a], -GK[a]);
+          const T ti_ = run_sum(GJ[a] + GK[a], xi), tj = run_sum(GJ[a], xj);
+          if (hi) atomicAdd(&Fs[3 * i + a], ti_);
+          if (hj) atomicAdd(&Fs[3 * j + a], -tj);
+          if (ok) atomicAdd(&Fs[3 * k + a], -GK[a]);
         }
         e_acc += static_cast<double>(ew);
         sg[0] -= static_cast<double>(d1[0] * GJ[0] + d2[0] * GK[0]);
