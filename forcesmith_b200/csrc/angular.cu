@@ -11,10 +11,11 @@
 //   With spline tables the reference's Jacobian is central differences; the
 //   device keeps that method (fd.cu, FP64 contexts).
 //
-// One CTA per configuration; threads take work items flat from a block scan:
-// one directed pair each (2-body), then one neighbour pair (j < k) of a
-// central atom each (3-body).  Forces accumulate in shared memory with
-// atomics; energy and stress are per-thread FP64 sums.
+// One CTA per configuration; each warp takes 32 consecutive work items from a
+// block scan: directed pairs (2-body), then neighbour pairs (j < k) of a
+// central atom (3-body).  Forces accumulate in shared memory, summed first
+// over each run of lanes that share an atom; energy and stress are
+// per-thread FP64 sums.
 #include "kern_common.cuh"
 
 #include <algorithm>
@@ -62,21 +63,33 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
   const uint32_t *nbp = A.c.nb_pack + start[0];
   const int npair = pfirst[N], ntri = tfirst[N];
   double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0}; // xx, yy, zz, xy, xz, yz
+  const int lane = threadIdx.x & 31;
+  // Each warp takes 32 consecutive work items (spare lanes repeat the last
+  // with ok false).  Items are ordered by central atom, so the forces on atom
+  // i (and, for neighbour pairs, on atom j) are summed over each run of lanes
+  // that share it and added once.
   // ---- 2-body: one thread per directed pair
-  for (int w = threadIdx.x; w < npair; w += blockDim.x) {
+  for (int w0 = threadIdx.x - lane; w0 < npair; w0 += blockDim.x) {
+    const int w = min(w0 + lane, npair - 1);
     const int i = owner_of(pfirst, N, w);
     int j;
     T d[3];
     pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
     const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    if (r < T(1e-14)) continue;
     const STab<T> &tb = tabs[pair_ord(typ[i], typ[j], nt)];
-    if (!in_span(tb, r)) continue;
+    const bool ok = w0 + lane < npair && r >= T(1e-14) && in_span(tb, r);
+    if (!__any_sync(0xffffffffu, ok)) continue;
+    bool hi;
+    const unsigned xi = run_links(i, lane, hi);
     const VD<T> ph = tab_vd<T, true>(tb, seg, A.vals, r);
-    const T s = ph.d / r;
+    const T s = ok ? ph.d / r : T(0);
     const T f[3] = {s * d[0], s * d[1], s * d[2]};
 #pragma unroll
-    for (int a = 0; a < 3; ++a) atomicAdd(&Fs[3 * i + a], f[a]);
+    for (int a = 0; a < 3; ++a) {
+      const T t = run_sum(f[a], xi);
+      if (hi) atomicAdd(&Fs[3 * i + a], t);
+    }
+    if (!ok) continue;
     e_acc += 0.5 * static_cast<double>(ph.v);
     sg[0] -= static_cast<double>(T(0.5) * d[0] * f[0]);
     sg[1] -= static_cast<double>(T(0.5) * d[1] * f[1]);
@@ -86,7 +99,8 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     sg[5] -= static_cast<double>(T(0.5) * d[1] * f[2]);
   }
   // ---- 3-body: one thread per neighbour pair (j < k) of a central atom i
-  for (int w = threadIdx.x; w < ntri; w += blockDim.x) {
+  for (int w0 = threadIdx.x - lane; w0 < ntri; w0 += blockDim.x) {
+    const int w = min(w0 + lane, ntri - 1);
     const int i = owner_of(tfirst, N, w);
     const int n = pfirst[i + 1] - pfirst[i];
     int u = w - tfirst[i], a0 = 0;
@@ -97,32 +111,35 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     T d1[3], d2[3];
     pair_vec(wpos, shift, i, nbp[pj], j, d1[0], d1[1], d1[2]);
     const T r1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
-    if (r1 < T(1e-14)) continue;
     const STab<T> &rj = tabs[np + pair_ord(ti, typ[j], nt)];
-    if (!in_span(rj, r1)) continue;
     pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
     const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
-    if (r2 < T(1e-14)) continue;
     const STab<T> &rk = tabs[np + pair_ord(ti, typ[k], nt)];
-    if (!in_span(rk, r2)) continue;
+    const bool ok = w0 + lane < ntri && r1 >= T(1e-14) && in_span(rj, r1) && r2 >= T(1e-14) && in_span(rk, r2);
+    if (!__any_sync(0xffffffffu, ok)) continue;
+    bool hi, hj;
+    const unsigned xi = run_links(i, lane, hi);
+    const unsigned xj = run_links(pj, lane, hj); // atom j: runs of the same neighbour slot
     const VD<T> F1 = tab_vd<T, true>(rj, seg, A.vals, r1), F2 = tab_vd<T, true>(rk, seg, A.vals, r2);
-    const T ir1 = T(1) / r1, ir2 = T(1) / r2;
+    // lanes without a term: zero inverse distances and c3, so every force below is zero
+    const T ir1 = ok ? T(1) / r1 : T(0), ir2 = ok ? T(1) / r2 : T(0);
     const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;
     const VD<T> G = tab_vd<T, true>(tabs[2 * np + ti], seg, A.vals, cth);
-    e_acc += static_cast<double>(F1.v * F2.v * G.v);
+    if (ok) e_acc += static_cast<double>(F1.v * F2.v * G.v);
     // three_body_forces (kernels.hpp:44-58)
     const T irr = ir1 * ir2;
     const T Aa = cth * ir1 * ir1 - irr, Bb = cth * ir2 * ir2 - irr;
-    const T c1 = F1.d * ir1 * F2.v * G.v, c2 = F1.v * F2.d * ir2 * G.v, c3 = F1.v * F2.v * G.d;
+    const T c1 = F1.d * ir1 * F2.v * G.v, c2 = F1.v * F2.d * ir2 * G.v, c3 = ok ? F1.v * F2.v * G.d : T(0);
     T Fj[3], Fk[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const T Fi = c1 * d1[a] + c2 * d2[a] - c3 * (Aa * d1[a] + Bb * d2[a]);
       Fj[a] = -(c1 * d1[a]) - c3 * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
       Fk[a] = -(c2 * d2[a]) - c3 * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
-      atomicAdd(&Fs[3 * i + a], Fi);
-      atomicAdd(&Fs[3 * j + a], Fj[a]);
-      atomicAdd(&Fs[3 * k + a], Fk[a]);
+      const T ti_ = run_sum(Fi, xi), tj = run_sum(Fj[a], xj);
+      if (hi) atomicAdd(&Fs[3 * i + a], ti_);
+      if (hj) atomicAdd(&Fs[3 * j + a], tj);
+      if (ok) atomicAdd(&Fs[3 * k + a], Fk[a]);
     }
     sg[0] += static_cast<double>(d1[0] * Fj[0] + d2[0] * Fk[0]);
     sg[1] += static_cast<double>(d1[1] * Fj[1] + d2[1] * Fk[1]);

@@ -88,6 +88,31 @@ template <int K> __device__ void block_sum_k(double (&v)[K], double *red) {
     }
 }
 
+// Runs of lanes with the same key, for keys that do not decrease across the
+// warp (flat work items are ordered by central atom, then by neighbour): bit s of
+// the links is set when lane + 2^s has this lane's key; head: the run's first
+// lane.  All 32 lanes call these together.
+__device__ __forceinline__ unsigned run_links(int key, int lane, bool &head) {
+  unsigned nx = 0;
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int kk = __shfl_down_sync(0xffffffffu, key, 1 << s);
+    if (lane + (1 << s) < 32 && kk == key) nx |= 1u << s;
+  }
+  const int kp = __shfl_up_sync(0xffffffffu, key, 1);
+  head = lane == 0 || kp != key;
+  return nx;
+}
+// Sum of v over this lane and the later lanes of its run (the whole run at its head).
+template <class T> __device__ __forceinline__ T run_sum(T v, unsigned nx) {
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const T t = __shfl_down_sync(0xffffffffu, v, 1 << s);
+    if (nx >> s & 1) v += t;
+  }
+  return v;
+}
+
 // An atom with n neighbours has n(n − 1)/2 neighbour pairs (j < k) in rows
 // a = 0 .. n − 2 of n − 1 − a pairs each, row a starting at a(2n − a − 1)/2.
 // For pair offset u: the row a (from the quadratic's root, then a one-step
