@@ -23,7 +23,7 @@
 // rows into the configuration's force-row block in shared memory, written out
 // once (or, when the block does not fit, straight into J, zeroed first); the
 // energy and stress rows, which every term hits, summed over the warp into J;
-// a column kernel forms Jᵀr.
+// a two-pass column reduction forms Jᵀr.
 #include "kern_common.cuh"
 
 #include <algorithm>
@@ -153,16 +153,10 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   // the configuration hits: summed over the warp and added once per row.
   // Lanes without a term pass zeros; all 32 lanes call this together.
   auto erows_warp = [&](int c0, T e, const T (&st)[6]) {
-    T v[7] = {we * e};
-#pragma unroll
-    for (int m = 0; m < 6; ++m) v[1 + m] = st[m];
-    T *Jc = A.J + static_cast<int64_t>(c0) * A.ld + row0 + rE;
-#pragma unroll
-    for (int m = 0; m < 7; ++m)
-      if (m < nrow) {
-        v[m] = warp_sum_group(v[m], 32);
-        if (lane == 0) atomicAdd(&Jc[m], v[m]);
-      }
+    const T v[8] = {we * e, st[0], st[1], st[2], st[3], st[4], st[5], T(0)};
+    const T t = warp_sum_tr<8>(v, lane); // lanes 4m hold row m
+    const int m = lane >> 2;
+    if ((lane & 3) == 0 && m < nrow) atomicAdd(&A.J[static_cast<int64_t>(c0) * A.ld + row0 + rE + m], t);
   };
   // the same rows from one lane
   auto erows_lane = [&](int cl, T e, const T (&st)[6]) {
@@ -298,6 +292,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       bool hi = false, hj = false;
       const unsigned xi = run_links(i, lane, hi);
       const unsigned xj = run_links(pj, lane, hj); // atom j: runs of the same neighbour slot
+      const bool iw = __all_sync(0xffffffffu, i == __shfl_sync(0xffffffffu, i, 0)); // one atom i for the warp
       T GJ[3] = {0, 0, 0}, GK[3] = {0, 0, 0}, ew = T(0);
       auto term = [&](int idx, T eta, T zeta, T lambda, T Cz, bool with_jk) {
         const T Aa = T(1) + lambda * costh;
@@ -334,11 +329,18 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
           const int c0 = __shfl_sync(0xffffffffu, cc, 0);
           if (__all_sync(0xffffffffu, cc == c0)) {
             if (c0 < 0) return;
+            if (iw) { // atom i's three rows by halving exchanges (lanes 8a hold row a)
+              const T v[4] = {gj[0] + gk[0], gj[1] + gk[1], gj[2] + gk[2], T(0)};
+              const T t = warp_sum_tr<4>(v, lane);
+              if ((lane & 7) == 0 && lane < 24) jadd(c0, 3 * i + (lane >> 3), t);
+            }
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              const T ti_ = run_sum(gj[a] + gk[a], xi);
+              if (!iw) {
+                const T ti_ = run_sum(gj[a] + gk[a], xi);
+                if (hi) jadd(c0, 3 * i + a, ti_);
+              }
               const T tj = run_sum(gj[a], xj);
-              if (hi) jadd(c0, 3 * i + a, ti_);
               if (hj) jadd(c0, 3 * j + a, -tj);
               if (on) jadd(c0, 3 * k + a, -gk[a]);
             }
@@ -367,10 +369,18 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
         term(L.base[4] + po * L.n5 + t, p5[3 * t], p5[3 * t + 1], p5[3 * t + 2], c5[t], false);
       if constexpr (!JAC) {
         // atoms i and j summed over their runs of lanes (zeros without a term)
+        if (iw) { // one atom i for the warp: halving exchanges (lanes 8a hold component a)
+          const T v[4] = {GJ[0] + GK[0], GJ[1] + GK[1], GJ[2] + GK[2], T(0)};
+          const T t = warp_sum_tr<4>(v, lane);
+          if ((lane & 7) == 0 && lane < 24) atomicAdd(&Fs[3 * i + (lane >> 3)], t);
+        }
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const T ti_ = run_sum(GJ[a] + GK[a], xi), tj = run_sum(GJ[a], xj);
-          if (hi) atomicAdd(&Fs[3 * i + a], ti_);
+          if (!iw) {
+            const T ti_ = run_sum(GJ[a] + GK[a], xi);
+            if (hi) atomicAdd(&Fs[3 * i + a], ti_);
+          }
+          const T tj = run_sum(GJ[a], xj);
           if (hj) atomicAdd(&Fs[3 * j + a], -tj);
           if (ok) atomicAdd(&Fs[3 * k + a], -GK[a]);
         }
@@ -456,14 +466,26 @@ __global__ void ac_sum_parts(const double *__restrict__ part, int n, double *__r
   if (threadIdx.x == 0) *out = s;
 }
 
-// Jᵀr: one CTA per column, FP64 sums over the rows.
+// Jᵀr in two passes: CTA (chunk, column) sums its slice of the column's rows
+// in FP64 into part[column][chunk], then one CTA per column adds the chunks
+// in order (deterministic).
+constexpr int kJtrChunks = 128;
 template <class T>
 __global__ void ac_jtr_kernel(const T *__restrict__ J, int64_t ld, int64_t M, const double *__restrict__ F,
-                              double *__restrict__ Jtr) {
+                              double *__restrict__ part) {
   __shared__ double r[32];
-  const T *Jc = J + static_cast<int64_t>(blockIdx.x) * ld;
+  const int64_t len = (M + gridDim.x - 1) / gridDim.x;
+  const int64_t k0 = static_cast<int64_t>(blockIdx.x) * len, k1 = min(M, k0 + len);
+  const T *Jc = J + static_cast<int64_t>(blockIdx.y) * ld;
   double s = 0.0;
-  for (int64_t k = threadIdx.x; k < M; k += blockDim.x) s += static_cast<double>(Jc[k]) * F[k];
+  for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) s += static_cast<double>(Jc[k]) * F[k];
+  s = block_sum(s, r);
+  if (threadIdx.x == 0) part[static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x] = s;
+}
+__global__ void ac_jtr_reduce(const double *__restrict__ part, int n, double *__restrict__ Jtr) {
+  __shared__ double r[32];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) s += part[static_cast<int64_t>(blockIdx.x) * n + k];
   s = block_sum(s, r);
   if (threadIdx.x == 0) Jtr[blockIdx.x] = s;
 }
@@ -527,6 +549,14 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
       FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
       FS_CUDA(cudaMalloc(&h->d_Jtr, std::max(D, 1) * sizeof(double)));
     }
+    if (D > 65535) return set_error(h, FS_ERR_UNSUPPORTED, "ACSF: more than 65535 free head values");
+    const size_t need = static_cast<size_t>(D) * kJtrChunks;
+    if (h->jtr_part_alloc < need || !h->d_jtr_part) {
+      if (h->d_jtr_part) cudaFree(h->d_jtr_part);
+      h->d_jtr_part = nullptr;
+      FS_CUDA(cudaMalloc(&h->d_jtr_part, need * sizeof(double)));
+      h->jtr_part_alloc = need;
+    }
     FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     a.J = static_cast<T *>(h->d_J);
     a.ld = ldj;
@@ -544,9 +574,11 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
   ++h->launches;
   if (jac) {
     if (D > 0) {
-      ac_jtr_kernel<T><<<D, 256, 0, h->stream>>>(static_cast<const T *>(h->d_J), h->ldj, M, h->d_F, h->d_Jtr);
+      ac_jtr_kernel<T><<<dim3(kJtrChunks, D), 256, 0, h->stream>>>(static_cast<const T *>(h->d_J), h->ldj, M, h->d_F,
+                                                                    h->d_jtr_part);
+      ac_jtr_reduce<<<D, 128, 0, h->stream>>>(h->d_jtr_part, kJtrChunks, h->d_Jtr);
       FS_CUDA(cudaGetLastError());
-      ++h->launches;
+      h->launches += 2;
     }
   } else {
     ac_sum_parts<<<1, 1024, 0, h->stream>>>(h->d_obj_part, h->n_cfg, h->d_obj);

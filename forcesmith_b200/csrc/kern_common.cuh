@@ -113,6 +113,33 @@ template <class T> __device__ __forceinline__ T run_sum(T v, unsigned nx) {
   return v;
 }
 
+// Warp sums of NV values (NV = 4 or 8) by halving exchanges: at each of the
+// first log2(NV) levels a lane keeps half of its values and trades the other
+// half with its partner, then the last levels sum one value.  Lane l ends
+// with the warp sum of value (l >> (5 − log2 NV)) & (NV − 1); every lane calls
+// this together.  NV − 1 + 5 − log2(NV) shuffles (8 values: 9, not 40).
+template <int NV, class T> __device__ __forceinline__ T warp_sum_tr(const T (&v)[NV], int lane) {
+  static_assert(NV == 4 || NV == 8, "NV is 4 or 8");
+  T a[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) a[q] = v[q];
+  int h = NV / 2, bit = 16;
+#pragma unroll
+  for (; h >= 1; h >>= 1, bit >>= 1) {
+    const bool up = lane & bit;
+#pragma unroll
+    for (int q = 0; q < h; ++q) {
+      const T send = up ? a[q] : a[q + h];
+      const T keep = up ? a[q + h] : a[q];
+      a[q] = keep + __shfl_xor_sync(0xffffffffu, send, bit);
+    }
+  }
+  T s = a[0];
+#pragma unroll
+  for (; bit >= 1; bit >>= 1) s += __shfl_xor_sync(0xffffffffu, s, bit);
+  return s;
+}
+
 // An atom with n neighbours has n(n − 1)/2 neighbour pairs (j < k) in rows
 // a = 0 .. n − 2 of n − 1 − a pairs each, row a starting at a(2n − a − 1)/2.
 // For pair offset u: the row a (from the quadratic's root, then a one-step
