@@ -33,21 +33,31 @@ namespace {
 
 constexpr int kAcThreads = 256;
 
-// exp and x^y: the hardware approximations in FP32 (a few ulp, inside the
-// FP32 path's stated tolerances), IEEE in FP64
+// exp, x^y, 1/x and the cutoff's sine and cosine (argument in [0, π]): the
+// hardware approximations in FP32 (a few ulp, or 2^-21 absolute for the
+// sine and cosine, inside the FP32 path's stated tolerances), IEEE in FP64
 __device__ __forceinline__ float ac_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double ac_exp(double x) { return exp(x); }
 __device__ __forceinline__ float ac_pow(float a, float z) { return __expf(z * __logf(a)); }
 __device__ __forceinline__ double ac_pow(double a, double z) { return pow(a, z); }
+__device__ __forceinline__ float ac_rcp(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double ac_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ void ac_sincos(float x, float &s, float &c) { __sincosf(x, &s, &c); }
+__device__ __forceinline__ void ac_sincos(double x, double &s, double &c) { sincos(x, &s, &c); }
+// sine and cosine of any argument (G3's κr): the full-range library functions
+__device__ __forceinline__ void ac_sincos_full(float x, float &s, float &c) { sincosf(x, &s, &c); }
+__device__ __forceinline__ void ac_sincos_full(double x, double &s, double &c) { sincos(x, &s, &c); }
 
-template <class T> __device__ __forceinline__ void ac_fc(T r, T rc, T &fc, T &fcp) {
+// f_c(r) = ½(1 + cos(πr/rc)) and its derivative; prc = π/rc
+template <class T> __device__ __forceinline__ void ac_fc(T r, T rc, T prc, T &fc, T &fcp) {
   if (r >= rc) {
     fc = fcp = T(0);
     return;
   }
-  const T x = T(3.14159265358979323846) * r / rc;
-  fc = T(0.5) * (T(1) + cos(x));
-  fcp = T(-0.5) * T(3.14159265358979323846) / rc * sin(x);
+  T sn, cs;
+  ac_sincos(prc * r, sn, cs);
+  fc = T(0.5) * (T(1) + cs);
+  fcp = T(-0.5) * prc * sn;
 }
 
 // The descriptor hyperparameters and layout (acsf.hpp:23-46), from the ACSF
@@ -130,6 +140,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   stage_work(start, N, pfirst, tfirst, wsum);
   __syncthreads();
   const T rc = par[0];
+  const T prc = static_cast<T>(3.14159265358979323846 / spec[0]);
   const T *p2 = par + 6, *p3 = p2 + 2 * L.n2, *p4 = p3 + L.n3, *p5 = p4 + 3 * L.n4;
   const T *c4 = cz, *c5 = cz + L.n4;
   const uint32_t *nbp = A.c.nb_pack + start[0];
@@ -176,10 +187,10 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
     const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
     const bool ok = w0 + lane < npair && r >= T(1e-14) && r < rc;
     if (!__any_sync(0xffffffffu, ok)) continue;
-    const T ir = ok ? T(1) / r : T(0);
+    const T ir = ok ? ac_rcp(r) : T(0);
     const T rh[3] = {d[0] * ir, d[1] * ir, d[2] * ir};
     T fc, fcp;
-    ac_fc(r, rc, fc, fcp);
+    ac_fc(r, rc, prc, fc, fcp);
     const int s = typ[j], ti = typ[i];
     const T *w_ = W + ti * (L.S + 1);
     const int *cl = col + ti * (L.S + 1);
@@ -227,7 +238,9 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       term(L.base[1] + s * L.n2 + t, gs * fc, gs * (T(-2) * eta * dr * fc + fcp));
     }
     for (int t = 0; t < L.n3; ++t) {
-      const T k = p3[t], cc = cos(k * r), ss = sin(k * r);
+      const T k = p3[t];
+      T ss, cc;
+      ac_sincos_full(k * r, ss, cc);
       term(L.base[2] + s * L.n3 + t, cc * fc, -k * ss * fc + cc * fcp);
     }
     if constexpr (!JAC) {
@@ -270,19 +283,21 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       const int ti = typ[i];
       const T *w_ = W + ti * (L.S + 1);
       const int *cl = col + ti * (L.S + 1);
-      const T ir1 = ok ? T(1) / r1 : T(0), ir2 = ok ? T(1) / r2 : T(0);
+      const T ir1 = ok ? ac_rcp(r1) : T(0), ir2 = ok ? ac_rcp(r2) : T(0);
       const T h1[3] = {d1[0] * ir1, d1[1] * ir1, d1[2] * ir1}, h2[3] = {d2[0] * ir2, d2[1] * ir2, d2[2] * ir2};
       T costh = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * (ir1 * ir2);
       costh = min(max(costh, T(-1)), T(1));
       const T djk[3] = {d2[0] - d1[0], d2[1] - d1[1], d2[2] - d1[2]};
       const T rjk = sqrt(djk[0] * djk[0] + djk[1] * djk[1] + djk[2] * djk[2]);
       T hjk[3] = {T(0), T(0), T(0)};
-      if (rjk > T(1e-14))
-        for (int a = 0; a < 3; ++a) hjk[a] = djk[a] / rjk;
+      if (rjk > T(1e-14)) {
+        const T irjk = ac_rcp(rjk);
+        for (int a = 0; a < 3; ++a) hjk[a] = djk[a] * irjk;
+      }
       T f1, fp1, f2, fp2, fjk, fpjk;
-      ac_fc(r1, rc, f1, fp1);
-      ac_fc(r2, rc, f2, fp2);
-      ac_fc(rjk, rc, fjk, fpjk);
+      ac_fc(r1, rc, prc, f1, fp1);
+      ac_fc(r2, rc, prc, f2, fp2);
+      ac_fc(rjk, rc, prc, fjk, fpjk);
       T dcj[3], dck[3];
       for (int a = 0; a < 3; ++a) {
         dcj[a] = (h2[a] - costh * h1[a]) * ir1;
@@ -299,7 +314,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
         const bool on = ok && Aa > T(1e-12);
         // 2^{1−ζ} per function (precomputed); ζ λ A^{ζ−1} = ζ λ A^ζ / A (A > 1e-12)
         const T Ab = on ? Aa : T(1);
-        const T C = Cz, ang = ac_pow(Ab, zeta), dang = zeta * lambda * ang / Ab;
+        const T C = Cz, ang = ac_pow(Ab, zeta), dang = zeta * lambda * ang * ac_rcp(Ab);
         const T rsum = r1 * r1 + r2 * r2 + (with_jk ? rjk * rjk : T(0));
         const T rad = ac_exp(-eta * rsum);
         const T fj = with_jk ? fjk : T(1);
