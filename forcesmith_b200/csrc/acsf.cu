@@ -24,6 +24,7 @@
 // once (or, when the block does not fit, straight into J, zeroed first); the
 // energy and stress rows, which every term hits, summed over the warp into J;
 // a two-pass column reduction forms Jᵀr.
+#include "jtr.cuh"
 #include "kern_common.cuh"
 
 #include <algorithm>
@@ -481,30 +482,6 @@ __global__ void ac_sum_parts(const double *__restrict__ part, int n, double *__r
   if (threadIdx.x == 0) *out = s;
 }
 
-// Jᵀr in two passes: CTA (chunk, column) sums its slice of the column's rows
-// in FP64 into part[column][chunk], then one CTA per column adds the chunks
-// in order (deterministic).
-constexpr int kJtrChunks = 128;
-template <class T>
-__global__ void ac_jtr_kernel(const T *__restrict__ J, int64_t ld, int64_t M, const double *__restrict__ F,
-                              double *__restrict__ part) {
-  __shared__ double r[32];
-  const int64_t len = (M + gridDim.x - 1) / gridDim.x;
-  const int64_t k0 = static_cast<int64_t>(blockIdx.x) * len, k1 = min(M, k0 + len);
-  const T *Jc = J + static_cast<int64_t>(blockIdx.y) * ld;
-  double s = 0.0;
-  for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) s += static_cast<double>(Jc[k]) * F[k];
-  s = block_sum(s, r);
-  if (threadIdx.x == 0) part[static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x] = s;
-}
-__global__ void ac_jtr_reduce(const double *__restrict__ part, int n, double *__restrict__ Jtr) {
-  __shared__ double r[32];
-  double s = 0.0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) s += part[static_cast<int64_t>(blockIdx.x) * n + k];
-  s = block_sum(s, r);
-  if (threadIdx.x == 0) Jtr[blockIdx.x] = s;
-}
-
 template <class T> size_t ac_smem(const fs_gpu *h, int mi) {
   AcLayout L;
   L.init(h->tables[0].v.data(), h->ntypes);
@@ -564,14 +541,6 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
       FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
       FS_CUDA(cudaMalloc(&h->d_Jtr, std::max(D, 1) * sizeof(double)));
     }
-    if (D > 65535) return set_error(h, FS_ERR_UNSUPPORTED, "ACSF: more than 65535 free head values");
-    const size_t need = static_cast<size_t>(D) * kJtrChunks;
-    if (h->jtr_part_alloc < need || !h->d_jtr_part) {
-      if (h->d_jtr_part) cudaFree(h->d_jtr_part);
-      h->d_jtr_part = nullptr;
-      FS_CUDA(cudaMalloc(&h->d_jtr_part, need * sizeof(double)));
-      h->jtr_part_alloc = need;
-    }
     FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     a.J = static_cast<T *>(h->d_J);
     a.ld = ldj;
@@ -589,11 +558,7 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
   ++h->launches;
   if (jac) {
     if (D > 0) {
-      ac_jtr_kernel<T><<<dim3(kJtrChunks, D), 256, 0, h->stream>>>(static_cast<const T *>(h->d_J), h->ldj, M, h->d_F,
-                                                                    h->d_jtr_part);
-      ac_jtr_reduce<<<D, 128, 0, h->stream>>>(h->d_jtr_part, kJtrChunks, h->d_Jtr);
-      FS_CUDA(cudaGetLastError());
-      h->launches += 2;
+      FS_TRY(launch_jtr<T>(h, static_cast<const T *>(h->d_J), h->ldj, M, D, h->d_F, h->d_Jtr));
     }
   } else {
     ac_sum_parts<<<1, 1024, 0, h->stream>>>(h->d_obj_part, h->n_cfg, h->d_obj);

@@ -1,9 +1,11 @@
 // Central-difference Jacobian on the device — the reference's own method
 // (opt::fd_jacobian, include/forcesmith/optimization/fd_jacobian.hpp:37-49:
 // h = 1e-5, x restored by the same add/subtract sequence), used for families
-// without an analytic device Jacobian in this build (ADP).  2·D residual
-// launches; FP64 contexts only (FP32 residuals are too coarse for h = 1e-5).
+// without an analytic device Jacobian in this build (ADP, Tersoff, Angular).
+// 2·D residual launches; FP64 contexts only (FP32 residuals are too coarse for
+// h = 1e-5).
 #include "internal.cuh"
+#include "jtr.cuh"
 
 #include <vector>
 
@@ -15,22 +17,6 @@ __global__ void fd_column(const double *__restrict__ Fp, const double *__restric
   for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < M;
        r += static_cast<int64_t>(gridDim.x) * blockDim.x)
     col[r] = (Fp[r] - Fm[r]) * inv2h;
-}
-
-__global__ void jtr_dense(const double *__restrict__ J, int64_t ld, int64_t M, const double *__restrict__ F,
-                          double *__restrict__ Jtr) {
-  __shared__ double red[32];
-  const int col = blockIdx.x;
-  double s = 0.0;
-  for (int64_t r = threadIdx.x; r < M; r += blockDim.x) s += J[col * ld + r] * F[r];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) t += red[k];
-    Jtr[col] = t;
-  }
 }
 
 } // namespace
@@ -86,11 +72,7 @@ int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s) {
   if (rc == FS_OK) rc = refresh_segments(h);
   h->params_dirty = false;
   FS_CUDA(cudaMemcpyAsync(h->d_F, Fbase, M * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  if (rc == FS_OK) {
-    jtr_dense<<<D, 256, 0, h->stream>>>(static_cast<const double *>(h->d_J), ldj, M, h->d_F, h->d_Jtr);
-    FS_CUDA(cudaGetLastError());
-    ++h->launches;
-  }
+  if (rc == FS_OK) rc = launch_jtr<double>(h, static_cast<const double *>(h->d_J), ldj, M, D, h->d_F, h->d_Jtr);
   cudaFreeAsync(Fbase, h->stream);
   cudaFreeAsync(Fp, h->stream);
   return rc;
