@@ -530,12 +530,13 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
   if (jac) {
     const int64_t ldj = (M + 31) / 32 * 32;
     const size_t jn = static_cast<size_t>(ldj) * D;
-    if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J) {
+    if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J || h->j_rowmajor) {
       if (h->d_J) cudaFree(h->d_J);
       h->d_J = nullptr;
       FS_CUDA(cudaMalloc(&h->d_J, std::max<size_t>(jn, 1) * sizeof(T)));
       h->jac_alloc = static_cast<int64_t>(jn);
       h->ldj = ldj;
+      h->j_rowmajor = false;
     }
     if (!h->d_JtJ) {
       FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));

@@ -661,6 +661,14 @@ int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F, double *J
       FS_CUDA(cudaMemcpy2DAsync(J, m * sizeof(double), h->d_J, h->ldj * sizeof(double), m * sizeof(double),
                                 h->D, cudaMemcpyDeviceToHost, h->stream));
       FS_TRY(sync(h));
+    } else if (h->j_rowmajor) { // row-major on the device (rows × ldj): transposed here
+      std::vector<float> tmp(n);
+      FS_CUDA(cudaMemcpy2DAsync(tmp.data(), h->D * sizeof(float), h->d_J, h->ldj * sizeof(float),
+                                h->D * sizeof(float), m, cudaMemcpyDeviceToHost, h->stream));
+      FS_TRY(sync(h));
+      const int64_t D = h->D;
+      for (int64_t r = 0; r < m; ++r)
+        for (int64_t c = 0; c < D; ++c) J[c * m + r] = tmp[r * D + c];
     } else {
       std::vector<float> tmp(n);
       FS_CUDA(cudaMemcpy2DAsync(tmp.data(), m * sizeof(float), h->d_J, h->ldj * sizeof(float), m * sizeof(float),

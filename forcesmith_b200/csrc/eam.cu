@@ -578,13 +578,13 @@ template <class T> struct JacArgs {
   const int32_t *seg_ws;
   double w_e, w_s;
   int64_t M;            // rows of J
-  int64_t ld;           // leading dimension of J (≥ M)
+  int64_t cs, rs;       // J element (row, col) at row·rs + col·cs: (1, ld) row-major, (ld, 1) column-major
   int D;
   const double *F;      // residual (for the fused Jᵀr)
   double *jtr_part;     // [config][D] Jᵀr partials (FP64)
   int dens_c0, ndens;   // contiguous density columns
   int stage;            // 1: the per-atom Jacobian data of a config fits in shared memory
-  T *J;                 // column-major M × D
+  T *J;                 // M × D, row- or column-major (cs, rs)
   T *gF, *cF, *over;    // [atom]: F'(ρ̄), F''(ρ̄), clamp overshoot term (0 = unclamped)
   T *drho;              // [atom][ndens]
   T *dgd;               // [atom][kWin]: ∂F'(ρ̄)/∂y over the embedding window
@@ -748,8 +748,8 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
   const int64_t rE = row0 + 3 * N, rL = rE + 1 + (A.w_s > 0.0 ? 6 : 0);
   for (int col = threadIdx.x; col < A.D; col += blockDim.x) {
-    A.J[col * A.ld + rE] = static_cast<T>(erow[col]);
-    A.J[col * A.ld + rL] = static_cast<T>(lrow[col]);
+    A.J[col * A.cs + rE * A.rs] = static_cast<T>(erow[col]);
+    A.J[col * A.cs + rL * A.rs] = static_cast<T>(lrow[col]);
   }
 }
 
@@ -1151,18 +1151,30 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     const double F0 = A.F[row0 + 3 * i], F1 = A.F[row0 + 3 * i + 1], F2 = A.F[row0 + 3 * i + 2];
     const T x0 = static_cast<T>(-2.0 * (wpos[3 * i] - ctr[0])), x1 = static_cast<T>(-2.0 * (wpos[3 * i + 1] - ctr[1])),
             x2 = static_cast<T>(-2.0 * (wpos[3 * i + 2] - ctr[2]));
-    // the atom's 3 rows of a column in two stores: a pair on its even row
-    // (ld is a multiple of 32, so the row parity is the address parity)
+    // Streaming stores: J is written once here and read once by JᵀJ, so it
+    // should not evict the ∂ρ/∂y rows this kernel rereads from L2.  Row-major
+    // J: each of the atom's 3 rows is one coalesced store per 32 columns.
+    // Column-major J: the atom's 3 rows of a column in two stores, a pair on
+    // its even row (ld is a multiple of 32, so the row parity is the address
+    // parity).
+    const bool rowm = A.cs == 1;
     const bool even = ((row0 + 3 * i) & 1) == 0;
+    T *Ji = A.J + (row0 + 3 * i) * A.rs;
     for (int col = lane; col < D; col += 32) {
       const T4 fr = frow[col];
-      T *Jc = A.J + static_cast<int64_t>(col) * A.ld + row0 + 3 * i;
-      if (even) {
-        *reinterpret_cast<T2 *>(Jc) = T2{fr.x, fr.y};
-        Jc[2] = fr.z;
+      if (rowm) {
+        __stcs(Ji + col, fr.x);
+        __stcs(Ji + A.rs + col, fr.y);
+        __stcs(Ji + 2 * A.rs + col, fr.z);
       } else {
-        Jc[0] = fr.x;
-        *reinterpret_cast<T2 *>(Jc + 1) = T2{fr.y, fr.z};
+        T *Jc = Ji + static_cast<int64_t>(col) * A.cs;
+        if (even) {
+          __stcs(reinterpret_cast<T2 *>(Jc), T2{fr.x, fr.y});
+          __stcs(Jc + 2, fr.z);
+        } else {
+          __stcs(Jc, fr.x);
+          __stcs(reinterpret_cast<T2 *>(Jc + 1), T2{fr.y, fr.z});
+        }
       }
       erow[col] += fr.w;
       jtr[col] += static_cast<double>(fr.x) * F0 + static_cast<double>(fr.y) * F1 + static_cast<double>(fr.z) * F2;
@@ -1191,14 +1203,15 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
       e += static_cast<double>(erow_all[static_cast<size_t>(ww) * D + col]);
       jr += jtr_all[static_cast<size_t>(ww) * D + col];
     }
-    T *Jc = A.J + static_cast<int64_t>(col) * A.ld;
+    T *Jc = A.J + static_cast<int64_t>(col) * A.cs; // row r of this column: Jc[r · rs]
+    const int64_t rs = A.rs;
     if constexpr (EAM)
-      Jc[rE] = static_cast<T>(static_cast<double>(Jc[rE]) + e);
+      Jc[rE * rs] = static_cast<T>(static_cast<double>(Jc[rE * rs]) + e);
     else
-      Jc[rE] = static_cast<T>(e);
+      Jc[rE * rs] = static_cast<T>(e);
     // Jᵀr over this configuration's rows: force rows (above), energy, stress, limit
-    jr += static_cast<double>(Jc[rE]) * A.F[rE];
-    if constexpr (EAM) jr += static_cast<double>(Jc[rL]) * A.F[rL];
+    jr += static_cast<double>(Jc[rE * rs]) * A.F[rE];
+    if constexpr (EAM) jr += static_cast<double>(Jc[rL * rs]) * A.F[rL];
     if (want_stress) {
       double s[6] = {0, 0, 0, 0, 0, 0};
       for (int ww = 0; ww < warps; ++ww) {
@@ -1211,11 +1224,11 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
         s[5] += static_cast<double>(sr[2].y);
       }
       for (int v = 0; v < 6; ++v) {
-        Jc[rE + 1 + v] = static_cast<T>(sc * s[v]);
-        jr += static_cast<double>(Jc[rE + 1 + v]) * A.F[rE + 1 + v];
+        Jc[(rE + 1 + v) * rs] = static_cast<T>(sc * s[v]);
+        jr += static_cast<double>(Jc[(rE + 1 + v) * rs]) * A.F[rE + 1 + v];
       }
     }
-    if constexpr (!EAM) Jc[rL] = T(0); // limit row: no embedding
+    if constexpr (!EAM) Jc[rL * rs] = T(0); // limit row: no embedding
     A.jtr_part[static_cast<int64_t>(c) * D + col] = jr;
   }
 }
@@ -1314,11 +1327,16 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   const bool eam = h->family == FS_FAMILY_EAM;
   const int64_t M = rows_of(h, w_s);
   const int D = h->D;
-  // J: column-major with the leading dimension rounded up to 32 rows (a
-  // 16-byte multiple, as a TMA row stride needs); padding rows stay zero
-  const int64_t ldj = (M + 31) / 32 * 32;
-  const size_t jn = static_cast<size_t>(ldj) * D;
-  if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J) {
+  // J, rows rounded up to 32 (padding rows stay zero).  FP32 with D ≤ 256
+  // (the tensor-core JᵀJ): row-major with the row stride rounded up to 4
+  // columns (16 bytes, as a TMA stride needs), so that an atom's rows are
+  // contiguous and its stores coalesce.  Otherwise column-major with the
+  // leading dimension the padded row count.
+  const bool rowmajor = sizeof(T) == 4 && D <= 256;
+  const int64_t rows = (M + 31) / 32 * 32;
+  const int64_t ldj = rowmajor ? (D + 3) / 4 * 4 : rows;
+  const size_t jn = static_cast<size_t>(rowmajor ? rows * ldj : ldj * D);
+  if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J || h->j_rowmajor != rowmajor) {
     if (h->d_J) cudaFree(h->d_J);
     h->d_J = nullptr;
     if (cudaMalloc(&h->d_J, std::max<size_t>(jn, 1) * sizeof(T)) != cudaSuccess)
@@ -1326,6 +1344,7 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
     FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     h->jac_alloc = static_cast<int64_t>(jn);
     h->ldj = ldj;
+    h->j_rowmajor = rowmajor;
   }
   {
     const size_t need = static_cast<size_t>(h->n_cfg) * D;
@@ -1383,7 +1402,8 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   a.w_e = w_e;
   a.w_s = w_s;
   a.M = M;
-  a.ld = ldj;
+  a.cs = rowmajor ? 1 : ldj;
+  a.rs = rowmajor ? ldj : 1;
   a.D = D;
   a.F = h->d_F;
   a.jtr_part = h->d_jtr_part;

@@ -172,8 +172,9 @@ struct fs_gpu {
   double *d_obj = nullptr;       // scalar
   // Jacobian buffers
   int64_t jac_alloc = 0;         // elements of J
-  void *d_J = nullptr;           // column-major ldj × D, FP32 or FP64 (rows ≥ M are zero)
-  int64_t ldj = 0;               // leading dimension of J (rows rounded up to 32)
+  void *d_J = nullptr;           // J, FP32 or FP64; rows rounded up to 32 (rows ≥ M are zero)
+  int64_t ldj = 0;               // column-major: the padded row count; row-major: the row stride (≥ D)
+  bool j_rowmajor = false;       // row-major J (FP32 EAM / pair Jacobians feeding the tensor-core JᵀJ)
   double *d_jtr_part = nullptr;  // per-config Jᵀr partials (FP64)
   size_t jtr_part_alloc = 0;
   int32_t *d_err = nullptr;      // device error word (bounded waits that gave up)
