@@ -135,6 +135,8 @@ void free_jacobian(fs_gpu *h) {
   dfree(h->d_gram_part);
   dfree(h->d_jtr_part);
   h->jtr_part_alloc = 0;
+  dfree(h->d_half_part);
+  h->half_part_alloc = 0;
   dfree(h->d_atom_scalars);
   dfree(h->d_drho);
   dfree(h->d_dgd);

@@ -579,6 +579,8 @@ template <class T> struct JacArgs {
   double w_e, w_s;
   int64_t M;            // rows of J
   int64_t cs, rs;       // J element (row, col) at row·rs + col·cs: (1, ld) row-major, (ld, 1) column-major
+  int halves;           // force-row pass: CTAs per configuration (1 or 2)
+  double *half_part;    // halves = 2: per (configuration, half) sums [8][D]: energy, 6 stress, Jᵀr
   int D;
   const double *F;      // residual (for the fused Jᵀr)
   double *jtr_part;     // [config][D] Jᵀr partials (FP64)
@@ -808,12 +810,45 @@ constexpr int kPairStep = 4; // pairs whose scatter terms are formed together
 // buffers of 11 warps fill the shared memory), 8 in FP64 (registers)
 template <class T> constexpr int kMaxK2Warps = sizeof(T) == 4 ? 11 : 8;
 
+// A configuration's column of the energy, stress and limit rows, from the
+// force-row pass's sums over its atoms (φ energy e, stress s, Jᵀr over the
+// force rows jr), and its Jᵀr over all its rows into jtr_part.
+template <class T, bool EAM>
+__device__ void finish_cfg_column(const JacArgs<T> &A, int c, int col, double e, const double (&s)[6], double jr) {
+  const CfgDev &cd = A.c.cfg[c];
+  const bool want_stress = A.w_s > 0.0;
+  const int64_t rows_per_extra = 2 + (want_stress ? 6 : 0);
+  const int64_t row0 = 3 * static_cast<int64_t>(cd.atom0) + static_cast<int64_t>(c) * rows_per_extra;
+  const int64_t rE = row0 + 3 * cd.natoms;
+  const int64_t rL = rE + 1 + (want_stress ? 6 : 0);
+  const double sc = -A.w_s * 0.5 / cd.volume;
+  T *Jc = A.J + static_cast<int64_t>(col) * A.cs; // row r of this column: Jc[r · rs]
+  const int64_t rs = A.rs;
+  if constexpr (EAM)
+    Jc[rE * rs] = static_cast<T>(static_cast<double>(Jc[rE * rs]) + e);
+  else
+    Jc[rE * rs] = static_cast<T>(e);
+  // Jᵀr over this configuration's rows: force rows (jr), energy, stress, limit
+  jr += static_cast<double>(Jc[rE * rs]) * A.F[rE];
+  if constexpr (EAM) jr += static_cast<double>(Jc[rL * rs]) * A.F[rL];
+  if (want_stress)
+    for (int v = 0; v < 6; ++v) {
+      Jc[(rE + 1 + v) * rs] = static_cast<T>(sc * s[v]);
+      jr += static_cast<double>(Jc[(rE + 1 + v) * rs]) * A.F[rE + 1 + v];
+    }
+  if constexpr (!EAM) Jc[rL * rs] = T(0); // limit row: no embedding
+  A.jtr_part[static_cast<int64_t>(c) * A.D + col] = jr;
+}
+
 template <class T, bool EAM, int STAGE>
 __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacArgs<T> A, int warps) {
   using T4 = typename Vec4T<T>::type;
   using T2 = typename V2T<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int c = blockIdx.x;
+  // halves = 2: two CTAs per configuration, taking alternate strides of its
+  // atoms (shorter CTAs fill the last wave of SMs better)
+  const int c = blockIdx.x / A.halves, half = blockIdx.x % A.halves;
+  const int astep = warps * A.halves;
   const CfgDev &cd = A.c.cfg[c];
   const int N = cd.natoms;
   const int D = A.D;
@@ -906,8 +941,9 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     pre_p0 = p;
     pk_next = lane < end - p ? A.c.nb_pack[p + lane] : 0u;
   };
-  if (w < N) prefetch(start[w], start[w + 1]);
-  for (int i = w; i < N; i += warps) {
+  const int i_first = w + half * warps;
+  if (i_first < N) prefetch(start[i_first], start[i_first + 1]);
+  for (int i = i_first; i < N; i += astep) {
     for (int k = lane; k <= D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
     const int ti = typ[i];
     T gFi = T(0), cFi = T(0);
@@ -927,7 +963,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
       {
         int np0 = p0 + 32, nend = start[i + 1];
         if (np0 >= nend) {
-          const int in = i + warps;
+          const int in = i + astep;
           np0 = in < N ? start[in] : 0;
           nend = in < N ? start[in + 1] : 0;
         }
@@ -1194,26 +1230,13 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     __syncwarp();
   }
   __syncthreads();
-  const int64_t rE = row0 + 3 * N;
-  const double sc = -A.w_s * 0.5 / cd.volume;
-  const int64_t rL = rE + 1 + (want_stress ? 6 : 0);
   for (int col = threadIdx.x; col < D; col += blockDim.x) {
-    double e = 0.0, jr = 0.0;
+    double e = 0.0, jr = 0.0, s[6] = {0, 0, 0, 0, 0, 0};
     for (int ww = 0; ww < warps; ++ww) {
       e += static_cast<double>(erow_all[static_cast<size_t>(ww) * D + col]);
       jr += jtr_all[static_cast<size_t>(ww) * D + col];
     }
-    T *Jc = A.J + static_cast<int64_t>(col) * A.cs; // row r of this column: Jc[r · rs]
-    const int64_t rs = A.rs;
-    if constexpr (EAM)
-      Jc[rE * rs] = static_cast<T>(static_cast<double>(Jc[rE * rs]) + e);
-    else
-      Jc[rE * rs] = static_cast<T>(e);
-    // Jᵀr over this configuration's rows: force rows (above), energy, stress, limit
-    jr += static_cast<double>(Jc[rE * rs]) * A.F[rE];
-    if constexpr (EAM) jr += static_cast<double>(Jc[rL * rs]) * A.F[rL];
-    if (want_stress) {
-      double s[6] = {0, 0, 0, 0, 0, 0};
+    if (want_stress)
       for (int ww = 0; ww < warps; ++ww) {
         const T2 *sr = srow_all + static_cast<size_t>(ww) * 3 * D + 3 * col;
         s[0] += static_cast<double>(sr[0].x);
@@ -1223,13 +1246,25 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
         s[4] += static_cast<double>(sr[2].x);
         s[5] += static_cast<double>(sr[2].y);
       }
-      for (int v = 0; v < 6; ++v) {
-        Jc[(rE + 1 + v) * rs] = static_cast<T>(sc * s[v]);
-        jr += static_cast<double>(Jc[(rE + 1 + v) * rs]) * A.F[rE + 1 + v];
-      }
+    if (A.halves == 1) {
+      finish_cfg_column<T, EAM>(A, c, col, e, s, jr);
+    } else { // the combine kernel adds the halves in order and finishes the column
+      double *hp = A.half_part + (static_cast<int64_t>(c) * 2 + half) * 8 * D + col;
+      hp[0] = e;
+      for (int v = 0; v < 6; ++v) hp[(1 + v) * D] = s[v];
+      hp[7 * D] = jr;
     }
-    if constexpr (!EAM) Jc[rL * rs] = T(0); // limit row: no embedding
-    A.jtr_part[static_cast<int64_t>(c) * D + col] = jr;
+  }
+}
+
+// halves = 2: configuration blockIdx.x's columns from its two CTAs' sums
+template <class T, bool EAM> __global__ void __launch_bounds__(256) jac_halves_combine(JacArgs<T> A) {
+  const int c = blockIdx.x, D = A.D;
+  const double *h0 = A.half_part + static_cast<int64_t>(c) * 2 * 8 * D, *h1 = h0 + 8 * D;
+  for (int col = threadIdx.x; col < D; col += blockDim.x) {
+    double s[6];
+    for (int v = 0; v < 6; ++v) s[v] = h0[(1 + v) * D + col] + h1[(1 + v) * D + col];
+    finish_cfg_column<T, EAM>(A, c, col, h0[col] + h1[col], s, h0[7 * D + col] + h1[7 * D + col]);
   }
 }
 
@@ -1404,6 +1439,8 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   a.M = M;
   a.cs = rowmajor ? 1 : ldj;
   a.rs = rowmajor ? ldj : 1;
+  a.halves = 1;
+  a.half_part = nullptr;
   a.D = D;
   a.F = h->d_F;
   a.jtr_part = h->d_jtr_part;
@@ -1476,8 +1513,37 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
                                   : jac_forces_kernel<T, true, 0>)
                 : jac_forces_kernel<T, false, 0>;
   FS_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm2)));
-  k2<<<h->n_cfg, 32 * warps, sm2, h->stream>>>(a, warps);
+  // Two CTAs per configuration when that fills the SMs' waves clearly better
+  // (e.g. 500 configurations on 148 SMs, one CTA each: 3.38 of 4 waves busy,
+  // 84 %; 1000 half-size CTAs: 6.76 of 7, 97 %), and every CTA keeps atoms.
+  {
+    int per_sm = 0, nsm = 0;
+    FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2, 32 * warps, sm2));
+    FS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const int64_t slots = static_cast<int64_t>(std::max(per_sm, 1)) * std::max(nsm, 1);
+    auto fill = [&](int64_t ctas) { return static_cast<double>(ctas) / (((ctas + slots - 1) / slots) * slots); };
+    int min_atoms = 1 << 30;
+    for (const CfgDev &cd : h->cfg_host) min_atoms = std::min(min_atoms, cd.natoms);
+    if (min_atoms >= 2 * warps && fill(2 * static_cast<int64_t>(h->n_cfg)) > fill(h->n_cfg) + 0.05) {
+      const size_t need = static_cast<size_t>(h->n_cfg) * 2 * 8 * D;
+      if (h->half_part_alloc < need || !h->d_half_part) {
+        if (h->d_half_part) cudaFree(h->d_half_part);
+        h->d_half_part = nullptr;
+        FS_CUDA(cudaMalloc(&h->d_half_part, need * sizeof(double)));
+        h->half_part_alloc = need;
+      }
+      a.halves = 2;
+      a.half_part = h->d_half_part;
+    }
+  }
+  k2<<<h->n_cfg * a.halves, 32 * warps, sm2, h->stream>>>(a, warps);
   FS_CUDA(cudaGetLastError());
+  if (a.halves == 2) {
+    auto comb = eam ? jac_halves_combine<T, true> : jac_halves_combine<T, false>;
+    comb<<<h->n_cfg, 256, 0, h->stream>>>(a);
+    FS_CUDA(cudaGetLastError());
+    ++h->launches;
+  }
   jtr_reduce_kernel<<<(D + 127) / 128, 128, 0, h->stream>>>(h->d_jtr_part, h->n_cfg, D, h->d_Jtr);
   FS_CUDA(cudaGetLastError());
   h->launches += 2;

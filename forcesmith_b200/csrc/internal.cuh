@@ -177,6 +177,8 @@ struct fs_gpu {
   bool j_rowmajor = false;       // row-major J (FP32 EAM / pair Jacobians feeding the tensor-core JᵀJ)
   double *d_jtr_part = nullptr;  // per-config Jᵀr partials (FP64)
   size_t jtr_part_alloc = 0;
+  double *d_half_part = nullptr; // force-row pass with two CTAs per configuration: their sums
+  size_t half_part_alloc = 0;
   int32_t *d_err = nullptr;      // device error word (bounded waits that gave up)
   double *d_JtJ = nullptr;       // D × D
   double *d_Jtr = nullptr;       // D

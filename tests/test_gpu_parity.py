@@ -173,6 +173,45 @@ def test_eam_jacobian_fp32(ternary_small):
     assert np.max(np.abs(res["Jtr"] - Jtr)) <= 1e-4 * np.max(np.abs(Jtr))
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_eam_jacobian_two_ctas_per_configuration(precision):
+    """20 configurations of 24 atoms fill the SMs' waves better as 40 CTAs, so
+    the force-row pass gives each configuration two CTAs (alternate strides of
+    its atoms) and a combine kernel adds their energy, stress and Jᵀr sums: one
+    launch more per step than 6 configurations take.  Against the analytic
+    oracle: FP64 J, JᵀJ, Jᵀr 1e-9·(1 + |x|); FP32 J 1e-4·max|J column|, JᵀJ
+    1e-3 of √(JᵀJ_aa·JᵀJ_bb), Jᵀr 1e-4 of its largest entry."""
+    from forcesmith_b200.gpu import launch_count
+    true, start = ternary_models(20)
+    ds = label(small_ternary(20, 24, seed=12), true, O.Oracle, 1.0, 0.1)
+    per_step = []
+    for sub in (ds, ds.subset(list(range(6)))):
+        g = _gpu(precision)
+        g.upload(sub)
+        g.set_model(start)
+        g.jacobian_async(1.0, 0.1)
+        n0 = launch_count(g)
+        g.jacobian_async(1.0, 0.1)
+        per_step.append(launch_count(g) - n0)
+    assert per_step[0] == per_step[1] + 1, per_step
+    g, o = _pair(ds, start, precision)
+    res = g.jacobian(1.0, 0.1)
+    Ja = o.jacobian_analytic(1.0, 0.1)
+    F = o.eval(1.0, 0.1)["F"]
+    JtJ, Jtr = O.normal_equations(Ja, F)
+    if precision == "fp64":
+        _close(res["J"], Ja, 1e-9, "J vs analytic oracle")
+        _close(res["JtJ"], JtJ, 1e-9, "JtJ")
+        _close(res["Jtr"], Jtr, 1e-9, "Jtr")
+    else:
+        colmax = np.abs(Ja).max(axis=0) + 1e-30
+        assert np.max(np.abs(res["J"] - Ja) / colmax) <= 1e-4
+        d = np.sqrt(np.outer(np.diag(JtJ), np.diag(JtJ)))
+        d = d + 1e-12 * d.max()
+        assert np.max(np.abs(res["JtJ"] - JtJ) / d) <= 1e-3
+        assert np.max(np.abs(res["Jtr"] - Jtr)) <= 1e-4 * np.max(np.abs(Jtr))
+
+
 def test_pair_jacobian_fp64():
     ds = small_ternary(2, 40, seed=13)
     ds.type[:] = ds.type % 2
