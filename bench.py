@@ -264,7 +264,7 @@ def three_body_leg(local, which, steps=20):
     atoms (sigma = 0.15 A, volumetric strain U[0.95, 1.05]).  Device: FP32
     residuals per second (CUDA events, 20 evaluations), and the FP64
     central-difference Jacobian (the reference's method for these families:
-    2 D + 1 residuals) per second, as the mean of 5 host-timed calls that each
+    2 D + 1 residuals) per second, the median of 5 host-timed calls that each
     end with the normal equations read back.  CPU: the oracle (16 threads, FP64), one
     residual timed, the Jacobian extrapolated as (2 D + 1) residuals."""
     import numpy as np
@@ -314,12 +314,13 @@ def three_body_leg(local, which, steps=20):
     D = g.D
     g.jacobian_async(W_E, W_S)
     g.normal_equations()
-    reps = 5
-    t0 = time.perf_counter()
-    for _ in range(reps):
+    times = []
+    for _ in range(5):
+        t0 = time.perf_counter()
         g.jacobian_async(W_E, W_S)
         g.normal_equations()
-    jac_s = (time.perf_counter() - t0) / reps
+        times.append(time.perf_counter() - t0)
+    jac_s = float(np.median(times))
     g.close()
     threads = set_threads(os.cpu_count() or 1)
     o = Oracle()

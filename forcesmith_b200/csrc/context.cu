@@ -137,6 +137,8 @@ void free_jacobian(fs_gpu *h) {
   h->jtr_part_alloc = 0;
   dfree(h->d_half_part);
   h->half_part_alloc = 0;
+  dfree(h->d_fd_scratch);
+  h->fd_scratch_alloc = 0;
   dfree(h->d_atom_scalars);
   dfree(h->d_drho);
   dfree(h->d_dgd);

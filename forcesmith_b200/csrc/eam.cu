@@ -1362,12 +1362,12 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   const bool eam = h->family == FS_FAMILY_EAM;
   const int64_t M = rows_of(h, w_s);
   const int D = h->D;
-  // J, rows rounded up to 32 (padding rows stay zero).  FP32 with D ≤ 256
-  // (the tensor-core JᵀJ): row-major with the row stride rounded up to 4
+  // J, rows rounded up to 32 (padding rows stay zero).  When the tensor cores
+  // form JᵀJ (FP32, 48 < D ≤ 256): row-major with the row stride rounded up to 4
   // columns (16 bytes, as a TMA stride needs), so that an atom's rows are
   // contiguous and its stores coalesce.  Otherwise column-major with the
   // leading dimension the padded row count.
-  const bool rowmajor = sizeof(T) == 4 && D <= 256;
+  const bool rowmajor = gram_on_tensor_cores(h->precision, D);
   const int64_t rows = (M + 31) / 32 * 32;
   const int64_t ldj = rowmajor ? (D + 3) / 4 * 4 : rows;
   const size_t jn = static_cast<size_t>(rowmajor ? rows * ldj : ldj * D);

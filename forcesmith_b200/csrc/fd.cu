@@ -41,9 +41,14 @@ int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s) {
     FS_CUDA(cudaMalloc(&h->d_JtJ, std::max(D * D, 1) * sizeof(double)));
     FS_CUDA(cudaMalloc(&h->d_Jtr, std::max(D, 1) * sizeof(double)));
   }
-  double *Fbase = nullptr, *Fp = nullptr;
-  FS_CUDA(cudaMallocAsync(&Fbase, M * sizeof(double), h->stream));
-  FS_CUDA(cudaMallocAsync(&Fp, M * sizeof(double), h->stream));
+  // the base residual and F(x + h e_j): scratch kept with the context
+  if (h->fd_scratch_alloc < static_cast<size_t>(2 * M) || !h->d_fd_scratch) {
+    if (h->d_fd_scratch) cudaFree(h->d_fd_scratch);
+    h->d_fd_scratch = nullptr;
+    FS_CUDA(cudaMalloc(&h->d_fd_scratch, 2 * M * sizeof(double)));
+    h->fd_scratch_alloc = static_cast<size_t>(2 * M);
+  }
+  double *Fbase = h->d_fd_scratch, *Fp = h->d_fd_scratch + M;
   FS_CUDA(cudaMemcpyAsync(Fbase, h->d_F, M * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   std::vector<double> x(D), xp;
   FS_TRY(fs_gpu_gather_params(h, x.data()));
@@ -74,8 +79,6 @@ int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s) {
   h->params_dirty = false;
   FS_CUDA(cudaMemcpyAsync(h->d_F, Fbase, M * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   if (rc == FS_OK) rc = launch_jtr<double>(h, static_cast<const double *>(h->d_J), ldj, M, D, h->d_F, h->d_Jtr);
-  cudaFreeAsync(Fbase, h->stream);
-  cudaFreeAsync(Fp, h->stream);
   return rc;
 }
 

@@ -179,6 +179,8 @@ struct fs_gpu {
   size_t jtr_part_alloc = 0;
   double *d_half_part = nullptr; // force-row pass with two CTAs per configuration: their sums
   size_t half_part_alloc = 0;
+  double *d_fd_scratch = nullptr; // central-difference Jacobian: base and perturbed residuals
+  size_t fd_scratch_alloc = 0;
   int32_t *d_err = nullptr;      // device error word (bounded waits that gave up)
   double *d_JtJ = nullptr;       // D × D
   double *d_Jtr = nullptr;       // D
@@ -257,6 +259,13 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s);
 // gram.cu
 int gram(fs_gpu *h, int64_t m, double *JtJ_dev, double *Jtr_dev);
 int gram_tc(fs_gpu *h, int64_t m, double *JtJ_dev); // tcgen05 (FP32 J)
+// JᵀJ paths: D ≤ kGramSmallD a row-slab kernel over the upper triangle;
+// else FP32 with D ≤ 256 the tensor cores (the only reader of a row-major J);
+// else 64 × 64 CUDA-core tiles
+constexpr int kGramSmallD = 48;
+inline bool gram_on_tensor_cores(int precision, int D) {
+  return precision == FS_PREC_FP32 && D > kGramSmallD && D <= 256;
+}
 
 // solve.cu
 int lm_solve(fs_gpu *h, double lambda, int mode, double *dx_host);
