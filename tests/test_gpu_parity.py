@@ -222,6 +222,31 @@ def test_pair_jacobian_fp64():
     _close(res["J"], o.jacobian_analytic(0.7, 0.2), 1e-9, "pair J")
 
 
+@pytest.mark.parametrize("nknots", [48, 49])
+def test_pair_jacobian_fp32_gram_paths(nknots):
+    """D = 48 free knots: column-major J and the small-D JᵀJ kernel; D = 49:
+    row-major J and the tensor-core JᵀJ.  J against the analytic oracle
+    (1e-4·max|J column|); JᵀJ against the returned J in FP64 (1e-5 of
+    √(JᵀJ_aa·JᵀJ_bb)), Jᵀr against the returned J and F (1e-5 of its largest
+    entry)."""
+    model = spline_pair_model(1, nknots)
+    assert model.free_values().size == nknots
+    ds = small_ternary(4, 40, seed=17)
+    ds.type[:] = 0
+    ds = label(ds, model.with_values(model.free_values() * 1.03), O.Oracle, 1.0, 0.2)
+    g, o = _pair(ds, model, "fp32")
+    res = g.jacobian(1.0, 0.2)
+    Ja = o.jacobian_analytic(1.0, 0.2)
+    colmax = np.abs(Ja).max(axis=0) + 1e-30
+    assert np.max(np.abs(res["J"] - Ja) / colmax) <= 1e-4
+    J = np.asarray(res["J"], np.float64)
+    JtJ, Jtr = J.T @ J, J.T @ np.asarray(res["F"], np.float64)
+    d = np.sqrt(np.outer(np.diag(JtJ), np.diag(JtJ)))
+    d = d + 1e-12 * d.max()
+    assert np.max(np.abs(res["JtJ"] - JtJ) / d) <= 1e-5
+    assert np.max(np.abs(res["Jtr"] - Jtr)) <= 1e-5 * np.max(np.abs(Jtr))
+
+
 def test_lm_and_lsq_steps_fp64(ternary_small):
     ds, _, start = ternary_small
     g = _gpu("fp64")
