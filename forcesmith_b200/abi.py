@@ -25,7 +25,7 @@ FS_ERR_NUMERIC = -7
 FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_FAMILY_ANGULAR = 0, 1, 2, 3, 4, 5
 FS_FAMILY_ACSF = 6
 FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA, FS_TABLE_TERSOFF = 0, 1, 2, 3, 4
-FS_TABLE_ACSF, FS_TABLE_LINEAR_HEAD = 5, 6
+FS_TABLE_ACSF, FS_TABLE_LINEAR_HEAD, FS_TABLE_STANDARDIZATION = 5, 6, 7
 TERSOFF_FIELDS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S", "omega")
 FS_PREC_FP32, FS_PREC_FP64 = 0, 1
 
@@ -160,6 +160,14 @@ class Table:
         return Table(FS_TABLE_LINEAR_HEAD, v, 0.0, 0.0, 0, fx)
 
     @staticmethod
+    def standardization(mean, inv_std):
+        """Per-species descriptor standardization {mean[S], inv_std[S]}: the
+        head sees (D − mean) ⊙ inv_std (MLBase, ml_force.hpp:607-623).  Not
+        fitted: every value is fixed."""
+        v = np.concatenate([np.asarray(mean, np.float64), np.asarray(inv_std, np.float64)])
+        return Table(FS_TABLE_STANDARDIZATION, v, 0.0, 0.0, 0, np.ones(v.size, np.uint8))
+
+    @staticmethod
     def lam(values, fixed=None):
         return Table(FS_TABLE_LAMBDA, np.ascontiguousarray(values, dtype=np.float64),
                      fixed=None if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8))
@@ -191,6 +199,15 @@ class Model:
             keep.append(t)
         m = fs_model(self.family, self.ntypes, len(self.tables), 0, arr)
         return m, keep
+
+    def with_standardization(self, mean, inv_std):
+        """An ACSF model with the per-species standardization tables set to
+        mean, inv_std (nt × S), replacing any it had."""
+        assert self.family == FS_FAMILY_ACSF
+        mean, inv_std = np.asarray(mean, np.float64), np.asarray(inv_std, np.float64)
+        tabs = [t.copy() for t in self.tables[:1 + self.ntypes]]
+        tabs += [Table.standardization(mean[t], inv_std[t]) for t in range(self.ntypes)]
+        return Model(self.family, self.ntypes, tabs)
 
     def free_values(self) -> np.ndarray:
         out = []
@@ -293,6 +310,7 @@ class Session:
     def set_model(self, model: Model, prepare=True):
         m, keep = model.to_c()
         self._keep = keep
+        self._model = model
         self._check(self._f("set_model")(self._h, C.byref(m)), "set_model")
         d = C.c_int32()
         self._check(self._f("param_count")(self._h, C.byref(d)), "param_count")
@@ -302,6 +320,19 @@ class Session:
 
     def prepare(self):
         self._check(self._f("prepare")(self._h), "prepare")
+
+    def acsf_standardization(self):
+        """ACSF models: per-species descriptor mean and 1/σ over every uploaded
+        atom, and the atoms per species (MLBase::compute_standardization).
+        Returns (mean nt × S, inv_std nt × S, count nt)."""
+        nt = self._model.ntypes
+        S = acsf_size(self._model.tables[0], nt)
+        mean, inv_std = np.zeros((nt, S)), np.zeros((nt, S))
+        count = np.zeros(nt, np.int64)
+        self._check(self._f("acsf_standardization")(self._h, _dp(mean), _dp(inv_std),
+                                                    count.ctypes.data_as(C.POINTER(C.c_int64))),
+                    "acsf_standardization")
+        return mean, inv_std, count
 
     def num_pairs(self):
         n = C.c_int64()

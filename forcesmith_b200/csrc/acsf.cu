@@ -28,6 +28,8 @@
 #include "kern_common.cuh"
 
 #include <algorithm>
+#include <cmath>
+#include <vector>
 
 namespace fsg {
 namespace {
@@ -94,10 +96,19 @@ template <class T> struct AcArgs {
   int64_t ld;
   int D;   // columns (free head values)
   int smj; // 1: the configuration's J block is summed in shared memory first
+  int std_on;   // 1: standardization tables follow the heads ({mean[S], inv_std[S]} per species)
+  double *desc; // MODE 2: per-atom descriptors [atom][S] (zeroed before)
 };
 
-// One CTA per configuration.  JAC = false: residual; JAC = true: J rows.
-template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_kernel(AcArgs<T> A) {
+// One CTA per configuration.  MODE 0: residual; 1: J rows; 2: each atom's
+// descriptors (for the standardization statistics).
+//
+// Standardized heads (the head sees (D − mean) ⊙ inv_std) act as heads of
+// raw descriptors with w' = w ⊙ inv_std and b' = b − Σ w·inv_std·mean; in the
+// Jacobian, w_k's column is inv_std_k times the raw one, and its energy row
+// also gets −w_e·inv_std_k·mean_k per atom of the species.
+template <class T, int MODE> __global__ void __launch_bounds__(kAcThreads) acsf_kernel(AcArgs<T> A) {
+  constexpr bool JAC = MODE == 1, DESC = MODE == 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int c = A.order ? A.order[blockIdx.x] : blockIdx.x;
   const CfgDev &cd = A.c.cfg[c];
@@ -121,6 +132,9 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
   int *tfirst = S.take<int>(N + 1);
   int *wsum = S.take<int>(32);
   T *cz = S.take<T>(L.n4 + L.n5); // 2^{1−ζ} of each G4, G5 function
+  // JAC with standardization: inv_std per (species, descriptor) and atoms per species
+  T *ivs = (JAC && A.std_on) ? S.take<T>(nt * L.S) : nullptr;
+  int *ntyp = (JAC && A.std_on) ? S.take<int>(nt) : nullptr;
   // JAC with smj: the 3N force rows (local) × D columns
   T *Jb = (JAC && A.smj) ? S.take<T>(static_cast<size_t>(3 * N) * A.D) : nullptr;
   if (Jb)
@@ -131,9 +145,25 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
     cz[k] = static_cast<T>(pow(2.0, 1.0 - zeta));
   }
   for (int k = threadIdx.x; k < nt * (L.S + 1); k += blockDim.x) {
-    const TableDesc &td = A.c.desc[1 + k / (L.S + 1)];
-    W[k] = static_cast<T>(A.vals[td.pv0 + k % (L.S + 1)]);
-    col[k] = A.c.cmap[td.cmap0 + k % (L.S + 1)];
+    const int t = k / (L.S + 1), q = k % (L.S + 1);
+    const TableDesc &td = A.c.desc[1 + t];
+    const double *w = A.vals + td.pv0;
+    double v = w[q];
+    if (A.std_on) { // w ⊙ inv_std; b − Σ w·inv_std·mean
+      const double *st = A.vals + A.c.desc[1 + nt + t].pv0; // mean[S], inv_std[S]
+      if (q < L.S) {
+        v = w[q] * st[L.S + q];
+      } else {
+        for (int u = 0; u < L.S; ++u) v -= w[u] * st[L.S + u] * st[u];
+      }
+    }
+    W[k] = static_cast<T>(v);
+    col[k] = A.c.cmap[td.cmap0 + q];
+  }
+  if (ivs) {
+    for (int k = threadIdx.x; k < nt * L.S; k += blockDim.x)
+      ivs[k] = static_cast<T>(A.vals[A.c.desc[1 + nt + k / L.S].pv0 + L.S + k % L.S]);
+    for (int k = threadIdx.x; k < nt; k += blockDim.x) ntyp[k] = 0;
   }
   for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) Fs[k] = T(0);
   stage_geometry(cd, A.c, wpos, shift, typ);
@@ -199,7 +229,14 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
     bool hi = false;
     const unsigned xi = run_links(i, lane, hi);
     auto term = [&](int idx, T g, T dg) {
-      if constexpr (JAC) {
+      if constexpr (DESC) {
+        if (ok) atomicAdd(&A.desc[(static_cast<int64_t>(cd.atom0) + i) * L.S + idx], static_cast<double>(g));
+      } else if constexpr (JAC) {
+        if (ivs) { // standardized: the column of w_idx scales by inv_std_idx
+          const T sv = ivs[ti * L.S + idx];
+          g *= sv;
+          dg *= sv;
+        }
         // force rows: +g on i, −g on j; stress −sw d ⊗ g
         T gv[3];
 #pragma unroll
@@ -244,7 +281,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
       ac_sincos_full(k * r, ss, cc);
       term(L.base[2] + s * L.n3 + t, cc * fc, -k * ss * fc + cc * fcp);
     }
-    if constexpr (!JAC) {
+    if constexpr (MODE == 0) {
       // atom i's force summed over its run of lanes (rh is zero without a term)
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
@@ -331,12 +368,16 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
           gj[a] = cij * h1[a] - cjk * hjk[a] + ccos * dcj[a];
           gk[a] = cik * h2[a] + cjk * hjk[a] + ccos * dck[a];
         }
-        if constexpr (JAC) {
+        if constexpr (DESC) {
+          if (on) atomicAdd(&A.desc[(static_cast<int64_t>(cd.atom0) + i) * L.S + idx], static_cast<double>(g));
+        } else if constexpr (JAC) {
           // rows: j gets −gj, k gets −gk, i gets gj + gk; stress d1 ⊗ −gj + d2 ⊗ −gk
+          // (standardized: the column of w_idx scales by inv_std_idx)
+          const T sv = ivs ? ivs[ti * L.S + idx] : T(1);
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            gj[a] = on ? gj[a] : T(0);
-            gk[a] = on ? gk[a] : T(0);
+            gj[a] = on ? gj[a] * sv : T(0);
+            gk[a] = on ? gk[a] * sv : T(0);
           }
           const T st[6] = {-sw * (d1[0] * gj[0] + d2[0] * gk[0]), -sw * (d1[1] * gj[1] + d2[1] * gk[1]),
                            -sw * (d1[2] * gj[2] + d2[2] * gk[2]), -sw * (d1[0] * gj[1] + d2[0] * gk[1]),
@@ -360,7 +401,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
               if (hj) jadd(c0, 3 * j + a, -tj);
               if (on) jadd(c0, 3 * k + a, -gk[a]);
             }
-            erows_warp(c0, on ? g : T(0), st);
+            erows_warp(c0, on ? g * sv : T(0), st);
           } else if (on && cc >= 0) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -368,7 +409,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
               jadd(cc, 3 * j + a, -gj[a]);
               jadd(cc, 3 * k + a, -gk[a]);
             }
-            erows_lane(cc, g, st);
+            erows_lane(cc, g * sv, st);
           }
         } else if (on) {
           ew += w_[idx] * g;
@@ -383,7 +424,7 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
         term(L.base[3] + po * L.n4 + t, p4[3 * t], p4[3 * t + 1], p4[3 * t + 2], c4[t], true);
       for (int t = 0; t < L.n5; ++t)
         term(L.base[4] + po * L.n5 + t, p5[3 * t], p5[3 * t + 1], p5[3 * t + 2], c5[t], false);
-      if constexpr (!JAC) {
+      if constexpr (MODE == 0) {
         // atoms i and j summed over their runs of lanes (zeros without a term)
         if (iw) { // one atom i for the warp: halving exchanges (lanes 8a hold component a)
           const T v[4] = {GJ[0] + GK[0], GJ[1] + GK[1], GJ[2] + GK[2], T(0)};
@@ -409,17 +450,29 @@ template <class T, bool JAC> __global__ void __launch_bounds__(kAcThreads) acsf_
         sg[5] -= static_cast<double>(d1[1] * GJ[2] + d2[1] * GK[2]);
       }
     }
+  if constexpr (DESC) return;
   // biases: one per atom
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int ti = typ[i];
     if constexpr (JAC) {
       const int cb = col[ti * (L.S + 1) + L.S];
       if (cb >= 0) jadd(cb, rE, we);
+      if (ntyp) atomicAdd(&ntyp[ti], 1);
     } else {
       e_acc += static_cast<double>(W[ti * (L.S + 1) + L.S]);
     }
   }
   if constexpr (JAC) {
+    if (ivs) { // standardized: ∂E/∂w_k also holds −inv_std_k·mean_k per atom of the species
+      __syncthreads();
+      for (int q = threadIdx.x; q < nt * L.S; q += blockDim.x) {
+        const int t = q / L.S, kk = q % L.S;
+        const int ck = col[t * (L.S + 1) + kk];
+        if (ck < 0 || ntyp[t] == 0) continue;
+        const double mu = A.vals[A.c.desc[1 + nt + t].pv0 + kk];
+        jadd(ck, rE, static_cast<T>(-A.w_e * static_cast<double>(ivs[q]) * mu * ntyp[t]));
+      }
+    }
     if (!Jb) return;
     __syncthreads();
     // the force rows to J (the energy, stress and limit rows are in J already)
@@ -489,10 +542,37 @@ template <class T> size_t ac_smem(const fs_gpu *h, int mi) {
   return align16(nspec * sizeof(T)) + align16(nt * (L.S + 1) * sizeof(T)) + align16(nt * (L.S + 1) * sizeof(int)) +
          align16((L.n4 + L.n5) * sizeof(T)) +
          align16(3 * N * sizeof(double)) + align16(3 * mi * sizeof(double)) + align16(N) + align16(3 * N * sizeof(T)) +
-         align16(8 * 32 * sizeof(double)) + 2 * align16((N + 1) * sizeof(int)) + align16(32 * sizeof(int)) + 160;
+         align16(8 * 32 * sizeof(double)) + 2 * align16((N + 1) * sizeof(int)) + align16(32 * sizeof(int)) +
+         align16(nt * L.S * sizeof(T)) + align16(nt * sizeof(int)) + 192;
 }
 
-template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) {
+// Σ D, Σ D² and the atom count of species q / S for descriptor q % S
+// (CTA q), in FP64 and a fixed order; out = [Σ D | Σ D² | count] × (nt·S)
+__global__ void ac_desc_stats(const double *__restrict__ Dsc, const int32_t *__restrict__ type, int64_t n_atoms,
+                              int S, double *__restrict__ out) {
+  __shared__ double r[32];
+  const int q = blockIdx.x, t = q / S, k = q % S;
+  double s1 = 0.0, s2 = 0.0, n = 0.0;
+  for (int64_t i = threadIdx.x; i < n_atoms; i += blockDim.x)
+    if (type[i] == t) {
+      const double v = Dsc[i * S + k];
+      s1 += v;
+      s2 += v * v;
+      n += 1.0;
+    }
+  s1 = block_sum(s1, r);
+  s2 = block_sum(s2, r);
+  n = block_sum(n, r);
+  if (threadIdx.x == 0) {
+    out[q] = s1;
+    out[gridDim.x + q] = s2;
+    out[2 * gridDim.x + q] = n;
+  }
+}
+
+// mode 0: residual; 1: Jacobian rows (+ Jᵀr); 2: descriptors into desc
+template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, int mode, double *desc = nullptr) {
+  const bool jac = mode == 1;
   AcArgs<T> a;
   a.c.cfg = h->d_cfg;
   a.c.wpos = h->d_wpos;
@@ -521,6 +601,8 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
   a.ld = 0;
   a.D = h->D;
   a.smj = 0;
+  a.std_on = static_cast<int>(h->tables.size()) == 1 + 2 * h->ntypes ? 1 : 0;
+  a.desc = desc;
   int mi = 1;
   for (const CfgDev &cd : h->cfg_host) mi = std::max(mi, (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1));
   size_t sm = ac_smem<T>(h, mi);
@@ -552,11 +634,12 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
       sm += jb;
     }
   }
-  auto k = jac ? acsf_kernel<T, true> : acsf_kernel<T, false>;
+  auto k = mode == 1 ? acsf_kernel<T, 1> : mode == 2 ? acsf_kernel<T, 2> : acsf_kernel<T, 0>;
   FS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
   k<<<h->n_cfg, kAcThreads, sm, h->stream>>>(a);
   FS_CUDA(cudaGetLastError());
   ++h->launches;
+  if (mode == 2) return FS_OK;
   if (jac) {
     if (D > 0) {
       FS_TRY(launch_jtr<T>(h, static_cast<const T *>(h->d_J), h->ldj, M, D, h->d_F, h->d_Jtr));
@@ -572,10 +655,68 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, bool jac) 
 } // namespace
 
 int eval_residual_acsf(fs_gpu *h, double w_e, double w_s) {
-  return h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, w_e, w_s, false) : launch_acsf<float>(h, w_e, w_s, false);
+  return h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, w_e, w_s, 0) : launch_acsf<float>(h, w_e, w_s, 0);
 }
 int eval_jacobian_acsf(fs_gpu *h, double w_e, double w_s) {
-  return h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, w_e, w_s, true) : launch_acsf<float>(h, w_e, w_s, true);
+  return h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, w_e, w_s, 1) : launch_acsf<float>(h, w_e, w_s, 1);
+}
+
+// Per-species descriptor statistics (MLBase::compute_standardization,
+// ml_force.hpp:644-688): the descriptors of every atom (formed in the context
+// precision, summed in FP64), then Σ D and Σ D² per (species, descriptor).
+int acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *count) {
+  AcLayout L;
+  L.init(h->tables[0].v.data(), h->ntypes);
+  const int nt = h->ntypes, S = L.S;
+  const int64_t na = h->n_atoms;
+  double *d_desc = nullptr, *d_out = nullptr;
+  FS_CUDA(cudaMalloc(&d_desc, std::max<int64_t>(na * S, 1) * sizeof(double)));
+  if (cudaMalloc(&d_out, std::max(3 * nt * S, 1) * sizeof(double)) != cudaSuccess) {
+    cudaFree(d_desc);
+    return set_error(h, FS_ERR_NOMEM, "cudaMalloc (ACSF statistics)");
+  }
+  int rc = FS_OK;
+  std::vector<double> out(static_cast<size_t>(3) * nt * S);
+  do {
+    if (cudaMemsetAsync(d_desc, 0, std::max<int64_t>(na * S, 1) * sizeof(double), h->stream) != cudaSuccess) {
+      rc = set_error(h, FS_ERR_CUDA, "cudaMemsetAsync");
+      break;
+    }
+    rc = h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, 1.0, 0.0, 2, d_desc)
+                                      : launch_acsf<float>(h, 1.0, 0.0, 2, d_desc);
+    if (rc != FS_OK) break;
+    if (nt * S > 0) {
+      ac_desc_stats<<<nt * S, 256, 0, h->stream>>>(d_desc, h->d_type, na, S, d_out);
+      ++h->launches;
+      if (cudaGetLastError() != cudaSuccess ||
+          cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        rc = set_error(h, FS_ERR_CUDA, "ACSF statistics");
+        break;
+      }
+    }
+  } while (false);
+  cudaFree(d_desc);
+  cudaFree(d_out);
+  if (rc != FS_OK) return rc;
+  // mean = Σ D / n, σ² = Σ D² / n − mean², inv_std = σ² > 1e-12 ? 1/σ : 0; no atoms: identity
+  for (int t = 0; t < nt; ++t) {
+    const double n = nt * S > 0 ? out[2 * nt * S + t * S] : 0.0;
+    count[t] = static_cast<int64_t>(n);
+    for (int k = 0; k < S; ++k) {
+      const size_t q = static_cast<size_t>(t) * S + k;
+      if (n == 0.0) {
+        mean[q] = 0.0;
+        inv_std[q] = 1.0;
+        continue;
+      }
+      const double mu = out[q] / n, var = out[nt * S + q] / n - mu * mu;
+      mean[q] = mu;
+      inv_std[q] = var > 1e-12 ? 1.0 / std::sqrt(var) : 0.0;
+    }
+  }
+  return FS_OK;
 }
 
 } // namespace fsg

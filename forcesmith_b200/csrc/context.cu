@@ -366,7 +366,9 @@ int fs_gpu_set_references(fs_gpu *h, const double *ref_force, const double *ref_
 int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
   if (!h || !m) return FS_ERR_ARG;
   if (m->ntypes < 1 || m->ntypes > 16) return set_error(h, FS_ERR_ARG, "set_model: ntypes out of range");
-  if (expected_tables(m->family, m->ntypes) != m->n_tables || !m->tables)
+  // ACSF models may carry standardization tables after the heads
+  const bool acsf_std = m->family == FS_FAMILY_ACSF && m->n_tables == 1 + 2 * m->ntypes;
+  if ((expected_tables(m->family, m->ntypes) != m->n_tables && !acsf_std) || !m->tables)
     return set_error(h, FS_ERR_ARG, "set_model: table count does not match the family");
   const int np = npair_of(m->ntypes);
   std::vector<HostTable> tabs(m->n_tables);
@@ -383,7 +385,8 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
     const bool sw_fam = m->family == FS_FAMILY_SW;
     if (m->family == FS_FAMILY_ACSF) {
       // the descriptor table {rcut, nG1..nG5, parameters}, then one linear head
-      // {w[S], b} per species
+      // {w[S], b} per species, then optionally one standardization
+      // {mean[S], inv_std[S]} per species, all fixed
       const fs_table &spec = m->tables[0];
       bool ok = spec.kind == FS_TABLE_ACSF && spec.n >= 6 && spec.values[0] > 0.0;
       int need = 6;
@@ -398,10 +401,17 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
         const int nt = m->ntypes, P = nt * (nt + 1) / 2;
         const int S = nt * static_cast<int>(spec.values[1] + spec.values[2] + spec.values[3]) +
                       P * static_cast<int>(spec.values[4] + spec.values[5]);
-        if (ft.kind != FS_TABLE_LINEAR_HEAD || ft.n != S + 1)
+        if (t <= nt && (ft.kind != FS_TABLE_LINEAR_HEAD || ft.n != S + 1))
           return set_error(h, FS_ERR_ARG, "set_model: ACSF heads are linear_head[nt] with S + 1 values");
+        if (t > nt) {
+          bool fixed = ft.fixed != nullptr;
+          for (int k = 0; fixed && k < ft.n; ++k) fixed = ft.fixed[k] != 0;
+          if (ft.kind != FS_TABLE_STANDARDIZATION || ft.n != 2 * S || !fixed)
+            return set_error(h, FS_ERR_ARG,
+                             "set_model: ACSF standardization tables hold {mean[S], inv_std[S]}, all fixed");
+        }
       }
-    } else if (ft.kind == FS_TABLE_ACSF || ft.kind == FS_TABLE_LINEAR_HEAD) {
+    } else if (ft.kind == FS_TABLE_ACSF || ft.kind == FS_TABLE_LINEAR_HEAD || ft.kind == FS_TABLE_STANDARDIZATION) {
       return set_error(h, FS_ERR_ARG, "set_model: ACSF tables belong to the ACSF family");
     } else if (m->family == FS_FAMILY_TERSOFF) {
       if (ft.kind != FS_TABLE_TERSOFF || ft.n != 12)
@@ -682,6 +692,14 @@ int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F, double *J
     }
   }
   return fs_gpu_fetch_normal_equations(h, JtJ, Jtr, obj);
+}
+
+int fs_gpu_acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *count) {
+  if (!h || !mean || !inv_std || !count) return FS_ERR_ARG;
+  FS_TRY(check_ready(h));
+  if (h->family != FS_FAMILY_ACSF) return set_error(h, FS_ERR_STATE, "acsf_standardization: not an ACSF model");
+  cudaSetDevice(h->device);
+  return acsf_standardization(h, mean, inv_std, count);
 }
 
 int fs_gpu_copy_normal_equations(fs_gpu *h, void *dst) {

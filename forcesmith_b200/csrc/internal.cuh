@@ -257,6 +257,8 @@ int eval_residual(fs_gpu *h, double w_e, double w_s);
 int eval_jacobian(fs_gpu *h, double w_e, double w_s);
 
 // gram.cu
+// ACSF: per-species descriptor mean and 1/σ over the uploaded atoms (acsf.cu)
+int acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *count);
 int gram(fs_gpu *h, int64_t m, double *JtJ_dev, double *Jtr_dev);
 int gram_tc(fs_gpu *h, int64_t m, double *JtJ_dev); // tcgen05 (FP32 J)
 // JᵀJ paths: D ≤ kGramSmallD a row-slab kernel over the upper triangle;

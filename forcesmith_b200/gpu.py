@@ -51,6 +51,7 @@ def lib() -> C.CDLL:
         L.fs_gpu_fetch_normal_equations.argtypes = [vp, pd, pd, pd]
         L.fs_gpu_lm_step.argtypes = [vp, dbl, i32, pd]
         L.fs_gpu_lsq_step.argtypes = [vp, dbl, pd]
+        L.fs_gpu_acsf_standardization.argtypes = [vp, pd, pd, C.POINTER(C.c_int64)]
         L.fs_gpu_eval_population.argtypes = [vp, dbl, dbl, pd, i32, pd]
         L.fs_gpu_de_init.argtypes = [vp, C.POINTER(fs_de_opts), pd, pd, pd]
         L.fs_gpu_de_run.argtypes = [vp, i32, i32, pd, pd, pd]

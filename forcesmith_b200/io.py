@@ -317,8 +317,6 @@ def _read_ml(j):
         raise FormatError("ml: missing 'descriptor' object with a string 'type'")
     if desc["type"] not in ("acsf", "symmetry_functions"):
         raise FormatError(f"ml: descriptor '{desc['type']}' is not supported by this build (acsf only)")
-    if "standardization" in j:
-        raise FormatError("ml: feature standardization is not supported by this build")
     g1 = desc.get("g1", 0)
     g1 = len(g1) if isinstance(g1, list) else int(g1) if isinstance(g1, (int, float)) else 0
     g2 = [(float(g["eta"]), float(g.get("rs", 0.0))) for g in desc.get("g2", [])]
@@ -343,7 +341,22 @@ def _read_ml(j):
         fixed[:S] = 1 if h.get("fixed", False) else 0
         fixed[S] = 1 if h.get("bias_fixed", True) else 0
         tabs.append(Table.linear_head(co, float(h.get("bias", 0.0)), fixed=fixed))
-    return Model(FS_FAMILY_ACSF, nt, tabs)
+    model = Model(FS_FAMILY_ACSF, nt, tabs)
+    if "standardization" in j:
+        # finish_ml (force_model_reader.cpp:261-281): one {mean, inv_std} per
+        # species, empty for a species without training atoms (identity here)
+        st = j["standardization"]
+        if not isinstance(st, list) or len(st) != nt:
+            raise FormatError(f"ml: standardization must be an array of {nt} entries")
+        mean, inv_std = np.zeros((nt, S)), np.ones((nt, S))
+        for t, e in enumerate(st):
+            mu, iv = e.get("mean", []), e.get("inv_std", [])
+            if len(mu) != len(iv) or (mu and len(mu) != S):
+                raise FormatError(f"ml: standardization mean/inv_std length {len(mu)} != descriptor size {S}")
+            if mu:
+                mean[t], inv_std[t] = mu, iv
+        model = model.with_standardization(mean, inv_std)
+    return model
 
 
 def _write_ml(model):
@@ -356,12 +369,18 @@ def _write_ml(model):
     g5 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n5)]
     desc = {"type": "acsf", "rcut": float(v[0]), "g1": g1, "g2": g2, "g3": g3, "g4": g4, "g5": g5}
     heads = []
-    for t in model.tables[1:]:
+    for t in model.tables[1:1 + model.ntypes]:
         fx = np.zeros(t.values.size, np.uint8) if t.fixed is None else t.fixed
         heads.append({"type": "linear", "coeffs": [float(x) for x in t.values[:-1]],
                       "fixed": bool(np.all(fx[:-1])) if t.values.size > 1 else False,
                       "bias": float(t.values[-1]), "bias_fixed": bool(fx[-1])})
-    return json.dumps({"model": "ml", "ntypes": model.ntypes, "descriptor": desc, "heads": heads}, indent=1)
+    out = {"model": "ml", "ntypes": model.ntypes, "descriptor": desc, "heads": heads}
+    if len(model.tables) == 1 + 2 * model.ntypes:  # add_standardization (output_writer.cpp:155-168)
+        S = acsf_size(model.tables[0], model.ntypes)
+        out["standardization"] = [{"mean": [float(x) for x in t.values[:S]],
+                                   "inv_std": [float(x) for x in t.values[S:]]}
+                                  for t in model.tables[1 + model.ntypes:]]
+    return json.dumps(out, indent=1)
 
 
 def _tersoff_json(t):

@@ -87,7 +87,9 @@ enum fs_family {
                             spline or analytic (angular_force.hpp:15-33)   */
   FS_FAMILY_ACSF = 6     /* tables: acsf[1] (descriptor), head[nt] (linear
                             energy head per species) (acsf.hpp:48-86,
-                            ml_force.hpp LinearHead)                       */
+                            ml_force.hpp LinearHead), and optionally
+                            standardization[nt] (MLBase mean_ / inv_std_,
+                            ml_force.hpp:194-199)                          */
 };
 
 enum fs_table_kind {
@@ -104,8 +106,12 @@ enum fs_table_kind {
                              (eta, zeta, lambda) × nG4, (eta, zeta, lambda) × nG5};
                             descriptor size S = nt(nG1 + nG2 + nG3)
                             + npair(nG4 + nG5) (AcsfLayout, acsf.hpp:23-33) */
-  FS_TABLE_LINEAR_HEAD = 6 /* E_i = w·D_i + b: {w[S], b}, n == S + 1; the
+  FS_TABLE_LINEAR_HEAD = 6, /* E_i = w·D_i + b: {w[S], b}, n == S + 1; the
                             bias is fixed unless `fixed` says otherwise    */
+  FS_TABLE_STANDARDIZATION = 7 /* per species, all values fixed: {mean[S],
+                            inv_std[S]}, n == 2S; the head then sees
+                            (D − mean) ⊙ inv_std (ml_force.hpp:607-623);
+                            mean 0 and inv_std 1 leave D unchanged        */
 };
 
 /* Analytic radial forms (include/forcesmith/potentials/analytic_potential.hpp). */
@@ -230,6 +236,15 @@ int fs_gpu_lm_step(fs_gpu *h, double lambda, int32_t mode, double *dx);
 /* NormalEquationsSolver step: λ = ridge > 0 ? ridge : 1e-8·max(mean diag,1);
  * dx = −(JᵀJ + λI)⁻¹ Jᵀr. */
 int fs_gpu_lsq_step(fs_gpu *h, double ridge, double *dx);
+
+/* ACSF models: per-species descriptor mean and 1/σ over every atom of the
+ * uploaded configurations (MLBase::compute_standardization,
+ * ml_force.hpp:644-688): σ² = E[D²] − E[D]², inv_std = σ² > 1e-12 ? 1/σ : 0.
+ * mean, inv_std: nt × S (species-major); count: atoms per species (nt).
+ * Descriptors are formed in the context precision, sums in FP64.  A model
+ * with standardization tables is standardized by them; these statistics are
+ * what such tables hold after the reference's prepare(). */
+int fs_gpu_acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *count);
 
 /* Copies [JᵀJ (D·D), Jᵀr (D), ‖F‖² (1)] as FP64 into a caller-owned DEVICE
  * buffer, ordered on the context stream (for a collective over ranks). */

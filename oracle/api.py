@@ -58,6 +58,8 @@ def lib():
         L.orc_residual_count.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_int64)]
         L.orc_eval.argtypes = [C.c_void_p, C.c_double, C.c_double] + [C.POINTER(C.c_double)] * 6
         L.orc_set_params.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int32]
+        L.orc_acsf_standardization.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                               C.POINTER(C.c_int64)]
     return _LIB
 
 

@@ -843,11 +843,30 @@ inline void acsf_fc(double r, double rc, double &fc, double &fcp) {
   fcp = -0.5 * kPi / rc * std::sin(x);
 }
 
+// Per-species effective head {w ⊙ inv_std, b − Σ w·inv_std·mean}: the linear
+// head of standardized descriptors (D − mean) ⊙ inv_std (ml_force.hpp:607-623)
+// as a head of raw descriptors; without standardization tables, the head.
+std::vector<double> acsf_head(const State &S, int t, int Sz) {
+  const std::vector<double> &w = S.tables[1 + t].v;
+  if (static_cast<int>(S.tables.size()) != 1 + 2 * S.ntypes) return w;
+  const std::vector<double> &st = S.tables[1 + S.ntypes + t].v; // mean[S], inv_std[S]
+  std::vector<double> h(Sz + 1);
+  double b = w[Sz];
+  for (int k = 0; k < Sz; ++k) {
+    h[k] = w[k] * st[Sz + k];
+    b -= h[k] * st[k];
+  }
+  h[Sz] = b;
+  return h;
+}
+
 void eval_acsf(const State &S, int c, Out &o) {
   const Config &cf = S.cfgs[c];
   const int nt = S.ntypes;
   const AcsfSpec A(S.tables[0].v.data());
   const int Sz = acsf_size(A, nt);
+  std::vector<std::vector<double>> heads(nt);
+  for (int t = 0; t < nt; ++t) heads[t] = acsf_head(S, t, Sz);
   struct Nb {
     int64_t p; // the entry in the atom's neighbour list
     Vec3 d, rh;
@@ -857,7 +876,7 @@ void eval_acsf(const State &S, int c, Out &o) {
   for (int i = 0; i < cf.natoms; ++i) {
     const int64_t gi = cf.atom0 + i;
     const int ti = S.type[gi];
-    const double *w = S.tables[1 + ti].v.data();
+    const double *w = heads[ti].data();
     const int64_t s0 = S.nb_start[gi], s1 = S.nb_start[gi + 1];
     std::vector<Nb> nb; // collect_neighbors (acsf.cpp:84-99): 1e-14 ≤ r < rcut
     for (int64_t p = s0; p < s1; ++p) {
@@ -940,6 +959,59 @@ void eval_acsf(const State &S, int c, Out &o) {
         for (int bb = 0; bb < 3; ++bb) o.stress[a][bb] += S.nb_d[p][a] * fj[bb];
     }
   }
+}
+
+// Descriptor values of atom i of configuration c (ACSF::get_descriptor,
+// acsf.cpp:84-196, values only) into D[Sz].
+void acsf_values_of(const State &S, int c, int i, double *D) {
+  const Config &cf = S.cfgs[c];
+  const int nt = S.ntypes;
+  const AcsfSpec A(S.tables[0].v.data());
+  const int Sz = acsf_size(A, nt);
+  std::fill(D, D + Sz, 0.0);
+  const int64_t gi = cf.atom0 + i;
+  struct Nb {
+    Vec3 d;
+    double r, fc;
+    int s;
+  };
+  std::vector<Nb> nb;
+  for (int64_t p = S.nb_start[gi]; p < S.nb_start[gi + 1]; ++p) {
+    const Vec3 &d = S.nb_d[p];
+    const double r = norm(d);
+    if (r < 1e-14 || r >= A.rcut) continue;
+    double fc, fcp;
+    acsf_fc(r, A.rcut, fc, fcp);
+    nb.push_back({d, r, fc, S.type[cf.atom0 + S.nb_j[p]]});
+  }
+  for (const Nb &n : nb) {
+    for (int t = 0; t < A.g1; ++t) D[A.index(0, n.s, t, nt)] += n.fc;
+    for (int t = 0; t < A.n2; ++t) {
+      const double dr = n.r - A.p2[2 * t + 1];
+      D[A.index(1, n.s, t, nt)] += std::exp(-A.p2[2 * t] * dr * dr) * n.fc;
+    }
+    for (int t = 0; t < A.n3; ++t) D[A.index(2, n.s, t, nt)] += std::cos(A.p3[t] * n.r) * n.fc;
+  }
+  for (size_t a = 0; a < nb.size(); ++a)
+    for (size_t b = a + 1; b < nb.size(); ++b) {
+      const Nb &J = nb[a], &K = nb[b];
+      const double costh = std::clamp(dot(J.d, K.d) / (J.r * K.r), -1.0, 1.0);
+      const double rjk = norm(K.d - J.d);
+      double fcjk, fcpjk;
+      acsf_fc(rjk, A.rcut, fcjk, fcpjk);
+      const int po = pair_ordinal(J.s, K.s, nt);
+      auto g = [&](double eta, double zeta, double lambda, bool with_jk) {
+        const double Aa = 1.0 + lambda * costh;
+        if (Aa <= 1e-12) return 0.0;
+        const double rsum = J.r * J.r + K.r * K.r + (with_jk ? rjk * rjk : 0.0);
+        return std::pow(2.0, 1.0 - zeta) * std::pow(Aa, zeta) * std::exp(-eta * rsum) * J.fc * K.fc *
+               (with_jk ? fcjk : 1.0);
+      };
+      for (int t = 0; t < A.n4; ++t)
+        D[A.index(3, po, t, nt)] += g(A.p4[3 * t], A.p4[3 * t + 1], A.p4[3 * t + 2], true);
+      for (int t = 0; t < A.n5; ++t)
+        D[A.index(4, po, t, nt)] += g(A.p5[3 * t], A.p5[3 * t + 1], A.p5[3 * t + 2], false);
+    }
 }
 
 // with_eval_scope (include/forcesmith/force/eval_scope.hpp:13-31): zero,
@@ -1302,7 +1374,8 @@ int orc_set_references(orc_state *h, const double *ref_force, const double *ref_
 
 int orc_set_model(orc_state *h, const fs_model *m) {
   if (!h || !m || m->ntypes < 1) return FS_ERR_ARG;
-  if (expected_tables(m->family, m->ntypes) != m->n_tables) return FS_ERR_ARG;
+  const bool acsf_std = m->family == FS_FAMILY_ACSF && m->n_tables == 1 + 2 * m->ntypes;
+  if (expected_tables(m->family, m->ntypes) != m->n_tables && !acsf_std) return FS_ERR_ARG;
   State &S = h->S;
   S.family = m->family;
   S.ntypes = m->ntypes;
@@ -1314,10 +1387,16 @@ int orc_set_model(orc_state *h, const fs_model *m) {
     if (ft.kind == FS_TABLE_ANALYTIC && form_nparams(ft.form) != ft.n) return FS_ERR_ARG;
     if ((m->family == FS_FAMILY_TERSOFF) != (ft.kind == FS_TABLE_TERSOFF)) return FS_ERR_ARG;
     if (m->family == FS_FAMILY_ACSF) {
-      const int want = t == 0 ? FS_TABLE_ACSF : FS_TABLE_LINEAR_HEAD;
+      const int want = t == 0 ? FS_TABLE_ACSF : t <= m->ntypes ? FS_TABLE_LINEAR_HEAD : FS_TABLE_STANDARDIZATION;
       if (ft.kind != want) return FS_ERR_ARG;
       if (t == 0 && acsf_values(ft.values, ft.n) != ft.n) return FS_ERR_ARG;
-      if (t > 0 && ft.n != acsf_size(AcsfSpec(m->tables[0].values), m->ntypes) + 1) return FS_ERR_ARG;
+      const int Sz = t > 0 ? acsf_size(AcsfSpec(m->tables[0].values), m->ntypes) : 0;
+      if (t > 0 && t <= m->ntypes && ft.n != Sz + 1) return FS_ERR_ARG;
+      if (t > m->ntypes) { // standardization: 2S values, none of them free
+        if (ft.n != 2 * Sz) return FS_ERR_ARG;
+        for (int k = 0; k < ft.n; ++k)
+          if (!ft.fixed || !ft.fixed[k]) return FS_ERR_ARG;
+      }
     }
     if (ft.kind == FS_TABLE_TERSOFF && ft.n != 12) return FS_ERR_ARG;
     S.tables[t].init(ft);
@@ -1506,6 +1585,43 @@ int orc_eval_population(orc_state *h, double w_e, double w_s, const double *xs, 
 }
 
 // JᵀJ and Jᵀr from a column-major J (FP64).
+int orc_acsf_standardization(orc_state *h, double *mean, double *inv_std, int64_t *count) {
+  if (!h || !mean || !inv_std || !count) return FS_ERR_ARG;
+  State &S = h->S;
+  if (!S.have_model || S.family != FS_FAMILY_ACSF || S.rcut_built < 0) return FS_ERR_STATE;
+  const int nt = S.ntypes;
+  const int Sz = acsf_size(AcsfSpec(S.tables[0].v.data()), nt);
+  // MLBase::compute_standardization (ml_force.hpp:644-688), atoms in order
+  std::vector<double> sum(static_cast<size_t>(nt) * Sz, 0.0), sq(sum.size(), 0.0), D(Sz);
+  std::vector<int64_t> n(nt, 0);
+  for (int c = 0; c < static_cast<int>(S.cfgs.size()); ++c)
+    for (int i = 0; i < S.cfgs[c].natoms; ++i) {
+      acsf_values_of(S, c, i, D.data());
+      const int t = S.type[S.cfgs[c].atom0 + i];
+      for (int k = 0; k < Sz; ++k) {
+        sum[static_cast<size_t>(t) * Sz + k] += D[k];
+        sq[static_cast<size_t>(t) * Sz + k] += D[k] * D[k];
+      }
+      ++n[t];
+    }
+  for (int t = 0; t < nt; ++t) {
+    count[t] = n[t];
+    for (int k = 0; k < Sz; ++k) {
+      const size_t q = static_cast<size_t>(t) * Sz + k;
+      if (n[t] == 0) {
+        mean[q] = 0.0;
+        inv_std[q] = 1.0;
+        continue;
+      }
+      const double mu = sum[q] / static_cast<double>(n[t]);
+      const double var = sq[q] / static_cast<double>(n[t]) - mu * mu;
+      mean[q] = mu;
+      inv_std[q] = var > 1e-12 ? 1.0 / std::sqrt(var) : 0.0;
+    }
+  }
+  return FS_OK;
+}
+
 int orc_normal_equations(const double *J, const double *F, int64_t m, int32_t D, double *JtJ,
                          double *Jtr) {
   if (!J || !F) return FS_ERR_ARG;

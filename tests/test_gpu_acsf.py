@@ -106,3 +106,58 @@ def test_acsf_lsq_step_recovers_labels(case):
     g.set_params(g.gather_params() + dx)
     after = g.eval(1.0, 0.2, want=("obj",))["obj"]
     assert after <= 1e-8 * before, (before, after)
+
+
+# ---- feature standardization (MLBase, ml_force.hpp:607-688)
+
+def test_acsf_standardization_statistics(case):
+    """Per-species descriptor mean and 1/σ over every atom against the oracle:
+    FP64 1e-10 relative, FP32 descriptors 1e-5 relative (mean) and 1e-4
+    (1/σ) (sums in FP64)."""
+    ds, start = case
+    for precision, tol in (("fp64", 1e-10), ("fp32", 1e-5)):
+        g, o = _pair(ds, start, precision)
+        mg, ig, cg = g.acsf_standardization()
+        mo, io_, co = o.acsf_standardization()
+        assert cg.tolist() == co.tolist()
+        np.testing.assert_allclose(mg, mo, rtol=tol, atol=tol * np.abs(mo).max())
+        np.testing.assert_allclose(ig, io_, rtol=tol * 10, atol=0)
+
+
+def _standardized(ds, start):
+    o = O.Oracle()
+    o.upload(ds)
+    o.set_model(start)
+    mean, inv_std, _ = o.acsf_standardization()
+    return start.with_standardization(mean, inv_std)
+
+
+def test_acsf_standardized_residual(case):
+    """With standardization tables: FP64 forces, energy, stress, F rows
+    1e-9·(1 + |x|); FP32 forces 2e-5·max|F|, objective 1e-4."""
+    ds, start = case
+    m = _standardized(ds, start)
+    g, o = _pair(ds, m, "fp64")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    for key in ("forces", "energy", "stress", "F"):
+        _close(rg[key], ro[key], 1e-9, key)
+    g, o = _pair(ds, m, "fp32")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    assert np.max(np.abs(rg["forces"] - ro["forces"])) <= 2e-5 * np.max(np.abs(ro["forces"]))
+    assert abs(rg["obj"] - ro["obj"]) <= 1e-4 * ro["obj"]
+
+
+@pytest.mark.parametrize("precision,rel,floor", [("fp64", 1e-6, 1e-9), ("fp32", 1e-4, 0.0)])
+def test_acsf_standardized_jacobian(case, precision, rel, floor):
+    """The exact Jacobian of a standardized head (columns of w scaled by
+    inv_std, energy rows shifted by −inv_std·mean per atom) against the
+    oracle's central differences, with the bars of test_acsf_jacobian."""
+    ds, start = case
+    m = _standardized(ds, start)
+    g, o = _pair(ds, m, precision)
+    res = g.jacobian(1.0, 0.2)
+    Jf = o.jacobian_fd(1.0, 0.2)
+    bar = rel * np.abs(Jf).max(axis=0) + floor + 1e-30
+    ratio = np.abs(res["J"] - Jf) / bar
+    r, c = np.unravel_index(np.argmax(ratio), ratio.shape)
+    assert ratio.max() <= 1.0, (ratio.max(), r, c, res["J"][r, c], Jf[r, c])

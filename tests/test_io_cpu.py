@@ -166,3 +166,22 @@ def test_read_setfl_matches_fixture_pin():
     o.set_model(model)
     e = o.eval(1.0, 0.0, want=("energy",))["energy"][0] / ideal.n_atoms
     assert abs(e + 3.36) < 1e-5
+
+
+def test_ml_standardization_round_trip():
+    """finish_ml / add_standardization (force_model_reader.cpp:261-281,
+    output_writer.cpp:155-168): one {mean, inv_std} per species; an empty
+    entry (a species without training atoms) reads as the identity."""
+    from forcesmith_b200.abi import FS_TABLE_STANDARDIZATION
+    j = {"model": "ml", "ntypes": 2,
+         "descriptor": {"type": "acsf", "rcut": 5.0, "g2": [{"eta": 0.5, "rs": 1.0}]},
+         "heads": [{"coeffs": [0.1, 0.2], "bias": -3.0}, {"coeffs": [0.3, 0.4], "bias": -2.0}],
+         "standardization": [{"mean": [0.5, 0.25], "inv_std": [2.0, 0.0]}, {"mean": [], "inv_std": []}]}
+    m = io.read_model(json.dumps(j))
+    assert len(m.tables) == 5 and m.tables[3].kind == FS_TABLE_STANDARDIZATION
+    assert m.tables[3].values.tolist() == [0.5, 0.25, 2.0, 0.0] and m.tables[4].values.tolist() == [0, 0, 1, 1]
+    assert np.all(m.tables[3].fixed == 1)
+    back = io.read_model(io.write_model(m))
+    _tables_equal(back, m)
+    with pytest.raises(io.FormatError):
+        io.read_model(json.dumps(dict(j, standardization=j["standardization"][:1])))

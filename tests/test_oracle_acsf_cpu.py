@@ -88,3 +88,82 @@ def test_beyond_cutoff_zero_and_species_channels():
     a = run(ENV, spec, [1.0, 0.0], nt=2, types=[0, 0, 0, 0])
     b = run(ENV, spec, [1.0, 5.0], nt=2, types=[0, 0, 0, 0])
     assert abs(a["energy"][0] - b["energy"][0]) <= 1e-14
+
+
+# ---- feature standardization (MLBase::compute_standardization and
+# standardize_in_place, ml_force.hpp:607-688), on the environment of the
+# reference's ML_Standardization_RoundTrips test (test_force_model_reader.cpp)
+STD_G2 = [(0.5, 0.0), (1.2, 1.5), (0.3, 2.5)]
+
+
+def _hand_descriptors(pos, g2, rc=6.0):
+    p = np.asarray(pos, np.float64)
+    D = np.zeros((len(p), len(g2)))
+    for i in range(len(p)):
+        r = np.linalg.norm(np.delete(p, i, 0) - p[i], axis=1)
+        for k, (eta, rs) in enumerate(g2):
+            D[i, k] = np.sum(np.exp(-eta * (r - rs) ** 2) * fc(r, rc))
+    return D
+
+
+def _std_model(w, b, mean, inv_std):
+    spec = Table.acsf(6.0, g2=STD_G2)
+    return Model(FS_FAMILY_ACSF, 1, [spec, Table.linear_head(w, b)]).with_standardization([mean], [inv_std])
+
+
+def test_standardization_statistics_and_energy():
+    """mean and 1/σ per descriptor over the four atoms against numpy on hand
+    descriptors (1e-12); the standardized head's energy
+    Σ_i b + w·(D_i − mean) ⊙ inv_std by hand (1e-12)."""
+    spec = Table.acsf(6.0, g2=STD_G2)
+    w, b = np.array([0.7, -0.4, 0.25]), 0.1
+    o = O.Oracle()
+    o.upload(cluster(ENV, 100.0))
+    o.set_model(Model(FS_FAMILY_ACSF, 1, [spec, Table.linear_head(w, b)]))
+    mean, inv_std, count = o.acsf_standardization()
+    D = _hand_descriptors(ENV, STD_G2)
+    mu, var = D.mean(axis=0), (D ** 2).mean(axis=0) - D.mean(axis=0) ** 2
+    assert count.tolist() == [4]
+    np.testing.assert_allclose(mean[0], mu, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(inv_std[0], 1.0 / np.sqrt(var), rtol=1e-10, atol=0)
+    o.set_model(_std_model(w, b, mean[0], inv_std[0]))
+    e = o.eval(1.0, 0.0)["energy"][0]
+    e_hand = np.sum(b + ((D - mean[0]) * inv_std[0]) @ w)
+    assert abs(e - e_hand) <= 1e-12 * (1 + abs(e_hand))
+
+
+def test_standardized_forces_match_energy_fd():
+    """Forces of the standardized model against central differences of its
+    energy (h = 1e-6, |Δ| ≤ 1e-7), and the same forces and energy as the
+    unstandardized head w ⊙ inv_std, b − Σ w·inv_std·mean (1e-13, 1e-12)."""
+    w, b = np.array([0.7, -0.4, 0.25]), 0.1
+    mean, inv_std = np.array([0.3, 0.6, 0.9]), np.array([1.7, 0.8, 2.2])
+    m = _std_model(w, b, mean, inv_std)
+    o = O.Oracle()
+    o.upload(cluster(ENV, 100.0))
+    o.set_model(m)
+    out = o.eval(1.0, 0.0)
+    weff, beff = w * inv_std, b - np.sum(w * inv_std * mean)
+    h = 1e-6
+    for a in range(4):
+        for x in range(3):
+            pp, pm = np.array(ENV, float), np.array(ENV, float)
+            pp[a, x] += h
+            pm[a, x] -= h
+            ep = run(pp, Table.acsf(6.0, g2=STD_G2), weff, beff)["energy"][0]
+            em = run(pm, Table.acsf(6.0, g2=STD_G2), weff, beff)["energy"][0]
+            assert abs(out["forces"][a][x] + (ep - em) / (2 * h)) <= 1e-7
+    raw = run(ENV, Table.acsf(6.0, g2=STD_G2), weff, beff)
+    np.testing.assert_allclose(out["forces"], raw["forces"], rtol=0, atol=1e-13)
+    assert abs(out["energy"][0] - raw["energy"][0]) <= 1e-12
+
+
+def test_standardization_tables_are_fixed():
+    """A standardization value marked free is rejected by set_model."""
+    from forcesmith_b200.abi import FsError
+    m = _std_model([0.7, -0.4, 0.25], 0.1, [0.3, 0.6, 0.9], [1.7, 0.8, 2.2])
+    m.tables[-1].fixed[0] = 0
+    o = O.Oracle()
+    o.upload(cluster(ENV, 100.0))
+    with pytest.raises(FsError):
+        o.set_model(m)
