@@ -22,7 +22,8 @@
 // shared memory; energy and stress as per-thread FP64 sums.  Jacobian: force
 // rows into the configuration's force-row block in shared memory, written out
 // once (or, when the block does not fit, straight into J, zeroed first); the
-// energy and stress rows, which every term hits, summed over the warp into J;
+// energy and stress rows, which every term hits, summed over the warp and
+// then in FP64 shared memory, written to J once;
 // a two-pass column reduction forms Jᵀr.
 #include "jtr.cuh"
 #include "kern_common.cuh"
@@ -137,6 +138,12 @@ template <class T, int MODE> __global__ void __launch_bounds__(kAcThreads) acsf_
   int *ntyp = (JAC && A.std_on) ? S.take<int>(nt) : nullptr;
   // JAC with smj: the 3N force rows (local) × D columns
   T *Jb = (JAC && A.smj) ? S.take<T>(static_cast<size_t>(3 * N) * A.D) : nullptr;
+  // JAC: the configuration's energy and 6 stress rows, summed in FP64 (every
+  // term of the configuration adds to them, and a standardized column then
+  // cancels most of its energy row against the mean shift)
+  double *E64 = JAC ? S.take<double>(static_cast<size_t>(7) * A.D) : nullptr;
+  if (E64)
+    for (int k = threadIdx.x; k < 7 * A.D; k += blockDim.x) E64[k] = 0.0;
   if (Jb)
     for (int k = threadIdx.x; k < 3 * N * A.D; k += blockDim.x) Jb[k] = T(0);
   for (int k = threadIdx.x; k < nspec; k += blockDim.x) par[k] = static_cast<T>(spec[k]);
@@ -198,13 +205,12 @@ template <class T, int MODE> __global__ void __launch_bounds__(kAcThreads) acsf_
     const T v[8] = {we * e, st[0], st[1], st[2], st[3], st[4], st[5], T(0)};
     const T t = warp_sum_tr<8>(v, lane); // lanes 4m hold row m
     const int m = lane >> 2;
-    if ((lane & 3) == 0 && m < nrow) atomicAdd(&A.J[static_cast<int64_t>(c0) * A.ld + row0 + rE + m], t);
+    if ((lane & 3) == 0 && m < nrow) atomicAdd(&E64[m * A.D + c0], static_cast<double>(t));
   };
   // the same rows from one lane
   auto erows_lane = [&](int cl, T e, const T (&st)[6]) {
-    T *Jc = A.J + static_cast<int64_t>(cl) * A.ld + row0 + rE;
-    atomicAdd(&Jc[0], we * e);
-    for (int m = 1; m < nrow; ++m) atomicAdd(&Jc[m], st[m - 1]);
+    atomicAdd(&E64[cl], static_cast<double>(we * e));
+    for (int m = 1; m < nrow; ++m) atomicAdd(&E64[m * A.D + cl], static_cast<double>(st[m - 1]));
   };
   // ---- G1–G3: one thread per directed pair; each warp takes 32 consecutive
   // items (the Jacobian's warp sums need every lane; spare lanes repeat the
@@ -456,26 +462,31 @@ template <class T, int MODE> __global__ void __launch_bounds__(kAcThreads) acsf_
     const int ti = typ[i];
     if constexpr (JAC) {
       const int cb = col[ti * (L.S + 1) + L.S];
-      if (cb >= 0) jadd(cb, rE, we);
+      if (cb >= 0) atomicAdd(&E64[cb], A.w_e);
       if (ntyp) atomicAdd(&ntyp[ti], 1);
     } else {
       e_acc += static_cast<double>(W[ti * (L.S + 1) + L.S]);
     }
   }
   if constexpr (JAC) {
-    if (ivs) { // standardized: ∂E/∂w_k also holds −inv_std_k·mean_k per atom of the species
-      __syncthreads();
+    __syncthreads();
+    if (ivs) // standardized: ∂E/∂w_k also holds −inv_std_k·mean_k per atom of the species
       for (int q = threadIdx.x; q < nt * L.S; q += blockDim.x) {
         const int t = q / L.S, kk = q % L.S;
         const int ck = col[t * (L.S + 1) + kk];
         if (ck < 0 || ntyp[t] == 0) continue;
         const double mu = A.vals[A.c.desc[1 + nt + t].pv0 + kk];
-        jadd(ck, rE, static_cast<T>(-A.w_e * static_cast<double>(ivs[q]) * mu * ntyp[t]));
+        atomicAdd(&E64[ck], -A.w_e * static_cast<double>(ivs[q]) * mu * ntyp[t]);
       }
+    __syncthreads();
+    // the energy and stress rows to J (J is zeroed; this CTA owns them)
+    for (int q = threadIdx.x; q < nrow * A.D; q += blockDim.x) {
+      const int m = q / A.D, cl = q % A.D;
+      A.J[static_cast<int64_t>(cl) * A.ld + row0 + rE + m] = static_cast<T>(E64[q]);
     }
     if (!Jb) return;
     __syncthreads();
-    // the force rows to J (the energy, stress and limit rows are in J already)
+    // the force rows to J (the limit row stays zero)
     for (int k = threadIdx.x; k < 3 * N * A.D; k += blockDim.x) {
       const int cl = k / (3 * N), r = k % (3 * N);
       A.J[static_cast<int64_t>(cl) * A.ld + row0 + r] = Jb[r * A.D + cl];
@@ -627,6 +638,7 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, int mode, 
     FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     a.J = static_cast<T *>(h->d_J);
     a.ld = ldj;
+    sm += align16(static_cast<size_t>(7) * D * sizeof(double)); // the FP64 energy and stress rows
     // the configuration's J block in shared memory when it fits
     const size_t jb = align16(static_cast<size_t>(3 * h->max_natoms) * D * sizeof(T));
     if (D > 0 && sm + jb <= 200 * 1024) {
