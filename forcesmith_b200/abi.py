@@ -209,6 +209,75 @@ class Model:
         tabs += [Table.standardization(mean[t], inv_std[t]) for t in range(self.ntypes)]
         return Model(self.family, self.ntypes, tabs)
 
+    def acsf_remapped(self, old_species, new_species):
+        """An ACSF model for the species list new_species, from this model's
+        heads for old_species (MLBase::remap, ml_force.hpp:165-190):
+        descriptor index k of the new layout takes the head coefficient of the
+        old index that describes the same species channel (remap_layout,
+        descriptor_layout.cpp:9-50); channels without an old counterpart get
+        coefficient 0 with the head's first coefficient's fixed flag
+        (LinearHead::remapped, ml_force.cpp:52-65).  A new species without an
+        old one gets a zero head, coefficients free and bias 0 fixed
+        (zero_like, :67-71).  Standardization is dropped, as remap drops it.
+
+        As in remap_layout, a block counts as per-species when its channel
+        count equals the new species count; with one new species that is also
+        true of the pair blocks (one pair channel)."""
+        assert self.family == FS_FAMILY_ACSF
+        old_of_new = [list(old_species).index(x) if x in old_species else None for x in new_species]
+        spec = self.tables[0]
+        S_old, S_new = self.ntypes, len(new_species)
+        g1, n2, n3, n4, n5 = (int(x) for x in spec.values[1:6])
+
+        def layout(nt):  # (base, count, nchan) per block: G1..G3 per species, G4, G5 per pair
+            P, base, out = nt * (nt + 1) // 2, 0, []
+            for count, nch in ((g1, nt), (n2, nt), (n3, nt), (n4, P), (n5, P)):
+                out.append((base, count, nch))
+                base += count * nch
+            return out, base
+
+        def ordinal(a, b, nt):  # pair_ordinal: upper triangle, row-major
+            a, b = min(a, b), max(a, b)
+            return a * nt - a * (a - 1) // 2 + (b - a)
+
+        Lo, _ = layout(S_old)
+        Ln, size = layout(S_new)
+        idx = [None] * size
+        for (bo, _, _), (bn, count, nch) in zip(Lo, Ln):
+            if nch == S_new:  # per species
+                for sn, so in enumerate(old_of_new):
+                    if so is not None:
+                        for t in range(count):
+                            idx[bn + sn * count + t] = bo + so * count + t
+            else:  # per pair
+                for a in range(S_new):
+                    for c in range(a, S_new):
+                        ao, co = old_of_new[a], old_of_new[c]
+                        if ao is None or co is None:
+                            continue
+                        pn, po = ordinal(a, c, S_new), ordinal(ao, co, S_old)
+                        for t in range(count):
+                            idx[bn + pn * count + t] = bo + po * count + t
+        heads = []
+        for so in old_of_new:
+            if so is None:
+                fx = np.zeros(size + 1, np.uint8)
+                fx[-1] = 1
+                heads.append(Table.linear_head(np.zeros(size), 0.0, fixed=fx))
+                continue
+            h = self.tables[1 + so]
+            hv = h.values
+            hf = h.fixed if h.fixed is not None else np.zeros(hv.size, np.uint8)
+            f0 = hf[0] if hv.size > 1 else 0
+            v = np.zeros(size + 1)
+            fx = np.full(size + 1, f0, np.uint8)
+            for k, src in enumerate(idx):
+                if src is not None:
+                    v[k], fx[k] = hv[src], hf[src]
+            v[-1], fx[-1] = hv[-1], hf[-1]
+            heads.append(Table.linear_head(v[:-1], v[-1], fixed=fx))
+        return Model(FS_FAMILY_ACSF, S_new, [spec.copy()] + heads)
+
     def free_values(self) -> np.ndarray:
         out = []
         for t in self.tables:

@@ -167,3 +167,61 @@ def test_standardization_tables_are_fixed():
     o.upload(cluster(ENV, 100.0))
     with pytest.raises(FsError):
         o.set_model(m)
+
+
+# ---- species re-ranking (MLBase::remap, ml_force.hpp:165-190; remap_layout,
+# descriptor_layout.cpp:9-50)
+REMAP_SPEC = Table.acsf(6.0, g1=1, g2=[(0.5, 1.0)], g3=[1.1], g4=[(0.1, 2.0, -1.0)], g5=[(0.2, 1.0, 1.0)])
+
+
+def _two_species_model(seed=4):
+    S = acsf_size(REMAP_SPEC, 2)
+    rng = np.random.default_rng(seed)
+    return Model(FS_FAMILY_ACSF, 2, [REMAP_SPEC] + [Table.linear_head(rng.normal(0, 0.3, S), -1.0 + t)
+                                                   for t in range(2)])
+
+
+def _eval(model, types, nt):
+    o = O.Oracle()
+    o.upload(cluster(ENV, 100.0, types=types))
+    o.set_model(model)
+    return o.eval(1.0, 0.0)
+
+
+def test_remap_swapped_species_is_a_relabelling():
+    """Remapping [A, B] → [B, A] and swapping every atom's species leaves the
+    energy and forces unchanged (1e-12): each coefficient moves with its
+    species channel, pair channels included."""
+    m = _two_species_model()
+    types = np.array([0, 1, 0, 1])
+    ref = _eval(m, types, 2)
+    r = m.acsf_remapped(["A", "B"], ["B", "A"])
+    out = _eval(r, 1 - types, 2)
+    assert abs(out["energy"][0] - ref["energy"][0]) <= 1e-12 * (1 + abs(ref["energy"][0]))
+    np.testing.assert_allclose(out["forces"], ref["forces"], rtol=0, atol=1e-12)
+
+
+def test_remap_added_species_changes_nothing():
+    """Remapping [A, B] → [A, B, C]: with no atom of species C, energies and
+    forces are those of the two-species model (1e-12); C's head is a zero
+    head with free coefficients and a fixed zero bias, and the channels that
+    involve C have coefficient 0."""
+    m = _two_species_model()
+    types = np.array([0, 1, 1, 0])
+    ref = _eval(m, types, 2)
+    r = m.acsf_remapped(["A", "B"], ["A", "B", "C"])
+    assert r.ntypes == 3 and len(r.tables) == 4
+    S3 = acsf_size(REMAP_SPEC, 3)
+    assert r.tables[3].values.tolist() == [0.0] * (S3 + 1)
+    assert r.tables[3].fixed[:-1].tolist() == [0] * S3 and r.tables[3].fixed[-1] == 1
+    out = _eval(r, types, 3)
+    assert abs(out["energy"][0] - ref["energy"][0]) <= 1e-12 * (1 + abs(ref["energy"][0]))
+    np.testing.assert_allclose(out["forces"], ref["forces"], rtol=0, atol=1e-12)
+
+
+def test_remap_drops_standardization():
+    """remap clears the (old-layout) standardization."""
+    m = _two_species_model()
+    S = acsf_size(REMAP_SPEC, 2)
+    ms = m.with_standardization(np.zeros((2, S)), np.ones((2, S)))
+    assert len(ms.acsf_remapped(["A", "B"], ["B", "A"]).tables) == 3
