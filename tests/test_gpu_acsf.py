@@ -183,3 +183,27 @@ def test_acsf_standardized_jacobian(case, precision, rel, floor):
     ratio = np.abs(res["J"] - Jf) / bar
     r, c = np.unravel_index(np.argmax(ratio), ratio.shape)
     assert ratio.max() <= 1.0, (ratio.max(), r, c, res["J"][r, c], Jf[r, c])
+
+
+def test_acsf_three_species_remapped():
+    """A three-species model made by species re-ranking ([A, B] → [A, B, C],
+    MLBase::remap) on configurations of all three species: FP64 residual rows
+    against the oracle 1e-9·(1 + |x|), and the exact FP64 Jacobian against the
+    oracle's central differences (1e-6·max|J column| + 1e-9)."""
+    ds = synth.diamond(3, cells=(2,), seed=17)
+    ds.type[:] = np.random.default_rng(5).integers(0, 3, ds.type.size)
+    m2 = model(2, 3)
+    m3 = m2.acsf_remapped(["A", "B"], ["A", "B", "C"])
+    rng = np.random.default_rng(6)
+    for t in m3.tables[1:]:
+        t.values[:-1] += rng.normal(0, 0.05, t.values.size - 1)  # every channel in use
+    ds = label(ds, m3, O.Oracle, 1.0, 0.2)
+    start = m3.with_values(m3.free_values() * 1.05)
+    g, o = _pair(ds, start, "fp64")
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    for key in ("forces", "energy", "stress", "F"):
+        _close(rg[key], ro[key], 1e-9, key)
+    res = g.jacobian(1.0, 0.2)
+    Jf = o.jacobian_fd(1.0, 0.2)
+    bar = 1e-6 * np.abs(Jf).max(axis=0) + 1e-9
+    assert np.max(np.abs(res["J"] - Jf) / bar) <= 1.0
