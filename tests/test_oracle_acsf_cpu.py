@@ -225,3 +225,22 @@ def test_remap_drops_standardization():
     S = acsf_size(REMAP_SPEC, 2)
     ms = m.with_standardization(np.zeros((2, S)), np.ones((2, S)))
     assert len(ms.acsf_remapped(["A", "B"], ["B", "A"]).tables) == 3
+
+
+def test_standardization_dead_features():
+    """A feature with no variance across the atoms (both atoms of a dimer see
+    the same environment) gets inv_std 0 (var ≤ 1e-12,
+    compute_standardization) and drops out of the head: the standardized
+    energy is N·b and the forces vanish (1e-12)."""
+    spec = Table.acsf(6.0, g2=STD_G2)
+    w, b = np.array([0.7, -0.4, 0.25]), 0.1
+    dimer = [[0.0, 0.0, 0.0], [2.3, 0.0, 0.0]]
+    o = O.Oracle()
+    o.upload(cluster(dimer, 100.0))
+    o.set_model(Model(FS_FAMILY_ACSF, 1, [spec, Table.linear_head(w, b)]))
+    mean, inv_std, count = o.acsf_standardization()
+    assert count.tolist() == [2] and np.all(inv_std == 0.0) and np.all(mean > 0)
+    o.set_model(_std_model(w, b, mean[0], inv_std[0]))
+    out = o.eval(1.0, 0.0)
+    assert abs(out["energy"][0] - 2 * b) <= 1e-12
+    assert np.max(np.abs(out["forces"])) <= 1e-12
