@@ -207,3 +207,28 @@ def test_acsf_three_species_remapped():
     Jf = o.jacobian_fd(1.0, 0.2)
     bar = 1e-6 * np.abs(Jf).max(axis=0) + 1e-9
     assert np.max(np.abs(res["J"] - Jf) / bar) <= 1.0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_acsf_standardization_dead_features(precision):
+    """Three identical dimers: every atom sees the same environment, so every
+    feature has no variance, inv_std is 0 (compute_standardization) and the
+    standardized head reduces to its bias.  Statistics, residual and Jacobian against the
+    oracle: the J columns of w vanish except for the energy row's mean
+    shift, which cancels Σ_i D_i exactly here (|J| ≤ 1e-6 in FP32, 1e-12 in
+    FP64); forces 1e-9 (FP64) / 1e-6 (FP32) absolute."""
+    from tests.helpers import cluster, concat
+    ds = concat(*[cluster([[0.0, 0.0, 0.0], [2.4, 0.0, 0.0]], 20.0) for _ in range(3)])
+    ds = label(ds, model(1, 1), O.Oracle, 1.0, 0.2)
+    start = model(1, 2)
+    g, o = _pair(ds, start, precision)
+    mg, ig, _ = g.acsf_standardization()
+    assert np.all(ig == 0.0), ig
+    m = start.with_standardization(mg, ig)
+    g, o = _pair(ds, m, precision)
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    tol = 1e-9 if precision == "fp64" else 1e-6
+    assert np.max(np.abs(rg["forces"])) <= tol and np.max(np.abs(ro["forces"])) <= 1e-12
+    _close(rg["energy"], ro["energy"], tol, "energy")
+    res = g.jacobian(1.0, 0.2)
+    assert np.max(np.abs(res["J"])) <= (1e-12 if precision == "fp64" else 1e-6)
