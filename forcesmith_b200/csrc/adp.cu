@@ -22,12 +22,13 @@ template <class T> struct AdpArgs {
   double *F, *forces, *energy, *stress9, *limit, *obj_part;
 };
 
-template <class T>
-__device__ __forceinline__ void gated(const STab<T> &tb, const typename Vec4T<T>::type *seg, T r, T &v, T &d) {
+template <class T, class R64>
+__device__ __forceinline__ void gated(const STab<T> &tb, const typename Vec4T<T>::type *seg, T r, R64 &&r64, T &v,
+                                      T &d) {
   v = d = T(0);
-  if (!in_span(tb, r)) return;
+  if (!gate_in(tb, r, r64)) return;
   T t;
-  const int e = seg_of(tb, r, t);
+  const int e = seg_of_r(tb, r, t, r64);
   v = seg_val<T>(seg[e], t);
   d = seg_der<T>(seg[e], t, tb.inv_h);
 }
@@ -63,16 +64,18 @@ __global__ void __launch_bounds__(256) adp_residual_kernel(AdpArgs<T> A) {
     for (int p = start[i]; p < start[i + 1]; ++p) {
       int j;
       T d[3];
-      pair_vec(wpos, shift, i, A.c.nb_pack[p], j, d[0], d[1], d[2]);
+      const uint32_t pk = A.c.nb_pack[p];
+      pair_vec(wpos, shift, i, pk, j, d[0], d[1], d[2]);
       const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (r < T(1e-14)) continue;
+      const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
       const int tj = typ[j], pt = pair_ord(ti, tj, nt);
       T v, dv;
-      gated(tabs[np + tj], seg, r, v, dv);
+      gated(tabs[np + tj], seg, r, r64, v, dv);
       rho += v;
-      gated(tabs[2 * nt + np + pt], seg, r, v, dv); // dipole u_{ij}
+      gated(tabs[2 * nt + np + pt], seg, r, r64, v, dv); // dipole u_{ij}
       for (int a = 0; a < 3; ++a) m[a] += v * d[a];
-      gated(tabs[2 * nt + 2 * np + pt], seg, r, v, dv); // quadrupole w_{ij}
+      gated(tabs[2 * nt + 2 * np + pt], seg, r, r64, v, dv); // quadrupole w_{ij}
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) L[3 * a + b] += v * (d[a] * d[b]);
     }
@@ -113,17 +116,19 @@ __global__ void __launch_bounds__(256) adp_residual_kernel(AdpArgs<T> A) {
     for (int p = start[i]; p < start[i + 1]; ++p) {
       int j;
       T d[3];
-      pair_vec(wpos, shift, i, A.c.nb_pack[p], j, d[0], d[1], d[2]);
+      const uint32_t pk = A.c.nb_pack[p];
+      pair_vec(wpos, shift, i, pk, j, d[0], d[1], d[2]);
       const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (r < T(1e-14)) continue;
+      const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
       const T ir = T(1) / r;
       const int tj = typ[j], pt = pair_ord(ti, tj, nt);
       T phi, dphi, rj, drj, ri, dri, u, du, w, dw;
-      gated(tabs[pt], seg, r, phi, dphi);
-      gated(tabs[np + tj], seg, r, rj, drj);
-      gated(tabs[np + ti], seg, r, ri, dri);
-      gated(tabs[2 * nt + np + pt], seg, r, u, du);
-      gated(tabs[2 * nt + 2 * np + pt], seg, r, w, dw);
+      gated(tabs[pt], seg, r, r64, phi, dphi);
+      gated(tabs[np + tj], seg, r, r64, rj, drj);
+      gated(tabs[np + ti], seg, r, r64, ri, dri);
+      gated(tabs[2 * nt + np + pt], seg, r, r64, u, du);
+      gated(tabs[2 * nt + 2 * np + pt], seg, r, r64, w, dw);
       T g[3];
       const T es = (dphi + gF[i] * drj + gF[j] * dri) * ir;
       const T *mi = mu + 3 * i, *mj = mu + 3 * j;

@@ -77,11 +77,13 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
     const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
     const STab<T> &tb = tabs[pair_ord(typ[i], typ[j], nt)];
-    const bool ok = w0 + lane < npair && r >= T(1e-14) && in_span(tb, r);
+    const uint32_t pw = nbp[w];
+    const auto r64 = [&] { return pair_len64(wpos, shift, i, pw); };
+    const bool ok = w0 + lane < npair && r >= T(1e-14) && gate_in(tb, r, r64);
     if (!__any_sync(0xffffffffu, ok)) continue;
     bool hi;
     const unsigned xi = run_links(i, lane, hi);
-    const VD<T> ph = tab_vd<T, true>(tb, seg, A.vals, r);
+    const VD<T> ph = tab_vd_r<T, true>(tb, seg, A.vals, r, r64);
     const T s = ok ? ph.d / r : T(0);
     const T f[3] = {s * d[0], s * d[1], s * d[2]};
 #pragma unroll
@@ -115,12 +117,16 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
     const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
     const STab<T> &rk = tabs[np + pair_ord(ti, typ[k], nt)];
-    const bool ok = w0 + lane < ntri && r1 >= T(1e-14) && in_span(rj, r1) && r2 >= T(1e-14) && in_span(rk, r2);
+    const uint32_t pwj = nbp[pj], pwk = nbp[pk];
+    const auto r64j = [&] { return pair_len64(wpos, shift, i, pwj); };
+    const auto r64k = [&] { return pair_len64(wpos, shift, i, pwk); };
+    const bool ok = w0 + lane < ntri && r1 >= T(1e-14) && gate_in(rj, r1, r64j) && r2 >= T(1e-14) &&
+                    gate_in(rk, r2, r64k);
     if (!__any_sync(0xffffffffu, ok)) continue;
     bool hi, hj;
     const unsigned xi = run_links(i, lane, hi);
     const unsigned xj = run_links(pj, lane, hj); // atom j: runs of the same neighbour slot
-    const VD<T> F1 = tab_vd<T, true>(rj, seg, A.vals, r1), F2 = tab_vd<T, true>(rk, seg, A.vals, r2);
+    const VD<T> F1 = tab_vd_r<T, true>(rj, seg, A.vals, r1, r64j), F2 = tab_vd_r<T, true>(rk, seg, A.vals, r2, r64k);
     // lanes without a term: zero inverse distances and c3, so every force below is zero
     const T ir1 = ok ? T(1) / r1 : T(0), ir2 = ok ? T(1) / r2 : T(0);
     const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;

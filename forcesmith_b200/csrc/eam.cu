@@ -70,10 +70,10 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
         for (int p = start[i] + l; p < start[i + 1]; p += LPA) {
           int j;
           T dx, dy, dz;
-          pair_vec(wpos, shift, i, A.c.nb_pack[p], j, dx, dy, dz);
-          const T r = sqrt_t(dx * dx + dy * dy + dz * dz);
+          const double r64 = pair_vec_len(wpos, shift, i, A.c.nb_pack[p], j, dx, dy, dz);
+          const T r = static_cast<T>(r64);
           const STab<T> &tb = tabs[np + typ[j]];
-          if (in_span(tb, r)) acc += tab_vd<T, AN>(tb, seg, A.c.vals, r).v;
+          if (gate64(tb, r64)) acc += tab_vd64<T, AN>(tb, seg, A.c.vals, r, r64).v;
         }
       }
       acc = warp_sum_group(acc, LPA);
@@ -112,22 +112,22 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
       for (int p = start[i] + l; p < start[i + 1]; p += LPA) {
         int j;
         T d[3];
-        pair_vec(wpos, shift, i, A.c.nb_pack[p], j, d[0], d[1], d[2]);
-        const T r = sqrt_t(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-        if (r < T(1e-14)) continue;
+        const double r64 = pair_vec_len(wpos, shift, i, A.c.nb_pack[p], j, d[0], d[1], d[2]);
+        const T r = static_cast<T>(r64);
+        if (r64 < 1e-14) continue;
         const int tj = typ[j];
         const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
         T phi = T(0), dphi = T(0);
         if constexpr (EAM) {
-          if (in_span(tp, r)) {
-            const VD<T> pv = tab_vd<T, AN>(tp, seg, A.c.vals, r);
+          if (gate64(tp, r64)) {
+            const VD<T> pv = tab_vd64<T, AN>(tp, seg, A.c.vals, r, r64);
             phi = pv.v;
             dphi = pv.d;
           }
         } else {
           // make_pair_bond's half-open gate [rmin, rmax) (pair_force.cpp:28)
-          if (r < tp.x0 || r >= tp.xmax) continue;
-          const VD<T> pv = tab_vd<T, AN>(tp, seg, A.c.vals, r);
+          if (!gate64<false>(tp, r64)) continue;
+          const VD<T> pv = tab_vd64<T, AN>(tp, seg, A.c.vals, r, r64);
           phi = pv.v;
           dphi = pv.d;
         }
@@ -135,8 +135,8 @@ __device__ double config_pass(const ResArgs<T> &A, int c, const CfgDev &cd, cons
         if constexpr (EAM) {
           const STab<T> &gj = tabs[np + tj], &gi = tabs[np + ti];
           T drho_j = T(0), drho_i = T(0);
-          if (in_span(gj, r)) drho_j = tab_vd<T, AN>(gj, seg, A.c.vals, r).d;
-          if (in_span(gi, r)) drho_i = tab_vd<T, AN>(gi, seg, A.c.vals, r).d;
+          if (gate64(gj, r64)) drho_j = tab_vd64<T, AN>(gj, seg, A.c.vals, r, r64).d;
+          if (gate64(gi, r64)) drho_i = tab_vd64<T, AN>(gi, seg, A.c.vals, r, r64).d;
           fs = dphi + gradF[i] * drho_j + gradF[j] * drho_i;
         }
         fs = fs * (T(1) / r);
@@ -383,12 +383,11 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
           if (p < p1) {
             int j;
             float dx, dy, dz;
-            pair_vec(wpos, shift, i, cur, j, dx, dy, dz);
-            const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+            const double r64 = pair_vec_len(wpos, shift, i, cur, j, dx, dy, dz);
             const STab<float> &tb = tabs[np + typ[j]];
-            if (in_span(tb, r)) {
+            if (gate64(tb, r64)) {
               float t;
-              rec.x = seg_of(tb, r, t);
+              rec.x = seg_of64(tb, static_cast<float>(r64), r64, t);
               rec.y = __float_as_int(t);
             }
           }
@@ -446,9 +445,9 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
           rec.a = rec.b = rec.c = rec.ih = make_float4(0.f, 0.f, 0.f, 0.f);
           int j;
           float dx, dy, dz;
-          pair_vec(wpos, shift, i, cur, j, dx, dy, dz);
-          const float r = sqrtf(dx * dx + dy * dy + dz * dz);
-          if (r >= 1e-14f) {
+          const double r64 = pair_vec_len(wpos, shift, i, cur, j, dx, dy, dz);
+          const float r = static_cast<float>(r64);
+          if (r64 >= 1e-14) {
             const float inv = 1.f / r, hi = 0.5f * inv;
             rec.d.x = j;
             rec.a = make_float4(dx * inv, dy * inv, dz * inv, 0.f);
@@ -457,24 +456,24 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
             const int tj = typ[j];
             const STab<float> &tp = tabs[pair_ord(ti, tj, nt)];
             // EAM: closed gate; pair: [rmin, rmax) (pair_force.cpp:28)
-            const bool gate = EAM ? in_span(tp, r) : (r >= tp.x0 && r < tp.xmax);
+            const bool gate = EAM ? gate64(tp, r64) : gate64<false>(tp, r64);
             if (gate) {
               float t;
-              rec.d.y = seg_of(tp, r, t);
+              rec.d.y = seg_of64(tp, r, r64, t);
               rec.a.w = t;
               rec.ih.x = tp.inv_h;
             }
             if constexpr (EAM) {
               const STab<float> &gj = tabs[np + tj], &gi = tabs[np + ti];
-              if (in_span(gj, r)) {
+              if (gate64(gj, r64)) {
                 float t;
-                rec.d.z = seg_of(gj, r, t);
+                rec.d.z = seg_of64(gj, r, r64, t);
                 rec.c.z = t;
                 rec.ih.y = gj.inv_h;
               }
-              if (in_span(gi, r)) {
+              if (gate64(gi, r64)) {
                 float t;
-                rec.d.w = seg_of(gi, r, t);
+                rec.d.w = seg_of64(gi, r, r64, t);
                 rec.c.w = t;
                 rec.ih.z = gi.inv_h;
               }
@@ -669,12 +668,14 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
     for (int p = start[i]; p < start[i + 1]; ++p) {
       int j;
       T dx, dy, dz;
-      pair_vec(wpos, shift, i, A.c.nb_pack[p], j, dx, dy, dz);
+      const uint32_t pk = A.c.nb_pack[p];
+      pair_vec(wpos, shift, i, pk, j, dx, dy, dz);
       const T r = sqrt_t(dx * dx + dy * dy + dz * dz);
       const STab<T> &tb = tabs[np + typ[j]];
-      if (!in_span(tb, r)) continue;
+      const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
+      if (!gate_in(tb, r, r64)) continue;
       T t;
-      const int e = seg_of(tb, r, t);
+      const int e = seg_of_r(tb, r, t, r64);
       rho += seg_val<T>(seg[e], t);
       const int ws = segws[e];
       const T *G = segg + e * 4 * kWin;
@@ -999,9 +1000,10 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
             v[4] = s0 * u[2];
             v[5] = s1 * u[2];
           }
+          const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
           auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt, T &tout) {
             T t;
-            const int e = seg_of(tb, rr, t);
+            const int e = seg_of_r(tb, rr, t, r64);
             R.si[s] = make_int4(e * 4 * kWin, tb.cmap0 + segws[e], 0, cross);
             R.sf[s].x = t;
             R.sf[s].y = wgt * tb.inv_h;
@@ -1010,19 +1012,19 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           };
           T t_;
           const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
-          const bool phi_in = EAM ? in_span(tp, r) : (r >= tp.x0 && r < tp.xmax);
+          const bool phi_in = EAM ? gate_in(tp, r, r64) : gate_in<false>(tp, r, r64);
           if (phi_in) set_slot(0, tp, r, T(1), t_);
           if constexpr (EAM) {
             const STab<T> &gj = tabs[np + tj], &gi_ = tabs[np + ti];
             const T gFj = gFa[j];
             cFj = cFa[j];
-            if (in_span(gj, r)) {
+            if (gate_in(gj, r, r64)) {
               const int e = set_slot(1, gj, r, tj == ti ? gFi + gFj : gFi, t_);
               dgj = seg_der<T>(seg[e], t_, gj.inv_h);
             }
-            if (in_span(gi_, r)) {
+            if (gate_in(gi_, r, r64)) {
               T t;
-              const int e = seg_of(gi_, r, t);
+              const int e = seg_of_r(gi_, r, t, r64);
               dgi = seg_der<T>(seg[e], t, gi_.inv_h);
               if (tj != ti) set_slot(2, gi_, r, gFj, t_);
             }

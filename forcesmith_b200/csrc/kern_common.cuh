@@ -66,6 +66,32 @@ __device__ __forceinline__ void pair_vec(const double *wpos, const double *shift
 
 template <class T> __device__ __forceinline__ T sqrt_t(T x) { return sqrt(x); }
 
+// pair_vec, also returning the pair's FP64 length (the FP64 path's r).
+template <class T>
+__device__ __forceinline__ double pair_vec_len(const double *wpos, const double *shift, int i, uint32_t pk, int &j,
+                                               T &dx, T &dy, T &dz) {
+  j = static_cast<int>(pk & 0xFFFFFu);
+  const int img = static_cast<int>(pk >> 20);
+  const double x = (wpos[3 * j] - wpos[3 * i]) + shift[3 * img];
+  const double y = (wpos[3 * j + 1] - wpos[3 * i + 1]) + shift[3 * img + 1];
+  const double z = (wpos[3 * j + 2] - wpos[3 * i + 2]) + shift[3 * img + 2];
+  dx = static_cast<T>(x);
+  dy = static_cast<T>(y);
+  dz = static_cast<T>(z);
+  return sqrt(x * x + y * y + z * z);
+}
+
+// FP64 length of pair_vec's pair vector, computed as the FP64 path computes
+// it; the FP32 kernels use it only to decide gates near a bound (gate_in).
+__device__ __forceinline__ double pair_len64(const double *wpos, const double *shift, int i, uint32_t pk) {
+  const int j = static_cast<int>(pk & 0xFFFFFu);
+  const int img = static_cast<int>(pk >> 20);
+  const double dx = (wpos[3 * j] - wpos[3 * i]) + shift[3 * img];
+  const double dy = (wpos[3 * j + 1] - wpos[3 * i + 1]) + shift[3 * img + 1];
+  const double dz = (wpos[3 * j + 2] - wpos[3 * i + 2]) + shift[3 * img + 2];
+  return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
 
 // Block sums of K values at once (one pair of barriers); valid on thread 0.
 // red holds K × 32 doubles.

@@ -11,9 +11,20 @@ namespace fsg {
 template <class T> struct STab {
   T x0, inv_h, xmax, h;
   double x0d, hd; // FP64 grid for the exact interval search
+  double xmaxd;   // FP64 upper gate bound
+  double inv_hd;  // FP64 1/h
+  // Gate bands of the working precision: r in (lo_in, hi_in) is inside the
+  // gate, r below lo_out or above hi_out is outside it, and a distance
+  // between is decided from its FP64 length (gate_in below).
+  T lo_in, hi_in, lo_out, hi_out;
   int n, seg0, cmap0, kind;
   int form, pv0; // analytic tables: fs_form and first parameter in the value array
 };
+
+// Relative width of the band around a gate bound inside which a length
+// computed in FP32 (from an FP64 pair vector rounded per component) may fall
+// on the other side of the bound than the FP64 length: a few FP32 ulps.
+constexpr double kGateBand = 4e-6;
 
 template <class T> __device__ __forceinline__ void load_stab(STab<T> &s, const TableDesc &d) {
   s.x0 = static_cast<T>(d.x0);
@@ -22,6 +33,13 @@ template <class T> __device__ __forceinline__ void load_stab(STab<T> &s, const T
   s.h = static_cast<T>(d.h);
   s.x0d = d.x0;
   s.hd = d.h;
+  s.xmaxd = d.xmax;
+  s.inv_hd = d.inv_h;
+  const double b0 = kGateBand * fabs(d.x0), b1 = kGateBand * fabs(d.xmax);
+  s.lo_in = static_cast<T>(d.x0 + b0);
+  s.lo_out = static_cast<T>(d.x0 - b0);
+  s.hi_in = static_cast<T>(d.xmax - b1);
+  s.hi_out = static_cast<T>(d.xmax + b1);
   s.n = d.n;
   s.seg0 = d.seg0;
   s.cmap0 = d.cmap0;
@@ -108,9 +126,29 @@ template <class T> __device__ __forceinline__ VD<T> form_vd(int form, const doub
   return o;
 }
 
-// Closed gate [x0, x_{n-1}] (force_calculator_concept.hpp:94-98).
+// Closed gate [x0, x_{n-1}] (force_calculator_concept.hpp:94-98), for
+// values that are not pair distances (ρ against the embedding span).
 template <class T> __device__ __forceinline__ bool in_span(const STab<T> &tb, T r) {
   return r >= tb.x0 && r <= tb.xmax;
+}
+
+// Range gate of a pair distance: closed [x0, x_{n-1}] (EAM, ADP, angular
+// radial tables; force_calculator_concept.hpp:94-118) or, when !CLOSED, the
+// pair calculator's half-open [x0, x_{n-1}) (pair_force.cpp:28).  In FP64
+// the distance r is compared directly.  In FP32, r carries a few ulps of
+// rounding, so a distance within kGateBand of a bound is decided from its
+// FP64 length r64() instead: the FP32 and FP64 paths then keep the same
+// pairs, and a pair at the cut-off is never dropped by rounding alone.
+template <bool CLOSED = true, class T, class R64>
+__device__ __forceinline__ bool gate_in(const STab<T> &tb, T r, R64 &&r64) {
+  if constexpr (std::is_same_v<T, double>) {
+    return CLOSED ? (r >= tb.x0 && r <= tb.xmax) : (r >= tb.x0 && r < tb.xmax);
+  } else {
+    if (r > tb.lo_in && r < tb.hi_in) return true;
+    if (r < tb.lo_out || r > tb.hi_out) return false;
+    const double q = r64();
+    return CLOSED ? (q >= tb.x0d && q <= tb.xmaxd) : (q >= tb.x0d && q < tb.xmaxd);
+  }
 }
 
 // Extended segment of r and its local coordinate t = (r - origin)/h, with the
@@ -145,6 +183,70 @@ template <class T> __device__ __forceinline__ int seg_of(const STab<T> &tb, T r,
   }
 }
 
+// seg_of for a pair distance.  The reference's derivative jumps at both end
+// knots: the makima end slope inside, the secant slope of the end interval
+// outside (spline.cpp:236-241).  In FP32, a distance within kGateBand of x0
+// or x_{n-1} therefore takes the branch that its FP64 length r64() takes, so
+// that rounding cannot move a pair onto the other side of the jump.
+template <class T, class R64> __device__ __forceinline__ int seg_of_r(const STab<T> &tb, T r, T &t, R64 &&r64) {
+  if constexpr (std::is_same_v<T, double>) {
+    return seg_of(tb, r, t);
+  } else {
+    int side = 0; // −1 lower linear, +1 upper linear, 0 makima segment
+    if (!(r > tb.lo_in && r < tb.hi_in)) {
+      if (r < tb.lo_out) side = -1;
+      else if (r > tb.hi_out) side = 1;
+      else {
+        const double q = r64();
+        side = q <= tb.x0d ? -1 : (q >= tb.xmaxd ? 1 : 0);
+      }
+    }
+    if (side < 0) {
+      t = (r - tb.x0) * tb.inv_h;
+      return tb.seg0;
+    }
+    if (side > 0) {
+      t = (r - tb.xmax) * tb.inv_h;
+      return tb.seg0 + tb.n;
+    }
+    const T u = (r - tb.x0) * tb.inv_h;
+    int i = static_cast<int>(u);
+    i = min(max(i, 0), tb.n - 2);
+    t = u - static_cast<T>(i);
+    return tb.seg0 + 1 + i;
+  }
+}
+
+// Gate and segment of a pair distance whose FP64 length r64 is at hand (the
+// residual and population kernels).  The gate and the branch are decided in
+// FP64, as the FP64 path decides them; in FP32 the local coordinate
+// t = (r − x_e)/h is also formed in FP64 and then rounded, which keeps t
+// accurate to an FP32 ulp of t rather than of r/h: on the steep repulsive
+// wall of a pair table (φ'' of a few hundred eV/Å²) an FP32 r alone would
+// put ~1e-5 eV/Å into each pair force.
+template <bool CLOSED = true, class T> __device__ __forceinline__ bool gate64(const STab<T> &tb, double r64) {
+  return CLOSED ? (r64 >= tb.x0d && r64 <= tb.xmaxd) : (r64 >= tb.x0d && r64 < tb.xmaxd);
+}
+template <class T> __device__ __forceinline__ int seg_of64(const STab<T> &tb, T r, double r64, T &t) {
+  if constexpr (std::is_same_v<T, double>) {
+    return seg_of(tb, r, t);
+  } else {
+    if (r64 <= tb.x0d) {
+      t = static_cast<T>((r64 - tb.x0d) * tb.inv_hd);
+      return tb.seg0;
+    }
+    if (r64 >= tb.xmaxd) {
+      t = static_cast<T>((r64 - tb.xmaxd) * tb.inv_hd);
+      return tb.seg0 + tb.n;
+    }
+    const double u = (r64 - tb.x0d) * tb.inv_hd;
+    int i = static_cast<int>(u);
+    i = min(max(i, 0), tb.n - 2);
+    t = static_cast<T>(u - static_cast<double>(i));
+    return tb.seg0 + 1 + i;
+  }
+}
+
 template <class T> struct Vec4T;
 template <> struct Vec4T<float> { using type = float4; };
 template <> struct Vec4T<double> { using type = double4; };
@@ -172,6 +274,30 @@ __device__ __forceinline__ VD<T> tab_vd(const STab<T> &tb, const typename Vec4T<
   }
   T t;
   const int e = seg_of(tb, r, t);
+  return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
+}
+
+// tab_vd at a pair distance: the makima branch chosen by seg_of_r.
+template <class T, bool AN, class R64>
+__device__ __forceinline__ VD<T> tab_vd_r(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
+                                          T r, R64 &&r64) {
+  if constexpr (AN) {
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
+  }
+  T t;
+  const int e = seg_of_r(tb, r, t, r64);
+  return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
+}
+
+// tab_vd at a pair distance with its FP64 length (seg_of64).
+template <class T, bool AN>
+__device__ __forceinline__ VD<T> tab_vd64(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
+                                          T r, double r64) {
+  if constexpr (AN) {
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
+  }
+  T t;
+  const int e = seg_of64(tb, r, r64, t);
   return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
 }
 
