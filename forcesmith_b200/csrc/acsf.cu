@@ -621,6 +621,13 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, int mode, 
   const int64_t M = rows_of(h, w_s);
   const int D = h->D;
   if (jac) {
+    // the Jacobian mode adds the FP64 energy and stress rows (7 × D doubles)
+    const size_t e64 = align16(static_cast<size_t>(7) * D * sizeof(double));
+    if (sm + e64 > 227 * 1024)
+      return set_error(h, FS_ERR_UNSUPPORTED,
+                       "ACSF Jacobian: " + std::to_string(sm + e64) + " bytes of shared memory for D = " +
+                           std::to_string(D) + " and " + std::to_string(h->max_natoms) +
+                           " atoms in the largest configuration (the limit is 232448)");
     const int64_t ldj = (M + 31) / 32 * 32;
     const size_t jn = static_cast<size_t>(ldj) * D;
     if (static_cast<size_t>(h->jac_alloc) != jn || h->ldj != ldj || !h->d_J || h->j_rowmajor) {
@@ -638,7 +645,7 @@ template <class T> int launch_acsf(fs_gpu *h, double w_e, double w_s, int mode, 
     FS_CUDA(cudaMemsetAsync(h->d_J, 0, std::max<size_t>(jn, 1) * sizeof(T), h->stream));
     a.J = static_cast<T *>(h->d_J);
     a.ld = ldj;
-    sm += align16(static_cast<size_t>(7) * D * sizeof(double)); // the FP64 energy and stress rows
+    sm += e64;
     // the configuration's J block in shared memory when it fits
     const size_t jb = align16(static_cast<size_t>(3 * h->max_natoms) * D * sizeof(T));
     if (D > 0 && sm + jb <= 200 * 1024) {

@@ -26,9 +26,9 @@ template <class T, class R64>
 __device__ __forceinline__ void gated(const STab<T> &tb, const typename Vec4T<T>::type *seg, T r, R64 &&r64, T &v,
                                       T &d) {
   v = d = T(0);
-  if (!gate_in(tb, r, r64)) return;
   T t;
-  const int e = seg_of_r(tb, r, t, r64);
+  const int e = gate_seg(tb, r, t, r64);
+  if (e < 0) return;
   v = seg_val<T>(seg[e], t);
   d = seg_der<T>(seg[e], t, tb.inv_h);
 }
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(256) adp_residual_kernel(AdpArgs<T> A) {
       pair_vec(wpos, shift, i, pk, j, d[0], d[1], d[2]);
       const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (r < T(1e-14)) continue;
-      const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
+      const auto r64 = [=] { return pair_len64(wpos, shift, i, pk); };
       const int tj = typ[j], pt = pair_ord(ti, tj, nt);
       T v, dv;
       gated(tabs[np + tj], seg, r, r64, v, dv);
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) adp_residual_kernel(AdpArgs<T> A) {
       pair_vec(wpos, shift, i, pk, j, d[0], d[1], d[2]);
       const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (r < T(1e-14)) continue;
-      const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
+      const auto r64 = [=] { return pair_len64(wpos, shift, i, pk); };
       const T ir = T(1) / r;
       const int tj = typ[j], pt = pair_ord(ti, tj, nt);
       T phi, dphi, rj, drj, ri, dri, u, du, w, dw;

@@ -34,7 +34,7 @@ template <class T> struct AgArgs {
   const int32_t *order; // configurations by work, heaviest first
 };
 
-template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(AgArgs<T> A) {
+template <class T> __global__ void __launch_bounds__(kAgThreads, sizeof(T) == 4 ? 3 : 1) angular_kernel(AgArgs<T> A) {
   using T4 = typename Vec4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int c = A.order ? A.order[blockIdx.x] : blockIdx.x;
@@ -78,12 +78,13 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
     const STab<T> &tb = tabs[pair_ord(typ[i], typ[j], nt)];
     const uint32_t pw = nbp[w];
-    const auto r64 = [&] { return pair_len64(wpos, shift, i, pw); };
-    const bool ok = w0 + lane < npair && r >= T(1e-14) && gate_in(tb, r, r64);
+    T tq;
+    const int eq = gate_seg(tb, r, tq, [=] { return pair_len64(wpos, shift, i, pw); });
+    const bool ok = w0 + lane < npair && r >= T(1e-14) && eq >= 0;
     if (!__any_sync(0xffffffffu, ok)) continue;
     bool hi;
     const unsigned xi = run_links(i, lane, hi);
-    const VD<T> ph = tab_vd_r<T, true>(tb, seg, A.vals, r, r64);
+    const VD<T> ph = tab_vd_at<T, true>(tb, seg, A.vals, r, eq >= 0 ? eq : tb.seg0, tq);
     const T s = ok ? ph.d / r : T(0);
     const T f[3] = {s * d[0], s * d[1], s * d[2]};
 #pragma unroll
@@ -118,15 +119,16 @@ template <class T> __global__ void __launch_bounds__(kAgThreads) angular_kernel(
     const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
     const STab<T> &rk = tabs[np + pair_ord(ti, typ[k], nt)];
     const uint32_t pwj = nbp[pj], pwk = nbp[pk];
-    const auto r64j = [&] { return pair_len64(wpos, shift, i, pwj); };
-    const auto r64k = [&] { return pair_len64(wpos, shift, i, pwk); };
-    const bool ok = w0 + lane < ntri && r1 >= T(1e-14) && gate_in(rj, r1, r64j) && r2 >= T(1e-14) &&
-                    gate_in(rk, r2, r64k);
+    T t1, t2;
+    const int e1 = gate_seg(rj, r1, t1, [=] { return pair_len64(wpos, shift, i, pwj); });
+    const int e2 = gate_seg(rk, r2, t2, [=] { return pair_len64(wpos, shift, i, pwk); });
+    const bool ok = w0 + lane < ntri && r1 >= T(1e-14) && e1 >= 0 && r2 >= T(1e-14) && e2 >= 0;
     if (!__any_sync(0xffffffffu, ok)) continue;
     bool hi, hj;
     const unsigned xi = run_links(i, lane, hi);
     const unsigned xj = run_links(pj, lane, hj); // atom j: runs of the same neighbour slot
-    const VD<T> F1 = tab_vd_r<T, true>(rj, seg, A.vals, r1, r64j), F2 = tab_vd_r<T, true>(rk, seg, A.vals, r2, r64k);
+    const VD<T> F1 = tab_vd_at<T, true>(rj, seg, A.vals, r1, e1 >= 0 ? e1 : rj.seg0, t1),
+                F2 = tab_vd_at<T, true>(rk, seg, A.vals, r2, e2 >= 0 ? e2 : rk.seg0, t2);
     // lanes without a term: zero inverse distances and c3, so every force below is zero
     const T ir1 = ok ? T(1) / r1 : T(0), ir2 = ok ? T(1) / r2 : T(0);
     const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;

@@ -143,6 +143,8 @@ void free_jacobian(fs_gpu *h) {
   dfree(h->d_drho);
   dfree(h->d_dgd);
   dfree(h->d_wsF);
+  dfree(h->d_jx);
+  h->jx_alloc = 0;
   h->jac_alloc = 0;
   h->gram_part_alloc = 0;
   h->atom_scratch_alloc = 0;
@@ -224,6 +226,7 @@ int fs_gpu_create(const fs_gpu_opts *opts, fs_gpu **out) {
     delete h;
     return FS_ERR_CUDA;
   }
+  fsg::noalloc_forget(h->device);
   *out = h;
   return FS_OK;
 }
@@ -560,6 +563,10 @@ int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D) {
   if (!h || !x) return FS_ERR_ARG;
   if (!h->have_model) return set_error(h, FS_ERR_STATE, "no model");
   if (D != h->D) return set_error(h, FS_ERR_ARG, "set_params: D mismatch");
+  for (int k = 0; k < D; ++k)
+    if (!std::isfinite(x[k]))
+      return set_error(h, FS_ERR_NUMERIC, "set_params: parameter " + std::to_string(k) +
+                                              " is not finite (the model is unchanged)");
   cudaSetDevice(h->device);
   for (HostTable &t : h->tables)
     for (int k = 0; k < t.n; ++k)
@@ -668,29 +675,8 @@ int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F, double *J
   FS_TRY(fs_gpu_eval_jacobian_async(h, w_e, w_s));
   const int64_t m = rows_of(h, w_s);
   if (F) FS_CUDA(cudaMemcpyAsync(F, h->d_F, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  if (J) {
-    // column-major m × D, from the device's padded leading dimension
-    const size_t n = static_cast<size_t>(m) * h->D;
-    if (h->precision == FS_PREC_FP64) {
-      FS_CUDA(cudaMemcpy2DAsync(J, m * sizeof(double), h->d_J, h->ldj * sizeof(double), m * sizeof(double),
-                                h->D, cudaMemcpyDeviceToHost, h->stream));
-      FS_TRY(sync(h));
-    } else if (h->j_rowmajor) { // row-major on the device (rows × ldj): transposed here
-      std::vector<float> tmp(n);
-      FS_CUDA(cudaMemcpy2DAsync(tmp.data(), h->D * sizeof(float), h->d_J, h->ldj * sizeof(float),
-                                h->D * sizeof(float), m, cudaMemcpyDeviceToHost, h->stream));
-      FS_TRY(sync(h));
-      const int64_t D = h->D;
-      for (int64_t r = 0; r < m; ++r)
-        for (int64_t c = 0; c < D; ++c) J[c * m + r] = tmp[r * D + c];
-    } else {
-      std::vector<float> tmp(n);
-      FS_CUDA(cudaMemcpy2DAsync(tmp.data(), m * sizeof(float), h->d_J, h->ldj * sizeof(float), m * sizeof(float),
-                                h->D, cudaMemcpyDeviceToHost, h->stream));
-      FS_TRY(sync(h));
-      for (size_t k = 0; k < n; ++k) J[k] = tmp[k];
-    }
-  }
+  // column-major m × D (Eigen's fjac), widened and transposed on the device
+  if (J) FS_TRY(fs_gpu_copy_jacobian_rows(h, 0, m, J, m));
   return fs_gpu_fetch_normal_equations(h, JtJ, Jtr, obj);
 }
 

@@ -672,10 +672,9 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
       pair_vec(wpos, shift, i, pk, j, dx, dy, dz);
       const T r = sqrt_t(dx * dx + dy * dy + dz * dz);
       const STab<T> &tb = tabs[np + typ[j]];
-      const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
-      if (!gate_in(tb, r, r64)) continue;
       T t;
-      const int e = seg_of_r(tb, r, t, r64);
+      const int e = gate_seg(tb, r, t, [=] { return pair_len64(wpos, shift, i, pk); });
+      if (e < 0) continue;
       rho += seg_val<T>(seg[e], t);
       const int ws = segws[e];
       const T *G = segg + e * 4 * kWin;
@@ -1000,33 +999,35 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
             v[4] = s0 * u[2];
             v[5] = s1 * u[2];
           }
-          const auto r64 = [&] { return pair_len64(wpos, shift, i, pk); };
-          auto set_slot = [&](int s, const STab<T> &tb, T rr, T wgt, T &tout) {
-            T t;
-            const int e = seg_of_r(tb, rr, t, r64);
+          const auto r64 = [=] { return pair_len64(wpos, shift, i, pk); };
+          auto set_slot = [&](int s, const STab<T> &tb, int e, T t, T wgt) {
             R.si[s] = make_int4(e * 4 * kWin, tb.cmap0 + segws[e], 0, cross);
             R.sf[s].x = t;
             R.sf[s].y = wgt * tb.inv_h;
-            tout = t;
-            return e;
           };
-          T t_;
           const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
-          const bool phi_in = EAM ? gate_in(tp, r, r64) : gate_in<false>(tp, r, r64);
-          if (phi_in) set_slot(0, tp, r, T(1), t_);
+          T tq;
+          const int ep = gate_seg<EAM>(tp, r, tq, r64);
+          if (ep >= 0) set_slot(0, tp, ep, tq, T(1));
           if constexpr (EAM) {
             const STab<T> &gj = tabs[np + tj], &gi_ = tabs[np + ti];
             const T gFj = gFa[j];
             cFj = cFa[j];
-            if (gate_in(gj, r, r64)) {
-              const int e = set_slot(1, gj, r, tj == ti ? gFi + gFj : gFi, t_);
-              dgj = seg_der<T>(seg[e], t_, gj.inv_h);
+            T tj_;
+            const int ej = gate_seg(gj, r, tj_, r64);
+            if (ej >= 0) {
+              set_slot(1, gj, ej, tj_, tj == ti ? gFi + gFj : gFi);
+              dgj = seg_der<T>(seg[ej], tj_, gj.inv_h);
             }
-            if (gate_in(gi_, r, r64)) {
-              T t;
-              const int e = seg_of_r(gi_, r, t, r64);
-              dgi = seg_der<T>(seg[e], t, gi_.inv_h);
-              if (tj != ti) set_slot(2, gi_, r, gFj, t_);
+            if (tj == ti) {
+              dgi = dgj; // the same table at the same distance
+            } else {
+              T ti_;
+              const int ei = gate_seg(gi_, r, ti_, r64);
+              if (ei >= 0) {
+                dgi = seg_der<T>(seg[ei], ti_, gi_.inv_h);
+                set_slot(2, gi_, ei, ti_, gFj);
+              }
             }
             // F_j window: coefficient dgd_j[q]·ρ'_{ti}(r)
             const STab<T> &te = tabs[np + nt + tj];
@@ -1769,15 +1770,24 @@ int launch_population_static(fs_gpu *h, double w_e, double w_s, const double *d_
   T4 *pop_seg = reinterpret_cast<T4 *>(scratch + L.seg);
   double *part = reinterpret_cast<double *>(scratch + L.part);
   const int n_tables = static_cast<int>(h->desc.size());
-  // every table is a spline here, so the table list is 0..n_tables−1; the
-  // configurations go in upload order (the order only balances the work)
-  iota_kernel<<<(h->n_cfg + 255) / 256, 256, 0, h->stream>>>(order, h->n_cfg);
+  // every table is a spline here, so the table list is 0..n_tables−1.  The
+  // configurations go heaviest first, in the order the context already keeps
+  // for its 3-body kernels (pairs + neighbour pairs per configuration, built
+  // with the neighbour lists); the order only balances the work, since the
+  // partial sums are indexed by configuration and added in a fixed order
+  if (h->d_cfg_by_work) {
+    FS_CUDA(cudaMemcpyAsync(order, h->d_cfg_by_work, h->n_cfg * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                            h->stream));
+  } else {
+    iota_kernel<<<(h->n_cfg + 255) / 256, 256, 0, h->stream>>>(order, h->n_cfg);
+    ++h->launches;
+  }
   iota_kernel<<<1, 256, 0, h->stream>>>(spl, n_tables);
   FS_CUDA(cudaGetLastError());
   dim3 g(static_cast<unsigned>(n_tables), static_cast<unsigned>(NP));
   pop_setup_kernel<T><<<g, 32, 0, h->stream>>>(h->d_desc, spl, h->d_vals, h->d_cmap, d_xs, h->D, h->n_segs, pop_seg);
   FS_CUDA(cudaGetLastError());
-  h->launches += 3;
+  h->launches += 2;
   ResArgs<T> a;
   a.c = make_common<T>(h);
   a.seg_a = nullptr;
@@ -1794,7 +1804,9 @@ int launch_population_static(fs_gpu *h, double w_e, double w_s, const double *d_
       pa.pop_seg = pop_seg;
       pa.NP = NP;
       pa.n_tiles = (NP + kPopLanes - 1) / kPopLanes;
-      pa.n_chunks = std::max(1, std::min(h->n_cfg, (4 * 148 + pa.n_tiles - 1) / pa.n_tiles));
+      // the allocating path's wave count (tuned by fs_gpu_autotune, else 4)
+      const int waves = h->tuned_pop_waves > 0 ? h->tuned_pop_waves : 4;
+      pa.n_chunks = std::max(1, std::min(h->n_cfg, (waves * 148 + pa.n_tiles - 1) / pa.n_tiles));
       pa.nseg_pd = nseg_pd;
       pa.max_atoms = h->max_natoms;
       pa.max_img = max_images(h);
@@ -1901,6 +1913,18 @@ void *g_noalloc_addr[kMaxDevices] = {};
 
 // The array's device address on h's device (looked up once per device, with
 // that device current).  The host-side symbol itself is not a device address.
+} // namespace
+
+// Forget the cached address of `device` (fs_gpu_create calls this): a
+// context created after a cudaDeviceReset looks the array up again in the
+// device's new CUDA context instead of using the old address.
+void noalloc_forget(int device) {
+  if (device < 0 || device >= kMaxDevices) return;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  g_noalloc_addr[device] = nullptr;
+}
+
+namespace {
 int noalloc_scratch(fs_gpu *h, unsigned char **out) {
   if (h->device < 0 || h->device >= kMaxDevices) return set_error(h, FS_ERR_ARG, "eval_population_noalloc: device ordinal");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1945,14 +1969,22 @@ extern "C" int fs_gpu_eval_population_noalloc(fs_gpu *h, double w_e, double w_s,
   const bool fp64 = h->precision == FS_PREC_FP64;
   const size_t need = fp64 ? noalloc_layout<double>(h, NP).total : noalloc_layout<float>(h, NP).total;
   if (need > kNoAllocScratchBytes) {
-    const size_t per_trial = fp64 ? noalloc_layout<double>(h, 2).total - noalloc_layout<double>(h, 1).total
-                                  : noalloc_layout<float>(h, 2).total - noalloc_layout<float>(h, 1).total;
-    const size_t fixed = (fp64 ? noalloc_layout<double>(h, 1).total : noalloc_layout<float>(h, 1).total) - per_trial;
-    const long long max_np = per_trial ? static_cast<long long>((kNoAllocScratchBytes - fixed) / per_trial) : 0;
+    // the largest NP whose layout fits, by bisection on the same layout the
+    // check uses (0 when not even one trial fits)
+    auto fits = [&](long long np) {
+      return (fp64 ? noalloc_layout<double>(h, static_cast<int>(np)).total
+                   : noalloc_layout<float>(h, static_cast<int>(np)).total) <= kNoAllocScratchBytes;
+    };
+    long long lo = 0, hi = NP; // fits(lo) or lo == 0; !fits(hi)
+    while (hi - lo > 1) {
+      const long long mid = lo + (hi - lo) / 2;
+      (mid > 0 && fits(mid) ? lo : hi) = mid;
+    }
+    const long long max_np = lo;
     return set_error(h, FS_ERR_ARG,
                      "eval_population_noalloc: NP = " + std::to_string(NP) + " needs " + std::to_string(need) +
                          " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
-                         " bytes (NP <= about " + std::to_string(max_np) + " for these configurations and model)");
+                         " bytes (NP <= " + std::to_string(max_np) + " for these configurations and model)");
   }
   unsigned char *scratch = nullptr;
   FS_TRY(noalloc_scratch(h, &scratch));

@@ -175,6 +175,8 @@ struct fs_gpu {
   void *d_J = nullptr;           // J, FP32 or FP64; rows rounded up to 32 (rows ≥ M are zero)
   int64_t ldj = 0;               // column-major: the padded row count; row-major: the row stride (≥ D)
   bool j_rowmajor = false;       // row-major J (FP32 EAM / pair Jacobians feeding the tensor-core JᵀJ)
+  double *d_jx = nullptr;        // FP64 column-major staging of an exported row block of J
+  size_t jx_alloc = 0;
   double *d_jtr_part = nullptr;  // per-config Jᵀr partials (FP64)
   size_t jtr_part_alloc = 0;
   double *d_half_part = nullptr; // force-row pass with two CTAs per configuration: their sums
@@ -229,6 +231,9 @@ struct fs_gpu {
 namespace fsg {
 
 int set_error(fs_gpu *h, int code, const std::string &m);
+// fs_gpu_eval_population_noalloc's cached scratch address of a device: dropped
+// when a context is created there, so a later first call looks it up again.
+void noalloc_forget(int device);
 // stream sync + the device error word of bounded waits
 int sync_checked(fs_gpu *h);
 

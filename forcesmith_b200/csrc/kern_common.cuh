@@ -82,7 +82,8 @@ __device__ __forceinline__ double pair_vec_len(const double *wpos, const double 
 }
 
 // FP64 length of pair_vec's pair vector, computed as the FP64 path computes
-// it; the FP32 kernels use it only to decide gates near a bound (gate_in).
+// it; the FP32 kernels use it only to decide a distance within a few ulps
+// of a gate bound (gate_seg).
 __device__ __forceinline__ double pair_len64(const double *wpos, const double *shift, int i, uint32_t pk) {
   const int j = static_cast<int>(pk & 0xFFFFFu);
   const int img = static_cast<int>(pk >> 20);

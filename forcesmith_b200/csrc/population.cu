@@ -173,7 +173,10 @@ __global__ void de_select_kernel(double *__restrict__ pop, double *__restrict__ 
 
 __global__ void de_advance_kernel(int64_t *gen_ctr) { *gen_ctr += 1; }
 
-__global__ void argmin_kernel(const double *__restrict__ v, int n, int *__restrict__ out) {
+// Index of the smallest of v[0..n) (lowest index on ties) into *out, and,
+// when rec is not null, that value into *rec.
+__global__ void argmin_kernel(const double *__restrict__ v, int n, int *__restrict__ out,
+                              double *__restrict__ rec = nullptr) {
   __shared__ double bv[1024];
   __shared__ int bi[1024];
   double best = INFINITY;
@@ -197,7 +200,10 @@ __global__ void argmin_kernel(const double *__restrict__ v, int n, int *__restri
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) *out = bi[0];
+  if (threadIdx.x == 0) {
+    *out = bi[0];
+    if (rec) *rec = bv[0];
+  }
 }
 
 } // namespace
@@ -210,6 +216,8 @@ struct DeState {
   double *pop = nullptr, *obj = nullptr, *trial = nullptr, *tobj = nullptr, *lo = nullptr, *hi = nullptr;
   int64_t *gen = nullptr;
   int *accepted = nullptr, *best = nullptr;
+  double *hist = nullptr; // best objective after each generation of a de_run call
+  int hist_n = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t generations = 0;
@@ -233,6 +241,7 @@ void de_free(DeState *s) {
   cudaFree(s->lo);
   cudaFree(s->hi);
   cudaFree(s->gen);
+  cudaFree(s->hist);
   cudaFree(s->accepted);
   cudaFree(s->best);
   delete s;
@@ -357,6 +366,13 @@ int de_run(fs_gpu *h, int generations, int use_graph, double *best_obj, double *
     FS_CUDA(cudaGraphInstantiate(&s->exec, g, 0));
     s->captured = graph_inputs(h);
   }
+  if (history && generations > s->hist_n) {
+    cudaFree(s->hist);
+    s->hist = nullptr;
+    s->hist_n = 0;
+    FS_CUDA(cudaMalloc(&s->hist, generations * sizeof(double)));
+    s->hist_n = generations;
+  }
   int64_t per_gen = 0;
   if (use_graph) {
     size_t nn = 0;
@@ -370,14 +386,14 @@ int de_run(fs_gpu *h, int generations, int use_graph, double *best_obj, double *
     } else {
       FS_TRY(de_generation(h, s));
     }
-    if (history) {
-      argmin_kernel<<<1, 1024, 0, h->stream>>>(s->obj, s->NP, s->best);
-      int b = 0;
-      FS_CUDA(cudaMemcpyAsync(&b, s->best, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-      FS_CUDA(cudaStreamSynchronize(h->stream));
-      FS_CUDA(cudaMemcpy(&history[g], s->obj + b, sizeof(double), cudaMemcpyDeviceToHost));
+    if (history) { // the generation's best into a device slot: no host wait per generation
+      argmin_kernel<<<1, 1024, 0, h->stream>>>(s->obj, s->NP, s->best, s->hist + g);
+      FS_CUDA(cudaGetLastError());
+      ++h->launches;
     }
   }
+  if (history && generations > 0)
+    FS_CUDA(cudaMemcpyAsync(history, s->hist, generations * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   s->generations += generations;
   argmin_kernel<<<1, 1024, 0, h->stream>>>(s->obj, s->NP, s->best);
   FS_CUDA(cudaGetLastError());

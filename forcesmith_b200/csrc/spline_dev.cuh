@@ -15,7 +15,7 @@ template <class T> struct STab {
   double inv_hd;  // FP64 1/h
   // Gate bands of the working precision: r in (lo_in, hi_in) is inside the
   // gate, r below lo_out or above hi_out is outside it, and a distance
-  // between is decided from its FP64 length (gate_in below).
+  // between is decided from its FP64 length (gate_seg below).
   T lo_in, hi_in, lo_out, hi_out;
   int n, seg0, cmap0, kind;
   int form, pv0; // analytic tables: fs_form and first parameter in the value array
@@ -132,25 +132,6 @@ template <class T> __device__ __forceinline__ bool in_span(const STab<T> &tb, T 
   return r >= tb.x0 && r <= tb.xmax;
 }
 
-// Range gate of a pair distance: closed [x0, x_{n-1}] (EAM, ADP, angular
-// radial tables; force_calculator_concept.hpp:94-118) or, when !CLOSED, the
-// pair calculator's half-open [x0, x_{n-1}) (pair_force.cpp:28).  In FP64
-// the distance r is compared directly.  In FP32, r carries a few ulps of
-// rounding, so a distance within kGateBand of a bound is decided from its
-// FP64 length r64() instead: the FP32 and FP64 paths then keep the same
-// pairs, and a pair at the cut-off is never dropped by rounding alone.
-template <bool CLOSED = true, class T, class R64>
-__device__ __forceinline__ bool gate_in(const STab<T> &tb, T r, R64 &&r64) {
-  if constexpr (std::is_same_v<T, double>) {
-    return CLOSED ? (r >= tb.x0 && r <= tb.xmax) : (r >= tb.x0 && r < tb.xmax);
-  } else {
-    if (r > tb.lo_in && r < tb.hi_in) return true;
-    if (r < tb.lo_out || r > tb.hi_out) return false;
-    const double q = r64();
-    return CLOSED ? (q >= tb.x0d && q <= tb.xmaxd) : (q >= tb.x0d && q < tb.xmaxd);
-  }
-}
-
 // Extended segment of r and its local coordinate t = (r - origin)/h, with the
 // reference's branch order (spline.cpp:215-252): r <= x0 → lower linear,
 // r >= x_{n-1} → upper linear, else the interval of upper_bound − 1
@@ -175,40 +156,6 @@ template <class T> __device__ __forceinline__ int seg_of(const STab<T> &tb, T r,
     t = (r - xi) / tb.hd;
     return tb.seg0 + 1 + i;
   } else {
-    const T u = (r - tb.x0) * tb.inv_h;
-    int i = static_cast<int>(u);
-    i = min(max(i, 0), tb.n - 2);
-    t = u - static_cast<T>(i);
-    return tb.seg0 + 1 + i;
-  }
-}
-
-// seg_of for a pair distance.  The reference's derivative jumps at both end
-// knots: the makima end slope inside, the secant slope of the end interval
-// outside (spline.cpp:236-241).  In FP32, a distance within kGateBand of x0
-// or x_{n-1} therefore takes the branch that its FP64 length r64() takes, so
-// that rounding cannot move a pair onto the other side of the jump.
-template <class T, class R64> __device__ __forceinline__ int seg_of_r(const STab<T> &tb, T r, T &t, R64 &&r64) {
-  if constexpr (std::is_same_v<T, double>) {
-    return seg_of(tb, r, t);
-  } else {
-    int side = 0; // −1 lower linear, +1 upper linear, 0 makima segment
-    if (!(r > tb.lo_in && r < tb.hi_in)) {
-      if (r < tb.lo_out) side = -1;
-      else if (r > tb.hi_out) side = 1;
-      else {
-        const double q = r64();
-        side = q <= tb.x0d ? -1 : (q >= tb.xmaxd ? 1 : 0);
-      }
-    }
-    if (side < 0) {
-      t = (r - tb.x0) * tb.inv_h;
-      return tb.seg0;
-    }
-    if (side > 0) {
-      t = (r - tb.xmax) * tb.inv_h;
-      return tb.seg0 + tb.n;
-    }
     const T u = (r - tb.x0) * tb.inv_h;
     int i = static_cast<int>(u);
     i = min(max(i, 0), tb.n - 2);
@@ -247,6 +194,58 @@ template <class T> __device__ __forceinline__ int seg_of64(const STab<T> &tb, T 
   }
 }
 
+// Gate and segment of a pair distance in one step, for kernels without the
+// FP64 length at hand: the extended segment of r (and t), or −1 when r is
+// outside the gate (closed [x0, x_{n-1}] for EAM, ADP and angular radial
+// tables, force_calculator_concept.hpp:94-118; half-open [x0, x_{n-1}) for
+// the pair calculator when !CLOSED, pair_force.cpp:28).  An FP32 distance
+// carries a few ulps of rounding, so one within kGateBand of either end is
+// decided by its FP64 length r64(): the gate as the FP64 path decides it,
+// and the branch too, since the reference's derivative jumps at both end
+// knots (makima end slope inside, the end interval's secant slope outside,
+// spline.cpp:236-241).  Distances away from the ends take the direct path.
+// Outside the gate t is set to 0.
+template <bool CLOSED, class T, class R64>
+__device__ __noinline__ int gate_seg_edge(const STab<T> &tb, T r, T &t, R64 r64) {
+  t = T(0);
+  if (r < tb.lo_out || r > tb.hi_out) return -1;
+  const double q = r64();
+  if (q < tb.x0d || (CLOSED ? q > tb.xmaxd : q >= tb.xmaxd)) return -1;
+  if (q <= tb.x0d) {
+    t = (r - tb.x0) * tb.inv_h;
+    return tb.seg0;
+  }
+  if (q >= tb.xmaxd) {
+    t = (r - tb.xmax) * tb.inv_h;
+    return tb.seg0 + tb.n;
+  }
+  const T u = (r - tb.x0) * tb.inv_h;
+  int i = static_cast<int>(u);
+  i = min(max(i, 0), tb.n - 2);
+  t = u - static_cast<T>(i);
+  return tb.seg0 + 1 + i;
+}
+
+template <bool CLOSED = true, class T, class R64>
+__device__ __forceinline__ int gate_seg(const STab<T> &tb, T r, T &t, R64 &&r64) {
+  if constexpr (std::is_same_v<T, double>) {
+    if (!(CLOSED ? (r >= tb.x0 && r <= tb.xmax) : (r >= tb.x0 && r < tb.xmax))) {
+      t = T(0);
+      return -1;
+    }
+    return seg_of(tb, r, t);
+  } else {
+    if (r > tb.lo_in && r < tb.hi_in) {
+      const T u = (r - tb.x0) * tb.inv_h;
+      int i = static_cast<int>(u);
+      i = min(max(i, 0), tb.n - 2);
+      t = u - static_cast<T>(i);
+      return tb.seg0 + 1 + i;
+    }
+    return gate_seg_edge<CLOSED>(tb, r, t, r64);
+  }
+}
+
 template <class T> struct Vec4T;
 template <> struct Vec4T<float> { using type = float4; };
 template <> struct Vec4T<double> { using type = double4; };
@@ -277,18 +276,6 @@ __device__ __forceinline__ VD<T> tab_vd(const STab<T> &tb, const typename Vec4T<
   return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
 }
 
-// tab_vd at a pair distance: the makima branch chosen by seg_of_r.
-template <class T, bool AN, class R64>
-__device__ __forceinline__ VD<T> tab_vd_r(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
-                                          T r, R64 &&r64) {
-  if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
-  }
-  T t;
-  const int e = seg_of_r(tb, r, t, r64);
-  return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
-}
-
 // tab_vd at a pair distance with its FP64 length (seg_of64).
 template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd64(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
@@ -298,6 +285,17 @@ __device__ __forceinline__ VD<T> tab_vd64(const STab<T> &tb, const typename Vec4
   }
   T t;
   const int e = seg_of64(tb, r, r64, t);
+  return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
+}
+
+// Value and d/dr at r from gate_seg's segment e and t (analytic tables,
+// when AN, from their closed form).
+template <class T, bool AN>
+__device__ __forceinline__ VD<T> tab_vd_at(const STab<T> &tb, const typename Vec4T<T>::type *seg,
+                                           const double *vals, T r, int e, T t) {
+  if constexpr (AN) {
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
+  }
   return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
 }
 

@@ -28,8 +28,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                : "memory");
 }
 
-// Bounded wait on an mbarrier phase; false when the cycle budget runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase; false when the cycle budget runs out
+// (kWaitCycles unless a shorter budget is given).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long budget = kWaitCycles) {
   const uint32_t a = smem_u32(bar);
   const long long t0 = clock64();
   while (true) {
@@ -44,7 +45,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > budget) return false;
   }
 }
 

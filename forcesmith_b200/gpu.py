@@ -48,6 +48,8 @@ def lib() -> C.CDLL:
         L.fs_gpu_eval.argtypes = [vp, dbl, dbl, pd, pd, pd, pd, pd, pd]
         L.fs_gpu_eval_jacobian.argtypes = [vp, dbl, dbl, pd, pd, pd, pd, pd]
         L.fs_gpu_eval_jacobian_async.argtypes = [vp, dbl, dbl]
+        L.fs_gpu_copy_jacobian_rows.argtypes = [vp, i64, i64, pd, i64]
+        L.fs_gpu_check_bounded_wait.argtypes = [vp, i64]
         L.fs_gpu_fetch_normal_equations.argtypes = [vp, pd, pd, pd]
         L.fs_gpu_lm_step.argtypes = [vp, dbl, i32, pd]
         L.fs_gpu_lsq_step.argtypes = [vp, dbl, pd]
@@ -107,6 +109,10 @@ class GpuSession(Session):
         except Exception:
             pass
 
+    def last_error(self) -> str:
+        """fs_gpu_last_error: the context's last error message."""
+        return _err(self._h)
+
     @property
     def stream(self) -> int:
         s = C.c_void_p()
@@ -134,6 +140,16 @@ class GpuSession(Session):
                                             C.byref(obj))
         self._check(rc, "eval_jacobian")
         return dict(F=F, J=None if J is None else J.T, JtJ=JtJ, Jtr=Jtr, obj=obj.value)
+
+    def jacobian_rows(self, row0, nrows, ld=None):
+        """fs_gpu_copy_jacobian_rows: rows [row0, row0 + nrows) of the last
+        Jacobian as an FP64 (nrows × D) array, from a column-major block of
+        leading dimension ld (default nrows)."""
+        ld = nrows if ld is None else ld
+        buf = np.full((self.D, ld), np.nan)  # column-major ld × D
+        self._check(self._lib.fs_gpu_copy_jacobian_rows(self._h, int(row0), int(nrows), _dp(buf), int(ld)),
+                    "copy_jacobian_rows")
+        return buf[:, :nrows].T, buf
 
     def jacobian_async(self, w_e=1.0, w_s=0.0):
         self._check(self._lib.fs_gpu_eval_jacobian_async(self._h, w_e, w_s), "eval_jacobian_async")

@@ -220,6 +220,18 @@ int fs_gpu_eval(fs_gpu *h, double w_e, double w_s, double *F, double *forces,
 int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F,
                          double *J, double *JtJ, double *Jtr, double *obj);
 
+/*
+ * Rows [row0, row0 + nrows) of the last evaluated Jacobian, FP64, into a
+ * host column-major block: element (row0 + r, c) goes to J[c·ldJ + r]
+ * (ldJ ≥ nrows).  With J = fjac.data() + row0 and ldJ = m this fills one
+ * configuration's row block of Eigen's column-major `fjac`, as
+ * ForceCalculator::eval_cached_jacobian does per configuration
+ * (include/forcesmith/force/force_calculator.hpp:62-159, called from
+ * df_cached_analytic, src/optimization/forcesmith_functor.cpp:111-132).
+ * The widening to FP64 and the transpose run on the device.  Synchronous.
+ */
+int fs_gpu_copy_jacobian_rows(fs_gpu *h, int64_t row0, int64_t nrows, double *J, int64_t ldJ);
+
 /* Device-resident variant: enqueues residual + Jacobian + JᵀJ + Jᵀr on the
  * context stream and returns without synchronising.  Results stay on the
  * device (fetch them with fs_gpu_fetch_normal_equations). */
@@ -261,6 +273,28 @@ int fs_gpu_copy_normal_equations(fs_gpu *h, void *dst_device);
 int fs_gpu_set_profiling(fs_gpu *h, int32_t max_steps);
 int fs_gpu_phase_times(fs_gpu *h, double *ms, int32_t n, int32_t *steps);
 int fs_gpu_launch_count(fs_gpu *h, int64_t *count);
+
+/*
+ * Failure detection (no reference counterpart: the reference has no device
+ * waits).  Every wait inside this library's kernels has a cycle budget
+ * (about 2 s); a wait that runs out sets the context's device error word,
+ * the kernel returns, and the next synchronising call returns
+ * FS_ERR_DEVICE, after which the context stays usable.
+ * fs_gpu_check_bounded_wait exercises that path: one CTA waits, with a
+ * budget of `cycles` (1 … 4e9) and the kernels' own wait routine, on a
+ * barrier phase that never completes and has no copy or MMA bound to it.
+ * It returns FS_ERR_DEVICE when the wait gave up and reported, as designed.
+ *
+ * Non-finite input: fs_gpu_set_params refuses a vector with a NaN or
+ * infinite entry (FS_ERR_NUMERIC; the model keeps its previous values).
+ * The population entry points evaluate rows as given: a non-finite entry
+ * reaches the objective through the spline segments it enters (as in the
+ * reference), so its row's objective turns non-finite when a pair reaches
+ * them, and other rows are unaffected.  fs_gpu_lm_step refuses λ < 0
+ * (FS_ERR_ARG) and returns FS_ERR_NUMERIC when JᵀJ + λ·diag is not
+ * positive definite.
+ */
+int fs_gpu_check_bounded_wait(fs_gpu *h, int64_t cycles);
 
 /*
  * Batched objective: obj[k] = ‖F(x_k)‖² for NP parameter vectors xs[NP·D]
@@ -306,7 +340,9 @@ int fs_gpu_autotune(fs_gpu *h, double w_e, double w_s, fs_tune_report *report);
  * with FS_ERR_ARG and a message giving the largest NP that fits (about 1000
  * trials for 500 configurations of a 12-table EAM model in FP32).
  *
- * Results equal fs_gpu_eval_population's (same kernels).  The call is
+ * Results equal fs_gpu_eval_population's (same kernels; configurations are
+ * taken heaviest first, in the order the context keeps from its neighbour
+ * lists, with the autotuned CTA waves).  The call is
  * asynchronous on the context's stream (fs_gpu_get_stream): obj_dev is ready
  * once that stream reaches it.  The context must have been prepared
  * (fs_gpu_prepare) with its configurations and model; EAM or pair family,
@@ -314,7 +350,9 @@ int fs_gpu_autotune(fs_gpu *h, double w_e, double w_s, fs_tune_report *report);
  *
  * The first call on each GPU looks up the array's device address (a
  * runtime query, no allocation); make that first call before any stream
- * capture.  All calls in the process share the one array and it keeps the
+ * capture.  fs_gpu_create drops the looked-up address of its device, so
+ * after a cudaDeviceReset (which invalidates every existing context) the
+ * first call of a newly created context looks it up again.  All calls in the process share the one array and it keeps the
  * previous call's contents; every byte a call reads it has written first,
  * so nothing needs clearing, but two calls whose kernels overlap on the
  * same GPU (two contexts, two streams) race on it — serialise them.
@@ -338,7 +376,7 @@ int fs_gpu_eval_population_noalloc(fs_gpu *h, double w_e, double w_s,
  * fs_gpu_upload_configs / fs_gpu_set_model discards the DE state.
  * fs_gpu_de_run: `generations` more generations; writes the best objective
  * and vector, and when history != NULL the best objective after each
- * generation (that adds one host sync per generation).
+ * generation (recorded on the device, copied back once at the end).
  * fs_gpu_de_population: copies the population (NP·D) and its objectives.
  */
 typedef struct fs_de_opts {

@@ -30,7 +30,10 @@ from forcesmith_b200 import synth  # noqa: E402
 from forcesmith_b200.io import read_setfl  # noqa: E402
 from oracle import api as O  # noqa: E402
 
-SETFL = os.environ.get("AL99_SETFL", "/root/reference/data/Al99.eam.alloy")
+# The reference's data/Al99.eam.alloy; give its path in AL99_SETFL, or the
+# Forcesmith source tree in FORCESMITH_SRC.
+SETFL = os.environ.get("AL99_SETFL") or os.path.join(os.environ.get("FORCESMITH_SRC", ""), "data",
+                                                      "Al99.eam.alloy")
 
 
 def main():

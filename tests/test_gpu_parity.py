@@ -445,3 +445,37 @@ def test_autotune_keeps_results(ternary_small, precision):
     np.testing.assert_allclose(ja["JtJ"], jb["JtJ"], rtol=tol if precision == "fp64" else 1e-3,
                                atol=(1e-12 if precision == "fp64" else 1e-3) * np.abs(jb["JtJ"]).max())
     np.testing.assert_allclose(pa, pb, rtol=tol)
+
+
+@pytest.mark.parametrize("precision,family", [("fp32", "eam"), ("fp64", "eam"), ("fp32", "sw")])
+def test_copy_jacobian_rows(ternary_small, precision, family):
+    """fs_gpu_copy_jacobian_rows (the row block a cached-Jacobian calculator
+    writes per configuration into Eigen's column-major fjac): every
+    configuration's block, copied into a larger leading dimension, equals
+    the matching rows of fs_gpu_eval_jacobian's J, bit for bit.  Layouts:
+    FP32 EAM row-major on the device, FP64 column-major, FP32 SW
+    column-major.  Rows past the residual count are refused."""
+    if family == "eam":
+        ds, _, model = ternary_small
+        w_s = 0.1
+    else:
+        from tests.helpers import small_diamond
+        ds = label(small_diamond(3, (2, 3), seed=31), synth.sw_model(), O.Oracle, 1.0, 0.2)
+        model, w_s = synth.sw_start_model(), 0.2
+    g = _gpu(precision)
+    g.upload(ds)
+    g.set_model(model)
+    J = g.jacobian(1.0, w_s)["J"]
+    m = J.shape[0]
+    extra = 2 + (6 if w_s > 0 else 0)
+    r0 = 0
+    for n in ds.natoms:
+        rows = 3 * int(n) + extra
+        blk, buf = g.jacobian_rows(r0, rows, ld=rows + 5)
+        assert np.array_equal(blk, J[r0:r0 + rows])
+        assert np.all(np.isnan(buf[:, rows:]))  # nothing written past the block
+        r0 += rows
+    assert r0 == m
+    from forcesmith_b200.abi import FsError
+    with pytest.raises(FsError):
+        g.jacobian_rows(m - 2, 3)

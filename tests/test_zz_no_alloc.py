@@ -7,7 +7,10 @@ Checked through the C ABI against fs_gpu_eval_population on the same trial
 vectors, twice in a row with different sizes (the array keeps the previous
 call's contents; a call must not depend on them): the two entry points run
 the same kernels, so the bar is relative 1e-12.  Too large an NP is refused
-with an error that states the limit.
+with an error that states the limit, and that limit itself is accepted.
+The call allocates nothing: on a fresh context (whose allocating population
+buffers do not exist yet) the device's free memory is the same before and
+after it.
 
 This file sorts last so that a run stopping at its first failure has already
 run every other test.
@@ -72,3 +75,47 @@ def test_noalloc_rejects_oversized_population(data):
     with pytest.raises(FsError) as e:
         g.eval_population_noalloc(xs_t.data_ptr(), NP, obj_t.data_ptr())
     assert "maximum" in str(e.value)
+
+
+def test_noalloc_allocates_nothing(data):
+    """Free device memory (cudaMemGetInfo) is unchanged across the first
+    no-alloc call of a fresh context.  A first context runs the call once so
+    that module loading and the address lookup are behind us."""
+    import torch
+    ds, start = data
+    warm = _session(ds, start, "fp32")
+    x0 = warm.gather_params()
+    xs = np.stack([x0 * synth.uniform(x0.size, 0.97, 1.03, 77 + k) for k in range(16)])
+    want = _noalloc(warm, xs, 1.0, 0.1)
+    g = _session(ds, start, "fp32")
+    xs_t = torch.from_numpy(xs).cuda()
+    obj_t = torch.zeros(xs.shape[0], dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    g.eval_population_noalloc(xs_t.data_ptr(), xs.shape[0], obj_t.data_ptr(), 1.0, 0.1)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    np.testing.assert_allclose(obj_t.cpu().numpy(), want, rtol=1e-12, atol=0.0)
+
+
+def test_noalloc_limit_in_message_is_exact(data):
+    """The NP the refusal names is the largest that fits: it is accepted, and
+    one more is refused."""
+    import re
+    import torch
+    ds, start = data
+    g = _session(ds, start, "fp32")
+    NP = 20000
+    xs_t = torch.zeros((NP + 1, g.D), dtype=torch.float64, device="cuda")
+    obj_t = torch.zeros(NP + 1, dtype=torch.float64, device="cuda")
+    with pytest.raises(FsError) as e:
+        g.eval_population_noalloc(xs_t.data_ptr(), NP, obj_t.data_ptr())
+    lim = int(re.search(r"NP <= (\d+)", str(e.value)).group(1))
+    assert 0 < lim < NP
+    xs_t[:lim] = torch.from_numpy(g.gather_params()).cuda()
+    g.eval_population_noalloc(xs_t.data_ptr(), lim, obj_t.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.isfinite(obj_t[:lim]).all()
+    with pytest.raises(FsError):
+        g.eval_population_noalloc(xs_t.data_ptr(), lim + 1, obj_t.data_ptr())
