@@ -67,6 +67,10 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=50,
                    help="configurations in the CPU central-difference sample of cpu_baseline")
     p.add_argument("--small", action="store_true", help="small case for profiler captures")
+    p.add_argument("--leg", default="all", choices=["all", "de"],
+                   help="de: only the DE and surrogate legs (profiler captures of their kernels)")
+    p.add_argument("--surrogate-seeds", type=int, default=len(SURROGATE_SEEDS),
+                   help="seeds of the surrogate comparison (the first N of 11, 12, 13)")
     p.add_argument("--de-generations", type=int, default=200,
                    help="generations of the DE and surrogate-screened DE legs (0: skip them)")
     return p.parse_args()
@@ -236,7 +240,7 @@ def jacobian_to_host_leg(g, x, M, D, steps=5):
                     "transposed on the device) and F into pageable host memory"}
 
 
-def de_legs(local, generations):
+def de_legs(local, generations, seeds=SURROGATE_SEEDS, cpu=True):
     """Batched DE on the 200-configuration set (32-512 atoms, NP = 15 D):
     throughput of the population objective, then the surrogate comparison -
     wall time of plain device DE over `generations` generations against the
@@ -280,11 +284,11 @@ def de_legs(local, generations):
           "roofline": {"bound": "fp32", "achieved": flops / 1e12, "peak": fp32_peak / 1e12,
                        "unit": "TFLOP/s", "frac": flops / fp32_peak, "peak_source": "nominal",
                        "algorithmic": "60 FLOP per pair-trial"}}
-    if generations <= 0:
+    if generations <= 0 or not seeds:
         g.close()
         return de, None
     runs = []
-    for seed in SURROGATE_SEEDS:
+    for seed in seeds:
         # plain DE, device-resident, graph replay: wall time of `generations`
         # generations, with the best objective after each one
         g.de_init(lb, ub, x0=x, NP=NP, seed=seed)
@@ -324,14 +328,15 @@ def de_legs(local, generations):
     pop = g.de_population()[0]
     g.close()
     sur = {"plain_generations": generations, "target": "plain final objective x 1.01",
-           "seeds": list(SURROGATE_SEEDS),
+           "seeds": list(seeds),
            "wall_ratio": float(np.median([r["wall_ratio"] for r in runs])),
            "wall_ratio_vs_plain_time_to_target": float(np.median(
                [r["wall_ratio_vs_plain_time_to_target"] for r in runs])),
            "all_reached": all(r["screened_reached"] for r in runs), "runs": runs,
            "model": "BF16 MLP D->256->256->1 (GELU, Adam lr 1e-3), 4 candidates per member, "
                     "warm start 5 generations, Spearman gate 0.8 on a 10% held-out slice"}
-    de["cpu_baseline"] = cpu_de_generation(ds, start, pop)
+    if cpu:
+        de["cpu_baseline"] = cpu_de_generation(ds, start, pop)
     return de, sur
 
 
@@ -682,6 +687,17 @@ def run_reference(args):
     return 0
 
 
+def run_de_only(args):
+    """The DE and surrogate legs alone on one GPU (profiler captures)."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    seeds = SURROGATE_SEEDS[:max(0, args.surrogate_seeds)]
+    de, sur = de_legs(local, args.de_generations, seeds, cpu=not args.no_cpu_baseline)
+    print(json.dumps({"de": de, "surrogate": sur}))
+    return 0
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -834,7 +850,7 @@ def run_ours(args):
         line["acsf"] = acsf_leg(local)
         line["al99_fit"] = al99_leg(local)
     if rank == 0 and world == 1 and not args.small and args.de_generations >= 0:
-        de, sur = de_legs(local, args.de_generations)
+        de, sur = de_legs(local, args.de_generations, SURROGATE_SEEDS[:max(0, args.surrogate_seeds)])
         line["de"] = de
         if sur is not None:
             line["surrogate"] = sur
@@ -852,6 +868,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.leg == "de":
+        return run_de_only(args)
     return run_ours(args)
 
 
