@@ -29,11 +29,17 @@ FS_TABLE_ACSF, FS_TABLE_LINEAR_HEAD, FS_TABLE_STANDARDIZATION = 5, 6, 7
 TERSOFF_FIELDS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S", "omega")
 FS_PREC_FP32, FS_PREC_FP64 = 0, 1
 
-FORMS = {
+FORMS = {  # name: (fs_form id, parameter count), analytic_potential.hpp:801-806
     "lj": (0, 2), "morse": (1, 3), "exp_decay": (2, 2), "sqrt": (3, 2),
     "power_decay": (4, 2), "mexp_decay": (5, 3), "harmonic": (6, 2),
     "exp_plus": (7, 3), "parabola": (8, 3), "const": (9, 1),
     "buckingham": (10, 3), "born": (11, 5),
+    "universal": (12, 4), "eopp": (13, 6), "eopp_exp": (14, 6), "meopp": (15, 7),
+    "gen_lj": (16, 5), "double_morse": (17, 7), "double_exp": (18, 5), "mishin": (19, 6),
+    "poly5": (20, 5), "stiweb_2": (21, 6), "stiweb_3": (22, 2), "tersoff": (23, 11),
+    "tersoff_mix": (24, 2), "tersoff_mod": (25, 16), "kawamura": (26, 9),
+    "kawamura_mix": (27, 12), "softshell": (28, 2), "strmm": (29, 5),
+    "lj_sc": (30, 3), "morse_sc": (31, 4), "exp_decay_sc": (32, 3), "eopp_sc": (33, 7),
 }
 
 

@@ -40,20 +40,49 @@ SYMBOLS = (
 Z_OF = {s: z + 1 for z, s in enumerate(SYMBOLS)}
 
 # analytic form names (and aliases) and parameter names, as the reference spells them
-FORM_SPEC = {
-    "lj": ("lj", ("epsilon", "sigma")), "pair_lj": ("lj", ("epsilon", "sigma")),
-    "morse": ("morse", ("De", "a", "re")),
-    "exp_decay": ("exp_decay", ("A", "B")), "exp": ("exp_decay", ("A", "B")),
-    "sqrt": ("sqrt", ("A", "B")),
-    "power_decay": ("power_decay", ("A", "n")), "power": ("power_decay", ("A", "n")),
-    "mexp_decay": ("mexp_decay", ("A", "B", "r0")), "mexp": ("mexp_decay", ("A", "B", "r0")),
-    "harmonic": ("harmonic", ("k", "r0")),
-    "exp_plus": ("exp_plus", ("A", "B", "C")), "expplus": ("exp_plus", ("A", "B", "C")),
-    "parabola": ("parabola", ("A", "B", "C")),
-    "const": ("const", ("C",)),
-    "buckingham": ("buckingham", ("A", "rho", "C")), "buck": ("buckingham", ("A", "rho", "C")),
-    "born": ("born", ("A", "B", "C", "D", "E")),
+_TERSOFF_P = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S")
+_EOPP_P = ("A", "n", "B", "m", "k", "phi")
+_KAW_P = ("A", "B", "C", "D", "E", "F", "G", "H", "I")
+# canonical name: (aliases, parameter names), analytic_potential.hpp:304-806
+_FORMS = {
+    "lj": (("pair_lj",), ("epsilon", "sigma")),
+    "morse": ((), ("De", "a", "re")),
+    "exp_decay": (("exp",), ("A", "B")),
+    "sqrt": ((), ("A", "B")),
+    "power_decay": (("power",), ("A", "n")),
+    "mexp_decay": (("mexp",), ("A", "B", "r0")),
+    "harmonic": ((), ("k", "r0")),
+    "exp_plus": (("expplus",), ("A", "B", "C")),
+    "parabola": ((), ("A", "B", "C")),
+    "const": ((), ("C",)),
+    "buckingham": (("buck",), ("A", "rho", "C")),
+    "born": ((), ("A", "B", "C", "D", "E")),
+    "universal": ((), ("E0", "a", "b", "c")),
+    "eopp": ((), _EOPP_P),
+    "eopp_exp": (("eopp_exp_",), ("A", "B", "C", "m", "k", "phi")),
+    "meopp": ((), ("A", "n", "B", "m", "k", "phi", "r0")),
+    "gen_lj": (("genlj",), ("A", "n", "m", "r0", "B")),
+    "double_morse": (("dbl_morse",), ("D1", "a1", "r1", "D2", "a2", "r2", "C")),
+    "double_exp": (("dbl_exp",), ("A", "B", "r1", "C", "r2")),
+    "mishin": ((), ("A", "B", "C", "r0", "n", "d")),
+    "poly5": ((), ("a0", "a1", "a2", "a3", "a4")),
+    "stiweb_2": (("sw2",), ("A", "B", "p", "q", "delta", "rc")),
+    "stiweb_3": (("sw3",), ("gamma", "a")),
+    "tersoff": (("tersoff_pot",), _TERSOFF_P),
+    "tersoff_mix": ((), ("chi", "omega")),
+    "tersoff_mod": (("tmod",), _TERSOFF_P + ("c1", "c2", "c3", "c4", "c5")),
+    "kawamura": ((), _KAW_P),
+    "kawamura_mix": ((), _KAW_P + ("J", "K", "L")),
+    "softshell": (("soft",), ("A", "n")),
+    "strmm": ((), ("A", "B", "C", "D", "E")),
+    "lj_sc": (("pair_lj_sc",), ("epsilon", "sigma", "h")),
+    "morse_sc": ((), ("De", "a", "re", "h")),
+    "exp_decay_sc": (("exp_sc",), ("A", "B", "h")),
+    "eopp_sc": ((), _EOPP_P + ("h",)),
 }
+# every spelling the reference accepts: name or alias → (canonical name, parameter names)
+FORM_SPEC = {alias: (canon, names) for canon, (aliases, names) in _FORMS.items()
+             for alias in (canon,) + aliases}
 FORM_NAME = {FORMS[canon][0]: canon for canon, _ in FORM_SPEC.values()}
 PARAM_NAMES = {FORMS[canon][0]: names for canon, names in FORM_SPEC.values()}
 SW_FIELDS = ("A", "B", "p", "q", "delta", "a1", "gamma", "a2")

@@ -51,7 +51,7 @@ def lib():
                                       C.POINTER(C.c_double)]
         L.orc_form_eval.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_int32, C.c_double,
                                     C.POINTER(C.c_double), C.POINTER(C.c_double),
-                                    C.POINTER(C.c_double)]
+                                    C.POINTER(C.c_double), C.c_double]
         L.orc_pbc.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double),
                               C.POINTER(C.c_double), C.POINTER(C.c_double),
                               C.POINTER(C.c_double)]
@@ -174,11 +174,14 @@ def spline_grad(x, y, r):
     return gv, gd, gdd
 
 
-def form_eval(form, params, r):
+def form_eval(form, params, r, rmax=0.0):
+    """Value, d/dr, d²/dr² and the parameter partials ∂v/∂θ, ∂²v/∂r∂θ of an
+    analytic form at r; rmax is the table's upper gate bound (the switching
+    point of the smooth-cutoff forms)."""
     p = np.ascontiguousarray(params, np.float64)
     out = np.zeros(3)
     g, dg = np.zeros(p.size), np.zeros(p.size)
-    rc = lib().orc_form_eval(form, _dp(p), p.size, r, _dp(out), _dp(g), _dp(dg))
+    rc = lib().orc_form_eval(form, _dp(p), p.size, r, _dp(out), _dp(g), _dp(dg), rmax)
     if rc != FS_OK:
         raise FsError(rc, "orc_form_eval")
     return out, g, dg

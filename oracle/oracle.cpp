@@ -77,13 +77,13 @@ struct Table {
     return r >= a && r <= b;
   }
   double eval(double r) const {
-    return kind == FS_TABLE_SPLINE ? sp.eval(r) : form_eval(form, v.data(), n, r, false).v;
+    return kind == FS_TABLE_SPLINE ? sp.eval(r) : form_eval(form, v.data(), n, r, false, rmax).v;
   }
   double deriv(double r) const {
-    return kind == FS_TABLE_SPLINE ? sp.deriv(r) : form_eval(form, v.data(), n, r, false).d;
+    return kind == FS_TABLE_SPLINE ? sp.deriv(r) : form_eval(form, v.data(), n, r, false, rmax).d;
   }
   double deriv2(double r) const {
-    return kind == FS_TABLE_SPLINE ? sp.deriv2(r) : form_eval(form, v.data(), n, r, false).d2;
+    return kind == FS_TABLE_SPLINE ? sp.deriv2(r) : form_eval(form, v.data(), n, r, false, rmax).d2;
   }
   // ∂v/∂θ, ∂v'/∂θ (and ∂v''/∂θ for splines) over the FREE parameters.
   void grad(double r, double *gv, double *gd, double *gdd = nullptr) const {
@@ -94,7 +94,7 @@ struct Table {
     if (kind == FS_TABLE_SPLINE) {
       spline_param_grad(sp, dS, r, bv.data(), bd.data(), gdd ? bdd.data() : nullptr);
     } else {
-      FormEval f = form_eval(form, v.data(), n, r, true);
+      FormEval f = form_eval(form, v.data(), n, r, true, rmax);
       for (int k = 0; k < n; ++k) {
         bv[k] = f.g[k];
         bd[k] = f.dg[k];
@@ -1700,9 +1700,9 @@ int orc_spline_grad(const double *x, const double *y, int32_t n, double r, doubl
   return FS_OK;
 }
 int orc_form_eval(int32_t form, const double *params, int32_t np, double r, double *out3,
-                  double *g, double *dg) {
+                  double *g, double *dg, double rmax) {
   if (form_nparams(form) != np || !params || !out3) return FS_ERR_ARG;
-  FormEval f = form_eval(form, params, np, r, g || dg);
+  FormEval f = form_eval(form, params, np, r, g || dg, rmax);
   out3[0] = f.v;
   out3[1] = f.d;
   out3[2] = f.d2;

@@ -501,28 +501,64 @@ inline HD hsqrt(HD x) {
   return lift(x, s, 0.5 / s, -0.25 / (s * x.a));
 }
 inline HD hlog(HD x) { return lift(x, std::log(x.a), 1.0 / x.a, -1.0 / (x.a * x.a)); }
-inline HD hpow(HD x, HD p) { return hexp(p * hlog(x)); }
+inline HD hcos(HD x) { return lift(x, std::cos(x.a), -std::sin(x.a), -std::cos(x.a)); }
+// min / max: the selected operand, derivatives included (ties take x)
+inline HD hmin(HD x, HD y) { return x.a <= y.a ? x : y; }
+inline HD hmax(HD x, HD y) { return x.a >= y.a ? x : y; }
+// x^p for a variable exponent: the value is std::pow, so a negative base with
+// an integral exponent keeps its value; ln x enters only through the
+// exponent's own derivative parts.
+inline HD hpow(HD x, HD p) {
+  const double v = std::pow(x.a, p.a);
+  const double fx = p.a * std::pow(x.a, p.a - 1.0);
+  const double fxx = p.a * (p.a - 1.0) * std::pow(x.a, p.a - 2.0);
+  HD o{v, fx * x.b, fx * x.c, fx * x.d + fxx * x.b * x.c};
+  if (p.b != 0.0 || p.c != 0.0 || p.d != 0.0) {
+    const double L = std::log(x.a);
+    const double fp = v * L, fpp = v * L * L, fxp = std::pow(x.a, p.a - 1.0) * (1.0 + p.a * L);
+    o.b += fp * p.b;
+    o.c += fp * p.c;
+    o.d += fp * p.d + fxp * (x.b * p.c + p.b * x.c) + fpp * p.b * p.c;
+  }
+  return o;
+}
 inline HD hpowc(HD x, double p) {
   const double v = std::pow(x.a, p);
   return lift(x, v, p * std::pow(x.a, p - 1.0), p * (p - 1.0) * std::pow(x.a, p - 2.0));
 }
 
+// Parameters per form: ids 0-11 as restated first, then the rest of the
+// reference's AnalyticForms list (analytic_potential.hpp:801-806).
 inline int form_nparams(int form) {
-  static const int np[] = {2, 3, 2, 2, 2, 3, 2, 3, 3, 1, 3, 5};
-  return (form >= 0 && form < 12) ? np[form] : -1;
+  static const int np[] = {2, 3, 2, 2, 2, 3, 2, 3, 3, 1, 3, 5,            // 0-11
+                           4, 6, 6, 7, 5, 7, 5, 6, 5, 6, 2,               // 12-22
+                           11, 2, 16, 9, 12, 2, 5, 3, 4, 3, 7};           // 23-33
+  return (form >= 0 && form < 34) ? np[form] : -1;
 }
 
-template <class T> T form_expr(int form, const T *p, T r) {
+// cosine_cutoff (analytic_potential.hpp:142-145)
+inline HD cos_cut(HD r, HD lo, HD hi) {
+  const double pi = 3.14159265358979323846;
+  return HD(0.5) + HD(0.5) * hcos(HD(pi) * (hmin(hmax(r, lo), hi) - lo) / (hi - lo));
+}
+// switching_factor (analytic_potential.hpp:147-151): u⁴/(1 + u⁴), u = min((r − r0)/h, 0)
+inline HD sw_factor(HD r, HD r0, HD h) {
+  const HD u = hmin((r - r0) / h, HD(0.0));
+  const HD u4 = (u * u) * (u * u);
+  return u4 / (HD(1.0) + u4);
+}
+
+// Every form's expression (analytic_potential.hpp:304-780), over hyper-duals.
+// rmax is the table's upper gate bound (the `_sc` forms' switching point).
+inline HD form_expr(int form, const HD *p, HD r, double rmax) {
   switch (form) {
   case 0: { // LennardJones 4ε(sr6² − sr6)
-    T sr = p[1] / r;
-    T sr2 = sr * sr;
-    T sr6 = sr2 * sr2 * sr2;
-    return T(4.0) * p[0] * (sr6 * sr6 - sr6);
+    HD sr6 = hpowc(p[1] / r, 6.0);
+    return HD(4.0) * p[0] * (sr6 * sr6 - sr6);
   }
   case 1: { // Morse
-    T e = hexp(-p[1] * (r - p[2]));
-    return p[0] * (T(1.0) - e) * (T(1.0) - e) - p[0];
+    HD e = hexp(-p[1] * (r - p[2]));
+    return p[0] * (HD(1.0) - e) * (HD(1.0) - e) - p[0];
   }
   case 2: return p[0] * hexp(-p[1] * r);                 // ExpDecay
   case 3: return p[0] * hsqrt(r / p[1]);                 // SqrtFunc
@@ -531,18 +567,94 @@ template <class T> T form_expr(int form, const T *p, T r) {
   case 6: return p[0] * (r - p[1]) * (r - p[1]);         // Harmonic
   case 7: return p[0] * hexp(-p[1] * r) + p[2];          // ExpPlus
   case 8: return p[0] * r * r + p[1] * r + p[2];         // Parabola
-  case 9: return p[0] + T(0.0) * r;                      // ConstFunc
+  case 9: return p[0] + HD(0.0) * r;                     // ConstFunc
   case 10: { // Buckingham
-    T x = (p[1] * p[1]) / (r * r);
+    HD x = (p[1] * p[1]) / (r * r);
     return p[0] * hexp(-r / p[1]) - p[2] * x * x * x;
   }
   case 11: { // Born
-    T r2 = r * r;
-    T r6 = r2 * r2 * r2;
+    HD r2 = r * r;
+    HD r6 = r2 * r2 * r2;
     return p[0] * hexp((p[2] - r) / p[1]) - p[3] / r6 + p[4] / (r6 * r2);
   }
+  case 12: // Universal {E0, a, b, c}
+    return p[0] * (p[2] / (p[2] - p[1]) * hpow(r, p[1]) - p[1] / (p[2] - p[1]) * hpow(r, p[2])) + p[3] * r;
+  case 13: // Eopp {A, n, B, m, k, phi}
+    return p[0] / hpow(r, p[1]) + (p[2] / hpow(r, p[3])) * hcos(p[4] * r + p[5]);
+  case 14: // EoppExp {A, B, C, m, k, phi}
+    return p[0] * hexp(-p[1] * r) + (p[2] / hpow(r, p[3])) * hcos(p[4] * r + p[5]);
+  case 15: // Meopp {A, n, B, m, k, phi, r0}
+    return p[0] / hpow(r - p[6], p[1]) + (p[2] / hpow(r, p[3])) * hcos(p[4] * r + p[5]);
+  case 16: { // GenLJ {A, n, m, r0, B}
+    HD x = r / p[3];
+    return p[0] / (p[2] - p[1]) * (p[2] * hpow(x, -p[1]) - p[1] * hpow(x, -p[2])) + p[4];
   }
-  return T(0.0);
+  case 17: { // DoubleMorse {D1, a1, r1, D2, a2, r2, C}
+    HD e1 = hexp(-p[1] * (r - p[2])), e2 = hexp(-p[4] * (r - p[5]));
+    return p[0] * ((HD(1.0) - e1) * (HD(1.0) - e1) - HD(1.0)) +
+           p[3] * ((HD(1.0) - e2) * (HD(1.0) - e2) - HD(1.0)) + p[6];
+  }
+  case 18: { // DoubleExp {A, B, r1, C, r2}
+    HD dr = r - p[2];
+    return p[0] * hexp(-p[1] * dr * dr) + hexp(-p[3] * (r - p[4]));
+  }
+  case 19: { // Mishin {A, B, C, r0, n, d}
+    HD z = r - p[3];
+    HD e = hexp(-p[5] * z);
+    return p[0] * hpow(z, p[4]) * e * (HD(1.0) + p[1] * e) + p[2];
+  }
+  case 20: { // Poly5 {a0..a4}
+    HD s1 = r - HD(1.0);
+    HD s2 = s1 * s1;
+    return p[0] + HD(0.5) * p[1] * s2 + p[2] * s1 * s2 + p[3] * s2 * s2 + p[4] * s2 * s2 * s1;
+  }
+  case 21: // StiwWeb2 {A, B, p, q, delta, rc}
+    return (p[0] * hpow(r, -p[2]) - p[1] * hpow(r, -p[3])) * hexp(p[4] / (r - p[5]));
+  case 22: // StiwWeb3 {gamma, a}
+    return hexp(p[0] / (r - p[1]));
+  case 23: // TersoffPot {A, B, lambda, mu, beta, n, c, d, h, R, S}
+    return cos_cut(r, p[9], p[10]) * (p[0] * hexp(-p[2] * r) - p[1] * hexp(-p[3] * r));
+  case 24: return p[0] * hexp(-p[1] * r);                // TersoffMix {chi, omega}
+  case 25: { // TersoffModPot {A, B, lambda, mu, beta, n, c, d, h, R, S, c1..c5}
+    HD r2 = r * r, r3 = r2 * r, r4 = r3 * r, r5 = r4 * r;
+    return cos_cut(r, p[9], p[10]) * (p[0] * hexp(-p[2] * r) - p[1] * hexp(-p[3] * r)) *
+           (HD(1.0) + p[11] * r + p[12] * r2 + p[13] * r3 + p[14] * r4 + p[15] * r5);
+  }
+  case 26: { // Kawamura {A..I}
+    HD s1 = p[5] + p[6], t = p[3] + p[4];
+    return p[0] * p[1] / r + p[2] * s1 * hexp((t - r) / s1) - p[7] * p[8] / hpowc(r, 6.0);
+  }
+  case 27: { // KawamuraMix {A..L}
+    HD s1 = p[5] + p[6], t = p[3] + p[4], w = r - p[11];
+    return p[0] * p[1] / r + p[2] * s1 * hexp((t - r) / s1) - p[7] * p[8] / hpowc(r, 6.0) +
+           p[2] * p[9] * (hexp(HD(-2.0) * p[10] * w) - HD(2.0) * hexp(-p[10] * w));
+  }
+  case 28: return hpow(p[0] / r, p[1]);                  // Softshell {A, n}
+  case 29: { // Strmm {A, B, C, D, E}
+    HD s1 = r - p[4];
+    return HD(2.0) * p[0] * hexp(-p[1] / HD(2.0) * s1) - p[2] * (HD(1.0) + p[3] * s1) * hexp(-p[3] * s1);
+  }
+  case 30: case 31: case 32: case 33: { // SmoothCutoff<LJ, Morse, ExpDecay, Eopp>: base × switch(r, rmax, h)
+    static const int base_form[4] = {0, 1, 2, 13};
+    const int b = base_form[form - 30];
+    const int nb = form_nparams(b);
+    return form_expr(b, p, r, rmax) * sw_factor(r, HD(rmax), p[nb]);
+  }
+  }
+  return HD(0.0);
+}
+
+// StiwWeb2 / StiwWeb3 are exactly zero past their cut-off, or where the
+// exponent would underflow (StiwWeb2::outside, analytic_potential.hpp:587-590).
+// The partials there are zero as well: the reference's generic param_grad
+// would differentiate the expression past rc (exp of a positive power).
+inline bool form_outside(int form, const double *params, double r) {
+  if (form == 21 || form == 22) {
+    const int k = form == 21 ? 5 : 1;
+    const double d = r - params[k];
+    return d >= 0.0 || params[k - 1] / d < -708.0;
+  }
+  return false;
 }
 
 struct FormEval {
@@ -551,13 +663,14 @@ struct FormEval {
 };
 
 inline FormEval form_eval(int form, const double *params, int np, double r,
-                          bool with_grad) {
+                          bool with_grad, double rmax = 0.0) {
   FormEval out;
+  if (form_outside(form, params, r)) return out;
   HD p[16];
   for (int k = 0; k < np; ++k) p[k] = HD(params[k]);
   {
     HD rr(r, 1.0, 1.0, 0.0); // ε1 = ε2 = dr → d = ∂²/∂r²
-    HD f = form_expr<HD>(form, p, rr);
+    HD f = form_expr(form, p, rr, rmax);
     out.v = f.a;
     out.d = f.b;
     out.d2 = f.d;
@@ -568,7 +681,7 @@ inline FormEval form_eval(int form, const double *params, int np, double r,
       for (int m = 0; m < np; ++m) q[m] = HD(params[m]);
       q[k] = HD(params[k], 0.0, 1.0, 0.0); // ε2 = dθ_k
       HD rr(r, 1.0, 0.0, 0.0);             // ε1 = dr
-      HD f = form_expr<HD>(form, q, rr);
+      HD f = form_expr(form, q, rr, rmax);
       out.g[k] = f.c;
       out.dg[k] = f.d;
     }
