@@ -1,5 +1,6 @@
 // The C ABI of include/forcesmith_gpu.h: context lifecycle, configuration
 // and model upload, parameter scatter, and the evaluate entry points.
+#include "forms_dev.cuh"
 #include "internal.cuh"
 
 #include <algorithm>
@@ -145,6 +146,8 @@ void free_jacobian(fs_gpu *h) {
   dfree(h->d_wsF);
   dfree(h->d_jx);
   h->jx_alloc = 0;
+  dfree(h->d_an);
+  h->an_alloc = 0;
   h->jac_alloc = 0;
   h->gram_part_alloc = 0;
   h->atom_scratch_alloc = 0;
@@ -432,8 +435,7 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
     } else if (ft.kind == FS_TABLE_ANALYTIC) {
       if (m->family != FS_FAMILY_EAM && m->family != FS_FAMILY_PAIR && m->family != FS_FAMILY_ANGULAR)
         return set_error(h, FS_ERR_UNSUPPORTED, "set_model: analytic tables in EAM, pair and angular models only");
-      static const int nparams[FS_FORM_COUNT] = {2, 3, 2, 2, 2, 3, 2, 3, 3, 1, 3, 5};
-      if (ft.form < 0 || ft.form >= FS_FORM_COUNT || ft.n != nparams[ft.form])
+      if (ft.form < 0 || ft.form >= FS_FORM_COUNT || ft.n != fsg::form_param_count(ft.form))
         return set_error(h, FS_ERR_ARG, "set_model: analytic form and parameter count do not match");
       if (!(ft.rmax >= ft.rmin)) return set_error(h, FS_ERR_ARG, "set_model: bad analytic gate span");
     } else {

@@ -1279,32 +1279,6 @@ __global__ void jtr_reduce_kernel(const double *__restrict__ part, int n_cfg, in
   Jtr[col] = s;
 }
 
-template <class T> Common make_common(fs_gpu *h) {
-  Common c;
-  c.cfg = h->d_cfg;
-  c.wpos = h->d_wpos;
-  c.type = h->d_type;
-  c.ref_force = h->d_ref_force;
-  c.nb_start = h->d_nb_start;
-  c.vals = h->d_vals;
-  c.nb_pack = h->d_nb_pack;
-  c.desc = h->d_desc;
-  c.cmap = h->d_cmap;
-  c.n_tables = static_cast<int>(h->desc.size());
-  c.n_segs = h->n_segs;
-  c.n_cmap = h->n_cmap;
-  c.ntypes = h->ntypes;
-  c.family = h->family;
-  c.cfg_count = h->n_cfg;
-  return c;
-}
-
-int max_images(const fs_gpu *h) {
-  int m = 1;
-  for (const CfgDev &cd : h->cfg_host) m = std::max(m, (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1));
-  return m;
-}
-
 int choose_lpa(const fs_gpu *h) {
   if (h->lanes_per_atom) return h->lanes_per_atom;
   if (h->tuned_lpa) return h->tuned_lpa;
@@ -1867,13 +1841,19 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s) {
     extern int eval_jacobian_other(fs_gpu * h, double w_e, double w_s);
     return eval_jacobian_other(h, w_e, w_s);
   }
-  for (const HostTable &t : h->tables)
-    if (t.kind == FS_TABLE_ANALYTIC) {
-      // analytic tables: the reference's central differences on the device
-      // (fd_jacobian.hpp:37-49); FP64 contexts only
-      extern int eval_jacobian_fd(fs_gpu * h, double w_e, double w_s);
-      return eval_jacobian_fd(h, w_e, w_s);
-    }
+  // every table analytic: the reference's analytic chain rule
+  // (forcesmith_functor.cpp:265-277); analytic and spline tables mixed: the
+  // reference's central differences (fd_jacobian.hpp:37-49), FP64 contexts only
+  int n_an = 0;
+  for (const HostTable &t : h->tables) n_an += t.kind == FS_TABLE_ANALYTIC;
+  if (n_an == static_cast<int>(h->tables.size())) {
+    extern int eval_jacobian_analytic(fs_gpu * h, double w_e, double w_s);
+    return eval_jacobian_analytic(h, w_e, w_s);
+  }
+  if (n_an > 0) {
+    extern int eval_jacobian_fd(fs_gpu * h, double w_e, double w_s);
+    return eval_jacobian_fd(h, w_e, w_s);
+  }
   return h->precision == FS_PREC_FP64 ? launch_jacobian_t<double>(h, w_e, w_s)
                                       : launch_jacobian_t<float>(h, w_e, w_s);
 }

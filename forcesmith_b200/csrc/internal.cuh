@@ -177,6 +177,8 @@ struct fs_gpu {
   bool j_rowmajor = false;       // row-major J (FP32 EAM / pair Jacobians feeding the tensor-core JᵀJ)
   double *d_jx = nullptr;        // FP64 column-major staging of an exported row block of J
   size_t jx_alloc = 0;
+  void *d_an = nullptr;          // analytic-table Jacobian: column table and per-atom scratch
+  size_t an_alloc = 0;
   double *d_jtr_part = nullptr;  // per-config Jᵀr partials (FP64)
   size_t jtr_part_alloc = 0;
   double *d_half_part = nullptr; // force-row pass with two CTAs per configuration: their sums

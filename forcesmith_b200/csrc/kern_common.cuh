@@ -234,4 +234,37 @@ __device__ void stage_work(const int32_t *nb, int N, int *pfirst, int *tfirst, i
 }
 
 } // namespace
+
+// Kernel-argument view of a context's configurations, neighbour lists and
+// tables.
+template <class T> inline Common make_common(fs_gpu *h) {
+  Common c;
+  c.cfg = h->d_cfg;
+  c.wpos = h->d_wpos;
+  c.type = h->d_type;
+  c.ref_force = h->d_ref_force;
+  c.nb_start = h->d_nb_start;
+  c.vals = h->d_vals;
+  c.nb_pack = h->d_nb_pack;
+  c.desc = h->d_desc;
+  c.cmap = h->d_cmap;
+  c.n_tables = static_cast<int>(h->desc.size());
+  c.n_segs = h->n_segs;
+  c.n_cmap = h->n_cmap;
+  c.ntypes = h->ntypes;
+  c.family = h->family;
+  c.cfg_count = h->n_cfg;
+  return c;
+}
+
+// The largest periodic-image count of the context's configurations.
+inline int max_images(const fs_gpu *h) {
+  int m = 1;
+  for (const CfgDev &cd : h->cfg_host) {
+    const int n = (2 * cd.sx + 1) * (2 * cd.sy + 1) * (2 * cd.sz + 1);
+    m = n > m ? n : m;
+  }
+  return m;
+}
+
 } // namespace fsg

@@ -1,6 +1,7 @@
 // Device-side spline evaluation shared by the evaluation kernels.
 #pragma once
 
+#include "forms_dev.cuh"
 #include "internal.cuh"
 
 #include <type_traits>
@@ -48,82 +49,15 @@ template <class T> __device__ __forceinline__ void load_stab(STab<T> &s, const T
   s.pv0 = d.pv0;
 }
 
-// Analytic radial forms (include/forcesmith/potentials/analytic_potential.hpp),
-// value and d/dr, parameters p[] as in the header's fs_form list.
+// Analytic radial forms: value and d/dr at r (forms_dev.cuh).  rmax is the
+// table's upper gate bound.
 template <class T> struct VD {
   T v, d;
 };
-template <class T> __device__ __forceinline__ VD<T> form_vd(int form, const double *pp, int n, T r) {
-  T p[5];
-  for (int k = 0; k < 5; ++k) p[k] = k < n ? static_cast<T>(pp[k]) : T(0);
-  VD<T> o{T(0), T(0)};
-  switch (form) {
-  case 0: { // LJ 4ε((σ/r)^12 − (σ/r)^6)
-    const T sr = p[1] / r, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2;
-    o.v = T(4) * p[0] * (sr6 * sr6 - sr6);
-    o.d = T(4) * p[0] * (T(-12) * sr6 * sr6 + T(6) * sr6) / r;
-    break;
-  }
-  case 1: { // Morse De(1 − e^{−a(r−re)})² − De
-    const T e = exp(-p[1] * (r - p[2]));
-    o.v = p[0] * (T(1) - e) * (T(1) - e) - p[0];
-    o.d = T(2) * p[0] * (T(1) - e) * p[1] * e;
-    break;
-  }
-  case 2: { // A e^{−Br}
-    o.v = p[0] * exp(-p[1] * r);
-    o.d = -p[1] * o.v;
-    break;
-  }
-  case 3: { // A √(r/B)
-    o.v = p[0] * sqrt(r / p[1]);
-    o.d = o.v / (T(2) * r);
-    break;
-  }
-  case 4: { // A / r^n
-    o.v = p[0] / pow(r, p[1]);
-    o.d = -p[1] * o.v / r;
-    break;
-  }
-  case 5: { // A e^{−B(r−r0)}
-    o.v = p[0] * exp(-p[1] * (r - p[2]));
-    o.d = -p[1] * o.v;
-    break;
-  }
-  case 6: { // k (r − r0)²
-    o.v = p[0] * (r - p[1]) * (r - p[1]);
-    o.d = T(2) * p[0] * (r - p[1]);
-    break;
-  }
-  case 7: { // A e^{−Br} + C
-    const T e = p[0] * exp(-p[1] * r);
-    o.v = e + p[2];
-    o.d = -p[1] * e;
-    break;
-  }
-  case 8: { // A r² + B r + C
-    o.v = p[0] * r * r + p[1] * r + p[2];
-    o.d = T(2) * p[0] * r + p[1];
-    break;
-  }
-  case 9: { // C
-    o.v = p[0];
-    break;
-  }
-  case 10: { // A e^{−r/ρ} − C (ρ²/r²)³
-    const T x = (p[1] * p[1]) / (r * r), e = p[0] * exp(-r / p[1]);
-    o.v = e - p[2] * x * x * x;
-    o.d = -e / p[1] + T(6) * p[2] * x * x * x / r;
-    break;
-  }
-  case 11: { // A e^{(C−r)/B} − D/r⁶ + E/r⁸
-    const T r2 = r * r, r6 = r2 * r2 * r2, e = p[0] * exp((p[2] - r) / p[1]);
-    o.v = e - p[3] / r6 + p[4] / (r6 * r2);
-    o.d = -e / p[1] + T(6) * p[3] / (r6 * r) - T(8) * p[4] / (r6 * r2 * r);
-    break;
-  }
-  }
-  return o;
+template <class T> __device__ __forceinline__ VD<T> form_vd(int form, const double *pp, int n, T r, T rmax) {
+  if (form_outside<T>(form, pp, r)) return VD<T>{T(0), T(0)};
+  const Hd<T> f = form_seeded<T>(form, pp, n, r, rmax, T(0), -1);
+  return VD<T>{f.a, f.b};
 }
 
 // Closed gate [x0, x_{n-1}] (force_calculator_concept.hpp:94-98), for
@@ -269,7 +203,7 @@ template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
                                         T r) {
   if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
   }
   T t;
   const int e = seg_of(tb, r, t);
@@ -281,7 +215,7 @@ template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd64(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
                                           T r, double r64) {
   if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
   }
   T t;
   const int e = seg_of64(tb, r, r64, t);
@@ -294,7 +228,7 @@ template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd_at(const STab<T> &tb, const typename Vec4T<T>::type *seg,
                                            const double *vals, T r, int e, T t) {
   if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r);
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
   }
   return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
 }

@@ -128,8 +128,39 @@ enum fs_form {
   FS_FORM_CONST = 9,       /* C                                  {C}         */
   FS_FORM_BUCKINGHAM = 10, /* A e^{−r/ρ} − C (ρ²/r²)³            {A,rho,C}   */
   FS_FORM_BORN = 11,       /* A e^{(C−r)/B} − D/r^6 + E/r^8      {A,B,C,D,E} */
-  FS_FORM_COUNT = 12
+  FS_FORM_UNIVERSAL = 12,  /* E0(b/(b−a) r^a − a/(b−a) r^b) + c r {E0,a,b,c} */
+  FS_FORM_EOPP = 13,       /* A/r^n + B/r^m cos(k r + φ)   {A,n,B,m,k,phi}   */
+  FS_FORM_EOPP_EXP = 14,   /* A e^{−Br} + C/r^m cos(k r + φ) {A,B,C,m,k,phi} */
+  FS_FORM_MEOPP = 15,      /* A/(r−r0)^n + B/r^m cos(k r + φ) {…,r0}        */
+  FS_FORM_GEN_LJ = 16,     /* A/(m−n)(m x^{−n} − n x^{−m}) + B, x = r/r0
+                                                           {A,n,m,r0,B}      */
+  FS_FORM_DOUBLE_MORSE = 17, /* Σ D_k((1−e_k)² − 1) + C {D1,a1,r1,D2,a2,r2,C} */
+  FS_FORM_DOUBLE_EXP = 18, /* A e^{−B(r−r1)²} + e^{−C(r−r2)}  {A,B,r1,C,r2}   */
+  FS_FORM_MISHIN = 19,     /* A z^n e^{−dz}(1 + B e^{−dz}) + C, z = r − r0
+                                                           {A,B,C,r0,n,d}    */
+  FS_FORM_POLY5 = 20,      /* a0 + ½a1 s² + a2 s³ + a3 s⁴ + a4 s⁵, s = r − 1 */
+  FS_FORM_STIWEB2 = 21,    /* (A r^{−p} − B r^{−q}) e^{δ/(r−rc)}, 0 past rc
+                                                           {A,B,p,q,delta,rc}*/
+  FS_FORM_STIWEB3 = 22,    /* e^{γ/(r−a)}, 0 past a             {gamma,a}  */
+  FS_FORM_TERSOFF = 23,    /* fc(r)(A e^{−λr} − B e^{−μr})
+                              {A,B,lambda,mu,beta,n,c,d,h,R,S}               */
+  FS_FORM_TERSOFF_MIX = 24, /* χ e^{−ωr}                         {chi,omega} */
+  FS_FORM_TERSOFF_MOD = 25, /* Tersoff × (1 + c1 r + … + c5 r⁵), 16 params  */
+  FS_FORM_KAWAMURA = 26,   /* AB/r + C(F+G) e^{(D+E−r)/(F+G)} − HI/r⁶ {A..I} */
+  FS_FORM_KAWAMURA_MIX = 27, /* Kawamura + CJ(e^{−2K(r−L)} − 2e^{−K(r−L)}) {A..L} */
+  FS_FORM_SOFTSHELL = 28,  /* (A/r)^n                              {A,n}      */
+  FS_FORM_STRMM = 29,      /* 2A e^{−B s/2} − C(1 + D s) e^{−D s}, s = r − E */
+  FS_FORM_LJ_SC = 30,      /* LJ × switch(r; rmax, h)          {eps,sigma,h} */
+  FS_FORM_MORSE_SC = 31,   /* Morse × switch                    {De,a,re,h}  */
+  FS_FORM_EXP_DECAY_SC = 32, /* ExpDecay × switch                  {A,B,h}   */
+  FS_FORM_EOPP_SC = 33,    /* Eopp × switch                     {…,h}        */
+  FS_FORM_COUNT = 34
 };
+/* switch(r; rmax, h) = u⁴/(1 + u⁴), u = min((r − rmax)/h, 0), with rmax the
+ * table's upper gate bound (SmoothCutoff, analytic_potential.hpp:782-793);
+ * fc is the cosine cutoff between R and S (analytic_potential.hpp:142-145).
+ * The order is the reference's AnalyticForms list (analytic_potential.hpp:801-806)
+ * after the first twelve. */
 
 typedef struct fs_table {
   int32_t kind;          /* fs_table_kind                                   */
