@@ -433,8 +433,10 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
     } else if (ft.kind == FS_TABLE_SPLINE) {
       if (ft.n < 2 || !(ft.rmax > ft.rmin)) return set_error(h, FS_ERR_ARG, "set_model: bad spline");
     } else if (ft.kind == FS_TABLE_ANALYTIC) {
-      if (m->family != FS_FAMILY_EAM && m->family != FS_FAMILY_PAIR && m->family != FS_FAMILY_ANGULAR)
-        return set_error(h, FS_ERR_UNSUPPORTED, "set_model: analytic tables in EAM, pair and angular models only");
+      if (m->family != FS_FAMILY_EAM && m->family != FS_FAMILY_PAIR && m->family != FS_FAMILY_ANGULAR &&
+          m->family != FS_FAMILY_ADP)
+        return set_error(h, FS_ERR_UNSUPPORTED,
+                         "set_model: analytic tables in EAM, pair, ADP and angular models only");
       if (ft.form < 0 || ft.form >= FS_FORM_COUNT || ft.n != fsg::form_param_count(ft.form))
         return set_error(h, FS_ERR_ARG, "set_model: analytic form and parameter count do not match");
       if (!(ft.rmax >= ft.rmin)) return set_error(h, FS_ERR_ARG, "set_model: bad analytic gate span");

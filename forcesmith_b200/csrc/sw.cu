@@ -644,9 +644,13 @@ int eval_jacobian_other(fs_gpu *h, double w_e, double w_s) {
   }
   // ACSF with linear heads: exact (the model is linear in its coefficients)
   if (h->family == FS_FAMILY_ACSF) return eval_jacobian_acsf(h, w_e, w_s);
-  // ADP, Tersoff, Angular: the reference's own central differences (FP64 contexts)
-  if (h->family == FS_FAMILY_ADP || h->family == FS_FAMILY_TERSOFF || h->family == FS_FAMILY_ANGULAR)
-    return eval_jacobian_fd(h, w_e, w_s);
+  // ADP: exact, forward mode (adp.cu)
+  if (h->family == FS_FAMILY_ADP) {
+    extern int eval_jacobian_adp(fs_gpu * h, double w_e, double w_s);
+    return eval_jacobian_adp(h, w_e, w_s);
+  }
+  // Tersoff, Angular: the reference's own central differences (FP64 contexts)
+  if (h->family == FS_FAMILY_TERSOFF || h->family == FS_FAMILY_ANGULAR) return eval_jacobian_fd(h, w_e, w_s);
   return set_error(h, FS_ERR_UNSUPPORTED, "Jacobian: family not handled by this build");
 }
 
