@@ -404,7 +404,8 @@ def test_sw_binary_residual_and_jacobian(precision, tol):
 
 # --------------------------------------------------------------- ADP ---
 
-def test_adp_residual_and_fd_jacobian_fp64():
+def test_adp_residual_fp64():
+    """ADP residual against the oracle (its exact Jacobian: test_gpu_adp.py)."""
     from tests.helpers import adp_spline_model
     ds = small_ternary(3, 32, seed=41)
     ds.type[:] = ds.type % 2
@@ -415,9 +416,6 @@ def test_adp_residual_and_fd_jacobian_fp64():
     _close(rg["forces"], ro["forces"], 1e-9, "ADP forces")
     _close(rg["energy"], ro["energy"], 1e-9, "ADP energy")
     _close(rg["F"], ro["F"], 1e-9, "ADP F")
-    res = g.jacobian(1.0, 0.1)
-    Jf = o.jacobian_fd(1.0, 0.1)
-    assert np.max(np.abs(res["J"] - Jf)) <= 1e-6 * (1 + np.abs(Jf).max())
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
