@@ -585,6 +585,13 @@ int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D) {
   return FS_OK;
 }
 
+int fs_gpu_max_cutoff(fs_gpu *h, double *rc) {
+  if (!h || !rc) return FS_ERR_ARG;
+  if (!h->have_model) return set_error(h, FS_ERR_STATE, "max_cutoff: no model");
+  *rc = model_max_cutoff(h);
+  return FS_OK;
+}
+
 int fs_gpu_residual_count(fs_gpu *h, double w_s, int64_t *m) {
   if (!h || !m) return FS_ERR_ARG;
   if (h->n_cfg == 0) return set_error(h, FS_ERR_STATE, "no configurations");

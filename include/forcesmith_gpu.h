@@ -46,13 +46,27 @@
  *                              plus the JᵀJ / Jᵀr products that
  *                              NormalEquationsSolver and LM consume
  *                              (src/optimization/solver.cpp:242-266)
+ *   fs_gpu_copy_jacobian_rows  the per-configuration block of fjac that
+ *                              CForceCalculator::eval_cached_jacobian fills
+ *                              (include/forcesmith/force/force_calculator_concept.hpp:62-67,
+ *                               src/optimization/forcesmith_functor.cpp:111-132)
+ *   fs_gpu_max_cutoff          CForceCalculator::max_cutoff
+ *                              (include/forcesmith/force/force_calculator_concept.hpp:210-225,288-292)
  *   fs_gpu_lm_step / fs_gpu_lsq_step
  *                              the LM / lsq step of EigenLMSolver and
  *                              NormalEquationsSolver (src/optimization/solver.cpp:67-85,242-266)
+ *   fs_gpu_eval_population[_noalloc]
+ *                              many parameter vectors' objectives in one launch
+ *                              (the inner loop of BoostDESolver and of the LM trials)
  *   fs_gpu_de_*                BoostDESolver's population evaluation
  *                              (src/optimization/solver.cpp:113-155)
  *   fs_gpu_surrogate_*         (no reference counterpart: the learned
  *                              pre-screen of DE trial vectors)
+ *   fs_gpu_check_bounded_wait  (no reference counterpart: a device wait that
+ *                              gives up and reports, for failure detection)
+ *
+ * include/forcesmith_gpu_adapter.hpp wraps these in C++ classes that satisfy
+ * the reference's CForceCalculator and CSolver concepts.
  */
 #ifndef FORCESMITH_GPU_H
 #define FORCESMITH_GPU_H
@@ -230,6 +244,10 @@ int fs_gpu_param_count(fs_gpu *h, int32_t *D);
 int fs_gpu_gather_params(fs_gpu *h, double *x);
 int fs_gpu_gather_bounds(fs_gpu *h, double *lo, double *hi);
 int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D);
+
+/* The model's interaction cut-off: CForceCalculator::max_cutoff
+ * (force_calculator_concept.hpp:210-221; SW: max(a1, a2), stiweb_force.cpp:234-239). */
+int fs_gpu_max_cutoff(fs_gpu *h, double *rc);
 
 /* rows = Σ_c 3N_c + 2 + (w_s > 0 ? 6 : 0)  (residual_layout.hpp:18-31) */
 int fs_gpu_residual_count(fs_gpu *h, double w_s, int64_t *m);
