@@ -6,9 +6,10 @@ surrogate screening over plain DE.
   gradient     per tensor ‖g_gpu − g_oracle‖ ≤ 1e-2 ‖g_oracle‖; loss 1e-4 rel
   Adam         one device step = the oracle's update of the device gradient,
                1e-5 relative + 1e-9
-  screening    surrogate-screened DE reaches plain DE's final objective
-               (within 1 %) in fewer generations, i.e. fewer exact
-               evaluations (NP per generation either way)
+  screening    over 3 seeds, surrogate-screened DE reaches plain DE's
+               80-generation objective (within 1 %) in a median ≤ 0.65 × 80
+               generations, and no seed needs more generations than plain DE
+               itself (NP exact evaluations per generation either way)
 """
 import numpy as np
 import pytest
@@ -98,19 +99,35 @@ def _de(problem_ds, start, screened, gens, seed, gate=0.8):
     return dict(history=hist)
 
 
+SEEDS = (21, 22, 23)
+GENS = 80
+GEN_RATIO = 0.65
+
+
 def test_screening_gains_over_plain_de():
+    """Surrogate-screened DE against plain DE from the same start and seed,
+    for three seeds: screened generations (NP exact evaluations each, like
+    plain DE's) to reach plain DE's final objective within 1 %.  Measured on
+    a B200: 42, 67, 43 of 80 (median ratio 0.54), where plain DE itself first
+    reaches that target at generation 69, 67, 71.  Asserted: median ratio ≤
+    GEN_RATIO, and no seed slower than plain DE to the target."""
     true, start = ternary_models(8)
     ds = label(small_ternary(3, 32, seed=11), true, O.Oracle, 1.0, 0.0)
-    gens = 80
-    plain = _de(ds, start, False, gens, 21)["history"]
-    scr = _de(ds, start, True, gens, 21)
-    target = 1.01 * plain[-1]
-    reached = np.nonzero(scr["history"] <= target)[0]
-    assert reached.size > 0, (plain[-1], scr["history"][-1], scr["rho"][-5:])
-    assert reached[0] + 1 < gens, (reached[0], plain[-1], scr["history"][-1])
-    assert scr["screened"].sum() > 0
-    # the exact objective decides acceptance: the best objective never increases
-    assert np.all(np.diff(scr["history"]) <= 0)
+    ratios = []
+    for seed in SEEDS:
+        plain = _de(ds, start, False, GENS, seed)["history"]
+        scr = _de(ds, start, True, GENS, seed)
+        target = 1.01 * plain[-1]
+        reached = np.nonzero(scr["history"] <= target)[0]
+        assert reached.size > 0, (seed, plain[-1], scr["history"][-1], scr["rho"][-5:])
+        g_scr = int(reached[0]) + 1
+        g_plain = int(np.nonzero(plain <= target)[0][0]) + 1
+        assert g_scr <= g_plain, (seed, g_scr, g_plain)
+        assert scr["screened"].sum() > 0
+        # the exact objective decides acceptance: the best objective never increases
+        assert np.all(np.diff(scr["history"]) <= 0)
+        ratios.append(g_scr / GENS)
+    assert np.median(ratios) <= GEN_RATIO, ratios
 
 
 def test_gate_closed_means_plain_de():
