@@ -65,7 +65,11 @@ class fs_table(C.Structure):
 
 class fs_model(C.Structure):
     _fields_ = [("family", C.c_int32), ("ntypes", C.c_int32), ("n_tables", C.c_int32),
-                ("reserved", C.c_int32), ("tables", C.POINTER(fs_table))]
+                ("reserved", C.c_int32), ("tables", C.POINTER(fs_table)),
+                ("n_globals", C.c_int32), ("n_links", C.c_int32),
+                ("global_values", C.POINTER(C.c_double)), ("global_fixed", C.POINTER(C.c_uint8)),
+                ("link_global", C.POINTER(C.c_int32)), ("link_table", C.POINTER(C.c_int32)),
+                ("link_param", C.POINTER(C.c_int32))]
 
 
 class fs_gpu_opts(C.Structure):
@@ -185,10 +189,45 @@ class Table:
 
 
 @dataclass
+class GlobalParam:
+    """A parameter shared by several analytic parameters (GlobalParam,
+    include/forcesmith/force/force_calculator_concept.hpp:21-44): its value,
+    fixed flag and links (table index in model order, parameter slot).  A
+    linked parameter is fixed in its table and takes the global's value
+    (finalize_globals, :230-237); a free global takes the column after every
+    table column, in global order."""
+    value: float
+    fixed: bool = False
+    links: list = field(default_factory=list)
+    name: str = ""
+
+    def copy(self):
+        return GlobalParam(float(self.value), bool(self.fixed), [tuple(lk) for lk in self.links], self.name)
+
+
+@dataclass
 class Model:
     family: int
     ntypes: int
     tables: list = field(default_factory=list)
+    globals: list = field(default_factory=list)
+
+    def _free_mask(self, k):
+        """Free values of table k: not fixed and not linked to a global."""
+        t = self.tables[k]
+        free = (t.fixed == 0) if t.fixed is not None else np.ones(t.values.size, bool)
+        for g in self.globals:
+            for tk, slot in g.links:
+                if tk == k:
+                    free[slot] = False
+        return free
+
+    def broadcast_globals(self):
+        """Each linked parameter takes its global's value (in place)."""
+        for g in self.globals:
+            for tk, slot in g.links:
+                self.tables[tk].values[slot] = g.value
+        return self
 
     def to_c(self):
         """Returns (fs_model, keepalive) — keep the second alive while in use."""
@@ -204,6 +243,16 @@ class Model:
             ft.upper = _dp(t.upper)
             keep.append(t)
         m = fs_model(self.family, self.ntypes, len(self.tables), 0, arr)
+        if self.globals:
+            gv = np.array([g.value for g in self.globals], np.float64)
+            gf = np.array([1 if g.fixed else 0 for g in self.globals], np.uint8)
+            links = [(gi, tk, slot) for gi, g in enumerate(self.globals) for tk, slot in g.links]
+            lg, lt, lp = (np.array([lk[q] for lk in links], np.int32) for q in range(3))
+            keep += [gv, gf, lg, lt, lp]
+            ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+            m.n_globals, m.n_links = len(self.globals), len(links)
+            m.global_values, m.global_fixed = _dp(gv), gf.ctypes.data_as(C.POINTER(C.c_uint8))
+            m.link_global, m.link_table, m.link_param = ip(lg), ip(lt), ip(lp)
         return m, keep
 
     def with_standardization(self, mean, inv_std):
@@ -285,24 +334,30 @@ class Model:
         return Model(FS_FAMILY_ACSF, S_new, [spec.copy()] + heads)
 
     def free_values(self) -> np.ndarray:
-        out = []
-        for t in self.tables:
-            fx = t.fixed if t.fixed is not None else np.zeros(t.values.size, np.uint8)
-            out.append(t.values[fx == 0])
-        return np.concatenate(out) if out else np.zeros(0)
+        """The parameter vector in gather order: every table's free values,
+        then the free globals (force_calculator_concept.hpp:171-208)."""
+        out = [t.values[self._free_mask(k)] for k, t in enumerate(self.tables)]
+        out.append(np.array([g.value for g in self.globals if not g.fixed], np.float64))
+        return np.concatenate(out)
 
     def with_values(self, x: np.ndarray) -> "Model":
-        m = Model(self.family, self.ntypes, [t.copy() for t in self.tables])
+        """scatter_params: a copy with x placed in gather order and the
+        globals broadcast to their links."""
+        m = self.copy()
         o = 0
-        for t in m.tables:
-            fx = t.fixed if t.fixed is not None else np.zeros(t.values.size, np.uint8)
-            k = int((fx == 0).sum())
-            t.values[fx == 0] = x[o:o + k]
-            o += k
-        return m
+        for k, t in enumerate(m.tables):
+            free = m._free_mask(k)
+            n = int(free.sum())
+            t.values[free] = x[o:o + n]
+            o += n
+        for g in m.globals:
+            if not g.fixed:
+                g.value = float(x[o])
+                o += 1
+        return m.broadcast_globals()
 
     def copy(self):
-        return Model(self.family, self.ntypes, [t.copy() for t in self.tables])
+        return Model(self.family, self.ntypes, [t.copy() for t in self.tables], [g.copy() for g in self.globals])
 
 
 @dataclass

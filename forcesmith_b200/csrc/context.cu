@@ -377,6 +377,29 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
   if ((expected_tables(m->family, m->ntypes) != m->n_tables && !acsf_std) || !m->tables)
     return set_error(h, FS_ERR_ARG, "set_model: table count does not match the family");
   const int np = npair_of(m->ntypes);
+  // global parameters: links (table, slot) → global
+  const int ng = m->n_globals, nl = m->n_links;
+  if (ng < 0 || nl < 0 || (ng > 0 && !m->global_values) ||
+      (nl > 0 && (!m->link_global || !m->link_table || !m->link_param)))
+    return set_error(h, FS_ERR_ARG, "set_model: malformed global parameter arrays");
+  if (ng > 0 && m->family != FS_FAMILY_EAM && m->family != FS_FAMILY_PAIR)
+    return set_error(h, FS_ERR_ARG, "set_model: global parameters belong to the pair and EAM families");
+  std::vector<std::vector<int>> link_of(m->n_tables);
+  for (int l = 0; l < nl; ++l) {
+    const int g = m->link_global[l], t = m->link_table[l], k = m->link_param[l];
+    if (g < 0 || g >= ng || t < 0 || t >= m->n_tables)
+      return set_error(h, FS_ERR_ARG, "set_model: global link " + std::to_string(l) + " out of range");
+    const fs_table &ft = m->tables[t];
+    if (ft.kind != FS_TABLE_ANALYTIC || k < 0 || k >= ft.n)
+      return set_error(h, FS_ERR_ARG,
+                       "set_model: global link " + std::to_string(l) + " is not a parameter of an analytic table");
+    if (link_of[t].empty()) link_of[t].assign(ft.n, -1);
+    if (link_of[t][k] >= 0) return set_error(h, FS_ERR_ARG, "set_model: a parameter linked to two globals");
+    link_of[t][k] = g;
+  }
+  for (int g = 0; g < ng; ++g)
+    if (!std::isfinite(m->global_values[g]))
+      return set_error(h, FS_ERR_ARG, "set_model: global " + std::to_string(g) + " is not finite");
   std::vector<HostTable> tabs(m->n_tables);
   int col = 0;
   for (int t = 0; t < m->n_tables; ++t) {
@@ -454,14 +477,32 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
         if (ft.lower) ht.lo[k] = ft.lower[k];
         if (ft.upper) ht.hi[k] = ft.upper[k];
       }
+      if (!link_of[t].empty() && link_of[t][k] >= 0) {
+        // finalize_globals: the linked slot is fixed at the global's value
+        ht.fixed[k] = 1;
+        ht.v[k] = m->global_values[link_of[t][k]];
+        ht.lo[k] = -std::numeric_limits<double>::infinity();
+        ht.hi[k] = std::numeric_limits<double>::infinity();
+      }
       if (!ht.fixed[k]) ht.cols[k] = col++;
     }
   }
+  // free globals take the columns after the tables'; their links share them
+  std::vector<double> gval(m->global_values, m->global_values + ng);
+  std::vector<int> gcol(ng, -1);
+  for (int g = 0; g < ng; ++g)
+    if (!(m->global_fixed && m->global_fixed[g])) gcol[g] = col++;
+  for (int t = 0; t < m->n_tables; ++t)
+    for (int k = 0; k < static_cast<int>(link_of[t].size()); ++k)
+      if (link_of[t][k] >= 0) tabs[t].cols[k] = gcol[link_of[t][k]];
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
   h->family = m->family;
   h->ntypes = m->ntypes;
   h->tables = std::move(tabs);
+  h->global_val = std::move(gval);
+  h->global_col = std::move(gcol);
+  h->shared_cols = nl > 0 && std::any_of(h->global_col.begin(), h->global_col.end(), [](int c) { return c >= 0; });
   h->D = col;
   h->have_model = true;
   h->rcut_built = -1.0;
@@ -548,6 +589,8 @@ int fs_gpu_gather_params(fs_gpu *h, double *x) {
   for (const HostTable &t : h->tables)
     for (int k = 0; k < t.n; ++k)
       if (t.cols[k] >= 0) x[t.cols[k]] = t.v[k];
+  for (size_t g = 0; g < h->global_col.size(); ++g)
+    if (h->global_col[g] >= 0) x[h->global_col[g]] = h->global_val[g];
   return FS_OK;
 }
 
@@ -560,6 +603,11 @@ int fs_gpu_gather_bounds(fs_gpu *h, double *lo, double *hi) {
         lo[t.cols[k]] = t.lo[k];
         hi[t.cols[k]] = t.hi[k];
       }
+  for (size_t g = 0; g < h->global_col.size(); ++g)
+    if (h->global_col[g] >= 0) {
+      lo[h->global_col[g]] = -std::numeric_limits<double>::infinity();
+      hi[h->global_col[g]] = std::numeric_limits<double>::infinity();
+    }
   return FS_OK;
 }
 
@@ -575,6 +623,8 @@ int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D) {
   for (HostTable &t : h->tables)
     for (int k = 0; k < t.n; ++k)
       if (t.cols[k] >= 0) t.v[k] = x[t.cols[k]];
+  for (size_t g = 0; g < h->global_col.size(); ++g)
+    if (h->global_col[g] >= 0) h->global_val[g] = x[h->global_col[g]];
   FS_TRY(upload_values(h));
   h->params_dirty = true;
   h->jac_valid = false;

@@ -1844,6 +1844,12 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s) {
   // every table analytic: the reference's analytic chain rule
   // (forcesmith_functor.cpp:265-277); analytic and spline tables mixed: the
   // reference's central differences (fd_jacobian.hpp:37-49), FP64 contexts only
+  // a free global parameter: central differences too, as the reference
+  // (analytic_jacobian_available, param_jacobian.hpp:44-57)
+  if (h->shared_cols) {
+    extern int eval_jacobian_fd(fs_gpu * h, double w_e, double w_s);
+    return eval_jacobian_fd(h, w_e, w_s);
+  }
   int n_an = 0;
   for (const HostTable &t : h->tables) n_an += t.kind == FS_TABLE_ANALYTIC;
   if (n_an == static_cast<int>(h->tables.size())) {
@@ -1861,6 +1867,18 @@ int eval_jacobian(fs_gpu *h, double w_e, double w_s) {
 } // namespace fsg
 
 namespace fsg {
+// FP64 segments of every spline table at the parameter vector d_x1 (D
+// values on the device), whatever the working precision: the per-trial setup
+// with one trial.  seg holds n_segs entries.
+int spline_segments_fp64(fs_gpu *h, const double *d_x1, double4 *seg) {
+  if (h->n_spl == 0) return FS_OK;
+  pop_setup_kernel<double><<<dim3(static_cast<unsigned>(h->n_spl), 1), 32, 0, h->stream>>>(
+      h->d_desc, h->d_spl, h->d_vals, h->d_cmap, d_x1, h->D, h->n_segs, seg);
+  FS_CUDA(cudaGetLastError());
+  ++h->launches;
+  return FS_OK;
+}
+
 // Σ‖F(x_k)‖² for NP device-resident trial vectors (EAM / pair families).
 int eval_population_device(fs_gpu *h, double w_e, double w_s, const double *d_xs, int NP, double *d_obj) {
   if (h->family != FS_FAMILY_EAM && h->family != FS_FAMILY_PAIR)

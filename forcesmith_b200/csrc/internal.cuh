@@ -144,6 +144,11 @@ struct fs_gpu {
   int family = 0, ntypes = 1;
   std::vector<fsg::HostTable> tables;
   int D = 0;                // free parameters
+  // global parameters: values and columns (−1 fixed); shared_cols when a
+  // free global has links, i.e. several values share one column
+  std::vector<double> global_val;
+  std::vector<int> global_col;
+  bool shared_cols = false;
   std::vector<fsg::TableDesc> desc;
   int n_segs = 0, n_cmap = 0, n_vals = 0;
   fsg::TableDesc *d_desc = nullptr;
@@ -257,6 +262,7 @@ int upload_tables(fs_gpu *h);          // structure + values (after set_model)
 int upload_values(fs_gpu *h);          // values only (after set_params), asynchronous
 int ensure_pinned(fs_gpu *h, double **buf, size_t *cap, size_t n);
 int refresh_segments(fs_gpu *h);       // recompute segment data from d_vals
+int spline_segments_fp64(fs_gpu *h, const double *d_x1, double4 *seg); // FP64 segments at x (n_segs)
 double model_max_cutoff(const fs_gpu *h);
 
 // eam.cu / pair

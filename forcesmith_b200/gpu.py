@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         L.fs_gpu_eval_jacobian_async.argtypes = [vp, dbl, dbl]
         L.fs_gpu_copy_jacobian_rows.argtypes = [vp, i64, i64, pd, i64]
         L.fs_gpu_check_bounded_wait.argtypes = [vp, i64]
+        L.fs_gpu_max_cutoff.argtypes = [vp, pd]
+        L.fs_gpu_tabulate.argtypes = [vp, C.c_int32, C.c_int32, pd, pd, pd]
         L.fs_gpu_fetch_normal_equations.argtypes = [vp, pd, pd, pd]
         L.fs_gpu_lm_step.argtypes = [vp, dbl, i32, pd]
         L.fs_gpu_lsq_step.argtypes = [vp, dbl, pd]
@@ -150,6 +152,21 @@ class GpuSession(Session):
         self._check(self._lib.fs_gpu_copy_jacobian_rows(self._h, int(row0), int(nrows), _dp(buf), int(ld)),
                     "copy_jacobian_rows")
         return buf[:, :nrows].T, buf
+
+    def max_cutoff(self):
+        """fs_gpu_max_cutoff: the model's interaction cut-off."""
+        rc = C.c_double()
+        self._check(self._lib.fs_gpu_max_cutoff(self._h, C.byref(rc)), "max_cutoff")
+        return rc.value
+
+    def tabulate(self, table, r):
+        """fs_gpu_tabulate: (value, d/dr) of radial table `table` at the
+        points r, FP64, at the current parameters."""
+        r = np.ascontiguousarray(r, np.float64)
+        v, dv = np.zeros(r.size), np.zeros(r.size)
+        self._check(self._lib.fs_gpu_tabulate(self._h, int(table), int(r.size), _dp(r), _dp(v), _dp(dv)),
+                    "tabulate")
+        return v, dv
 
     def jacobian_async(self, w_e=1.0, w_s=0.0):
         self._check(self._lib.fs_gpu_eval_jacobian_async(self._h, w_e, w_s), "eval_jacobian_async")

@@ -15,8 +15,17 @@
       objects, "lambda").  A table section is {"format", "potentials": [...]}
       with tabulated {rmin, rmax, knots, fixed?} or analytic {type, rmin,
       rmax, <parameter>: number | {value, min?, max?, fixed?}} entries
-      (src/io/potential_reader.cpp:60-200).  Global parameters ("globals")
-      are not supported here.
+      (src/io/potential_reader.cpp:60-200).  Pair and EAM models may carry
+      global parameters: {"globals": {name: {value, fixed?}}} and
+      {"global": name} in place of an analytic parameter
+      (force_model_reader.cpp:59-117).
+  read_potential  a bare potential section → list of tables
+      (parse_potential, src/io/potential_reader.cpp).
+  write_native / write_lammps / write_imd / write_model_file  the sampled
+      writers of src/io/output_writer.cpp and write_model.cpp: every radial
+      table on 500 uniform points of its span, values (and derivatives for
+      LAMMPS) from a sampler — fs_gpu_tabulate on the device through
+      session_sampler.
   read_setfl  a single-element LAMMPS setfl file as three makima tables on
       the file's own grids (φ = r·φ / r from the second r point on).
 """
@@ -30,7 +39,8 @@ import numpy as np
 
 from .abi import (FS_FAMILY_ACSF, FS_FAMILY_ADP, FS_FAMILY_ANGULAR, FS_FAMILY_EAM, FS_FAMILY_PAIR,
                   FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_TABLE_ANALYTIC, FS_TABLE_LAMBDA, FS_TABLE_SPLINE,
-                  FS_TABLE_SW, FS_TABLE_TERSOFF, FORMS, TERSOFF_FIELDS, Dataset, Model, Table, acsf_size)
+                  FS_TABLE_SW, FS_TABLE_TERSOFF, FORMS, TERSOFF_FIELDS, Dataset, GlobalParam, Model, Table,
+                  acsf_size)
 
 SYMBOLS = (
     "H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
@@ -109,6 +119,24 @@ def _text(src):
     return src
 
 
+def _json(src):
+    """Parsed JSON, with a syntax error reported as a FormatError."""
+    try:
+        return json.loads(_text(src))
+    except json.JSONDecodeError as e:
+        raise FormatError(f"invalid JSON: {e}") from None
+
+
+def _vec3(v, what):
+    try:
+        a = np.asarray(v, np.float64)
+    except (TypeError, ValueError):
+        raise FormatError(f"{what}: must be an array of 3 numbers") from None
+    if a.shape != (3,):
+        raise FormatError(f"{what}: must be an array of 3 numbers")
+    return a
+
+
 # ---------------------------------------------------------------------------
 # configurations
 
@@ -122,7 +150,7 @@ def species_slots(symbols):
 
 def read_configs(src):
     """Configuration JSON → (Dataset, species symbols by slot, names, weights)."""
-    j = json.loads(_text(src))
+    j = _json(src)
     if not isinstance(j, list):
         raise FormatError("top-level JSON must be an array of configurations")
     syms = [a["element"] for c in j if isinstance(c, dict) for a in c.get("atoms", [])
@@ -137,9 +165,7 @@ def read_configs(src):
         for k in ("X", "Y", "Z", "E", "atoms"):
             if k not in c:
                 raise FormatError(f"{ctx}: missing key '{k}'")
-        cols = [np.asarray(c[k], np.float64) for k in ("X", "Y", "Z")]
-        if any(v.shape != (3,) for v in cols):
-            raise FormatError(f"{ctx}: X, Y, Z must be arrays of 3 doubles")
+        cols = [_vec3(c[k], f"{ctx} '{k}'") for k in ("X", "Y", "Z")]
         box9.append(np.stack(cols, axis=1).ravel())  # lattice vectors as columns, row-major
         ene.append(float(c["E"]))
         weights.append(float(c.get("W", 1.0)))
@@ -162,8 +188,8 @@ def read_configs(src):
             if "element" not in a or "position" not in a:
                 raise FormatError(f"{ctx} atom[{ai}]: needs 'element' and 'position'")
             typ.append(slot_of[a["element"]])
-            pos.append(np.asarray(a["position"], np.float64))
-            frc.append(np.asarray(a.get("force", (0.0, 0.0, 0.0)), np.float64))
+            pos.append(_vec3(a["position"], f"{ctx} atom[{ai}] 'position'"))
+            frc.append(_vec3(a.get("force", (0.0, 0.0, 0.0)), f"{ctx} atom[{ai}] 'force'"))
     ds = Dataset(np.asarray(natoms, np.int32), np.asarray(box9).reshape(-1, 9),
                  np.asarray(pos).reshape(-1, 3), np.asarray(typ, np.int32), np.asarray(frc).reshape(-1, 3),
                  np.asarray(ene), np.asarray(st9).reshape(-1, 9))
@@ -222,7 +248,11 @@ def _potential(p):
                               fixed=np.array([x[3] for x in vals], np.uint8),
                               lower=np.array([x[1] for x in vals]), upper=np.array([x[2] for x in vals]))
     if "knots" in p:
-        y = np.asarray(p["knots"], np.float64)
+        knots = p["knots"]
+        if not isinstance(knots, list) or not all(
+                isinstance(v, (int, float)) and not isinstance(v, bool) for v in knots):
+            raise FormatError("tabulated potential: 'knots' must be an array of numbers")
+        y = np.asarray(knots, np.float64)
         if y.size < 2:
             raise FormatError("tabulated potential needs at least 2 knots")
         rmin, rmax = float(p["rmin"]), float(p["rmax"])
@@ -246,12 +276,56 @@ def _section(sub, want, label):
     return [_potential(p) for p in pots]
 
 
+def read_potential(src):
+    """A potential section {"format", "potentials": [...]} → list of Tables
+    (parse_potential, src/io/potential_reader.cpp)."""
+    j = _json(src)
+    if not isinstance(j, dict):
+        raise FormatError("potential file must be a JSON object")
+    pots = j.get("potentials")
+    return _section(j, len(pots) if isinstance(pots, list) else -1, "potential")
+
+
+def _build_globals(j, regions):
+    """build_globals (src/io/force_model_reader.cpp:59-117): the "globals"
+    object {name: {value, fixed?}} (min and max are not read), then every
+    analytic parameter given as {"global": name} in the region sections is
+    linked to that global and replaced by its seed value.  regions: (section
+    JSON, first table index of the section)."""
+    out, by_name = [], {}
+    for gname, spec in (j.get("globals") or {}).items():
+        if not isinstance(spec, dict) or "value" not in spec:
+            raise FormatError(f"globals: global '{gname}' missing 'value'")
+        by_name[gname] = len(out)
+        out.append(GlobalParam(float(spec["value"]), bool(spec.get("fixed", False)), [], gname))
+    for sub, t0 in regions:
+        pots = sub.get("potentials") if isinstance(sub, dict) else None
+        if not isinstance(pots, list):
+            continue
+        for i, pot in enumerate(pots):
+            if not isinstance(pot, dict) or "type" not in pot:
+                continue
+            for key in [k for k, v in pot.items() if isinstance(v, dict) and "global" in v]:
+                gname = pot[key]["global"]
+                if gname not in by_name:
+                    raise FormatError(f"globals: reference to undefined global '{gname}'")
+                spec = FORM_SPEC.get(pot["type"])
+                if spec is None or key not in spec[1]:
+                    raise FormatError(f"globals: global ref on parameter '{key}' not valid for analytic "
+                                      f"type '{pot['type']}'")
+                g = out[by_name[gname]]
+                g.links.append((t0 + i, spec[1].index(key)))
+                pot[key] = g.value
+    return out
+
+
 def read_model(src):
     """Force-model JSON → Model (families pair, eam, adp, angular, stiweb,
-    tersoff, and ml with an ACSF descriptor and linear heads)."""
-    j = json.loads(_text(src))
-    if "globals" in j:
-        raise FormatError("global parameters are not supported by this reader")
+    tersoff, and ml with an ACSF descriptor and linear heads).  Pair and EAM
+    models may carry global parameters ("globals")."""
+    j = _json(src)
+    if not isinstance(j, dict):
+        raise FormatError("force-model file must be a JSON object")
     if "model" not in j:
         count = len(j.get("potentials", [])) if isinstance(j.get("potentials"), list) else 0
         nt = 1
@@ -259,7 +333,8 @@ def read_model(src):
             nt += 1
         if nt * (nt + 1) // 2 != count:
             raise FormatError(f"bare pair file: {count} potentials is not a valid pair count for any ntypes")
-        return Model(FS_FAMILY_PAIR, nt, _section(j, count, "pair"))
+        glob = _build_globals(j, [(j, 0)])
+        return _finish_globals(Model(FS_FAMILY_PAIR, nt, _section(j, count, "pair")), glob)
     name = j["model"]
     if name == "ml":
         return _read_ml(j)
@@ -307,16 +382,45 @@ def read_model(src):
                           np.array([v[3] for v in vals], np.uint8), np.array([v[1] for v in vals]),
                           np.array([v[2] for v in vals])))
         return Model(fam, nt, tabs)
-    tabs = []
+    subs, regions, t0 = [], [], 0
     for key in TABLE_KEYS[fam]:
         sub = j if (name == "pair" and key == "pair" and "pair" not in j) else j.get(key)
         if sub is None:
             raise FormatError(f"{name}: missing section '{key}'")
-        tabs += _section(sub, npair if PER_PAIR[key] else nt, f"{name}.{key}")
-    return Model(fam, nt, tabs)
+        n = npair if PER_PAIR[key] else nt
+        subs.append((sub, n, f"{name}.{key}"))
+        regions.append((sub, t0))
+        t0 += n
+    # global parameters belong to the pair and EAM calculators (with_globals<>,
+    # pair_force.hpp:27, eam_force.hpp:18)
+    glob = _build_globals(j, regions) if fam in (FS_FAMILY_PAIR, FS_FAMILY_EAM) else []
+    tabs = []
+    for sub, n, label in subs:
+        tabs += _section(sub, n, label)
+    return _finish_globals(Model(fam, nt, tabs), glob)
 
 
-def _pot_json(t):
+def _finish_globals(model, glob):
+    """finalize_globals (force_calculator_concept.hpp:230-237): linked
+    parameters fixed, then every global broadcast to its links."""
+    model.globals = glob
+    for g in glob:
+        for tk, slot in g.links:
+            t = model.tables[tk]
+            if t.fixed is None:
+                t.fixed = np.zeros(t.values.size, np.uint8)
+            t.fixed[slot] = 1
+            if t.lower is not None:
+                t.lower[slot] = -math.inf
+            if t.upper is not None:
+                t.upper[slot] = math.inf
+    return model.broadcast_globals()
+
+
+def _pot_json(t, refs=None):
+    """One potential entry; refs maps a parameter slot to the name of the
+    global it is linked to (written as {"global": name})."""
+    refs = refs or {}
     if t.kind == FS_TABLE_SPLINE:
         d = {"rmin": t.rmin, "rmax": t.rmax, "knots": [float(v) for v in t.values]}
         if t.fixed is not None and np.all(t.fixed):
@@ -325,6 +429,9 @@ def _pot_json(t):
     name = FORM_NAME[t.form]
     d = {"type": name, "rmin": t.rmin, "rmax": t.rmax}
     for k, nm in enumerate(PARAM_NAMES[t.form]):
+        if k in refs:
+            d[nm] = {"global": refs[k]}
+            continue
         lo = -math.inf if t.lower is None else float(t.lower[k])
         hi = math.inf if t.upper is None else float(t.upper[k])
         fx = False if t.fixed is None else bool(t.fixed[k])
@@ -429,8 +536,10 @@ def _tersoff_json(t):
 
 
 def write_model(model):
-    """Model → force-model JSON text (families pair, eam, adp, angular,
-    tersoff, and ml with an ACSF descriptor)."""
+    """Model → force-model JSON text, lossless: analytic tables keep their
+    closed forms and parameter specs (families pair, eam, adp, angular,
+    stiweb, tersoff, and ml with an ACSF descriptor).  write_native samples
+    every radial table instead, as the reference's writer does."""
     nt, fam = model.ntypes, model.family
     npair = nt * (nt + 1) // 2
     if fam == FS_FAMILY_ACSF:
@@ -438,16 +547,39 @@ def write_model(model):
     if fam == FS_FAMILY_TERSOFF:
         return json.dumps({"model": "tersoff", "ntypes": nt,
                            "potentials": [_tersoff_json(t) for t in model.tables]}, indent=1)
+    if fam == FS_FAMILY_SW:
+        # write_native for stiweb (output_writer.cpp:125-135): SWParams per
+        # pair, then the triplet λ array
+        def entry(t, k):
+            lo = -math.inf if t.lower is None else float(t.lower[k])
+            hi = math.inf if t.upper is None else float(t.upper[k])
+            fx = False if t.fixed is None else bool(t.fixed[k])
+            if math.isinf(lo) and math.isinf(hi) and not fx:
+                return float(t.values[k])
+            return {"value": float(t.values[k]), "fixed": fx,
+                    **({} if math.isinf(lo) else {"min": lo}), **({} if math.isinf(hi) else {"max": hi})}
+        pots = [{nm: entry(t, k) for k, nm in enumerate(SW_FIELDS)} for t in model.tables[:npair]]
+        lam = model.tables[npair]
+        return json.dumps({"model": "stiweb", "ntypes": nt, "potentials": pots,
+                           "lambda": [entry(lam, k) for k in range(lam.values.size)]}, indent=1)
     if fam not in TABLE_KEYS:
-        raise FormatError("write_model: pair, eam, adp, angular and tersoff families")
+        raise FormatError("write_model: unsupported model family")
     out = {"model": NAME_OF[fam], "ntypes": nt}
+    names = [g.name or f"g{i}" for i, g in enumerate(model.globals)]
+    refs = {}
+    for g, gname in zip(model.globals, names):
+        for tk, slot in g.links:
+            refs.setdefault(tk, {})[slot] = gname
+    if model.globals:
+        out["globals"] = {gname: {"value": float(g.value), "fixed": bool(g.fixed)}
+                          for g, gname in zip(model.globals, names)}
     k = 0
     for key in TABLE_KEYS[fam]:
         n = npair if PER_PAIR[key] else nt
         tabs = model.tables[k:k + n]
-        k += n
         fmt = "analytic" if all(t.kind == FS_TABLE_ANALYTIC for t in tabs) else "tabulated"
-        out[key] = {"format": fmt, "potentials": [_pot_json(t) for t in tabs]}
+        out[key] = {"format": fmt, "potentials": [_pot_json(t, refs.get(k + i)) for i, t in enumerate(tabs)]}
+        k += n
     return json.dumps(out, indent=1)
 
 
@@ -475,3 +607,117 @@ def read_setfl(path):
                                      Table.spline(0.0, drho * (nrho - 1), F)])
     header = dict(element=lines[3].split()[1], nrho=nrho, drho=drho, nr=nr, dr=dr, rc=rc)
     return model, header
+
+
+# ---------------------------------------------------------------------------
+# sampled writers (src/io/output_writer.cpp, src/io/write_model.cpp)
+
+DEFAULT_KNOTS = 500  # kDefaultKnots, include/forcesmith/io/output_writer.hpp:19
+
+
+def _span(t):
+    """RadialPotential::span: the knot span of a spline, the gate span of an
+    analytic form."""
+    return float(t.rmin), float(t.rmax)
+
+
+def _grid(t, nknots):
+    lo, hi = _span(t)
+    step = (hi - lo) / (nknots - 1)
+    return lo, hi, lo + np.arange(nknots) * step
+
+
+def _sampled(model, k, sample, nknots):
+    """sample_one (output_writer.cpp:22-40): {rmin, rmax, knots} of table k
+    on nknots uniform points of its span; a non-finite value is an error."""
+    lo, hi, r = _grid(model.tables[k], nknots)
+    v, _ = sample(k, r)
+    bad = np.nonzero(~np.isfinite(v))[0]
+    if bad.size:
+        q = int(bad[0])
+        raise FormatError(f"non-finite potential value ({v[q]}) at r={r[q]:.6f}; "
+                          "cannot tabulate potential for output")
+    return {"rmin": lo, "rmax": hi, "knots": [float(x) for x in v]}
+
+
+def session_sampler(sess):
+    """The sampler of a GpuSession holding the model: fs_gpu_tabulate."""
+    return lambda k, r: sess.tabulate(k, r)
+
+
+def write_native(model, sample, nknots=DEFAULT_KNOTS):
+    """write_native (output_writer.cpp:42-119): every radial table sampled
+    onto nknots knots.  A pair model is a bare potential section; EAM, ADP and
+    angular models are {"model", "ntypes", <section>: …}; Stillinger–Weber,
+    Tersoff and ACSF models carry their parameters as they are.
+    sample(k, r) → (values, derivatives) of table k at the points r."""
+    fam, nt = model.family, model.ntypes
+    if fam in (FS_FAMILY_TERSOFF, FS_FAMILY_ACSF, FS_FAMILY_SW):
+        return write_model(model)
+    if fam not in TABLE_KEYS:
+        raise FormatError("write_native: unsupported model family")
+    npair = nt * (nt + 1) // 2
+    if fam == FS_FAMILY_PAIR:
+        return json.dumps({"format": "tabulated",
+                           "potentials": [_sampled(model, k, sample, nknots) for k in range(npair)]}, indent=2)
+    out, k = {"model": NAME_OF[fam], "ntypes": nt}, 0
+    for key in TABLE_KEYS[fam]:
+        n = npair if PER_PAIR[key] else nt
+        out[key] = {"format": "tabulated",
+                    "potentials": [_sampled(model, k + i, sample, nknots) for i in range(n)]}
+        k += n
+    return json.dumps(out, indent=2)
+
+
+def _g(x):
+    """A double as a default-formatted C++ stream writes it (6 significant
+    digits, %g style)."""
+    return format(float(x), "g")
+
+
+def write_lammps(model, sample):
+    """write_lammps (output_writer.cpp:266-289), pair models: per pair table
+    a "# pair potential k" / "POT_k" / "N 500 R lo hi" block, then one
+    "index r φ(r) φ'(r)" line per knot."""
+    if model.family != FS_FAMILY_PAIR:
+        raise FormatError("write_lammps: pair models only")
+    lines = []
+    for k, t in enumerate(model.tables):
+        lo, hi, r = _grid(t, DEFAULT_KNOTS)
+        v, dv = sample(k, r)
+        lines += [f"# pair potential {k}", f"POT_{k}", f"N {DEFAULT_KNOTS} R {_g(lo)} {_g(hi)}", ""]
+        lines += [f"{q + 1} {_g(r[q])} {_g(v[q])} {_g(dv[q])}" for q in range(DEFAULT_KNOTS)]
+        lines.append("")
+    return "\n".join(lines) + "\n"
+
+
+def write_imd(model, sample):
+    """write_imd (output_writer.cpp:291-310), pair models: the "#F 3 n",
+    "#T IMD", "#E" header, one "lo hi 500" line per table, then every
+    table's 500 values, one per line."""
+    if model.family != FS_FAMILY_PAIR:
+        raise FormatError("write_imd: pair models only")
+    lines = [f"#F 3 {len(model.tables)}", "#T IMD", "#E"]
+    lines += [f"{_g(_span(t)[0])} {_g(_span(t)[1])} {DEFAULT_KNOTS}" for t in model.tables]
+    for k, t in enumerate(model.tables):
+        _, _, r = _grid(t, DEFAULT_KNOTS)
+        lines += [_g(x) for x in sample(k, r)[0]]
+    return "\n".join(lines) + "\n"
+
+
+def write_model_file(model, path, fmt, sample):
+    """write_model (src/io/write_model.cpp:22-55): "lammps" and "imd" for
+    pair models, native JSON otherwise (another format for another family
+    writes native JSON with a warning on stderr)."""
+    import sys
+    if model.family == FS_FAMILY_PAIR and fmt == "lammps":
+        text = write_lammps(model, sample)
+    elif model.family == FS_FAMILY_PAIR and fmt == "imd":
+        text = write_imd(model, sample)
+    else:
+        if fmt != "native" and model.family != FS_FAMILY_PAIR:
+            print(f"warning: '{fmt}' output unsupported for {NAME_OF.get(model.family, 'ml')}; "
+                  "writing native JSON", file=sys.stderr)
+        text = write_native(model, sample)
+    with open(path, "w") as f:
+        f.write(text if text.endswith("\n") else text + "\n")

@@ -52,6 +52,8 @@
  *                               src/optimization/forcesmith_functor.cpp:111-132)
  *   fs_gpu_max_cutoff          CForceCalculator::max_cutoff
  *                              (include/forcesmith/force/force_calculator_concept.hpp:210-225,288-292)
+ *   fs_gpu_tabulate            RadialPotential::eval / deriv as the model writers
+ *                              sample them (src/io/output_writer.cpp:22-40,266-310)
  *   fs_gpu_lm_step / fs_gpu_lsq_step
  *                              the LM / lsq step of EigenLMSolver and
  *                              NormalEquationsSolver (src/optimization/solver.cpp:67-85,242-266)
@@ -194,6 +196,22 @@ typedef struct fs_model {
   int32_t n_tables; /* must equal the family's table count                  */
   int32_t reserved;
   const fs_table *tables; /* in the reference's gather order                */
+  /* Global parameters (GlobalParam, force_calculator_concept.hpp:21-44;
+   * pair and EAM families, analytic tables): n_globals values and fixed
+   * flags (nullable: all free), and n_links links (global, table in model
+   * order, parameter slot).  A linked parameter is fixed in its table and
+   * takes the global's value (finalize_globals, :235-242); a free global's
+   * column follows every table column, in global order (:171-208).  The
+   * global's own min/max are not kept (build_globals reads only value and
+   * fixed, force_model_reader.cpp:64-75): its bounds are ±inf.  Zero
+   * everything for a model without globals. */
+  int32_t n_globals;
+  int32_t n_links;
+  const double *global_values;
+  const uint8_t *global_fixed;
+  const int32_t *link_global;
+  const int32_t *link_table;
+  const int32_t *link_param;
 } fs_model;
 
 /* ---- context ----------------------------------------------------------- */
@@ -248,6 +266,14 @@ int fs_gpu_set_params(fs_gpu *h, const double *x, int32_t D);
 /* The model's interaction cut-off: CForceCalculator::max_cutoff
  * (force_calculator_concept.hpp:210-221; SW: max(a1, a2), stiweb_force.cpp:234-239). */
 int fs_gpu_max_cutoff(fs_gpu *h, double *rc);
+
+/* Value and d/dr of radial table `table` (model order; a spline or analytic
+ * table) at the current parameters, at n points r[]: what the reference's
+ * writers sample with RadialPotential::eval / deriv (output_writer.cpp:22-40,
+ * 266-310).  Always FP64, whatever the context precision; a spline outside
+ * its knot span gives its linear extension.  Other table kinds: FS_ERR_ARG.
+ * Needs a model only (no configurations). */
+int fs_gpu_tabulate(fs_gpu *h, int32_t table, int32_t n, const double *r, double *value, double *deriv);
 
 /* rows = Σ_c 3N_c + 2 + (w_s > 0 ? 6 : 0)  (residual_layout.hpp:18-31) */
 int fs_gpu_residual_count(fs_gpu *h, double w_s, int64_t *m);

@@ -140,6 +140,11 @@ struct State {
   bool have_model = false;
   int family = 0, ntypes = 1;
   std::vector<Table> tables;
+  // global parameters (GlobalParam, force_calculator_concept.hpp:21-44):
+  // values, fixed flags, links (global, table, slot)
+  std::vector<double> gval;
+  std::vector<uint8_t> gfixed;
+  std::vector<std::array<int, 3>> links;
   // spline sites per pair per role (φ, g_j, g_i, u, w); −1 = not cached
   std::vector<Site> site[5];
   std::vector<uint8_t> site_ok[5];
@@ -1053,22 +1058,32 @@ int64_t write_residuals(const State &S, int c, const Out &o, double w_e, double 
   return row;
 }
 
+// TableParams (force_calculator_concept.hpp:171-208): tables in order, then
+// the free globals; scatter broadcasts each global to its links (:225-229).
 int param_count(const State &S) {
   int D = 0;
   for (const Table &t : S.tables) D += t.param_count();
+  for (uint8_t f : S.gfixed) D += f ? 0 : 1;
   return D;
 }
 void gather(const State &S, double *x) {
   int o = 0;
   for (const Table &t : S.tables)
     for (int k : t.free_idx) x[o++] = t.v[k];
+  for (std::size_t g = 0; g < S.gval.size(); ++g)
+    if (!S.gfixed[g]) x[o++] = S.gval[g];
+}
+void broadcast_globals(State &S) {
+  for (const auto &lk : S.links) S.tables[lk[1]].v[lk[2]] = S.gval[lk[0]];
 }
 void scatter(State &S, const double *x) {
   int o = 0;
-  for (Table &t : S.tables) {
+  for (Table &t : S.tables)
     for (int k : t.free_idx) t.v[k] = x[o++];
-    t.refresh();
-  }
+  for (std::size_t g = 0; g < S.gval.size(); ++g)
+    if (!S.gfixed[g]) S.gval[g] = x[o++];
+  broadcast_globals(S);
+  for (Table &t : S.tables) t.refresh();
 }
 
 std::vector<int64_t> row_offsets(const State &S, double w_s) {
@@ -1401,6 +1416,30 @@ int orc_set_model(orc_state *h, const fs_model *m) {
     if (ft.kind == FS_TABLE_TERSOFF && ft.n != 12) return FS_ERR_ARG;
     S.tables[t].init(ft);
   }
+  // globals: pair and EAM only, links on analytic parameters; a linked
+  // parameter is fixed and takes the global's value (finalize_globals)
+  S.gval.assign(m->global_values, m->global_values + std::max(m->n_globals, 0));
+  S.gfixed.assign(S.gval.size(), 0);
+  S.links.clear();
+  if (m->n_globals > 0 && S.family != FS_FAMILY_EAM && S.family != FS_FAMILY_PAIR) return FS_ERR_ARG;
+  for (std::size_t g = 0; g < S.gval.size(); ++g) S.gfixed[g] = m->global_fixed && m->global_fixed[g] ? 1 : 0;
+  for (int l = 0; l < m->n_links; ++l) {
+    const int g = m->link_global[l], t = m->link_table[l], k = m->link_param[l];
+    if (g < 0 || g >= m->n_globals || t < 0 || t >= m->n_tables) return FS_ERR_ARG;
+    Table &tb = S.tables[t];
+    if (tb.kind != FS_TABLE_ANALYTIC || k < 0 || k >= tb.n) return FS_ERR_ARG;
+    tb.fixed[k] = 1;
+    tb.lo[k] = -std::numeric_limits<double>::infinity();
+    tb.hi[k] = std::numeric_limits<double>::infinity();
+    S.links.push_back({g, t, k});
+  }
+  for (Table &tb : S.tables) {
+    tb.free_idx.clear();
+    for (int k = 0; k < tb.n; ++k)
+      if (!tb.fixed[k]) tb.free_idx.push_back(k);
+  }
+  broadcast_globals(S);
+  for (Table &tb : S.tables) tb.refresh();
   S.have_model = true;
   S.rcut_built = -1;
   return FS_OK;
@@ -1454,6 +1493,12 @@ int orc_gather_bounds(orc_state *h, double *lo, double *hi) {
     for (int k : t.free_idx) {
       lo[o] = t.lo[k];
       hi[o] = t.hi[k];
+      ++o;
+    }
+  for (std::size_t g = 0; g < h->S.gval.size(); ++g) // build_globals keeps no min/max
+    if (!h->S.gfixed[g]) {
+      lo[o] = -std::numeric_limits<double>::infinity();
+      hi[o] = std::numeric_limits<double>::infinity();
       ++o;
     }
   return FS_OK;
@@ -1549,6 +1594,8 @@ int orc_eval_jacobian_analytic(orc_state *h, double w_e, double w_s, double *J) 
   State &S = h->S;
   if (S.rcut_built < 0) return FS_ERR_STATE;
   if (S.family != FS_FAMILY_EAM && S.family != FS_FAMILY_PAIR) return FS_ERR_UNSUPPORTED;
+  for (uint8_t f : S.gfixed) // analytic_jacobian_available (param_jacobian.hpp:44-57)
+    if (!f) return FS_ERR_UNSUPPORTED;
   const auto ro = row_offsets(S, w_s);
   const int64_t m = ro.back();
   const int D = param_count(S);

@@ -45,7 +45,7 @@ def test_create_without_device_fails_cleanly():
 
 def test_struct_layout_matches_header():
     assert C.sizeof(fs_table) == 4 * 4 + 2 * 8 + 4 * 8
-    assert C.sizeof(fs_model) == 4 * 4 + 8
+    assert C.sizeof(fs_model) == 4 * 4 + 8 + 2 * 4 + 5 * 8
 
 
 def test_synthetic_workloads_are_deterministic():

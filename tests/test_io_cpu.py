@@ -135,8 +135,9 @@ def test_model_json_forms_and_errors():
     bad = dict(eam, pair={"format": "analytic", "potentials": [{"type": "nope", "rmin": 0, "rmax": 1}]})
     with pytest.raises(io.FormatError):
         io.read_model(json.dumps(bad))
-    with pytest.raises(io.FormatError):
-        io.read_model(json.dumps(dict(eam, globals={"g": {"value": 1.0}})))
+    # a global without links is still a free parameter, after the tables'
+    g = io.read_model(json.dumps(dict(eam, globals={"g": {"value": 1.5}})))
+    assert g.free_values()[-1] == 1.5 and g.free_values().size == m.free_values().size + 1
 
 
 def test_evaluate_report_sums_to_objective():
