@@ -75,11 +75,21 @@ struct GpuTable {
   std::vector<double> lower, upper; // empty: unbounded
 };
 
+// A global parameter (GlobalParam, force_calculator_concept.hpp:21-44): its
+// value, fixed flag and links (table in model order, parameter slot).  Pair
+// and EAM models only; a free global's column follows the tables' columns.
+struct GpuGlobal {
+  double value = 0.0;
+  bool fixed = false;
+  std::vector<std::pair<int, int>> links;
+};
+
 // A model in the reference's gather order (force_calculator_concept.hpp:171-284).
 struct GpuModel {
   int family = FS_FAMILY_EAM;
   int ntypes = 1;
   std::vector<GpuTable> tables;
+  std::vector<GpuGlobal> globals;
 };
 
 namespace gpu_detail {
@@ -87,8 +97,20 @@ namespace gpu_detail {
 // The ABI view of a model (pointers into `m`, valid while `m` lives).
 struct ModelView {
   std::vector<fs_table> t;
+  std::vector<double> gv;
+  std::vector<uint8_t> gf;
+  std::vector<int32_t> lg, lt, lp;
   fs_model m{};
   explicit ModelView(const GpuModel &g) : t(g.tables.size()) {
+    for (std::size_t k = 0; k < g.globals.size(); ++k) {
+      gv.push_back(g.globals[k].value);
+      gf.push_back(g.globals[k].fixed ? 1 : 0);
+      for (const auto &[tab, slot] : g.globals[k].links) {
+        lg.push_back(static_cast<int32_t>(k));
+        lt.push_back(tab);
+        lp.push_back(slot);
+      }
+    }
     for (std::size_t k = 0; k < g.tables.size(); ++k) {
       const GpuTable &s = g.tables[k];
       fs_table &d = t[k];
@@ -108,6 +130,13 @@ struct ModelView {
     m.n_tables = static_cast<int32_t>(t.size());
     m.reserved = 0;
     m.tables = t.data();
+    m.n_globals = static_cast<int32_t>(gv.size());
+    m.n_links = static_cast<int32_t>(lg.size());
+    m.global_values = gv.empty() ? nullptr : gv.data();
+    m.global_fixed = gf.empty() ? nullptr : gf.data();
+    m.link_global = lg.empty() ? nullptr : lg.data();
+    m.link_table = lt.empty() ? nullptr : lt.data();
+    m.link_param = lp.empty() ? nullptr : lp.data();
   }
 };
 
