@@ -835,3 +835,12 @@ int fs_gpu_eval_population(fs_gpu *h, double w_e, double w_s, const double *xs, 
 }
 
 } // extern "C"
+
+extern "C" int fs_gpu_abi_sizes(int64_t *sizes, int32_t n) {
+  const int64_t s[6] = {static_cast<int64_t>(sizeof(fs_table)),       static_cast<int64_t>(sizeof(fs_model)),
+                        static_cast<int64_t>(sizeof(fs_gpu_opts)),    static_cast<int64_t>(sizeof(fs_tune_report)),
+                        static_cast<int64_t>(sizeof(fs_de_opts)),     static_cast<int64_t>(sizeof(fs_surrogate_opts))};
+  if (!sizes || n < 0) return FS_ERR_ARG;
+  for (int k = 0; k < n && k < 6; ++k) sizes[k] = s[k];
+  return 6;
+}

@@ -11,13 +11,24 @@ import os
 
 import numpy as np
 
-from .abi import (fs_de_opts, fs_surrogate_opts, fs_tune_report, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
+from .abi import (fs_de_opts, fs_surrogate_opts, fs_table, fs_tune_report, FS_OK, FS_PREC_FP32, FS_PREC_FP64, FsError, Session, _dp, _ip, fs_gpu_opts,
                   fs_model, load_library)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libforcesmith_b200.so")
 
 _LIB = None
+
+
+def _check_abi(L):
+    """The library's struct sizes against these bindings' (a stale build
+    would otherwise write past a caller's struct)."""
+    ours = [C.sizeof(t) for t in (fs_table, fs_model, fs_gpu_opts, fs_tune_report, fs_de_opts, fs_surrogate_opts)]
+    got = (C.c_int64 * 6)()
+    L.fs_gpu_abi_sizes.argtypes = [C.POINTER(C.c_int64), C.c_int32]
+    if L.fs_gpu_abi_sizes(got, 6) != 6 or list(got) != ours:
+        raise ImportError(f"{LIB_PATH} was built against another forcesmith_gpu.h (struct sizes {list(got)}, "
+                          f"bindings {ours}); rebuild it with `python -m forcesmith_b200.build`")
 
 
 def lib() -> C.CDLL:
@@ -27,6 +38,7 @@ def lib() -> C.CDLL:
             raise FileNotFoundError(
                 f"{LIB_PATH} is not built; run `python -m forcesmith_b200.build` (nvcc, sm_100a)")
         L = load_library(LIB_PATH)
+        _check_abi(L)
         vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
         pd, pi = C.POINTER(C.c_double), C.POINTER(C.c_int32)
         L.fs_gpu_create.argtypes = [C.POINTER(fs_gpu_opts), C.POINTER(vp)]

@@ -371,6 +371,13 @@ int fs_gpu_launch_count(fs_gpu *h, int64_t *count);
  */
 int fs_gpu_check_bounded_wait(fs_gpu *h, int64_t cycles);
 
+/* sizeof of the ABI's structs as this library was compiled, in the order
+ * fs_table, fs_model, fs_gpu_opts, fs_tune_report, fs_de_opts,
+ * fs_surrogate_opts, into sizes[0..n): a binding compares them with its own
+ * declarations when it loads the library, so that a stale build fails at
+ * load rather than writing past a caller's struct.  Returns the count. */
+int fs_gpu_abi_sizes(int64_t *sizes, int32_t n);
+
 /*
  * Batched objective: obj[k] = ‖F(x_k)‖² for NP parameter vectors xs[NP·D]
  * (row-major), all configurations, one launch.  The DE population kernel.
