@@ -34,7 +34,7 @@ template <class T> struct AgArgs {
   const int32_t *order; // configurations by work, heaviest first
 };
 
-template <class T> __global__ void __launch_bounds__(kAgThreads, sizeof(T) == 4 ? 3 : 1) angular_kernel(AgArgs<T> A) {
+template <class T> __global__ void __launch_bounds__(kAgThreads, sizeof(T) == 4 ? 3 : 2) angular_kernel(AgArgs<T> A) {
   using T4 = typename Vec4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int c = A.order ? A.order[blockIdx.x] : blockIdx.x;

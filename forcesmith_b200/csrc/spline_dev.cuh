@@ -60,6 +60,14 @@ template <class T> __device__ __forceinline__ VD<T> form_vd(int form, const doub
   return VD<T>{f.a, f.b};
 }
 
+// form_vd out of line, for the table helpers below that kernels taking both
+// spline and analytic tables call at every pair: the 34 forms' code then
+// stays out of those kernels' register allocation (a call only where a table
+// is analytic).
+template <class T> __device__ __noinline__ VD<T> form_vd_call(int form, const double *pp, int n, T r, T rmax) {
+  return form_vd<T>(form, pp, n, r, rmax);
+}
+
 // Closed gate [x0, x_{n-1}] (force_calculator_concept.hpp:94-98), for
 // values that are not pair distances (ρ against the embedding span).
 template <class T> __device__ __forceinline__ bool in_span(const STab<T> &tb, T r) {
@@ -203,7 +211,7 @@ template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
                                         T r) {
   if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd_call<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
   }
   T t;
   const int e = seg_of(tb, r, t);
@@ -215,7 +223,7 @@ template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd64(const STab<T> &tb, const typename Vec4T<T>::type *seg, const double *vals,
                                           T r, double r64) {
   if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd_call<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
   }
   T t;
   const int e = seg_of64(tb, r, r64, t);
@@ -228,7 +236,7 @@ template <class T, bool AN>
 __device__ __forceinline__ VD<T> tab_vd_at(const STab<T> &tb, const typename Vec4T<T>::type *seg,
                                            const double *vals, T r, int e, T t) {
   if constexpr (AN) {
-    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
+    if (tb.kind == FS_TABLE_ANALYTIC) return form_vd_call<T>(tb.form, vals + tb.pv0, tb.n, r, tb.xmax);
   }
   return VD<T>{seg_val<T>(seg[e], t), seg_der<T>(seg[e], t, tb.inv_h)};
 }
