@@ -110,6 +110,11 @@ void free_configs(fs_gpu *h) {
   dfree(h->d_nb_count);
   dfree(h->d_cfg_by_work);
   h->max_cfg_work = 0;
+  dfree(h->d_run_a);
+  dfree(h->d_run_b);
+  dfree(h->d_run_cnt);
+  dfree(h->d_run_r);
+  h->runs_valid = false;
   dfree(h->d_F);
   dfree(h->d_forces);
   dfree(h->d_energy);
@@ -507,6 +512,7 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
   h->have_model = true;
   h->rcut_built = -1.0;
   h->jac_valid = false;
+  h->runs_valid = false; // the pair runs depend on the model's knot grid
   free_jacobian(h);
   fsg::de_free(h->de);
   h->de = nullptr;

@@ -304,6 +304,13 @@ struct PopArgs {
   const int32_t *order;               // configurations by decreasing size
   double *part;                       // [trial][config]
   double w_e, w_s;
+  // RUNS: each atom's pairs sorted by (neighbour species, segment) on the
+  // grid shared by the pair and density tables (pair_runs.cu)
+  const float4 *run_a; // u, t
+  const int2 *run_b;   // packed neighbour entry, key
+  const float *run_r;  // length (−1: coincident atoms)
+  const int32_t *run_cnt;
+  int run_np1;         // knots of the shared grid + 1
 };
 
 size_t pop_lanes_smem(int n_tables, int nseg_pd, int max_atoms, int max_img, bool eam) {
@@ -323,7 +330,12 @@ size_t pop_lanes_smem(int n_tables, int nseg_pd, int max_atoms, int max_img, boo
 __device__ __forceinline__ float poly_val(const float4 &a, float t) { return a.x + t * (a.y + t * (a.z + t * a.w)); }
 __device__ __forceinline__ float poly_der(const float4 &a, float t) { return a.y + t * (2.f * a.z + 3.f * t * a.w); }
 
-template <bool EAM>
+// RUNS (EAM, pair and density tables on one knot grid): the pairs come
+// from the sorted pair runs instead of the neighbour list; a run of pairs
+// with one (neighbour species, segment) key shares the φ_{t_i t_j}, ρ_{t_j}
+// and ρ_{t_i} segments, so each lane loads its trial's coefficients once per
+// run, and the pair geometry is read instead of rebuilt for every tile.
+template <bool EAM, bool RUNS>
 __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tile = blockIdx.x % A.n_tiles, chunk = blockIdx.x / A.n_tiles;
@@ -367,6 +379,38 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
     double sg[6] = {0, 0, 0, 0, 0, 0};
 
     if constexpr (EAM) {
+     if constexpr (RUNS) {
+      // ρ_i per trial (closed gate, eam_force.cpp:59-66) over the atom's runs
+      int2 *wst2 = reinterpret_cast<int2 *>(wst);
+      for (int i = w; i < N; i += kPopWarps) {
+        const int64_t gi = static_cast<int64_t>(cd.atom0) + i;
+        const int p0 = start[i], cnt = A.run_cnt[gi];
+        float acc = 0.f;
+        int cur = -1;
+        float4 cf = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int pb = 0; pb < cnt; pb += 32) {
+          int2 rec = make_int2(-1, 0);
+          if (pb + l < cnt) {
+            const int key = A.run_b[p0 + pb + l].y;
+            const int tj = key / A.run_np1, e = key - tj * A.run_np1;
+            rec = make_int2(tabs[np + tj].seg0 + e, __float_as_int(A.run_a[p0 + pb + l].w));
+          }
+          wst2[l] = rec;
+          __syncwarp();
+          const int c = min(32, cnt - pb);
+          for (int q = 0; q < c; ++q) {
+            const int2 rr = wst2[q];
+            if (rr.x != cur) { // a new run (warp-uniform)
+              cur = rr.x;
+              cf = coef[cur * kPopLanes + l];
+            }
+            acc += poly_val(cf, __int_as_float(rr.y));
+          }
+          __syncwarp();
+        }
+        rf[i * kPopLanes + l] = acc;
+      }
+     } else {
       // ρ_i per trial (closed gate, eam_force.cpp:59-66)
       int2 *wst2 = reinterpret_cast<int2 *>(wst);
       uint32_t pk = first_batch(w);
@@ -402,6 +446,7 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
         }
         rf[i * kPopLanes + l] = acc;
       }
+     }
       __syncthreads();
       // clamp + F(ρ), F'(ρ) per (atom, trial) (kernels.hpp:19-31; eam_force.cpp:68-73)
       for (int i = w; i < N; i += kPopWarps) {
@@ -426,6 +471,75 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
       __syncthreads();
     }
     // forces, ½φ energy, −½ d fᵀ stress (eam_force.cpp:75-100; kernels.hpp:33-38)
+    if constexpr (RUNS) {
+      static_assert(EAM, "pair runs: EAM models");
+      const float inv_h = tabs[0].inv_h; // the shared grid
+      for (int i = w; i < N; i += kPopWarps) {
+        const int ti = typ[i];
+        const int64_t ga = static_cast<int64_t>(cd.atom0) + i;
+        const int p0 = start[i], cnt = A.run_cnt[ga];
+        const float gFi = rf[i * kPopLanes + l];
+        const double fr0 = A.c.ref_force[3 * ga], fr1 = A.c.ref_force[3 * ga + 1], fr2 = A.c.ref_force[3 * ga + 2];
+        float f0 = 0.f, f1 = 0.f, f2 = 0.f, ep = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f;
+        int cur = -1;
+        float4 aP = make_float4(0.f, 0.f, 0.f, 0.f), aJ = aP, aI = aP;
+        for (int pb = 0; pb < cnt; pb += 32) {
+          if (pb + l < cnt) {
+            const int p = p0 + pb + l;
+            const float4 ua = A.run_a[p];
+            const int2 b = A.run_b[p];
+            const float r = A.run_r[p];
+            const int tj = b.y / A.run_np1, e = b.y - tj * A.run_np1;
+            const float hr = 0.5f * r;
+            PopRec rec;
+            rec.a = ua;
+            rec.b = make_float4(hr * ua.x * ua.x, hr * ua.y * ua.y, hr * ua.z * ua.z, hr * ua.x * ua.y);
+            rec.c = make_float4(hr * ua.x * ua.z, hr * ua.y * ua.z, 0.f, 0.f);
+            rec.ih = make_float4(0.f, 0.f, 0.f, 0.f);
+            rec.d = make_int4(b.x & 0xFFFFF, r >= 0.f ? tabs[pair_ord(ti, tj, nt)].seg0 + e : -1, tabs[np + tj].seg0 + e,
+                              tabs[np + ti].seg0 + e);
+            wst[l] = rec;
+          }
+          __syncwarp();
+          const int c = min(32, cnt - pb);
+          for (int q = 0; q < c; ++q) {
+            const float4 ra = wst[q].a, rb = wst[q].b, rc = wst[q].c;
+            const int4 rd = wst[q].d;
+            if (rd.y < 0) continue; // coincident atoms: no pair term (warp-uniform)
+            if (rd.y != cur) {      // a new run (warp-uniform): this trial's three segments
+              cur = rd.y;
+              aP = coef[rd.y * kPopLanes + l];
+              aJ = coef[rd.z * kPopLanes + l];
+              aI = coef[rd.w * kPopLanes + l];
+            }
+            ep += poly_val(aP, ra.w);
+            const float g = (poly_der(aP, ra.w) + gFi * poly_der(aJ, ra.w) +
+                             rf[rd.x * kPopLanes + l] * poly_der(aI, ra.w)) * inv_h;
+            f0 += g * ra.x;
+            f1 += g * ra.y;
+            f2 += g * ra.z;
+            s0 -= g * rb.x;
+            s1 -= g * rb.y;
+            s2 -= g * rb.z;
+            s3 -= g * rb.w;
+            s4 -= g * rc.x;
+            s5 -= g * rc.y;
+          }
+          __syncwarp();
+        }
+        const double r0 = static_cast<double>(f0) - fr0;
+        const double r1 = static_cast<double>(f1) - fr1;
+        const double r2 = static_cast<double>(f2) - fr2;
+        objf += r0 * r0 + r1 * r1 + r2 * r2;
+        e_pair += 0.5 * static_cast<double>(ep);
+        sg[0] += s0;
+        sg[1] += s1;
+        sg[2] += s2;
+        sg[3] += s3;
+        sg[4] += s4;
+        sg[5] += s5;
+      }
+    } else {
     uint32_t pk = first_batch(w);
     for (int i = w; i < N; i += kPopWarps) {
       const int ti = typ[i];
@@ -521,6 +635,7 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
       sg[4] += s4;
       sg[5] += s5;
     }
+    } // RUNS
     // per-(warp, trial) partials into the staging area (16 × 32 × 10 doubles),
     // then a fixed-order sum over warps
     __syncthreads();
@@ -1675,7 +1790,19 @@ int launch_population_t(fs_gpu *h, double w_e, double w_s, const double *d_xs, i
       pa.part = part;
       pa.w_e = w_e;
       pa.w_s = w_s;
-      auto kl = pop_lanes_kernel<EAM>;
+      pa.run_a = h->d_run_a;
+      pa.run_b = h->d_run_b;
+      pa.run_r = h->d_run_r;
+      pa.run_cnt = h->d_run_cnt;
+      pa.run_np1 = 0;
+      auto kl = pop_lanes_kernel<EAM, false>;
+      if constexpr (EAM) {
+        RunGrid rg;
+        if (h->runs_valid && pair_runs_grid(h, &rg)) {
+          kl = pop_lanes_kernel<EAM, true>;
+          pa.run_np1 = rg.n + 1;
+        }
+      }
       FS_CUDA(cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sml)));
       kl<<<static_cast<unsigned>(pa.n_chunks) * pa.n_tiles, kPopWarps * 32, sml, h->stream>>>(pa);
       FS_CUDA(cudaGetLastError());
@@ -1788,7 +1915,19 @@ int launch_population_static(fs_gpu *h, double w_e, double w_s, const double *d_
       pa.part = part;
       pa.w_e = w_e;
       pa.w_s = w_s;
-      auto kl = pop_lanes_kernel<EAM>;
+      pa.run_a = h->d_run_a;
+      pa.run_b = h->d_run_b;
+      pa.run_r = h->d_run_r;
+      pa.run_cnt = h->d_run_cnt;
+      pa.run_np1 = 0;
+      auto kl = pop_lanes_kernel<EAM, false>;
+      if constexpr (EAM) {
+        RunGrid rg;
+        if (h->runs_valid && pair_runs_grid(h, &rg)) {
+          kl = pop_lanes_kernel<EAM, true>;
+          pa.run_np1 = rg.n + 1;
+        }
+      }
       FS_CUDA(cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sml)));
       kl<<<static_cast<unsigned>(pa.n_chunks) * pa.n_tiles, kPopWarps * 32, sml, h->stream>>>(pa);
       FS_CUDA(cudaGetLastError());

@@ -201,6 +201,14 @@ struct fs_gpu {
   void *d_dgd = nullptr;          // [n_atoms][kWin]
   int32_t *d_wsF = nullptr;       // [n_atoms]
   int64_t atom_scratch_alloc = 0;
+  // population kernel on a knot grid shared by the pair and density tables:
+  // each atom's in-gate pairs sorted by (neighbour species, segment of the
+  // grid), built once per neighbour list and grid (pair_runs.cuh)
+  float4 *d_run_a = nullptr;      // [pair]: u_x, u_y, u_z, t  (pair slots of the neighbour list)
+  int2 *d_run_b = nullptr;        // [pair]: packed neighbour entry, key = species·(n + 1) + segment
+  int32_t *d_run_cnt = nullptr;   // [atom]: in-gate pairs
+  float *d_run_r = nullptr;       // [pair]: FP64 length rounded to FP32
+  bool runs_valid = false;        // built for the current neighbour lists and model grid
   double last_ws = -1.0, last_we = 0.0;
   bool jac_valid = false;
 
@@ -256,6 +264,17 @@ inline void mark(fs_gpu *h, int boundary) {
 
 // neighbour.cu
 int build_neighbors(fs_gpu *h, double rcut);
+
+// pair_runs.cu: each atom's pairs sorted by (neighbour species, segment) on
+// the knot grid shared by the pair and density tables
+constexpr int kRunMaxT = 4;  // species
+constexpr int kRunMaxN = 64; // knots of the shared grid
+struct RunGrid {
+  double x0, xmax, inv_h;
+  int n;
+};
+bool pair_runs_grid(const fs_gpu *h, RunGrid *g);
+int build_pair_runs(fs_gpu *h); // after every neighbour build (no-op without a shared grid)
 
 // tables.cu
 int upload_tables(fs_gpu *h);          // structure + values (after set_model)

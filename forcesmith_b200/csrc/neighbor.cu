@@ -301,6 +301,7 @@ int build_neighbors(fs_gpu *h, double rcut) {
     return set_error(h, FS_ERR_UNSUPPORTED, "neighbour list: more than 4096 periodic images (box far smaller than the cutoff)");
   const bool none = !(rcut > 0.0 && std::isfinite(rcut));
   const double rcut2 = none ? -1.0 : rcut * rcut;
+  h->runs_valid = false; // pair runs index the neighbour lists
   FS_CUDA(cudaMemcpyAsync(h->d_cfg, h->cfg_host.data(), n_cfg * sizeof(CfgDev), cudaMemcpyHostToDevice,
                           h->stream));
   wrap_kernel<<<n_cfg, 128, 0, h->stream>>>(h->d_cfg, n_cfg, h->d_pos, h->d_wpos);
@@ -419,7 +420,7 @@ int build_neighbors(fs_gpu *h, double rcut) {
 #undef FS_NB
   release();
   h->rcut_built = none ? 0.0 : rcut;
-  return FS_OK;
+  return build_pair_runs(h);
 }
 
 } // namespace fsg

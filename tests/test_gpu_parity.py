@@ -271,14 +271,25 @@ def test_population_objective(ternary_small):
     _close(og, oo, 1e-9, "population objective")
 
 
-@pytest.mark.parametrize("family", ["eam", "pair"])
+def _two_grid_model(start):
+    """The ternary start model with its density tables on [1.8, 5.5] instead
+    of the pair tables' [1.8, 6.0]: no knot grid shared by all r-functions."""
+    tabs = list(start.tables)
+    for a in range(3):
+        tabs[6 + a] = Table.spline(tabs[6 + a].rmin, 5.5, tabs[6 + a].values)
+    return Model(FS_FAMILY_EAM, 3, tabs)
+
+
+@pytest.mark.parametrize("family", ["eam", "pair", "eam_two_grids"])
 def test_population_objective_fp32_lanes(ternary_small, family):
     """FP32 population path (one lane per trial vector): against the FP64
     oracle (relative 1e-4, the FP32 objective bar) and against the FP32
     single-vector residual path (relative 1e-5); NP = 37 leaves a partial
-    tile of trials."""
+    tile of trials.  "eam": the pair and density tables share a knot grid, so
+    the kernel walks the sorted pair runs; "eam_two_grids" and "pair": it
+    walks the neighbour list."""
     ds, _, start = ternary_small
-    model = start if family == "eam" else spline_pair_model(3, 14)
+    model = {"eam": start, "pair": spline_pair_model(3, 14), "eam_two_grids": _two_grid_model(start)}[family]
     g, o = _pair(ds.subset([0, 1, 2, 3]), model, "fp32")
     x0 = g.gather_params()
     xs = np.stack([x0 * synth.uniform(x0.size, 0.97, 1.03, 200 + k) for k in range(37)])
