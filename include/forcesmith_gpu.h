@@ -248,7 +248,12 @@ int fs_gpu_set_references(fs_gpu *h, const double *ref_force,
                           const double *ref_energy, const double *ref_stress9);
 
 int fs_gpu_set_model(fs_gpu *h, const fs_model *model);
-/* Builds the device neighbour lists at the model's max cutoff. */
+/* Builds the device neighbour lists at the model's max cutoff: device cell
+ * lists (slabs at least the cutoff wide per lattice direction), the
+ * reference's FP64 distance test on every candidate, then each atom's list
+ * sorted into the reference's order.  For an FP32 EAM model whose pair and
+ * density tables share one knot grid it also sorts each atom's pairs by
+ * (neighbour species, segment) for the population kernel. */
 int fs_gpu_prepare(fs_gpu *h);
 
 int fs_gpu_num_pairs(fs_gpu *h, int64_t *n_pairs);
