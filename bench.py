@@ -308,7 +308,7 @@ def de_legs(local, generations, seeds=SURROGATE_SEEDS, cpu=True):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         done, gens, best_s, screened = 0, 0, float("inf"), 0
-        chunk = 5
+        chunk = 1  # the target is checked after every generation
         while gens < generations:
             b, _, info = g.de_run_screened(min(chunk, generations - gens))
             gens += min(chunk, generations - gens)

@@ -237,14 +237,27 @@ __global__ void gelu_back_kernel(const float *__restrict__ dH, const float *__re
   }
 }
 
-// out[j] = Σ_r X[r·ncols + j]·(s ? s[r] : 1), fixed order
-__global__ void colsum_kernel(const float *__restrict__ X, const float *__restrict__ s, int rows, int ncols,
-                              float *__restrict__ out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ncols) return;
+// out[j] = Σ_r X[r·ncols + j]·(s ? s[r] : 1), fixed order.  A block of
+// kColsumRows × 32 threads takes 32 columns: thread (x, y) sums rows
+// y, y + kColsumRows, … of column x (coalesced across x), and the partial
+// sums meet in shared memory in the order of y.
+constexpr int kColsumRows = 8;
+__global__ void __launch_bounds__(32 * kColsumRows) colsum_kernel(const float *__restrict__ X,
+                                                                  const float *__restrict__ s, int rows, int ncols,
+                                                                  float *__restrict__ out) {
+  __shared__ float part[kColsumRows][33];
+  const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + x;
   float acc = 0.f;
-  for (int r = 0; r < rows; ++r) acc += X[static_cast<int64_t>(r) * ncols + j] * (s ? s[r] : 1.f);
-  out[j] = acc;
+  if (j < ncols)
+    for (int r = y; r < rows; r += kColsumRows) acc += X[static_cast<int64_t>(r) * ncols + j] * (s ? s[r] : 1.f);
+  part[y][x] = acc;
+  __syncthreads();
+  if (y == 0 && j < ncols) {
+    float t = 0.f;
+    for (int q = 0; q < kColsumRows; ++q) t += part[q][x];
+    out[j] = t;
+  }
 }
 
 __global__ void sum_kernel_f(const float *__restrict__ v, int n, float *__restrict__ out) {
@@ -580,10 +593,11 @@ int mlp_gradient_dev(fs_gpu *h, Mlp *s, int rows) {
   FS_CUDA(cudaGetLastError());
   // dW1 = dZ1ᵀ X  (columns padded to Dp; the pad columns of X are zero)
   FS_TRY(gemm(h, s, s->dZ1T, rows, s->XT, rows, kH, s->Dp, rows, s->g + s->oW1, s->Dp, splits));
-  colsum_kernel<<<1, kH, 0, h->stream>>>(s->dZ1, nullptr, rows, kH, s->g + s->ob1);
-  colsum_kernel<<<1, kH, 0, h->stream>>>(s->dZ2, nullptr, rows, kH, s->g + s->ob2);
-  colsum_kernel<<<1, kH, 0, h->stream>>>(s->H2, s->dy, rows, kH, s->g + s->ow3);
-  colsum_kernel<<<1, 1, 0, h->stream>>>(s->dy, nullptr, rows, 1, s->g + s->ob3);
+  const unsigned cb = (kH + 31) / 32;
+  colsum_kernel<<<cb, 32 * kColsumRows, 0, h->stream>>>(s->dZ1, nullptr, rows, kH, s->g + s->ob1);
+  colsum_kernel<<<cb, 32 * kColsumRows, 0, h->stream>>>(s->dZ2, nullptr, rows, kH, s->g + s->ob2);
+  colsum_kernel<<<cb, 32 * kColsumRows, 0, h->stream>>>(s->H2, s->dy, rows, kH, s->g + s->ow3);
+  colsum_kernel<<<1, 32 * kColsumRows, 0, h->stream>>>(s->dy, nullptr, rows, 1, s->g + s->ob3);
   sum_kernel_f<<<1, 256, 0, h->stream>>>(s->sq, rows, s->loss);
   FS_CUDA(cudaGetLastError());
   h->launches += 10;
