@@ -746,6 +746,24 @@ __device__ void stage_tables(const JacArgs<T> &A, STab<T> *tabs, typename Vec4T<
   for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
 }
 
+// stage_tables with the knot-derivative blocks as one 4-vector per (segment,
+// window knot), so that a lane reads its knot's four coefficients in one load
+template <class T>
+__device__ void stage_tables_g4(const JacArgs<T> &A, STab<T> *tabs, typename Vec4T<T>::type *seg,
+                                typename Vec4T<T>::type *G4, int32_t *segws, int32_t *cmap) {
+  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
+  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
+    seg[k] = A.seg_a[k];
+    segws[k] = A.seg_ws[k];
+  }
+  for (int k = threadIdx.x; k < A.c.n_segs * kWin; k += blockDim.x) {
+    const int sg = k / kWin, q = k - sg * kWin;
+    const T *g = A.seg_g + static_cast<size_t>(sg) * 4 * kWin + q;
+    G4[k] = typename Vec4T<T>::type{g[0], g[kWin], g[2 * kWin], g[3 * kWin]};
+  }
+  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   using T4 = typename Vec4T<T>::type;
@@ -973,7 +991,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   Smem S(smem_raw);
   STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
   T4 *seg = S.take<T4>(A.c.n_segs);
-  T *segg = S.take<T>(A.c.n_segs * 4 * kWin);
+  T4 *G4 = S.take<T4>(static_cast<size_t>(A.c.n_segs) * kWin); // [seg][q]: ∂a_0..3/∂y_{ws+q}
   int32_t *segws = S.take<int32_t>(A.c.n_segs);
   int32_t *cmap = S.take<int32_t>(A.c.n_cmap);
   double *wpos = S.take<double>(3 * N);
@@ -1019,7 +1037,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     wsFa = s_ws;
     dgda = s_dgd;
   }
-  stage_tables(A, tabs, seg, segg, segws, cmap);
+  stage_tables_g4(A, tabs, seg, G4, segws, cmap);
   for (int k = threadIdx.x; k < warps * 3 * D; k += blockDim.x) srow_all[k] = T2{T(0), T(0)};
   for (int k = threadIdx.x; k < warps * D; k += blockDim.x) {
     erow_all[k] = T(0);
@@ -1116,7 +1134,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           }
           const auto r64 = [=] { return pair_len64(wpos, shift, i, pk); };
           auto set_slot = [&](int s, const STab<T> &tb, int e, T t, T wgt) {
-            R.si[s] = make_int4(e * 4 * kWin, tb.cmap0 + segws[e], 0, cross);
+            R.si[s] = make_int4(e * kWin, tb.cmap0 + segws[e], 0, cross);
             R.sf[s].x = t;
             R.sf[s].y = wgt * tb.inv_h;
           };
@@ -1199,8 +1217,8 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           const int c0 = cmap[si.y + q]; // −1: no term (padding, fixed knot, unused slot)
           const T2 sf = R.sf[slot_c];
           const T tt = sf.x;
-          const T *G = segg + si.x;
-          const T g0 = G[q], g1 = G[kWin + q], g2 = G[2 * kWin + q], g3 = G[3 * kWin + q];
+          const T4 G = G4[si.x + q];
+          const T g0 = G.x, g1 = G.y, g2 = G.z, g3 = G.w;
           T base = g1 + tt * (T(2) * g2 + T(3) * tt * g3);
           if constexpr (EAM)
             if (slot_c == 3) base = fwin[u]; // F window of j: ∂F'_j/∂y_q
