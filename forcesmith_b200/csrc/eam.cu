@@ -920,22 +920,39 @@ template <class T> struct V2T;
 template <> struct V2T<float> { using type = float2; };
 template <> struct V2T<double> { using type = double2; };
 
-// One pair, laid out for vector loads: a scatter lane reads its slot's
-// integers with one 128-bit load and (t, weight) with one 64/128-bit load.
+// One pair, laid out for vector loads: a scatter lane reads its slot with
+// one 128-bit load (FP32), and the neighbour terms read (weight, j) at once.
+// Per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window): index of
+// the segment's first knot-derivative 4-vector, column-map index of the
+// window's first knot (0, the map's leading block of −1, when the slot adds
+// nothing; knots past the table's end read the −1 padding after it), local
+// coordinate t, weight × the table's 1/h (F window: ρ'_{ti}(r)).
+template <class T> struct SlotRec;
+template <> struct __align__(16) SlotRec<float> {
+  int g, c;
+  float t, w;
+};
+template <> struct __align__(16) SlotRec<double> {
+  int g, c, pad0, pad1;
+  double t, w;
+};
+// F''_j ρ'_{ti}(r) (the dense ρ-chain weight); j, with bit 31 set when the
+// pair leaves the cell and stress is wanted
+template <class T> struct JW;
+template <> struct __align__(8) JW<float> {
+  float w;
+  int jc;
+};
+template <> struct __align__(16) JW<double> {
+  double w;
+  int jc, pad;
+};
 template <class T> struct PairRec {
-  // per slot (0: φ, 1: ρ_{tj} direct, 2: ρ_{ti} direct, 3: F_j window):
-  // offset of the segment's knot-derivative block (4 × kWin coefficients),
-  // column-map index of the window's first knot (0, the map's leading block
-  // of −1, when the slot adds nothing; knots past the table's end read the
-  // −1 padding after it), unused, 1 if the pair leaves the cell and stress
-  // is wanted
-  int4 si[4];
-  typename V2T<T>::type sf[4]; // local coordinate t; weight × the table's 1/h (F window: ρ'_{ti}(r))
-  typename Vec4T<T>::type uv;  // u_x, u_y, u_z, v_xx     (v = s ⊗ u for pairs that leave the
-  typename Vec4T<T>::type vv;  // v_yy, v_zz, v_xy, v_xz  cell, image shift s; zero otherwise)
-  typename V2T<T>::type vd;    // v_yz, ρ'_{ti}(r)
-  T cFj;                       // F''_j
-  int j;
+  SlotRec<T> s[4];
+  typename Vec4T<T>::type uv; // u_x, u_y, u_z, v_xx     (v = s ⊗ u for pairs that leave the
+  typename Vec4T<T>::type vv; // v_yy, v_zz, v_xy, v_xz  cell, image shift s; zero otherwise)
+  T vyz;                      // v_yz
+  JW<T> jw;
 };
 
 constexpr int kPairStep = 4; // pairs whose scatter terms are formed together
@@ -1112,10 +1129,10 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
         const int tj = typ[j];
         const int img = static_cast<int>(pk >> 20);
         const int cross = want_stress && img != home; // the pair leaves the cell: image shift s ≠ 0
-        R.j = j;
+        R.jw.jc = static_cast<int>(static_cast<uint32_t>(j) | (cross ? 0x80000000u : 0u));
         for (int s = 0; s < 4; ++s) {
-          R.si[s] = make_int4(0, 0, 0, 0);
-          R.sf[s].x = R.sf[s].y = T(0);
+          R.s[s].g = R.s[s].c = 0;
+          R.s[s].t = R.s[s].w = T(0);
         }
         T dgi = T(0), cFj = T(0), u[3] = {0, 0, 0}, v[6] = {0, 0, 0, 0, 0, 0};
         T dgj = T(0);
@@ -1134,9 +1151,10 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           }
           const auto r64 = [=] { return pair_len64(wpos, shift, i, pk); };
           auto set_slot = [&](int s, const STab<T> &tb, int e, T t, T wgt) {
-            R.si[s] = make_int4(e * kWin, tb.cmap0 + segws[e], 0, cross);
-            R.sf[s].x = t;
-            R.sf[s].y = wgt * tb.inv_h;
+            R.s[s].g = e * kWin;
+            R.s[s].c = tb.cmap0 + segws[e];
+            R.s[s].t = t;
+            R.s[s].w = wgt * tb.inv_h;
           };
           const STab<T> &tp = tabs[pair_ord(ti, tj, nt)];
           T tq;
@@ -1165,15 +1183,14 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
             // F_j window: coefficient dgd_j[q]·ρ'_{ti}(r)
             const STab<T> &te = tabs[np + nt + tj];
             const int wsj = wsFa[j];
-            R.si[3] = make_int4(0, te.cmap0 + wsj, 0, 0);
-            R.sf[3].y = dgi;
+            R.s[3].c = te.cmap0 + wsj;
+            R.s[3].w = dgi;
           }
         }
         R.uv = {u[0], u[1], u[2], v[0]};
         R.vv = {v[1], v[2], v[3], v[4]};
-        R.vd.x = v[5];
-        R.vd.y = dgi;
-        R.cFj = cFj;
+        R.vyz = v[5];
+        R.jw.w = cFj * dgi;
         rec[lane] = R;
         for (int a = 0; a < 3; ++a) V[a] += dgj * u[a];
         for (int a = 0; a < 6; ++a) P[a] += dgj * v[a];
@@ -1192,16 +1209,19 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
         bool st[kPairStep];
         T4 uvs[kPairStep];
         T dval[kPairStep][2], dwgt[kPairStep], fwin[kPairStep];
+        bool crs[kPairStep];
         if constexpr (EAM) {
           // per-atom loads go out first: the F-window terms ∂F'_j/∂y_q (slot 3
           // lanes) and the dense ρ-chain's ∂ρ_j/∂y, used after the row updates
 #pragma unroll
           for (int u = 0; u < kPairStep; ++u) {
             const bool live = k0 + u < cnt;
-            const PairRec<T> &R = rec[live ? k0 + u : k0];
-            fwin[u] = slot_c == 3 ? dgda[R.j * kWin + q] : T(0);
-            dwgt[u] = live ? R.cFj * R.vd.y : T(0);
-            const T *drj = drho + R.j * dstr;
+            const JW<T> jw = rec[live ? k0 + u : k0].jw;
+            const int jj = jw.jc & 0x7FFFFFFF;
+            crs[u] = jw.jc < 0;
+            fwin[u] = slot_c == 3 ? dgda[jj * kWin + q] : T(0);
+            dwgt[u] = live ? jw.w : T(0);
+            const T *drj = drho + jj * dstr;
 #pragma unroll
             for (int s2 = 0; s2 < 2; ++s2) {
               const int m = lane + 32 * s2;
@@ -1213,20 +1233,20 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
         for (int u = 0; u < kPairStep; ++u) {
           const bool live = k0 + u < cnt;
           const PairRec<T> &R = rec[live ? k0 + u : k0];
-          const int4 si = R.si[slot_c];
-          const int c0 = cmap[si.y + q]; // −1: no term (padding, fixed knot, unused slot)
-          const T2 sf = R.sf[slot_c];
-          const T tt = sf.x;
-          const T4 G = G4[si.x + q];
+          const SlotRec<T> sr = R.s[slot_c];
+          const int c0 = cmap[sr.c + q]; // −1: no term (padding, fixed knot, unused slot)
+          const T tt = sr.t;
+          const T4 G = G4[sr.g + q];
+          if constexpr (!EAM) crs[u] = R.jw.jc < 0;
           const T g0 = G.x, g1 = G.y, g2 = G.z, g3 = G.w;
           T base = g1 + tt * (T(2) * g2 + T(3) * tt * g3);
           if constexpr (EAM)
             if (slot_c == 3) base = fwin[u]; // F window of j: ∂F'_j/∂y_q
           const bool use = live && lane_ok && c0 >= 0;
           col[u] = use ? c0 : D;
-          cf[u] = use ? sf.y * base : T(0);
+          cf[u] = use ? sr.w * base : T(0);
           dv[u] = (use && slot == 0) ? half_we * (g0 + tt * (g1 + tt * (g2 + tt * g3))) : T(0);
-          st[u] = use && si.w != 0;
+          st[u] = use && crs[u] && slot < 3; // the F window carries no stress term here
           uvs[u] = R.uv;
         }
 #pragma unroll
@@ -1241,7 +1261,7 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
           if (st[u]) { // stress scatter: pairs that leave the cell only
             const PairRec<T> &R = rec[k0 + u];
             const T4 vv = R.vv;
-            const T v5 = R.vd.x, c = cf[u];
+            const T v5 = R.vyz, c = cf[u];
             T2 s0 = srow[3 * cu], s1 = srow[3 * cu + 1], s2 = srow[3 * cu + 2];
             s0.x += c * uvs[u].w;
             s0.y += c * vv.x;
