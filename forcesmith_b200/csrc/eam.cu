@@ -734,20 +734,10 @@ template <class T> size_t atom_stage_smem(int max_atoms, int ndens) {
          align16(static_cast<size_t>(max_atoms) * kWin * sizeof(T)) + 96;
 }
 
-template <class T>
-__device__ void stage_tables(const JacArgs<T> &A, STab<T> *tabs, typename Vec4T<T>::type *seg, T *segg,
-                             int32_t *segws, int32_t *cmap) {
-  for (int t = threadIdx.x; t < A.c.n_tables; t += blockDim.x) load_stab(tabs[t], A.c.desc[t]);
-  for (int k = threadIdx.x; k < A.c.n_segs; k += blockDim.x) {
-    seg[k] = A.seg_a[k];
-    segws[k] = A.seg_ws[k];
-  }
-  for (int k = threadIdx.x; k < A.c.n_segs * 4 * kWin; k += blockDim.x) segg[k] = A.seg_g[k];
-  for (int k = threadIdx.x; k < A.c.n_cmap; k += blockDim.x) cmap[k] = A.c.cmap[k];
-}
 
-// stage_tables with the knot-derivative blocks as one 4-vector per (segment,
-// window knot), so that a lane reads its knot's four coefficients in one load
+// Stage the tables, segment coefficients, window starts and column map, with
+// the knot-derivative blocks as one 4-vector per (segment, window knot), so
+// that a thread reads a knot's four coefficients in one load
 template <class T>
 __device__ void stage_tables_g4(const JacArgs<T> &A, STab<T> *tabs, typename Vec4T<T>::type *seg,
                                 typename Vec4T<T>::type *G4, int32_t *segws, int32_t *cmap) {
@@ -777,7 +767,7 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   Smem S(smem_raw);
   STab<T> *tabs = S.take<STab<T>>(A.c.n_tables);
   T4 *seg = S.take<T4>(A.c.n_segs);
-  T *segg = S.take<T>(A.c.n_segs * 4 * kWin);
+  T4 *G4 = S.take<T4>(static_cast<size_t>(A.c.n_segs) * kWin); // [seg][q]: ∂a_0..3/∂y_{ws+q}
   int32_t *segws = S.take<int32_t>(A.c.n_segs);
   int32_t *cmap = S.take<int32_t>(A.c.n_cmap);
   double *wpos = S.take<double>(3 * N);
@@ -788,7 +778,7 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
   T *drs = S.take<T>(static_cast<size_t>(N) * ds); // ∂ρ_i/∂y rows (staged)
   T *sgf = S.take<T>(N);
   T *sov = S.take<T>(N);
-  stage_tables(A, tabs, seg, segg, segws, cmap);
+  stage_tables_g4(A, tabs, seg, G4, segws, cmap);
   for (int k = threadIdx.x; k < A.D; k += blockDim.x) erow[k] = lrow[k] = 0.0;
   for (int k = threadIdx.x; k < N * ds; k += blockDim.x) drs[k] = T(0);
   stage_geometry(cd, A.c, wpos, shift, typ);
@@ -810,7 +800,7 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
       if (e < 0) continue;
       rho += seg_val<T>(seg[e], t);
       const int ws = segws[e];
-      const T *G = segg + e * 4 * kWin;
+      const T4 *G = G4 + e * kWin;
       // the window's knots are distinct columns: load all, add, store all
       // (knots past the table's end and fixed knots add zero to the pad column nd)
       int m[kWin];
@@ -819,7 +809,8 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
       for (int q = 0; q < kWin; ++q) {
         const int col = ws + q < tb.n ? cmap[tb.cmap0 + ws + q] : -1;
         m[q] = col >= 0 ? col - A.dens_c0 : nd;
-        add[q] = col >= 0 ? G[q] + t * (G[kWin + q] + t * (G[2 * kWin + q] + t * G[3 * kWin + q])) : T(0);
+        const T4 g = G[q];
+        add[q] = col >= 0 ? g.x + t * (g.y + t * (g.z + t * g.w)) : T(0);
       }
 #pragma unroll
       for (int q = 0; q < kWin; ++q) cur[q] = dr[m[q]];
@@ -847,11 +838,12 @@ __global__ void __launch_bounds__(256) jac_atoms_kernel(JacArgs<T> A) {
     sov[i] = static_cast<T>(over);
     const int ws = segws[e];
     A.wsF[ga] = ws;
-    const T *G = segg + e * 4 * kWin;
+    const T4 *G = G4 + e * kWin;
     for (int q = 0; q < kWin; ++q) {
       const bool ok = ws + q < te.n;
-      const T dv = G[q] + t * (G[kWin + q] + t * (G[2 * kWin + q] + t * G[3 * kWin + q]));
-      const T dd = (G[kWin + q] + t * (T(2) * G[2 * kWin + q] + T(3) * t * G[3 * kWin + q])) * te.inv_h;
+      const T4 g = G[q];
+      const T dv = g.x + t * (g.y + t * (g.z + t * g.w));
+      const T dd = (g.y + t * (T(2) * g.z + T(3) * t * g.w)) * te.inv_h;
       A.dgd[ga * kWin + q] = ok ? dd : T(0);
       if (!ok) continue;
       const int col = cmap[te.cmap0 + ws + q];
