@@ -310,7 +310,7 @@ struct PopArgs {
   const int2 *run_b;   // packed neighbour entry, key
   const float *run_r;  // length (−1: coincident atoms)
   const int32_t *run_cnt;
-  int run_np1;         // knots of the shared grid + 1
+  int runs;            // 1: walk the pair runs
 };
 
 size_t pop_lanes_smem(int n_tables, int nseg_pd, int max_atoms, int max_img, bool eam) {
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
           int2 rec = make_int2(-1, 0);
           if (pb + l < cnt) {
             const int key = A.run_b[p0 + pb + l].y;
-            const int tj = key / A.run_np1, e = key - tj * A.run_np1;
+            const int tj = key >> kRunKeyBits, e = key & ((1 << kRunKeyBits) - 1);
             rec = make_int2(tabs[np + tj].seg0 + e, __float_as_int(A.run_a[p0 + pb + l].w));
           }
           wst2[l] = rec;
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
             const float4 ua = A.run_a[p];
             const int2 b = A.run_b[p];
             const float r = A.run_r[p];
-            const int tj = b.y / A.run_np1, e = b.y - tj * A.run_np1;
+            const int tj = b.y >> kRunKeyBits, e = b.y & ((1 << kRunKeyBits) - 1);
             const float hr = 0.5f * r;
             PopRec rec;
             rec.a = ua;
@@ -705,6 +705,13 @@ template <class T> struct JacArgs {
   T *drho;              // [atom][ndens]
   T *dgd;               // [atom][kWin]: ∂F'(ρ̄)/∂y over the embedding window
   int32_t *wsF;         // [atom]: embedding window start (knot)
+  // FP32 EAM on a knot grid shared by the pair and density tables: each
+  // atom's pairs from the sorted pair runs (pair_runs.cu), with u, t and the
+  // segment already found (runs = 1)
+  const float4 *run_a;  // u, t
+  const int2 *run_b;    // packed neighbour entry, run key
+  const int32_t *run_cnt;
+  int runs;
 };
 
 template <class T> size_t jac_common_smem(int n_tables, int n_segs, int n_cmap, int max_atoms, int max_img) {
@@ -1079,12 +1086,24 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
   // each chunk's packed neighbour entries are loaded one chunk ahead
   int pre_p0 = -1;
   uint32_t pk_next = 0;
+  float4 ra_next = make_float4(0.f, 0.f, 0.f, 0.f);
+  int2 rb_next = make_int2(0, 0);
+  constexpr bool kRunsOK = EAM && std::is_same_v<T, float>;
+  const bool runs = kRunsOK && A.runs;
+  // end of atom ii's pairs: its in-gate pair runs, else its neighbour list
+  auto end_of = [&](int ii) { return runs ? start[ii] + A.run_cnt[cd.atom0 + ii] : start[ii + 1]; };
   auto prefetch = [&](int p, int end) {
     pre_p0 = p;
-    pk_next = lane < end - p ? A.c.nb_pack[p + lane] : 0u;
+    const bool in = lane < end - p;
+    if (runs) {
+      rb_next = in ? A.run_b[p + lane] : make_int2(0, 0);
+      ra_next = in ? A.run_a[p + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      pk_next = in ? A.c.nb_pack[p + lane] : 0u;
+    }
   };
   const int i_first = w + half * warps;
-  if (i_first < N) prefetch(start[i_first], start[i_first + 1]);
+  if (i_first < N) prefetch(start[i_first], end_of(i_first));
   for (int i = i_first; i < N; i += astep) {
     for (int k = lane; k <= D; k += 32) frow[k] = T4{T(0), T(0), T(0), T(0)};
     const int ti = typ[i];
@@ -1098,20 +1117,87 @@ __global__ void __launch_bounds__(32 * kMaxK2Warps<T>, 1) jac_forces_kernel(JacA
     T V[3] = {0, 0, 0}, P[6] = {0, 0, 0, 0, 0, 0};
     T dacc[2][3] = {{0, 0, 0}, {0, 0, 0}}; // dense ρ-chain, columns m = lane, lane + 32
     __syncwarp();
-    for (int p0 = start[i]; p0 < start[i + 1]; p0 += 32) {
-      const int cnt = min(32, start[i + 1] - p0);
+    const int iend = end_of(i);
+    for (int p0 = start[i]; p0 < iend; p0 += 32) {
+      const int cnt = min(32, iend - p0);
       uint32_t pk_cur = pk_next;
-      if (pre_p0 != p0) pk_cur = lane < cnt ? A.c.nb_pack[p0 + lane] : 0u; // (after an atom without pairs)
+      float4 ra_cur = ra_next;
+      int2 rb_cur = rb_next;
+      if (pre_p0 != p0) { // (after an atom without pairs)
+        if (runs) {
+          rb_cur = lane < cnt ? A.run_b[p0 + lane] : make_int2(0, 0);
+          ra_cur = lane < cnt ? A.run_a[p0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+          pk_cur = lane < cnt ? A.c.nb_pack[p0 + lane] : 0u;
+        }
+      }
       {
-        int np0 = p0 + 32, nend = start[i + 1];
+        int np0 = p0 + 32, nend = iend;
         if (np0 >= nend) {
           const int in = i + astep;
           np0 = in < N ? start[in] : 0;
-          nend = in < N ? start[in + 1] : 0;
+          nend = in < N ? end_of(in) : 0;
         }
         prefetch(np0, nend);
       }
-      if (lane < cnt) {
+      if constexpr (kRunsOK) {
+        if (runs && lane < cnt) {
+          // a pair run record: u and t on the shared grid, the segment in the key
+          PairRec<T> R;
+          const uint32_t pk = static_cast<uint32_t>(rb_cur.x);
+          const int j = static_cast<int>(pk & 0xFFFFFu), img = static_cast<int>(pk >> 20);
+          const int tj = rb_cur.y >> kRunKeyBits, e = rb_cur.y & ((1 << kRunKeyBits) - 1);
+          const int cross = want_stress && img != home;
+          const T t = ra_cur.w, u[3] = {ra_cur.x, ra_cur.y, ra_cur.z};
+          R.jw.jc = static_cast<int>(static_cast<uint32_t>(j) | (cross ? 0x80000000u : 0u));
+          for (int s = 0; s < 4; ++s) {
+            R.s[s].g = R.s[s].c = 0;
+            R.s[s].t = R.s[s].w = T(0);
+          }
+          T dgi = T(0), dgj = T(0), cFj = T(0), v[6] = {0, 0, 0, 0, 0, 0};
+          if (u[0] != T(0) || u[1] != T(0) || u[2] != T(0)) { // (coincident atoms: no pair term)
+            if (cross) {
+              const T s0 = static_cast<T>(shift[3 * img]), s1 = static_cast<T>(shift[3 * img + 1]),
+                      s2 = static_cast<T>(shift[3 * img + 2]);
+              v[0] = s0 * u[0];
+              v[1] = s1 * u[1];
+              v[2] = s2 * u[2];
+              v[3] = s0 * u[1];
+              v[4] = s0 * u[2];
+              v[5] = s1 * u[2];
+            }
+            auto set_slot = [&](int sl, const STab<T> &tb, int sg, T wgt) {
+              R.s[sl].g = sg * kWin;
+              R.s[sl].c = tb.cmap0 + segws[sg];
+              R.s[sl].t = t;
+              R.s[sl].w = wgt * tb.inv_h;
+            };
+            const STab<T> &tp = tabs[pair_ord(ti, tj, nt)], &gj = tabs[np + tj], &gi_ = tabs[np + ti];
+            set_slot(0, tp, tp.seg0 + e, T(1));
+            const T gFj = gFa[j];
+            cFj = cFa[j];
+            set_slot(1, gj, gj.seg0 + e, tj == ti ? gFi + gFj : gFi);
+            dgj = seg_der<T>(seg[gj.seg0 + e], t, gj.inv_h);
+            if (tj == ti) {
+              dgi = dgj;
+            } else {
+              dgi = seg_der<T>(seg[gi_.seg0 + e], t, gi_.inv_h);
+              set_slot(2, gi_, gi_.seg0 + e, gFj);
+            }
+            const STab<T> &te = tabs[np + nt + tj];
+            R.s[3].c = te.cmap0 + wsFa[j];
+            R.s[3].w = dgi;
+          }
+          R.uv = {u[0], u[1], u[2], v[0]};
+          R.vv = {v[1], v[2], v[3], v[4]};
+          R.vyz = v[5];
+          R.jw.w = cFj * dgi;
+          rec[lane] = R;
+          for (int a = 0; a < 3; ++a) V[a] += dgj * u[a];
+          for (int a = 0; a < 6; ++a) P[a] += dgj * v[a];
+        }
+      }
+      if (!runs && lane < cnt) {
         PairRec<T> R;
         int j;
         T d[3];
@@ -1579,6 +1665,14 @@ template <class T> int launch_jacobian_t(fs_gpu *h, double w_e, double w_s) {
   a.drho = static_cast<T *>(h->d_drho);
   a.dgd = static_cast<T *>(h->d_dgd);
   a.wsF = h->d_wsF;
+  a.run_a = h->d_run_a;
+  a.run_b = h->d_run_b;
+  a.run_cnt = h->d_run_cnt;
+  a.runs = 0;
+  if constexpr (std::is_same_v<T, float>) {
+    RunGrid rg;
+    a.runs = eam && h->runs_valid && pair_runs_grid(h, &rg) ? 1 : 0;
+  }
   a.stage = 0;
   const size_t common = jac_common_smem<T>(a.c.n_tables, h->n_segs, h->n_cmap, h->max_natoms, max_images(h));
   if (eam) {
@@ -1824,13 +1918,13 @@ int launch_population_t(fs_gpu *h, double w_e, double w_s, const double *d_xs, i
       pa.run_b = h->d_run_b;
       pa.run_r = h->d_run_r;
       pa.run_cnt = h->d_run_cnt;
-      pa.run_np1 = 0;
+      pa.runs = 0;
       auto kl = pop_lanes_kernel<EAM, false>;
       if constexpr (EAM) {
         RunGrid rg;
         if (h->runs_valid && pair_runs_grid(h, &rg)) {
           kl = pop_lanes_kernel<EAM, true>;
-          pa.run_np1 = rg.n + 1;
+          pa.runs = 1;
         }
       }
       FS_CUDA(cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sml)));
@@ -1949,13 +2043,13 @@ int launch_population_static(fs_gpu *h, double w_e, double w_s, const double *d_
       pa.run_b = h->d_run_b;
       pa.run_r = h->d_run_r;
       pa.run_cnt = h->d_run_cnt;
-      pa.run_np1 = 0;
+      pa.runs = 0;
       auto kl = pop_lanes_kernel<EAM, false>;
       if constexpr (EAM) {
         RunGrid rg;
         if (h->runs_valid && pair_runs_grid(h, &rg)) {
           kl = pop_lanes_kernel<EAM, true>;
-          pa.run_np1 = rg.n + 1;
+          pa.runs = 1;
         }
       }
       FS_CUDA(cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sml)));

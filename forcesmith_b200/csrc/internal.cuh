@@ -205,7 +205,7 @@ struct fs_gpu {
   // each atom's in-gate pairs sorted by (neighbour species, segment of the
   // grid), built once per neighbour list and grid (pair_runs.cuh)
   float4 *d_run_a = nullptr;      // [pair]: u_x, u_y, u_z, t  (pair slots of the neighbour list)
-  int2 *d_run_b = nullptr;        // [pair]: packed neighbour entry, key = species·(n + 1) + segment
+  int2 *d_run_b = nullptr;        // [pair]: packed neighbour entry, key = (species << 8) | segment
   int32_t *d_run_cnt = nullptr;   // [atom]: in-gate pairs
   float *d_run_r = nullptr;       // [pair]: FP64 length rounded to FP32
   bool runs_valid = false;        // built for the current neighbour lists and model grid
@@ -269,6 +269,7 @@ int build_neighbors(fs_gpu *h, double rcut);
 // the knot grid shared by the pair and density tables
 constexpr int kRunMaxT = 4;  // species
 constexpr int kRunMaxN = 64; // knots of the shared grid
+constexpr int kRunKeyBits = 8; // run key = (neighbour species << 8) | segment (segments ≤ kRunMaxN)
 struct RunGrid {
   double x0, xmax, inv_h;
   int n;

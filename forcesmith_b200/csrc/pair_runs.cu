@@ -4,7 +4,7 @@
 //
 // On a shared grid a pair's segment e and local coordinate t are the same in
 // every radial table and depend only on the geometry, so they are found once
-// per neighbour list.  Sorted by key = t_j·(n + 1) + e, consecutive pairs of
+// per neighbour list.  Sorted by key = (t_j << 8) | e, consecutive pairs of
 // an atom with one key (a run; 1.8 pairs on average in the ternary
 // benchmark) use the same segment of φ_{t_i t_j}, ρ_{t_j} and ρ_{t_i}: the
 // population kernel loads each trial's coefficients once per run instead of
@@ -36,7 +36,6 @@ __global__ void __launch_bounds__(256) run_pairs_kernel(Common C, RunGrid G, int
   stage_geometry(cd, C, wpos, shift, typ);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int np1 = G.n + 1;
   constexpr int kOut = 0x7fffffff;
   // segment and local coordinate on the grid, as seg_of64 forms them
   auto locate = [&](double r64, int &e, float &t) {
@@ -75,7 +74,7 @@ __global__ void __launch_bounds__(256) run_pairs_kernel(Common C, RunGrid G, int
         int e;
         float t;
         locate(r64, e, t);
-        key = typ[j] * np1 + e;
+        key = (typ[j] << kRunKeyBits) | e;
         ++in_gate;
       }
       keys_tmp[s0 + q] = key;
