@@ -335,7 +335,9 @@ __device__ __forceinline__ float poly_der(const float4 &a, float t) { return a.y
 // with one (neighbour species, segment) key shares the φ_{t_i t_j}, ρ_{t_j}
 // and ρ_{t_i} segments, so each lane loads its trial's coefficients once per
 // run, and the pair geometry is read instead of rebuilt for every tile.
-template <bool EAM, bool RUNS>
+// STRESS (w_s > 0): the per-trial virial sums; the DE objective of a fit
+// without stress rows skips them.
+template <bool EAM, bool RUNS, bool STRESS>
 __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tile = blockIdx.x % A.n_tiles, chunk = blockIdx.x / A.n_tiles;
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
           __syncwarp();
           const int c = min(32, cnt - pb);
           for (int q = 0; q < c; ++q) {
-            const float4 ra = wst[q].a, rb = wst[q].b, rc = wst[q].c;
+            const float4 ra = wst[q].a;
             const int4 rd = wst[q].d;
             if (rd.y < 0) continue; // coincident atoms: no pair term (warp-uniform)
             if (rd.y != cur) {      // a new run (warp-uniform): this trial's three segments
@@ -518,12 +520,15 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
             f0 += g * ra.x;
             f1 += g * ra.y;
             f2 += g * ra.z;
-            s0 -= g * rb.x;
-            s1 -= g * rb.y;
-            s2 -= g * rb.z;
-            s3 -= g * rb.w;
-            s4 -= g * rc.x;
-            s5 -= g * rc.y;
+            if constexpr (STRESS) {
+              const float4 rb = wst[q].b, rc = wst[q].c;
+              s0 -= g * rb.x;
+              s1 -= g * rb.y;
+              s2 -= g * rb.z;
+              s3 -= g * rb.w;
+              s4 -= g * rc.x;
+              s5 -= g * rc.y;
+            }
           }
           __syncwarp();
         }
@@ -599,7 +604,7 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
         const int cnt = min(32, p1 - pb);
         for (int q = 0; q < cnt; ++q) {
           // the whole record as five 128-bit broadcast loads
-          const float4 ra = wst[q].a, rb = wst[q].b, rc = wst[q].c, rh = wst[q].ih;
+          const float4 ra = wst[q].a, rc = wst[q].c, rh = wst[q].ih;
           const int4 rd = wst[q].d;
           float g = 0.f;
           if (rd.y >= 0) {
@@ -614,12 +619,15 @@ __global__ void __launch_bounds__(kPopWarps * 32, 1) pop_lanes_kernel(PopArgs A)
           f0 += g * ra.x;
           f1 += g * ra.y;
           f2 += g * ra.z;
-          s0 -= g * rb.x;
-          s1 -= g * rb.y;
-          s2 -= g * rb.z;
-          s3 -= g * rb.w;
-          s4 -= g * rc.x;
-          s5 -= g * rc.y;
+          if constexpr (STRESS) {
+            const float4 rb = wst[q].b;
+            s0 -= g * rb.x;
+            s1 -= g * rb.y;
+            s2 -= g * rb.z;
+            s3 -= g * rb.w;
+            s4 -= g * rc.x;
+            s5 -= g * rc.y;
+          }
         }
         __syncwarp();
       }
@@ -1919,11 +1927,12 @@ int launch_population_t(fs_gpu *h, double w_e, double w_s, const double *d_xs, i
       pa.run_r = h->d_run_r;
       pa.run_cnt = h->d_run_cnt;
       pa.runs = 0;
-      auto kl = pop_lanes_kernel<EAM, false>;
+      const bool stress = w_s > 0.0;
+      auto kl = stress ? pop_lanes_kernel<EAM, false, true> : pop_lanes_kernel<EAM, false, false>;
       if constexpr (EAM) {
         RunGrid rg;
         if (h->runs_valid && pair_runs_grid(h, &rg)) {
-          kl = pop_lanes_kernel<EAM, true>;
+          kl = stress ? pop_lanes_kernel<EAM, true, true> : pop_lanes_kernel<EAM, true, false>;
           pa.runs = 1;
         }
       }
@@ -2044,11 +2053,12 @@ int launch_population_static(fs_gpu *h, double w_e, double w_s, const double *d_
       pa.run_r = h->d_run_r;
       pa.run_cnt = h->d_run_cnt;
       pa.runs = 0;
-      auto kl = pop_lanes_kernel<EAM, false>;
+      const bool stress = w_s > 0.0;
+      auto kl = stress ? pop_lanes_kernel<EAM, false, true> : pop_lanes_kernel<EAM, false, false>;
       if constexpr (EAM) {
         RunGrid rg;
         if (h->runs_valid && pair_runs_grid(h, &rg)) {
-          kl = pop_lanes_kernel<EAM, true>;
+          kl = stress ? pop_lanes_kernel<EAM, true, true> : pop_lanes_kernel<EAM, true, false>;
           pa.runs = 1;
         }
       }
