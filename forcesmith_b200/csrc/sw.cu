@@ -159,6 +159,7 @@ template <class T> struct SwArgs {
 };
 
 constexpr int kSwThreads = 256;
+constexpr int kSwChunk = 4; // consecutive 3-body items per thread
 
 
 template <class T>
@@ -202,6 +203,55 @@ template <class T, int NQ> struct RowAcc {
   }
 };
 
+
+// The force and Jacobian rows of one central atom i, summed in registers over
+// a thread's consecutive work items while i and the items' columns stay the
+// same, and added to shared memory when they change.
+template <class T, int NQ, bool JAC> struct AtomAcc {
+  T f[3];
+  T g[NQ][3];
+  int col[NQ];
+  int i = -1;
+  __device__ AtomAcc() {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[a] = T(0);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      col[q] = -1;
+      g[q][0] = g[q][1] = g[q][2] = T(0);
+    }
+  }
+  __device__ __forceinline__ void flush(T *Fs, T *Jb, int D) {
+    if (i < 0) return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      atomicAdd(&Fs[3 * i + a], f[a]);
+      f[a] = T(0);
+    }
+    if constexpr (JAC)
+#pragma unroll
+      for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          add_row(Jb, D, 3 * i + a, col[q], g[q][a]);
+          g[q][a] = T(0);
+        }
+    i = -1;
+  }
+  // start summing for atom ii with columns cols (flushing what was summed)
+  __device__ __forceinline__ void use(int ii, const int (&cols)[NQ], T *Fs, T *Jb, int D) {
+    bool same = ii == i;
+    if constexpr (JAC)
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) same = same && cols[q] == col[q];
+    if (!same) {
+      flush(Fs, Jb, D);
+      i = ii;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) col[q] = cols[q];
+    }
+  }
+};
 
 template <class T, bool JAC>
 __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(SwArgs<T> A) {
@@ -262,10 +312,14 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
   }
   double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0};
   const int rowE = 3 * N; // local rows of the block: 3N force, E, 6 stress
-  // ---- 2-body: one thread per directed pair (½ v₂ each, force on i)
+  // ---- 2-body: one thread per directed pair (½ v₂ each, force on i).  A
+  // thread takes kSwChunk consecutive pairs, which mostly share atom i.
   {
     RowAcc<T, JAC ? 6 : 1> ra;
-    for (int w = threadIdx.x; w < npair; w += blockDim.x) {
+    AtomAcc<T, JAC ? 6 : 1, JAC> ia;
+    for (int w0 = threadIdx.x * kSwChunk; w0 < npair; w0 += blockDim.x * kSwChunk) {
+    const int w1 = min(w0 + kSwChunk, npair);
+    for (int w = w0; w < w1; ++w) {
       const int i = own ? static_cast<int>(own[w]) : owner_of(pfirst, N, w);
       int j;
       T d[3];
@@ -286,9 +340,12 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
         s = dv2p / r;
       }
       const T f[3] = {s * d[0], s * d[1], s * d[2]};
-      atomicAdd(&Fs[3 * i], f[0]);
-      atomicAdd(&Fs[3 * i + 1], f[1]);
-      atomicAdd(&Fs[3 * i + 2], f[2]);
+      if constexpr (!JAC) {
+        const int nocol[1] = {-1};
+        ia.use(i, nocol, Fs, Jb, D);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ia.f[a] += f[a];
+      }
       e_acc += 0.5 * static_cast<double>(v2v);
       const T hx = T(0.5) * d[0], hy = T(0.5) * d[1], hz = T(0.5) * d[2];
       sg[0] -= hx * f[0];
@@ -302,13 +359,16 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
 #pragma unroll
         for (int k = 0; k < 6; ++k) cols[k] = pcol[8 * sl + k];
         ra.use(cols, Jb, D, rowE);
+        ia.use(i, cols, Fs, Jb, D);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ia.f[a] += f[a];
         const T we = static_cast<T>(0.5 * A.w_e), ir = rcp_t(r);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
           const T ds = dv2.d[k] * ir;
           const T df[3] = {ds * d[0], ds * d[1], ds * d[2]};
 #pragma unroll
-          for (int a = 0; a < 3; ++a) add_row(Jb, D, 3 * i + a, cols[k], df[a]);
+          for (int a = 0; a < 3; ++a) ia.g[k][a] += df[a];
           ra.a[k][0] += we * v2.d[k];
           ra.a[k][1] -= hx * df[0];
           ra.a[k][2] -= hy * df[1];
@@ -319,12 +379,19 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
         }
       }
     }
+    ia.flush(Fs, Jb, D);
+    }
     if constexpr (JAC) ra.flush(Jb, D, rowE);
   }
-  // ---- 3-body: one thread per neighbour pair (j < k) of a central atom i
+  // ---- 3-body: one thread per neighbour pair (j < k) of a central atom i.
+  // A thread takes kSwChunk consecutive items, which mostly share their
+  // central atom i (its force and Jacobian rows go through AtomAcc).
   {
     RowAcc<T, JAC ? 5 : 1> rb;
-    for (int w = threadIdx.x; w < ntri; w += blockDim.x) {
+    AtomAcc<T, JAC ? 5 : 1, JAC> ia;
+    for (int w0 = threadIdx.x * kSwChunk; w0 < ntri; w0 += blockDim.x * kSwChunk) {
+    const int w1 = min(w0 + kSwChunk, ntri);
+    for (int w = w0; w < w1; ++w) {
       int i, a0, u;
       if (own) {
         const uint32_t v = own[npair + w];
@@ -378,9 +445,14 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
         Fj[a] = -(c1.v * d1[a]) - c3.v * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
         Fk[a] = -(c2.v * d2[a]) - c3.v * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
         Fi[a] = -(Fj[a] + Fk[a]); // the three forces sum to zero
-        atomicAdd(&Fs[3 * i + a], Fi[a]);
         atomicAdd(&Fs[3 * j + a], Fj[a]);
         atomicAdd(&Fs[3 * k + a], Fk[a]);
+      }
+      if constexpr (!JAC) {
+        const int nocol[1] = {-1};
+        ia.use(i, nocol, Fs, Jb, D);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ia.f[a] += Fi[a];
       }
       e_acc += static_cast<double>(e3.v);
       sg[0] += d1[0] * Fj[0] + d2[0] * Fk[0];
@@ -402,6 +474,9 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
             cols[q] = -1;
           }
         rb.use(cols, Jb, D, rowE);
+        ia.use(i, cols, Fs, Jb, D);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ia.f[a] += Fi[a];
         const T we = static_cast<T>(A.w_e);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -410,7 +485,7 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
           for (int a = 0; a < 3; ++a) {
             gj[a] = -(c1.d[q] * d1[a]) - c3.d[q] * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
             gk[a] = -(c2.d[q] * d2[a]) - c3.d[q] * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
-            add_row(Jb, D, 3 * i + a, cols[q], -(gj[a] + gk[a]));
+            ia.g[q][a] -= gj[a] + gk[a];
             add_row(Jb, D, 3 * j + a, cols[q], gj[a]);
             add_row(Jb, D, 3 * k + a, cols[q], gk[a]);
           }
@@ -423,6 +498,8 @@ __global__ void __launch_bounds__(kSwThreads, sizeof(T) == 4 ? 2 : 1) sw_kernel(
           rb.a[q][6] += d1[1] * gj[2] + d2[1] * gk[2];
         }
       }
+    }
+    ia.flush(Fs, Jb, D);
     }
     if constexpr (JAC) rb.flush(Jb, D, rowE);
   }
