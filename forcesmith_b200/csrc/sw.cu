@@ -159,7 +159,7 @@ template <class T> struct SwArgs {
 };
 
 constexpr int kSwThreads = 256;
-constexpr int kSwChunk = 4; // consecutive 3-body items per thread
+constexpr int kSwChunk = 4; // consecutive 2-body and 3-body items per thread
 
 
 template <class T>

@@ -141,13 +141,18 @@ template <class T> __global__ void __launch_bounds__(kTsThreads) tersoff_kernel(
     e_acc += 0.5 * static_cast<double>(fc * (VR - b * VA));
     const T pc = T(0.5) * (dfc * (VR - b * VA) + fc * (VRp - b * VAp)) / r1;
     const T Fp[3] = {pc * d1[0], pc * d1[1], pc * d1[2]};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      atomicAdd(&Fs[3 * i + a], Fp[a]);
-      atomicAdd(&Fs[3 * j + a], -Fp[a]);
-    }
     add_stress(d1, Fp, T(-0.5));
-    if (zeta == T(0)) continue;
+    // the forces on i and j of this bond and of its three-body terms, summed
+    // here and added once (k's are added per neighbour)
+    T fi[3] = {Fp[0], Fp[1], Fp[2]}, fj[3] = {-Fp[0], -Fp[1], -Fp[2]};
+    if (zeta == T(0)) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        atomicAdd(&Fs[3 * i + a], fi[a]);
+        atomicAdd(&Fs[3 * j + a], fj[a]);
+      }
+      continue;
+    }
     // accumulate_three_body
     const T Pz = T(0.5) * fc * VA * db;
     const T ir1 = T(1) / r1;
@@ -172,12 +177,17 @@ template <class T> __global__ void __launch_bounds__(kTsThreads) tersoff_kernel(
         Fi[a] = Pz * (wk * (-dfck * ir2 * gv * d2[a] + fck * dgv * (Ac * d1[a] + Bc * d2[a])));
         Fj[a] = Pz * (wk * fck * dgv * (ir1 * ir2 * d2[a] - cth * ir1 * ir1 * d1[a]));
         Fk[a] = Pz * (wk * (dfck * ir2 * gv * d2[a] + fck * dgv * (ir1 * ir2 * d1[a] - cth * ir2 * ir2 * d2[a])));
-        atomicAdd(&Fs[3 * i + a], Fi[a]);
-        atomicAdd(&Fs[3 * j + a], Fj[a]);
+        fi[a] += Fi[a];
+        fj[a] += Fj[a];
         atomicAdd(&Fs[3 * k + a], Fk[a]);
       }
       add_stress(d1, Fj, T(1));
       add_stress(d2, Fk, T(1));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      atomicAdd(&Fs[3 * i + a], fi[a]);
+      atomicAdd(&Fs[3 * j + a], fj[a]);
     }
   }
   __syncthreads();
