@@ -11,10 +11,10 @@
 //   With spline tables the reference's Jacobian is central differences; the
 //   device keeps that method (fd.cu, FP64 contexts).
 //
-// One CTA per configuration; each warp takes 32 consecutive work items from a
-// block scan: directed pairs (2-body), then neighbour pairs (j < k) of a
-// central atom (3-body).  Forces accumulate in shared memory, summed first
-// over each run of lanes that share an atom; energy and stress are
+// One CTA per configuration; each thread takes 4 consecutive work items from
+// a block scan: directed pairs (2-body), then neighbour pairs (j < k) of a
+// central atom (3-body).  Forces accumulate in shared memory, summed first in
+// registers over a thread's items that share an atom; energy and stress are
 // per-thread FP64 sums.
 #include "kern_common.cuh"
 
@@ -24,6 +24,7 @@ namespace fsg {
 namespace {
 
 constexpr int kAgThreads = 256;
+constexpr int kAgChunk = 4; // consecutive work items per thread
 
 template <class T> struct AgArgs {
   Common c;
@@ -63,98 +64,118 @@ template <class T> __global__ void __launch_bounds__(kAgThreads, sizeof(T) == 4 
   const uint32_t *nbp = A.c.nb_pack + start[0];
   const int npair = pfirst[N], ntri = tfirst[N];
   double e_acc = 0.0, sg[6] = {0, 0, 0, 0, 0, 0}; // xx, yy, zz, xy, xz, yz
-  const int lane = threadIdx.x & 31;
-  // Each warp takes 32 consecutive work items (spare lanes repeat the last
-  // with ok false).  Items are ordered by central atom, so the forces on atom
-  // i (and, for neighbour pairs, on atom j) are summed over each run of lanes
-  // that share it and added once.
-  // ---- 2-body: one thread per directed pair
-  for (int w0 = threadIdx.x - lane; w0 < npair; w0 += blockDim.x) {
-    const int w = min(w0 + lane, npair - 1);
-    const int i = owner_of(pfirst, N, w);
-    int j;
-    T d[3];
-    pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
-    const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    const STab<T> &tb = tabs[pair_ord(typ[i], typ[j], nt)];
-    const uint32_t pw = nbp[w];
-    T tq;
-    const int eq = gate_seg(tb, r, tq, [=] { return pair_len64(wpos, shift, i, pw); });
-    const bool ok = w0 + lane < npair && r >= T(1e-14) && eq >= 0;
-    if (!__any_sync(0xffffffffu, ok)) continue;
-    bool hi;
-    const unsigned xi = run_links(i, lane, hi);
-    const VD<T> ph = tab_vd_at<T, true>(tb, seg, A.vals, r, eq >= 0 ? eq : tb.seg0, tq);
-    const T s = ok ? ph.d / r : T(0);
-    const T f[3] = {s * d[0], s * d[1], s * d[2]};
+  // Each thread takes kAgChunk consecutive work items.  Items are ordered by
+  // central atom (then by neighbour), so consecutive items mostly share atom
+  // i (and, for neighbour pairs, atom j): their forces on i and j are summed
+  // in registers and added to shared memory when the atom changes.
+  struct Acc {
+    T f[3] = {T(0), T(0), T(0)};
+    int at = -1;
+    __device__ __forceinline__ void to(int a, T *Fs) {
+      if (a == at) return;
+      if (at >= 0)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const T t = run_sum(f[a], xi);
-      if (hi) atomicAdd(&Fs[3 * i + a], t);
+        for (int q = 0; q < 3; ++q) {
+          atomicAdd(&Fs[3 * at + q], f[q]);
+          f[q] = T(0);
+        }
+      at = a;
     }
-    if (!ok) continue;
-    e_acc += 0.5 * static_cast<double>(ph.v);
-    sg[0] -= static_cast<double>(T(0.5) * d[0] * f[0]);
-    sg[1] -= static_cast<double>(T(0.5) * d[1] * f[1]);
-    sg[2] -= static_cast<double>(T(0.5) * d[2] * f[2]);
-    sg[3] -= static_cast<double>(T(0.5) * d[0] * f[1]);
-    sg[4] -= static_cast<double>(T(0.5) * d[0] * f[2]);
-    sg[5] -= static_cast<double>(T(0.5) * d[1] * f[2]);
+  };
+  // ---- 2-body: one item per directed pair
+  for (int w0 = threadIdx.x * kAgChunk; w0 < npair; w0 += blockDim.x * kAgChunk) {
+    const int w1 = min(w0 + kAgChunk, npair);
+    int i = owner_of(pfirst, N, w0);
+    Acc ai;
+    for (int w = w0; w < w1; ++w) {
+      while (pfirst[i + 1] <= w) ++i;
+      int j;
+      T d[3];
+      pair_vec(wpos, shift, i, nbp[w], j, d[0], d[1], d[2]);
+      const T r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      if (r < T(1e-14)) continue;
+      const STab<T> &tb = tabs[pair_ord(typ[i], typ[j], nt)];
+      const uint32_t pw = nbp[w];
+      T tq;
+      const int eq = gate_seg(tb, r, tq, [=] { return pair_len64(wpos, shift, i, pw); });
+      if (eq < 0) continue;
+      const VD<T> ph = tab_vd_at<T, true>(tb, seg, A.vals, r, eq, tq);
+      const T s = ph.d / r;
+      const T f[3] = {s * d[0], s * d[1], s * d[2]};
+      ai.to(i, Fs);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) ai.f[a] += f[a];
+      e_acc += 0.5 * static_cast<double>(ph.v);
+      sg[0] -= static_cast<double>(T(0.5) * d[0] * f[0]);
+      sg[1] -= static_cast<double>(T(0.5) * d[1] * f[1]);
+      sg[2] -= static_cast<double>(T(0.5) * d[2] * f[2]);
+      sg[3] -= static_cast<double>(T(0.5) * d[0] * f[1]);
+      sg[4] -= static_cast<double>(T(0.5) * d[0] * f[2]);
+      sg[5] -= static_cast<double>(T(0.5) * d[1] * f[2]);
+    }
+    ai.to(-1, Fs);
   }
-  // ---- 3-body: one thread per neighbour pair (j < k) of a central atom i
-  for (int w0 = threadIdx.x - lane; w0 < ntri; w0 += blockDim.x) {
-    const int w = min(w0 + lane, ntri - 1);
-    const int i = owner_of(tfirst, N, w);
-    const int n = pfirst[i + 1] - pfirst[i];
-    int u = w - tfirst[i], a0 = 0;
-    pair_row(n, u, a0);
-    const int pj = pfirst[i] + a0, pk = pj + 1 + u;
-    const int ti = typ[i];
-    int j, k;
-    T d1[3], d2[3];
-    pair_vec(wpos, shift, i, nbp[pj], j, d1[0], d1[1], d1[2]);
-    const T r1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
-    const STab<T> &rj = tabs[np + pair_ord(ti, typ[j], nt)];
-    pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
-    const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
-    const STab<T> &rk = tabs[np + pair_ord(ti, typ[k], nt)];
-    const uint32_t pwj = nbp[pj], pwk = nbp[pk];
-    T t1, t2;
-    const int e1 = gate_seg(rj, r1, t1, [=] { return pair_len64(wpos, shift, i, pwj); });
-    const int e2 = gate_seg(rk, r2, t2, [=] { return pair_len64(wpos, shift, i, pwk); });
-    const bool ok = w0 + lane < ntri && r1 >= T(1e-14) && e1 >= 0 && r2 >= T(1e-14) && e2 >= 0;
-    if (!__any_sync(0xffffffffu, ok)) continue;
-    bool hi, hj;
-    const unsigned xi = run_links(i, lane, hi);
-    const unsigned xj = run_links(pj, lane, hj); // atom j: runs of the same neighbour slot
-    const VD<T> F1 = tab_vd_at<T, true>(rj, seg, A.vals, r1, e1 >= 0 ? e1 : rj.seg0, t1),
-                F2 = tab_vd_at<T, true>(rk, seg, A.vals, r2, e2 >= 0 ? e2 : rk.seg0, t2);
-    // lanes without a term: zero inverse distances and c3, so every force below is zero
-    const T ir1 = ok ? T(1) / r1 : T(0), ir2 = ok ? T(1) / r2 : T(0);
-    const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;
-    const VD<T> G = tab_vd<T, true>(tabs[2 * np + ti], seg, A.vals, cth);
-    if (ok) e_acc += static_cast<double>(F1.v * F2.v * G.v);
-    // three_body_forces (kernels.hpp:44-58)
-    const T irr = ir1 * ir2;
-    const T Aa = cth * ir1 * ir1 - irr, Bb = cth * ir2 * ir2 - irr;
-    const T c1 = F1.d * ir1 * F2.v * G.v, c2 = F1.v * F2.d * ir2 * G.v, c3 = ok ? F1.v * F2.v * G.d : T(0);
-    T Fj[3], Fk[3];
+  // ---- 3-body: one item per neighbour pair (j < k) of a central atom i
+  for (int w0 = threadIdx.x * kAgChunk; w0 < ntri; w0 += blockDim.x * kAgChunk) {
+    const int w1 = min(w0 + kAgChunk, ntri);
+    int i = owner_of(tfirst, N, w0);
+    Acc ai, aj;
+    for (int w = w0; w < w1; ++w) {
+      while (tfirst[i + 1] <= w) ++i;
+      const int n = pfirst[i + 1] - pfirst[i];
+      int u = w - tfirst[i], a0 = 0;
+      pair_row(n, u, a0);
+      const int pj = pfirst[i] + a0, pk = pj + 1 + u;
+      const int ti = typ[i];
+      int j, k;
+      T d1[3], d2[3];
+      pair_vec(wpos, shift, i, nbp[pj], j, d1[0], d1[1], d1[2]);
+      const T r1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+      if (r1 < T(1e-14)) continue;
+      const STab<T> &rj = tabs[np + pair_ord(ti, typ[j], nt)];
+      const uint32_t pwj = nbp[pj];
+      T t1;
+      const int e1 = gate_seg(rj, r1, t1, [=] { return pair_len64(wpos, shift, i, pwj); });
+      if (e1 < 0) continue;
+      pair_vec(wpos, shift, i, nbp[pk], k, d2[0], d2[1], d2[2]);
+      const T r2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
+      if (r2 < T(1e-14)) continue;
+      const STab<T> &rk = tabs[np + pair_ord(ti, typ[k], nt)];
+      const uint32_t pwk = nbp[pk];
+      T t2;
+      const int e2 = gate_seg(rk, r2, t2, [=] { return pair_len64(wpos, shift, i, pwk); });
+      if (e2 < 0) continue;
+      const VD<T> F1 = tab_vd_at<T, true>(rj, seg, A.vals, r1, e1, t1),
+                  F2 = tab_vd_at<T, true>(rk, seg, A.vals, r2, e2, t2);
+      const T ir1 = T(1) / r1, ir2 = T(1) / r2;
+      const T cth = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) * ir1 * ir2;
+      const VD<T> G = tab_vd<T, true>(tabs[2 * np + ti], seg, A.vals, cth);
+      e_acc += static_cast<double>(F1.v * F2.v * G.v);
+      // three_body_forces (kernels.hpp:44-58)
+      const T irr = ir1 * ir2;
+      const T Aa = cth * ir1 * ir1 - irr, Bb = cth * ir2 * ir2 - irr;
+      const T c1 = F1.d * ir1 * F2.v * G.v, c2 = F1.v * F2.d * ir2 * G.v, c3 = F1.v * F2.v * G.d;
+      T Fj[3], Fk[3];
+      ai.to(i, Fs);
+      aj.to(j, Fs);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const T Fi = c1 * d1[a] + c2 * d2[a] - c3 * (Aa * d1[a] + Bb * d2[a]);
-      Fj[a] = -(c1 * d1[a]) - c3 * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
-      Fk[a] = -(c2 * d2[a]) - c3 * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
-      const T ti_ = run_sum(Fi, xi), tj = run_sum(Fj[a], xj);
-      if (hi) atomicAdd(&Fs[3 * i + a], ti_);
-      if (hj) atomicAdd(&Fs[3 * j + a], tj);
-      if (ok) atomicAdd(&Fs[3 * k + a], Fk[a]);
+      for (int a = 0; a < 3; ++a) {
+        const T Fi = c1 * d1[a] + c2 * d2[a] - c3 * (Aa * d1[a] + Bb * d2[a]);
+        Fj[a] = -(c1 * d1[a]) - c3 * (irr * d2[a] - cth * ir1 * ir1 * d1[a]);
+        Fk[a] = -(c2 * d2[a]) - c3 * (irr * d1[a] - cth * ir2 * ir2 * d2[a]);
+        ai.f[a] += Fi;
+        aj.f[a] += Fj[a];
+        atomicAdd(&Fs[3 * k + a], Fk[a]);
+      }
+      sg[0] += static_cast<double>(d1[0] * Fj[0] + d2[0] * Fk[0]);
+      sg[1] += static_cast<double>(d1[1] * Fj[1] + d2[1] * Fk[1]);
+      sg[2] += static_cast<double>(d1[2] * Fj[2] + d2[2] * Fk[2]);
+      sg[3] += static_cast<double>(d1[0] * Fj[1] + d2[0] * Fk[1]);
+      sg[4] += static_cast<double>(d1[0] * Fj[2] + d2[0] * Fk[2]);
+      sg[5] += static_cast<double>(d1[1] * Fj[2] + d2[1] * Fk[2]);
     }
-    sg[0] += static_cast<double>(d1[0] * Fj[0] + d2[0] * Fk[0]);
-    sg[1] += static_cast<double>(d1[1] * Fj[1] + d2[1] * Fk[1]);
-    sg[2] += static_cast<double>(d1[2] * Fj[2] + d2[2] * Fk[2]);
-    sg[3] += static_cast<double>(d1[0] * Fj[1] + d2[0] * Fk[1]);
-    sg[4] += static_cast<double>(d1[0] * Fj[2] + d2[0] * Fk[2]);
-    sg[5] += static_cast<double>(d1[1] * Fj[2] + d2[1] * Fk[2]);
+    ai.to(-1, Fs);
+    aj.to(-1, Fs);
   }
   __syncthreads();
   // residual rows of the configuration (residual_layout.hpp:37-54)
