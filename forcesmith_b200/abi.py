@@ -24,8 +24,10 @@ FS_ERR_NUMERIC = -7
 
 FS_FAMILY_PAIR, FS_FAMILY_EAM, FS_FAMILY_ADP, FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_FAMILY_ANGULAR = 0, 1, 2, 3, 4, 5
 FS_FAMILY_ACSF = 6
+FS_FAMILY_LMBTR = 7
 FS_TABLE_SPLINE, FS_TABLE_ANALYTIC, FS_TABLE_SW, FS_TABLE_LAMBDA, FS_TABLE_TERSOFF = 0, 1, 2, 3, 4
 FS_TABLE_ACSF, FS_TABLE_LINEAR_HEAD, FS_TABLE_STANDARDIZATION = 5, 6, 7
+FS_TABLE_LMBTR = 8
 TERSOFF_FIELDS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S", "omega")
 FS_PREC_FP32, FS_PREC_FP64 = 0, 1
 
@@ -48,6 +50,19 @@ def acsf_size(spec, nt):
     acsf.hpp:23-33): nt(nG1 + nG2 + nG3) + npair(nG4 + nG5)."""
     g1, n2, n3, n4, n5 = (int(x) for x in spec.values[1:6])
     return nt * (g1 + n2 + n3) + nt * (nt + 1) // 2 * (n4 + n5)
+
+
+def lmbtr_size(spec, nt):
+    """Descriptor length of an LMBTR table for nt species (LmbtrLayout,
+    lmbtr.hpp:13-38): nt·n2 + npair·n3, a term with n = 0 absent."""
+    n2, n3 = int(spec.values[3]), int(spec.values[7])
+    return nt * n2 + nt * (nt + 1) // 2 * n3
+
+
+def descriptor_size(model):
+    """Descriptor length S of an ACSF or LMBTR model."""
+    spec = model.tables[0]
+    return lmbtr_size(spec, model.ntypes) if model.family == FS_FAMILY_LMBTR else acsf_size(spec, model.ntypes)
 
 
 class FsError(RuntimeError):
@@ -160,6 +175,20 @@ class Table:
         return Table(FS_TABLE_ACSF, v, 0.0, 0.0, 0, np.ones(v.size, np.uint8))
 
     @staticmethod
+    def lmbtr(rcut=6.0, weight_scale=3.0, normalize=True, k2=(0.0, 6.0, 50, 0.3), k3=(-1.0, 1.0, 50, 0.1)):
+        """LMBTR descriptor (the reference's LMBTR fields and defaults,
+        lmbtr.hpp:40-47): k2 and k3 grids as (min, max, n, sigma) or None
+        for an absent term; distances r_ij on the k2 grid, cos θ_ijk on the
+        k3 grid.  Descriptor hyperparameters are not fitted."""
+        def grid(g):
+            if g is None:
+                return [0, 0.0, 0.0, 0.0]
+            lo, hi, n, sig = g
+            return [int(n), float(lo), float(hi), float(sig)]
+        v = np.array([rcut, weight_scale, 1.0 if normalize else 0.0] + grid(k2) + grid(k3), np.float64)
+        return Table(FS_TABLE_LMBTR, v, 0.0, 0.0, 0, np.ones(v.size, np.uint8))
+
+    @staticmethod
     def linear_head(coeffs, bias=0.0, bias_fixed=True, fixed=None):
         """LinearHead E_i = w·D_i + b (ml_force.hpp); the bias is fixed unless
         bias_fixed is False, as the reference declares it."""
@@ -256,9 +285,9 @@ class Model:
         return m, keep
 
     def with_standardization(self, mean, inv_std):
-        """An ACSF model with the per-species standardization tables set to
-        mean, inv_std (nt × S), replacing any it had."""
-        assert self.family == FS_FAMILY_ACSF
+        """An ACSF or LMBTR model with the per-species standardization tables
+        set to mean, inv_std (nt × S), replacing any it had."""
+        assert self.family in (FS_FAMILY_ACSF, FS_FAMILY_LMBTR)
         mean, inv_std = np.asarray(mean, np.float64), np.asarray(inv_std, np.float64)
         tabs = [t.copy() for t in self.tables[:1 + self.ntypes]]
         tabs += [Table.standardization(mean[t], inv_std[t]) for t in range(self.ntypes)]
@@ -452,11 +481,12 @@ class Session:
         self._check(self._f("prepare")(self._h), "prepare")
 
     def acsf_standardization(self):
-        """ACSF models: per-species descriptor mean and 1/σ over every uploaded
-        atom, and the atoms per species (MLBase::compute_standardization).
-        Returns (mean nt × S, inv_std nt × S, count nt)."""
+        """ACSF and LMBTR models: per-species descriptor mean and 1/σ over
+        every uploaded atom, and the atoms per species
+        (MLBase::compute_standardization).  Returns (mean nt × S, inv_std
+        nt × S, count nt)."""
         nt = self._model.ntypes
-        S = acsf_size(self._model.tables[0], nt)
+        S = descriptor_size(self._model)
         mean, inv_std = np.zeros((nt, S)), np.zeros((nt, S))
         count = np.zeros(nt, np.int64)
         self._check(self._f("acsf_standardization")(self._h, _dp(mean), _dp(inv_std),

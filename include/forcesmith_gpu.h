@@ -101,11 +101,14 @@ enum fs_family {
   FS_FAMILY_TERSOFF = 4, /* tables: tersoff[npair] (12 params each)        */
   FS_FAMILY_ANGULAR = 5, /* tables: pair[npair], radial[npair], angular[nt]:
                             spline or analytic (angular_force.hpp:15-33)   */
-  FS_FAMILY_ACSF = 6     /* tables: acsf[1] (descriptor), head[nt] (linear
+  FS_FAMILY_ACSF = 6,    /* tables: acsf[1] (descriptor), head[nt] (linear
                             energy head per species) (acsf.hpp:48-86,
                             ml_force.hpp LinearHead), and optionally
                             standardization[nt] (MLBase mean_ / inv_std_,
                             ml_force.hpp:194-199)                          */
+  FS_FAMILY_LMBTR = 7    /* tables: lmbtr[1] (descriptor), head[nt], and
+                            optionally standardization[nt], as for ACSF
+                            (include/forcesmith/potentials/lmbtr.hpp:40-63) */
 };
 
 enum fs_table_kind {
@@ -124,10 +127,15 @@ enum fs_table_kind {
                             + npair(nG4 + nG5) (AcsfLayout, acsf.hpp:23-33) */
   FS_TABLE_LINEAR_HEAD = 6, /* E_i = w·D_i + b: {w[S], b}, n == S + 1; the
                             bias is fixed unless `fixed` says otherwise    */
-  FS_TABLE_STANDARDIZATION = 7 /* per species, all values fixed: {mean[S],
+  FS_TABLE_STANDARDIZATION = 7, /* per species, all values fixed: {mean[S],
                             inv_std[S]}, n == 2S; the head then sees
                             (D − mean) ⊙ inv_std (ml_force.hpp:607-623);
                             mean 0 and inv_std 1 leave D unchanged        */
+  FS_TABLE_LMBTR = 8     /* LMBTR descriptor, all values fixed:
+                            {rcut, weight_scale, normalize (0/1),
+                             n2, min2, max2, sigma2, n3, min3, max3, sigma3};
+                            a term with n = 0 is absent; descriptor size
+                            S = nt·n2 + npair·n3 (LmbtrLayout, lmbtr.hpp:13-38) */
 };
 
 /* Analytic radial forms (include/forcesmith/potentials/analytic_potential.hpp). */

@@ -60,6 +60,7 @@ def lib():
         L.orc_set_params.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int32]
         L.orc_acsf_standardization.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                C.POINTER(C.c_int64)]
+        L.orc_descriptor.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
     return _LIB
 
 
@@ -95,6 +96,12 @@ class Oracle(Session):
                                          _dp(d))
         self._check(rc, "get_neighbors")
         return j, img.reshape(-1, 3), d.reshape(-1, 3)
+
+    def descriptor(self, c, i, size):
+        """Descriptor values of atom i of configuration c (ACSF or LMBTR)."""
+        D = np.zeros(size, np.float64)
+        self._check(self._lib.orc_descriptor(self._h, c, i, _dp(D)), "descriptor")
+        return D
 
     def jacobian_fd(self, w_e=1.0, w_s=0.0, c0=0, c1=-1):
         m = self.residual_count(w_s)

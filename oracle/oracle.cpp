@@ -164,6 +164,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_TERSOFF: return np;
   case FS_FAMILY_ANGULAR: return 2 * np + nt;
   case FS_FAMILY_ACSF: return 1 + nt;
+  case FS_FAMILY_LMBTR: return 1 + nt;
   }
   return -1;
 }
@@ -180,6 +181,7 @@ double max_cutoff(const State &S) {
     return m;
   }
   if (S.family == FS_FAMILY_ACSF) return S.tables[0].v[0]; // descriptor_cutoff (acsf.hpp:73)
+  if (S.family == FS_FAMILY_LMBTR) return S.tables[0].v[0]; // descriptor_cutoff (lmbtr.hpp:47)
   if (S.family == FS_FAMILY_TERSOFF) { // max S over pair slots (tersoff_force.cpp:259-265)
     for (int p = 0; p < np; ++p) m = std::max(m, S.tables[p].v[10]);
     return m;
@@ -274,7 +276,7 @@ void prime_sites(State &S) {
   for (auto &v : S.site) v.assign(P, Site{});
   for (auto &v : S.site_ok) v.assign(P, 0);
   if (S.family == FS_FAMILY_SW || S.family == FS_FAMILY_TERSOFF || S.family == FS_FAMILY_ANGULAR ||
-      S.family == FS_FAMILY_ACSF)
+      S.family == FS_FAMILY_ACSF || S.family == FS_FAMILY_LMBTR)
     return;
   const Roles R{npair_of(S.ntypes), S.ntypes};
 #pragma omp parallel for schedule(dynamic)
@@ -1019,6 +1021,161 @@ void acsf_values_of(const State &S, int c, int i, double *D) {
     }
 }
 
+// LMBTR descriptors (src/force/lmbtr.cpp) with a linear energy head per
+// species, evaluated as MLBase::eval_forces (ml_force.hpp:462-480).  LMBTR
+// has no analytic descriptor gradient (analytic_grads() is false,
+// lmbtr.hpp:48), so MLBase::descriptor_with_grad (ml_force.hpp:544-572)
+// forms it by central differences, h = 1e-4, moving one neighbour-list
+// displacement component at a time and recomputing the whole descriptor.
+struct LmbtrGrid {
+  int n;
+  double min, max, sigma;
+};
+struct LmbtrSpec {
+  double rcut, ws;
+  bool normalize;
+  LmbtrGrid k2, k3; // n == 0: the term is absent
+  explicit LmbtrSpec(const double *v)
+      : rcut(v[0]), ws(v[1]), normalize(v[2] != 0.0),
+        k2{static_cast<int>(v[3]), v[4], v[5], v[6]}, k3{static_cast<int>(v[7]), v[8], v[9], v[10]} {}
+};
+inline int lmbtr_size(const LmbtrSpec &L, int nt) { return nt * L.k2.n + nt * (nt + 1) / 2 * L.k3.n; }
+// 11 values, counts non-negative integers, at least one term, positive
+// rcut, weight scale and widths of the present terms
+bool lmbtr_valid(const double *v, int n) {
+  if (n != 11 || !(v[0] > 0.0) || !(v[1] > 0.0)) return false;
+  for (int k : {3, 7})
+    if (v[k] < 0 || v[k] != std::floor(v[k]) || (v[k] > 0 && !(v[k + 3] > 0.0))) return false;
+  return v[3] + v[7] > 0;
+}
+
+// broaden (lmbtr.cpp:31-55): a Gaussian of width sigma at geom, scaled by
+// w / (sigma sqrt(2π)), added to the grid bins within 5 sigma; successive
+// bins by the constant-ratio recurrence of make_kernel (lmbtr.cpp:21-29).
+void lmbtr_broaden(double *block, const LmbtrGrid &g, double geom, double w) {
+  const double inv = 1.0 / (g.sigma * std::sqrt(2.0 * kPi)), s2 = 2.0 * g.sigma * g.sigma;
+  const double a = w * inv;
+  if (g.n <= 1) {
+    const double dx = g.min - geom;
+    block[0] += a * std::exp(-dx * dx / s2);
+    return;
+  }
+  const double step = (g.max - g.min) / (g.n - 1), ratio = std::exp(-2.0 * step * step / s2);
+  const double center = (geom - g.min) / step, rad = 5.0 * g.sigma / step;
+  const int b0 = std::max(0, static_cast<int>(std::ceil(center - rad)));
+  const int b1 = std::min(g.n - 1, static_cast<int>(std::floor(center + rad)));
+  if (b0 > b1) return;
+  const double dx0 = g.min + static_cast<double>(b0) * step - geom;
+  double f = std::exp(-dx0 * dx0 / s2), u = std::exp(-(2.0 * dx0 * step + step * step) / s2);
+  for (int b = b0; b <= b1; ++b) {
+    block[b] += a * f;
+    f *= u;
+    u *= ratio;
+  }
+}
+
+// get_descriptor (lmbtr.cpp:64-121) of one atom from its neighbour-list
+// displacements d[0..n) and species s[0..n): neighbours with 1e-14 ≤ r < rcut
+// (descriptor_neighbor, ml_force.hpp:85-97), the k2 term per neighbour, the
+// k3 term per neighbour pair j < k in list order, then the L2 normalisation.
+void lmbtr_descriptor(const LmbtrSpec &L, int nt, const Vec3 *d, const int *s, int n, double *D) {
+  const int Sz = lmbtr_size(L, nt), base3 = nt * L.k2.n;
+  std::fill(D, D + Sz, 0.0);
+  struct Nb {
+    double r;
+    Vec3 d;
+    int s;
+  };
+  std::vector<Nb> nb;
+  for (int p = 0; p < n; ++p) {
+    const double r = norm(d[p]);
+    if (r < 1e-14 || r >= L.rcut) continue;
+    nb.push_back({r, d[p], s[p]});
+  }
+  if (L.k2.n > 0)
+    for (const Nb &j : nb) lmbtr_broaden(D + j.s * L.k2.n, L.k2, j.r, std::exp(-j.r / L.ws));
+  if (L.k3.n > 0)
+    for (size_t a = 0; a < nb.size(); ++a)
+      for (size_t b = a + 1; b < nb.size(); ++b) {
+        const Nb &J = nb[a], &K = nb[b];
+        const double costh = std::clamp(dot(J.d, K.d) / (J.r * K.r), -1.0, 1.0);
+        const double rjk = norm(K.d - J.d);
+        const double w = std::exp(-(J.r + K.r + rjk) / L.ws);
+        lmbtr_broaden(D + base3 + pair_ordinal(J.s, K.s, nt) * L.k3.n, L.k3, costh, w);
+      }
+  if (L.normalize) {
+    double ss = 0.0;
+    for (int k = 0; k < Sz; ++k) ss += D[k] * D[k];
+    const double nrm = std::sqrt(ss);
+    if (nrm > 1e-300)
+      for (int k = 0; k < Sz; ++k) D[k] /= nrm;
+  }
+}
+
+// Atom i's neighbour-list displacements and species.
+void lmbtr_env(const State &S, int c, int i, std::vector<Vec3> &d, std::vector<int> &s) {
+  const Config &cf = S.cfgs[c];
+  const int64_t gi = cf.atom0 + i;
+  d.clear();
+  s.clear();
+  for (int64_t p = S.nb_start[gi]; p < S.nb_start[gi + 1]; ++p) {
+    d.push_back(S.nb_d[p]);
+    s.push_back(S.type[cf.atom0 + S.nb_j[p]]);
+  }
+}
+
+void lmbtr_values_of(const State &S, int c, int i, double *D) {
+  std::vector<Vec3> d;
+  std::vector<int> s;
+  lmbtr_env(S, c, i, d, s);
+  lmbtr_descriptor(LmbtrSpec(S.tables[0].v.data()), S.ntypes, d.data(), s.data(), static_cast<int>(d.size()), D);
+}
+
+void eval_lmbtr(const State &S, int c, Out &o) {
+  const Config &cf = S.cfgs[c];
+  const int nt = S.ntypes;
+  const LmbtrSpec L(S.tables[0].v.data());
+  const int Sz = lmbtr_size(L, nt);
+  std::vector<std::vector<double>> heads(nt);
+  for (int t = 0; t < nt; ++t) heads[t] = acsf_head(S, t, Sz); // standardization folded in
+  std::vector<Vec3> d;
+  std::vector<int> s;
+  std::vector<double> D(Sz), Dp(Sz), Dm(Sz);
+  constexpr double h = 1e-4; // descriptor_with_grad (ml_force.hpp:553)
+  for (int i = 0; i < cf.natoms; ++i) {
+    const int64_t gi = cf.atom0 + i;
+    const double *w = heads[S.type[gi]].data();
+    lmbtr_env(S, c, i, d, s);
+    const int n = static_cast<int>(d.size());
+    lmbtr_descriptor(L, nt, d.data(), s.data(), n, D.data());
+    double e = w[Sz];
+    for (int k = 0; k < Sz; ++k) e += w[k] * D[k];
+    o.energy += e;
+    // grad_neigh by central differences, contracted with dE/dD = w;
+    // accumulate_atom_forces (ml_force.hpp:595-605)
+    for (int p = 0; p < n; ++p) {
+      Vec3 gw{0, 0, 0};
+      for (int a = 0; a < 3; ++a) {
+        const double x0 = d[p][a];
+        d[p][a] = x0 + h;
+        lmbtr_descriptor(L, nt, d.data(), s.data(), n, Dp.data());
+        d[p][a] = x0 - h;
+        lmbtr_descriptor(L, nt, d.data(), s.data(), n, Dm.data());
+        d[p][a] = x0;
+        double t = 0.0;
+        for (int k = 0; k < Sz; ++k) t += w[k] * ((Dp[k] - Dm[k]) / (2.0 * h));
+        gw[a] = t;
+      }
+      const Vec3 fj = -1.0 * gw;
+      o.force[i] = o.force[i] + gw; // −grad_selfᵀ w, grad_self = −Σ grad_neigh
+      const int j = S.nb_j[S.nb_start[gi] + p];
+      o.force[j] = o.force[j] + fj;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) o.stress[a][b] += d[p][a] * fj[b];
+    }
+  }
+}
+
 // with_eval_scope (include/forcesmith/force/eval_scope.hpp:13-31): zero,
 // run the kernel, σ /= V.
 void eval_config(const State &S, int c, Out &o) {
@@ -1034,6 +1191,7 @@ void eval_config(const State &S, int c, Out &o) {
   case FS_FAMILY_TERSOFF: eval_tersoff(S, c, o); break;
   case FS_FAMILY_ANGULAR: eval_angular(S, c, o); break;
   case FS_FAMILY_ACSF: eval_acsf(S, c, o); break;
+  case FS_FAMILY_LMBTR: eval_lmbtr(S, c, o); break;
   }
   const double V = cf.pbc.volume;
   for (auto &row : o.stress)
@@ -1389,7 +1547,8 @@ int orc_set_references(orc_state *h, const double *ref_force, const double *ref_
 
 int orc_set_model(orc_state *h, const fs_model *m) {
   if (!h || !m || m->ntypes < 1) return FS_ERR_ARG;
-  const bool acsf_std = m->family == FS_FAMILY_ACSF && m->n_tables == 1 + 2 * m->ntypes;
+  const bool ml = m->family == FS_FAMILY_ACSF || m->family == FS_FAMILY_LMBTR;
+  const bool acsf_std = ml && m->n_tables == 1 + 2 * m->ntypes;
   if (expected_tables(m->family, m->ntypes) != m->n_tables && !acsf_std) return FS_ERR_ARG;
   State &S = h->S;
   S.family = m->family;
@@ -1401,11 +1560,16 @@ int orc_set_model(orc_state *h, const fs_model *m) {
     if (ft.kind == FS_TABLE_SPLINE && (ft.n < 2 || !(ft.rmax > ft.rmin))) return FS_ERR_ARG;
     if (ft.kind == FS_TABLE_ANALYTIC && form_nparams(ft.form) != ft.n) return FS_ERR_ARG;
     if ((m->family == FS_FAMILY_TERSOFF) != (ft.kind == FS_TABLE_TERSOFF)) return FS_ERR_ARG;
-    if (m->family == FS_FAMILY_ACSF) {
-      const int want = t == 0 ? FS_TABLE_ACSF : t <= m->ntypes ? FS_TABLE_LINEAR_HEAD : FS_TABLE_STANDARDIZATION;
+    if (ml) {
+      const bool lm = m->family == FS_FAMILY_LMBTR;
+      const int want = t == 0 ? (lm ? FS_TABLE_LMBTR : FS_TABLE_ACSF)
+                              : t <= m->ntypes ? FS_TABLE_LINEAR_HEAD : FS_TABLE_STANDARDIZATION;
       if (ft.kind != want) return FS_ERR_ARG;
-      if (t == 0 && acsf_values(ft.values, ft.n) != ft.n) return FS_ERR_ARG;
-      const int Sz = t > 0 ? acsf_size(AcsfSpec(m->tables[0].values), m->ntypes) : 0;
+      if (t == 0 && !lm && acsf_values(ft.values, ft.n) != ft.n) return FS_ERR_ARG;
+      if (t == 0 && lm && !lmbtr_valid(ft.values, ft.n)) return FS_ERR_ARG;
+      const int Sz = t == 0 ? 0
+                     : lm   ? lmbtr_size(LmbtrSpec(m->tables[0].values), m->ntypes)
+                            : acsf_size(AcsfSpec(m->tables[0].values), m->ntypes);
       if (t > 0 && t <= m->ntypes && ft.n != Sz + 1) return FS_ERR_ARG;
       if (t > m->ntypes) { // standardization: 2S values, none of them free
         if (ft.n != 2 * Sz) return FS_ERR_ARG;
@@ -1631,19 +1795,38 @@ int orc_eval_population(orc_state *h, double w_e, double w_s, const double *xs, 
   return FS_OK;
 }
 
+// Descriptor values of atom i of configuration c (ACSF or LMBTR models).
+int orc_descriptor(orc_state *h, int32_t c, int32_t i, double *D) {
+  if (!h || !D) return FS_ERR_ARG;
+  State &S = h->S;
+  if (!S.have_model || S.rcut_built < 0) return FS_ERR_STATE;
+  if (c < 0 || c >= static_cast<int>(S.cfgs.size()) || i < 0 || i >= S.cfgs[c].natoms) return FS_ERR_ARG;
+  if (S.family == FS_FAMILY_LMBTR)
+    lmbtr_values_of(S, c, i, D);
+  else if (S.family == FS_FAMILY_ACSF)
+    acsf_values_of(S, c, i, D);
+  else
+    return FS_ERR_STATE;
+  return FS_OK;
+}
+
 // JᵀJ and Jᵀr from a column-major J (FP64).
 int orc_acsf_standardization(orc_state *h, double *mean, double *inv_std, int64_t *count) {
   if (!h || !mean || !inv_std || !count) return FS_ERR_ARG;
   State &S = h->S;
-  if (!S.have_model || S.family != FS_FAMILY_ACSF || S.rcut_built < 0) return FS_ERR_STATE;
+  const bool lm = S.family == FS_FAMILY_LMBTR;
+  if (!S.have_model || (S.family != FS_FAMILY_ACSF && !lm) || S.rcut_built < 0) return FS_ERR_STATE;
   const int nt = S.ntypes;
-  const int Sz = acsf_size(AcsfSpec(S.tables[0].v.data()), nt);
+  const int Sz = lm ? lmbtr_size(LmbtrSpec(S.tables[0].v.data()), nt) : acsf_size(AcsfSpec(S.tables[0].v.data()), nt);
   // MLBase::compute_standardization (ml_force.hpp:644-688), atoms in order
   std::vector<double> sum(static_cast<size_t>(nt) * Sz, 0.0), sq(sum.size(), 0.0), D(Sz);
   std::vector<int64_t> n(nt, 0);
   for (int c = 0; c < static_cast<int>(S.cfgs.size()); ++c)
     for (int i = 0; i < S.cfgs[c].natoms; ++i) {
-      acsf_values_of(S, c, i, D.data());
+      if (lm)
+        lmbtr_values_of(S, c, i, D.data());
+      else
+        acsf_values_of(S, c, i, D.data());
       const int t = S.type[S.cfgs[c].atom0 + i];
       for (int k = 0; k < Sz; ++k) {
         sum[static_cast<size_t>(t) * Sz + k] += D[k];

@@ -1,0 +1,114 @@
+"""The oracle's LMBTR + linear-head restatement, pinned against the
+reference's unit tests (tests/unit/test_lmbtr.cpp): the 4-atom environment
+(origin plus three neighbours) in a 100 Å box, rcut = 6, weight_scale = 3,
+k2 grid (0, 6, 6 bins, σ 0.4), k3 grid (−1, 1, 6 bins, σ 0.2).
+
+  DescriptorSizeFormula    S·n2 + P·n3, either term absent
+  K3OnlyMatchesTail        k3-only descriptor = the k3 tail of both      1e-14
+  L2Normalized             ‖D‖ = 1                                        1e-12
+  Translation / Rotation / PermutationInvariant                          1e-10 / 1e-9 / 1e-12
+  SensitiveToGeometry      moving a neighbour changes D by > 1e-3
+  ForceMatchesEnergyFD     forces (central-difference descriptor gradient)
+                           against −ΔE/Δx, Δx = 1e-5                   1e-4·|fd| + 1e-5
+plus a dimer's k2 bins by hand (Gaussian of r, weight e^{−r/3}) and
+Newton's third law.
+"""
+import numpy as np
+
+from forcesmith_b200.abi import FS_FAMILY_LMBTR, Model, Table, lmbtr_size
+from oracle import api as O
+from tests.helpers import cluster
+
+ENV = np.array([[0.0, 0.0, 0.0], [2.1, 0.3, -0.2], [0.4, 2.0, 0.5], [-1.3, 0.7, 1.9]])
+K2 = (0.0, 6.0, 6, 0.4)
+K3 = (-1.0, 1.0, 6, 0.2)
+
+
+def spec(k2=K2, k3=K3, normalize=True):
+    return Table.lmbtr(6.0, 3.0, normalize, k2, k3)
+
+
+def oracle(pos, sp, coeffs=None, nt=1, types=None):
+    S = lmbtr_size(sp, nt)
+    w = np.zeros(S) if coeffs is None else coeffs
+    o = O.Oracle()
+    o.upload(cluster(pos, 100.0, types=types))
+    o.set_model(Model(FS_FAMILY_LMBTR, nt, [sp] + [Table.linear_head(w, 0.0) for _ in range(nt)]))
+    return o, S
+
+
+def desc(pos, sp, i=0):
+    o, S = oracle(pos, sp)
+    return o.descriptor(0, i, S)
+
+
+def test_descriptor_size_formula():
+    for S in (1, 2):
+        P = S * (S + 1) // 2
+        assert lmbtr_size(spec(), S) == S * 6 + P * 6
+        assert lmbtr_size(spec(k3=None), S) == S * 6
+        assert lmbtr_size(spec(k2=None), S) == P * 6
+
+
+def test_k3_only_matches_tail():
+    both = desc(ENV, spec(normalize=False))
+    k3 = desc(ENV, spec(k2=None, normalize=False))
+    assert k3.size == both.size - 6
+    assert np.linalg.norm(k3 - both[6:]) <= 1e-14
+    assert np.linalg.norm(k3) > 1e-6
+
+
+def test_l2_normalized():
+    assert abs(np.linalg.norm(desc(ENV, spec())) - 1.0) <= 1e-12
+
+
+def test_invariances():
+    v0 = desc(ENV, spec())
+    assert np.linalg.norm(desc(ENV + np.array([3.7, -1.2, 0.9]), spec()) - v0) <= 1e-10
+    ax = np.array([0.3, -0.8, 0.5])
+    ax /= np.linalg.norm(ax)
+    th = 0.7
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    R = np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+    assert np.linalg.norm(desc(ENV @ R.T, spec()) - v0) <= 1e-9
+    perm = ENV[[0, 3, 2, 1]]
+    assert np.linalg.norm(desc(perm, spec()) - v0) <= 1e-12
+
+
+def test_sensitive_to_geometry():
+    v0 = desc(ENV, spec(normalize=False))
+    moved = ENV.copy()
+    moved[1] += [0.4, -0.3, 0.2]
+    assert np.linalg.norm(desc(moved, spec(normalize=False)) - v0) > 1e-3
+
+
+def test_dimer_k2_bins_by_hand():
+    r = 2.3
+    v = desc([[0, 0, 0], [r, 0, 0]], spec(k3=None, normalize=False))
+    lo, hi, n, sig = K2
+    x = np.linspace(lo, hi, n)
+    g = np.exp(-r / 3.0) / (sig * np.sqrt(2 * np.pi)) * np.exp(-(x - r) ** 2 / (2 * sig * sig))
+    g[np.abs(x - r) > 5 * sig] = 0.0  # outside the 5σ window
+    assert np.abs(v - g).max() <= 1e-14 * np.abs(g).max() * 10
+
+
+def test_force_matches_energy_fd_and_newton():
+    S = lmbtr_size(spec(), 1)
+    w = 0.1 + 0.03 * np.arange(S)
+    o, _ = oracle(ENV, spec(), w)
+    out = o.eval(1.0, 0.0)
+    F = out["forces"].reshape(-1, 3)
+    assert np.abs(F.sum(axis=0)).max() <= 1e-10 * np.abs(F).max()
+
+    def energy(pos):
+        oo, _ = oracle(pos, spec(), w)
+        return oo.eval(1.0, 0.0)["energy"][0]
+
+    dr = 1e-5
+    for a in range(4):
+        for c in range(3):
+            p, m = ENV.copy(), ENV.copy()
+            p[a, c] += dr / 2
+            m[a, c] -= dr / 2
+            fd = -(energy(p) - energy(m)) / dr
+            assert abs(F[a, c] - fd) <= 1e-4 * abs(fd) + 1e-5, (a, c)
