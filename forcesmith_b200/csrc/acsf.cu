@@ -683,10 +683,15 @@ int eval_jacobian_acsf(fs_gpu *h, double w_e, double w_s) {
 // Per-species descriptor statistics (MLBase::compute_standardization,
 // ml_force.hpp:644-688): the descriptors of every atom (formed in the context
 // precision, summed in FP64), then Σ D and Σ D² per (species, descriptor).
+int lmbtr_descriptors(fs_gpu *h, double *desc);
+
 int acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *count) {
+  const bool lm = h->family == FS_FAMILY_LMBTR;
   AcLayout L;
   L.init(h->tables[0].v.data(), h->ntypes);
-  const int nt = h->ntypes, S = L.S;
+  const double *lv = h->tables[0].v.data();
+  const int nt = h->ntypes;
+  const int S = lm ? nt * static_cast<int>(lv[3]) + nt * (nt + 1) / 2 * static_cast<int>(lv[7]) : L.S;
   const int64_t na = h->n_atoms;
   double *d_desc = nullptr, *d_out = nullptr;
   FS_CUDA(cudaMalloc(&d_desc, std::max<int64_t>(na * S, 1) * sizeof(double)));
@@ -701,8 +706,9 @@ int acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *coun
       rc = set_error(h, FS_ERR_CUDA, "cudaMemsetAsync");
       break;
     }
-    rc = h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, 1.0, 0.0, 2, d_desc)
-                                      : launch_acsf<float>(h, 1.0, 0.0, 2, d_desc);
+    rc = lm                             ? lmbtr_descriptors(h, d_desc)
+         : h->precision == FS_PREC_FP64 ? launch_acsf<double>(h, 1.0, 0.0, 2, d_desc)
+                                        : launch_acsf<float>(h, 1.0, 0.0, 2, d_desc);
     if (rc != FS_OK) break;
     if (nt * S > 0) {
       ac_desc_stats<<<nt * S, 256, 0, h->stream>>>(d_desc, h->d_type, na, S, d_out);

@@ -77,6 +77,7 @@ int expected_tables(int family, int nt) {
   case FS_FAMILY_TERSOFF: return np;
   case FS_FAMILY_ANGULAR: return 2 * np + nt;
   case FS_FAMILY_ACSF: return 1 + nt;
+  case FS_FAMILY_LMBTR: return 1 + nt;
   }
   return -1;
 }
@@ -115,6 +116,7 @@ void free_configs(fs_gpu *h) {
   dfree(h->d_run_cnt);
   dfree(h->d_run_r);
   h->runs_valid = false;
+  h->max_list = -1;
   dfree(h->d_F);
   dfree(h->d_forces);
   dfree(h->d_energy);
@@ -377,8 +379,9 @@ int fs_gpu_set_references(fs_gpu *h, const double *ref_force, const double *ref_
 int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
   if (!h || !m) return FS_ERR_ARG;
   if (m->ntypes < 1 || m->ntypes > 16) return set_error(h, FS_ERR_ARG, "set_model: ntypes out of range");
-  // ACSF models may carry standardization tables after the heads
-  const bool acsf_std = m->family == FS_FAMILY_ACSF && m->n_tables == 1 + 2 * m->ntypes;
+  // ACSF and LMBTR models may carry standardization tables after the heads
+  const bool ml_fam = m->family == FS_FAMILY_ACSF || m->family == FS_FAMILY_LMBTR;
+  const bool acsf_std = ml_fam && m->n_tables == 1 + 2 * m->ntypes;
   if ((expected_tables(m->family, m->ntypes) != m->n_tables && !acsf_std) || !m->tables)
     return set_error(h, FS_ERR_ARG, "set_model: table count does not match the family");
   const int np = npair_of(m->ntypes);
@@ -445,8 +448,36 @@ int fs_gpu_set_model(fs_gpu *h, const fs_model *m) {
                              "set_model: ACSF standardization tables hold {mean[S], inv_std[S]}, all fixed");
         }
       }
-    } else if (ft.kind == FS_TABLE_ACSF || ft.kind == FS_TABLE_LINEAR_HEAD || ft.kind == FS_TABLE_STANDARDIZATION) {
-      return set_error(h, FS_ERR_ARG, "set_model: ACSF tables belong to the ACSF family");
+    } else if (m->family == FS_FAMILY_LMBTR) {
+      // the descriptor table {rcut, weight_scale, normalize, n2, min2, max2,
+      // sigma2, n3, min3, max3, sigma3}, then the heads and optional
+      // standardization tables as for ACSF
+      const fs_table &spec = m->tables[0];
+      const double *v = spec.values;
+      bool ok = spec.kind == FS_TABLE_LMBTR && spec.n == 11 && v[0] > 0.0 && v[1] > 0.0 && v[3] + v[7] > 0;
+      for (int k : {3, 7})
+        ok = ok && v[k] >= 0 && v[k] == std::floor(v[k]) && v[k] < 1e6 && (v[k] == 0 || v[k + 3] > 0.0) &&
+             std::isfinite(v[k + 1]) && std::isfinite(v[k + 2]) && (v[k] <= 1 || v[k + 2] > v[k + 1]);
+      if (!ok)
+        return set_error(h, FS_ERR_ARG,
+                         "set_model: LMBTR table {rcut, weight_scale, normalize, n2, min2, max2, sigma2, n3, min3, "
+                         "max3, sigma3} is malformed");
+      if (t > 0) {
+        const int nt = m->ntypes, P = nt * (nt + 1) / 2;
+        const int S = nt * static_cast<int>(v[3]) + P * static_cast<int>(v[7]);
+        if (t <= nt && (ft.kind != FS_TABLE_LINEAR_HEAD || ft.n != S + 1))
+          return set_error(h, FS_ERR_ARG, "set_model: LMBTR heads are linear_head[nt] with S + 1 values");
+        if (t > nt) {
+          bool fixed = ft.fixed != nullptr;
+          for (int k = 0; fixed && k < ft.n; ++k) fixed = ft.fixed[k] != 0;
+          if (ft.kind != FS_TABLE_STANDARDIZATION || ft.n != 2 * S || !fixed)
+            return set_error(h, FS_ERR_ARG,
+                             "set_model: LMBTR standardization tables hold {mean[S], inv_std[S]}, all fixed");
+        }
+      }
+    } else if (ft.kind == FS_TABLE_ACSF || ft.kind == FS_TABLE_LINEAR_HEAD || ft.kind == FS_TABLE_STANDARDIZATION ||
+               ft.kind == FS_TABLE_LMBTR) {
+      return set_error(h, FS_ERR_ARG, "set_model: descriptor tables belong to the ACSF and LMBTR families");
     } else if (m->family == FS_FAMILY_TERSOFF) {
       if (ft.kind != FS_TABLE_TERSOFF || ft.n != 12)
         return set_error(h, FS_ERR_ARG, "set_model: Tersoff tables are tersoff[npair] with 12 params");
@@ -750,7 +781,8 @@ int fs_gpu_eval_jacobian(fs_gpu *h, double w_e, double w_s, double *F, double *J
 int fs_gpu_acsf_standardization(fs_gpu *h, double *mean, double *inv_std, int64_t *count) {
   if (!h || !mean || !inv_std || !count) return FS_ERR_ARG;
   FS_TRY(check_ready(h));
-  if (h->family != FS_FAMILY_ACSF) return set_error(h, FS_ERR_STATE, "acsf_standardization: not an ACSF model");
+  if (h->family != FS_FAMILY_ACSF && h->family != FS_FAMILY_LMBTR)
+    return set_error(h, FS_ERR_STATE, "acsf_standardization: not an ACSF or LMBTR model");
   cudaSetDevice(h->device);
   return acsf_standardization(h, mean, inv_std, count);
 }

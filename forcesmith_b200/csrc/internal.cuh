@@ -137,6 +137,7 @@ struct fs_gpu {
   // of one configuration, and the configurations ordered by that count,
   // heaviest first (launch order of the per-configuration 3-body kernels)
   int64_t max_cfg_work = 0;
+  int max_list = -1; // the longest neighbour list (LMBTR warp slices); −1: not yet counted
   int32_t *d_cfg_by_work = nullptr;
 
   // model

@@ -302,6 +302,7 @@ int build_neighbors(fs_gpu *h, double rcut) {
   const bool none = !(rcut > 0.0 && std::isfinite(rcut));
   const double rcut2 = none ? -1.0 : rcut * rcut;
   h->runs_valid = false; // pair runs index the neighbour lists
+  h->max_list = -1;
   FS_CUDA(cudaMemcpyAsync(h->d_cfg, h->cfg_host.data(), n_cfg * sizeof(CfgDev), cudaMemcpyHostToDevice,
                           h->stream));
   wrap_kernel<<<n_cfg, 128, 0, h->stream>>>(h->d_cfg, n_cfg, h->d_pos, h->d_wpos);

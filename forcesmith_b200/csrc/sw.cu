@@ -699,6 +699,8 @@ int eval_residual_tersoff(fs_gpu *h, double w_e, double w_s);
 int eval_residual_angular(fs_gpu *h, double w_e, double w_s);
 int eval_residual_acsf(fs_gpu *h, double w_e, double w_s);
 int eval_jacobian_acsf(fs_gpu *h, double w_e, double w_s);
+int eval_residual_lmbtr(fs_gpu *h, double w_e, double w_s);
+int eval_jacobian_lmbtr(fs_gpu *h, double w_e, double w_s);
 int eval_jacobian_fd(fs_gpu *h, double w_e, double w_s);
 
 int eval_residual_other(fs_gpu *h, double w_e, double w_s) {
@@ -708,6 +710,7 @@ int eval_residual_other(fs_gpu *h, double w_e, double w_s) {
   if (h->family == FS_FAMILY_TERSOFF) return eval_residual_tersoff(h, w_e, w_s);
   if (h->family == FS_FAMILY_ANGULAR) return eval_residual_angular(h, w_e, w_s);
   if (h->family == FS_FAMILY_ACSF) return eval_residual_acsf(h, w_e, w_s);
+  if (h->family == FS_FAMILY_LMBTR) return eval_residual_lmbtr(h, w_e, w_s);
   return set_error(h, FS_ERR_UNSUPPORTED, "residual: family not handled by this build");
 }
 
@@ -721,6 +724,8 @@ int eval_jacobian_other(fs_gpu *h, double w_e, double w_s) {
   }
   // ACSF with linear heads: exact (the model is linear in its coefficients)
   if (h->family == FS_FAMILY_ACSF) return eval_jacobian_acsf(h, w_e, w_s);
+  // LMBTR with linear heads: exact, like ACSF
+  if (h->family == FS_FAMILY_LMBTR) return eval_jacobian_lmbtr(h, w_e, w_s);
   // ADP: exact, forward mode (adp.cu)
   if (h->family == FS_FAMILY_ADP) {
     extern int eval_jacobian_adp(fs_gpu * h, double w_e, double w_s);

@@ -20,6 +20,7 @@ double model_max_cutoff(const fs_gpu *h) {
     return m;
   }
   if (h->family == FS_FAMILY_ACSF) return h->tables[0].v[0]; // descriptor_cutoff (acsf.hpp:73)
+  if (h->family == FS_FAMILY_LMBTR) return h->tables[0].v[0]; // descriptor_cutoff (lmbtr.hpp:47)
   if (h->family == FS_FAMILY_TERSOFF) { // max S over pair slots (tersoff_force.cpp:259-265)
     for (int p = 0; p < np; ++p) m = std::max(m, h->tables[p].v[10]);
     return m;

@@ -337,7 +337,7 @@ int fs_gpu_lm_step(fs_gpu *h, double lambda, int32_t mode, double *dx);
  * dx = −(JᵀJ + λI)⁻¹ Jᵀr. */
 int fs_gpu_lsq_step(fs_gpu *h, double ridge, double *dx);
 
-/* ACSF models: per-species descriptor mean and 1/σ over every atom of the
+/* ACSF and LMBTR models: per-species descriptor mean and 1/σ over every atom of the
  * uploaded configurations (MLBase::compute_standardization,
  * ml_force.hpp:644-688): σ² = E[D²] − E[D]², inv_std = σ² > 1e-12 ? 1/σ : 0.
  * mean, inv_std: nt × S (species-major); count: atoms per species (nt).

@@ -1138,11 +1138,16 @@ void eval_lmbtr(const State &S, int c, Out &o) {
   const int Sz = lmbtr_size(L, nt);
   std::vector<std::vector<double>> heads(nt);
   for (int t = 0; t < nt; ++t) heads[t] = acsf_head(S, t, Sz); // standardization folded in
-  std::vector<Vec3> d;
-  std::vector<int> s;
-  std::vector<double> D(Sz), Dp(Sz), Dm(Sz);
   constexpr double h = 1e-4; // descriptor_with_grad (ml_force.hpp:553)
+  // per atom: its energy and, per neighbour-list entry, (∂D/∂d)ᵀ w; formed
+  // in parallel over the atoms, summed below in atom order
+  std::vector<double> ea(cf.natoms);
+  std::vector<std::vector<Vec3>> gwa(cf.natoms);
+#pragma omp parallel for schedule(dynamic) if (!omp_in_parallel())
   for (int i = 0; i < cf.natoms; ++i) {
+    std::vector<Vec3> d;
+    std::vector<int> s;
+    std::vector<double> D(Sz), Dp(Sz), Dm(Sz);
     const int64_t gi = cf.atom0 + i;
     const double *w = heads[S.type[gi]].data();
     lmbtr_env(S, c, i, d, s);
@@ -1150,11 +1155,10 @@ void eval_lmbtr(const State &S, int c, Out &o) {
     lmbtr_descriptor(L, nt, d.data(), s.data(), n, D.data());
     double e = w[Sz];
     for (int k = 0; k < Sz; ++k) e += w[k] * D[k];
-    o.energy += e;
-    // grad_neigh by central differences, contracted with dE/dD = w;
-    // accumulate_atom_forces (ml_force.hpp:595-605)
-    for (int p = 0; p < n; ++p) {
-      Vec3 gw{0, 0, 0};
+    ea[i] = e;
+    // grad_neigh by central differences, contracted with dE/dD = w
+    gwa[i].assign(n, Vec3{0, 0, 0});
+    for (int p = 0; p < n; ++p)
       for (int a = 0; a < 3; ++a) {
         const double x0 = d[p][a];
         d[p][a] = x0 + h;
@@ -1164,14 +1168,22 @@ void eval_lmbtr(const State &S, int c, Out &o) {
         d[p][a] = x0;
         double t = 0.0;
         for (int k = 0; k < Sz; ++k) t += w[k] * ((Dp[k] - Dm[k]) / (2.0 * h));
-        gw[a] = t;
+        gwa[i][p][a] = t;
       }
+  }
+  // accumulate_atom_forces (ml_force.hpp:595-605)
+  for (int i = 0; i < cf.natoms; ++i) {
+    const int64_t gi = cf.atom0 + i;
+    o.energy += ea[i];
+    for (size_t p = 0; p < gwa[i].size(); ++p) {
+      const Vec3 &gw = gwa[i][p];
       const Vec3 fj = -1.0 * gw;
       o.force[i] = o.force[i] + gw; // −grad_selfᵀ w, grad_self = −Σ grad_neigh
-      const int j = S.nb_j[S.nb_start[gi] + p];
+      const int64_t q = S.nb_start[gi] + static_cast<int64_t>(p);
+      const int j = S.nb_j[q];
       o.force[j] = o.force[j] + fj;
       for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) o.stress[a][b] += d[p][a] * fj[b];
+        for (int b = 0; b < 3; ++b) o.stress[a][b] += S.nb_d[q][a] * fj[b];
     }
   }
 }
@@ -1254,6 +1266,15 @@ void residual(const State &S, double w_e, double w_s, double *F,
               const std::vector<int64_t> &ro, std::vector<Out> *keep = nullptr) {
   const int nc = static_cast<int>(S.cfgs.size());
   if (keep) keep->resize(nc);
+  if (S.family == FS_FAMILY_LMBTR) { // parallel over each configuration's atoms instead (eval_lmbtr)
+    Out o;
+    for (int c = 0; c < nc; ++c) {
+      Out &oo = keep ? (*keep)[c] : o;
+      eval_config(S, c, oo);
+      write_residuals(S, c, oo, w_e, w_s, F, ro[c]);
+    }
+    return;
+  }
 #pragma omp parallel
   {
     Out o;
