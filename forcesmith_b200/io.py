@@ -37,10 +37,10 @@ import os
 
 import numpy as np
 
-from .abi import (FS_FAMILY_ACSF, FS_FAMILY_ADP, FS_FAMILY_ANGULAR, FS_FAMILY_EAM, FS_FAMILY_PAIR,
+from .abi import (FS_FAMILY_ACSF, FS_FAMILY_LMBTR, FS_FAMILY_ADP, FS_FAMILY_ANGULAR, FS_FAMILY_EAM, FS_FAMILY_PAIR,
                   FS_FAMILY_SW, FS_FAMILY_TERSOFF, FS_TABLE_ANALYTIC, FS_TABLE_LAMBDA, FS_TABLE_SPLINE,
                   FS_TABLE_SW, FS_TABLE_TERSOFF, FORMS, TERSOFF_FIELDS, Dataset, GlobalParam, Model, Table,
-                  acsf_size)
+                  acsf_size, descriptor_size, lmbtr_size)
 
 SYMBOLS = (
     "H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
@@ -445,14 +445,17 @@ def _pot_json(t, refs=None):
 
 def _read_ml(j):
     """build_ml / finish_ml / parse_linear_head (src/io/force_model_reader.cpp:
-    217-333): an ACSF ("acsf" or "symmetry_functions") descriptor and one
-    linear head per species."""
+    217-389): an ACSF ("acsf" or "symmetry_functions") or LMBTR descriptor and
+    one linear head per species."""
     nt = int(j.get("ntypes", 1))
     desc = j.get("descriptor")
     if not isinstance(desc, dict) or not isinstance(desc.get("type"), str):
         raise FormatError("ml: missing 'descriptor' object with a string 'type'")
+    if desc["type"] == "lmbtr":
+        spec = _read_lmbtr(desc)
+        return _read_heads(j, FS_FAMILY_LMBTR, nt, spec, lmbtr_size(spec, nt))
     if desc["type"] not in ("acsf", "symmetry_functions"):
-        raise FormatError(f"ml: descriptor '{desc['type']}' is not supported by this build (acsf only)")
+        raise FormatError(f"ml: unknown descriptor type '{desc['type']}' (acsf and lmbtr are built; soap is not)")
     g1 = desc.get("g1", 0)
     g1 = len(g1) if isinstance(g1, list) else int(g1) if isinstance(g1, (int, float)) else 0
     g2 = [(float(g["eta"]), float(g.get("rs", 0.0))) for g in desc.get("g2", [])]
@@ -463,6 +466,36 @@ def _read_ml(j):
     S = acsf_size(spec, nt)
     if S == 0:
         raise FormatError("ml: acsf descriptor needs at least one of g1/g2/g3/g4/g5")
+    return _read_heads(j, FS_FAMILY_ACSF, nt, spec, S)
+
+
+def _read_lmbtr(desc):
+    """The lmbtr branch of build_ml (force_model_reader.cpp:350-382): rcut
+    (6), weight_scale (rcut/2), normalize (true); k2 and k3 grids {min, max,
+    n, sigma} defaulting to (0, rcut, 50, 0.3) and (−1, 1, 50, 0.1); naming
+    either grid drops the one not named."""
+    rcut = float(desc.get("rcut", 6.0))
+    ws = float(desc.get("weight_scale", rcut / 2.0))
+    norm = bool(desc.get("normalize", True))
+
+    def grid(key, lo, hi, n, sig):
+        g = desc.get(key)
+        if isinstance(g, dict):
+            lo, hi = float(g.get("min", lo)), float(g.get("max", hi))
+            n, sig = int(g.get("n", n)), float(g.get("sigma", sig))
+        return (lo, hi, n, sig)
+
+    named = "k2" in desc or "k3" in desc
+    k2 = grid("k2", 0.0, rcut, 50, 0.3) if (not named or "k2" in desc) else None
+    k3 = grid("k3", -1.0, 1.0, 50, 0.1) if (not named or "k3" in desc) else None
+    if (k2[2] if k2 else 0) + (k3[2] if k3 else 0) <= 0:
+        raise FormatError("ml: lmbtr descriptor needs k2 and/or k3 with n > 0")
+    return Table.lmbtr(rcut, ws, norm, k2, k3)
+
+
+def _read_heads(j, family, nt, spec, S):
+    """finish_ml / parse_linear_head: one linear head per species, then the
+    optional per-species standardization."""
     heads = j.get("heads")
     if not isinstance(heads, list) or len(heads) != nt:
         raise FormatError(f"ml: expected {nt} heads")
@@ -477,7 +510,7 @@ def _read_ml(j):
         fixed[:S] = 1 if h.get("fixed", False) else 0
         fixed[S] = 1 if h.get("bias_fixed", True) else 0
         tabs.append(Table.linear_head(co, float(h.get("bias", 0.0)), fixed=fixed))
-    model = Model(FS_FAMILY_ACSF, nt, tabs)
+    model = Model(family, nt, tabs)
     if "standardization" in j:
         # finish_ml (force_model_reader.cpp:261-281): one {mean, inv_std} per
         # species, empty for a species without training atoms (identity here)
@@ -497,13 +530,19 @@ def _read_ml(j):
 
 def _write_ml(model):
     v = model.tables[0].values
-    g1, n2, n3, n4, n5 = (int(x) for x in v[1:6])
-    p = list(v[6:])
-    g2 = [{"eta": p.pop(0), "rs": p.pop(0)} for _ in range(n2)]
-    g3 = [{"kappa": p.pop(0)} for _ in range(n3)]
-    g4 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n4)]
-    g5 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n5)]
-    desc = {"type": "acsf", "rcut": float(v[0]), "g1": g1, "g2": g2, "g3": g3, "g4": g4, "g5": g5}
+    if model.family == FS_FAMILY_LMBTR:  # write_native for LMBTR (output_writer.cpp:238-267)
+        desc = {"type": "lmbtr", "rcut": float(v[0]), "weight_scale": float(v[1]), "normalize": bool(v[2] != 0.0)}
+        for key, o in (("k2", 3), ("k3", 7)):
+            if int(v[o]) > 0:
+                desc[key] = {"min": float(v[o + 1]), "max": float(v[o + 2]), "n": int(v[o]), "sigma": float(v[o + 3])}
+    else:
+        g1, n2, n3, n4, n5 = (int(x) for x in v[1:6])
+        p = list(v[6:])
+        g2 = [{"eta": p.pop(0), "rs": p.pop(0)} for _ in range(n2)]
+        g3 = [{"kappa": p.pop(0)} for _ in range(n3)]
+        g4 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n4)]
+        g5 = [{"eta": p.pop(0), "zeta": p.pop(0), "lambda": p.pop(0)} for _ in range(n5)]
+        desc = {"type": "acsf", "rcut": float(v[0]), "g1": g1, "g2": g2, "g3": g3, "g4": g4, "g5": g5}
     heads = []
     for t in model.tables[1:1 + model.ntypes]:
         fx = np.zeros(t.values.size, np.uint8) if t.fixed is None else t.fixed
@@ -512,7 +551,7 @@ def _write_ml(model):
                       "bias": float(t.values[-1]), "bias_fixed": bool(fx[-1])})
     out = {"model": "ml", "ntypes": model.ntypes, "descriptor": desc, "heads": heads}
     if len(model.tables) == 1 + 2 * model.ntypes:  # add_standardization (output_writer.cpp:155-168)
-        S = acsf_size(model.tables[0], model.ntypes)
+        S = descriptor_size(model)
         out["standardization"] = [{"mean": [float(x) for x in t.values[:S]],
                                    "inv_std": [float(x) for x in t.values[S:]]}
                                   for t in model.tables[1 + model.ntypes:]]
@@ -542,7 +581,7 @@ def write_model(model):
     every radial table instead, as the reference's writer does."""
     nt, fam = model.ntypes, model.family
     npair = nt * (nt + 1) // 2
-    if fam == FS_FAMILY_ACSF:
+    if fam in (FS_FAMILY_ACSF, FS_FAMILY_LMBTR):
         return _write_ml(model)
     if fam == FS_FAMILY_TERSOFF:
         return json.dumps({"model": "tersoff", "ntypes": nt,
@@ -652,7 +691,7 @@ def write_native(model, sample, nknots=DEFAULT_KNOTS):
     Tersoff and ACSF models carry their parameters as they are.
     sample(k, r) → (values, derivatives) of table k at the points r."""
     fam, nt = model.family, model.ntypes
-    if fam in (FS_FAMILY_TERSOFF, FS_FAMILY_ACSF, FS_FAMILY_SW):
+    if fam in (FS_FAMILY_TERSOFF, FS_FAMILY_ACSF, FS_FAMILY_LMBTR, FS_FAMILY_SW):
         return write_model(model)
     if fam not in TABLE_KEYS:
         raise FormatError("write_native: unsupported model family")

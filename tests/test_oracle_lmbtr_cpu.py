@@ -112,3 +112,63 @@ def test_force_matches_energy_fd_and_newton():
             m[a, c] -= dr / 2
             fd = -(energy(p) - energy(m)) / dr
             assert abs(F[a, c] - fd) <= 1e-4 * abs(fd) + 1e-5, (a, c)
+
+
+# ---- the model JSON (force_model_reader.cpp:350-382, output_writer.cpp:238-267)
+
+def test_reader_round_trip_case():
+    """The reference's Lmbtr.ReaderRoundTrip input: 8-bin k2 and k3 grids,
+    one species, so S = 16."""
+    import json
+    from forcesmith_b200 import io
+    text = json.dumps({
+        "model": "ml", "ntypes": 1,
+        "descriptor": {"type": "lmbtr", "rcut": 6.0, "weight_scale": 3.0, "normalize": True,
+                       "k2": {"min": 0.0, "max": 6.0, "n": 8, "sigma": 0.3},
+                       "k3": {"min": -1.0, "max": 1.0, "n": 8, "sigma": 0.1}},
+        "heads": [{"type": "linear", "coeffs": [0] * 16, "bias": 0.0}]})
+    m = io.read_model(text)
+    assert m.family == FS_FAMILY_LMBTR and lmbtr_size(m.tables[0], 1) == 16
+    v = m.tables[0].values
+    assert int(v[3]) == 8 and int(v[7]) == 8
+    m2 = io.read_model(io.write_model(m))
+    assert np.array_equal(m2.tables[0].values, v)
+    assert np.array_equal(m2.tables[1].values, m.tables[1].values)
+
+
+def test_reader_defaults_and_errors():
+    import json
+    import pytest
+    from forcesmith_b200 import io
+
+    def read(desc, nt=1, S=None):
+        sp = io._read_lmbtr(desc)
+        S = lmbtr_size(sp, nt) if S is None else S
+        return io.read_model(json.dumps({"model": "ml", "ntypes": nt, "descriptor": desc,
+                                         "heads": [{"coeffs": [0.0] * S} for _ in range(nt)]}))
+
+    m = read({"type": "lmbtr", "rcut": 5.0})
+    v = m.tables[0].values
+    # weight_scale = rcut / 2; both grids at their defaults, k2 up to rcut
+    assert v[1] == 2.5 and v[2] == 1.0 and list(v[3:7]) == [50, 0.0, 5.0, 0.3] and list(v[7:]) == [50, -1.0, 1.0, 0.1]
+    m = read({"type": "lmbtr", "k3": {"n": 12}}, nt=2)  # naming k3 drops k2
+    v = m.tables[0].values
+    assert v[3] == 0 and v[7] == 12 and lmbtr_size(m.tables[0], 2) == 36
+    with pytest.raises(io.FormatError):
+        io._read_lmbtr({"type": "lmbtr", "k2": {"n": 0}})
+    with pytest.raises(io.FormatError):  # head length must match S
+        io.read_model(json.dumps({"model": "ml", "ntypes": 1, "descriptor": {"type": "lmbtr"},
+                                  "heads": [{"coeffs": [0.0] * 5}]}))
+
+
+def test_standardization_block_round_trip():
+    from forcesmith_b200 import io
+    sp = spec()
+    S = lmbtr_size(sp, 2)
+    rng = np.random.default_rng(4)
+    m = Model(FS_FAMILY_LMBTR, 2, [sp] + [Table.linear_head(rng.normal(size=S), 0.5) for _ in range(2)])
+    m = m.with_standardization(rng.normal(size=(2, S)), rng.uniform(0.5, 2, (2, S)))
+    m2 = io.read_model(io.write_model(m))
+    assert len(m2.tables) == 5
+    for a, b in zip(m.tables, m2.tables):
+        assert np.array_equal(a.values, b.values)
