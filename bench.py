@@ -503,6 +503,73 @@ def acsf_leg(local, steps=20):
                              "kind": "port", "sample": f"one FP64 residual ({t_res * 1e3:.0f} ms)"}}
 
 
+def lmbtr_leg(local, steps=10, n_cfg=1000, cpu_cfgs=4):
+    """LMBTR descriptors at the reference's defaults (rcut 6 A, weight scale
+    3 A, k2 grid 0-6 A x 50 bins, sigma 0.3; k3 grid cos 0 in [-1, 1] x 50
+    bins, sigma 0.1; L2 normalised) with a linear head on diamond Si,
+    n_cfg configurations of 64/216/512 atoms.  Device FP32: residuals per
+    second (forces from the exact descriptor derivative), and residual +
+    exact head Jacobian + JtJ per second.  CPU: the oracle's residual (all
+    host threads, FP64), whose forces are the reference's central
+    differences of the whole descriptor (6 descriptors per neighbour of
+    every atom); timed on the first cpu_cfgs configurations and scaled to
+    n_cfg by atom count."""
+    import numpy as np
+    import torch
+    from forcesmith_b200 import gpu as G, synth
+    from forcesmith_b200.abi import FS_FAMILY_LMBTR, Model, Table, lmbtr_size
+    from oracle.api import Oracle, set_threads
+    spec = Table.lmbtr()
+    S = lmbtr_size(spec, 1)
+    rng = np.random.default_rng(6)
+
+    def model(w):
+        return Model(FS_FAMILY_LMBTR, 1, [spec, Table.linear_head(w, -4.0)])
+    w_true = rng.normal(0, 0.3, S)
+    ds = label_on_gpu(synth.diamond(n_cfg), model(w_true), local)
+    start = model(w_true * (1 + 0.1 * rng.normal(size=S)))
+    g = G.GpuSession(local, "fp32")
+    g.upload(ds)
+    g.set_model(start)
+    for _ in range(3):
+        g.jacobian_async(W_E, W_S)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(g.stream)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+        for _ in range(steps):
+            fn()
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+    res_ms = timed(lambda: g._lib.fs_gpu_eval(g._h, W_E, W_S, None, None, None, None, None, None))
+    jac_ms = timed(lambda: g.jacobian_async(W_E, W_S))
+    P = g.num_pairs()
+    g.close()
+    threads = set_threads(os.cpu_count() or 1)
+    sub = ds.subset(range(cpu_cfgs))
+    o = Oracle()
+    o.upload(sub)
+    o.set_model(start)
+    t0 = time.perf_counter()
+    o.eval(W_E, W_S, want=("F",))
+    t_sub = time.perf_counter() - t0
+    t_res = t_sub * ds.n_atoms / sub.n_atoms
+    return {"workload": f"LMBTR (reference defaults, S = {S}) + linear head, Si, {ds.n_cfg} configs x "
+                        f"64/216/512 atoms ({ds.n_atoms} atoms, {P} pairs), w_e=1, w_s=0.1",
+            "residual_fp32": {"value": 1000.0 / res_ms, "unit": "evals/s", "ms_per_eval": res_ms},
+            "jacobian_fp32": {"value": 1000.0 / jac_ms, "unit": "evals/s", "ms_per_eval": jac_ms,
+                              "method": "exact (linear head): residual + J + JtJ + Jtr"},
+            "cpu_baseline": {"residual": {"value": 1.0 / t_res, "unit": "evals/s"}, "cores": threads,
+                             "kind": "port",
+                             "sample": f"one FP64 residual of the first {sub.n_cfg} configurations "
+                                       f"({sub.n_atoms} atoms, {t_sub:.2f} s), scaled by atom count"}}
+
+
 def sw_leg(local, steps=20):
     """Stillinger-Weber Si: 1000 diamond configurations of 64, 216 or 512
     atoms (sigma = 0.15 A, volumetric strain U[0.95, 1.05]), 7 perturbed SW
@@ -848,6 +915,7 @@ def run_ours(args):
         line["tersoff"] = three_body_leg(local, "tersoff")
         line["angular"] = three_body_leg(local, "angular")
         line["acsf"] = acsf_leg(local)
+        line["lmbtr"] = lmbtr_leg(local)
         line["al99_fit"] = al99_leg(local)
     if rank == 0 and world == 1 and not args.small and args.de_generations >= 0:
         de, sur = de_legs(local, args.de_generations, SURROGATE_SEEDS[:max(0, args.surrogate_seeds)])
