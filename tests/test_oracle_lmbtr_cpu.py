@@ -172,3 +172,26 @@ def test_standardization_block_round_trip():
     assert len(m2.tables) == 5
     for a, b in zip(m.tables, m2.tables):
         assert np.array_equal(a.values, b.values)
+
+
+def test_model_validation():
+    """Malformed LMBTR tables and heads of the wrong length are refused."""
+    import pytest
+    from forcesmith_b200.abi import FsError
+    o = O.Oracle()
+    o.upload(cluster(ENV, 100.0))
+    good = spec()
+    S = lmbtr_size(good, 1)
+    o.set_model(Model(FS_FAMILY_LMBTR, 1, [good, Table.linear_head(np.zeros(S))]))
+    bad = []
+    for k, v in ((0, 0.0), (1, -1.0), (3, 2.5), (6, 0.0)):  # rcut, weight scale, fractional n, sigma
+        t = spec()
+        t.values[k] = v
+        bad.append(Model(FS_FAMILY_LMBTR, 1, [t, Table.linear_head(np.zeros(S))]))
+    t = spec()
+    t.values[3] = t.values[7] = 0  # no term
+    bad.append(Model(FS_FAMILY_LMBTR, 1, [t, Table.linear_head(np.zeros(1))]))
+    bad.append(Model(FS_FAMILY_LMBTR, 1, [good, Table.linear_head(np.zeros(S + 1))]))
+    for m in bad:
+        with pytest.raises(FsError):
+            o.set_model(m)
