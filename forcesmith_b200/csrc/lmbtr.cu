@@ -43,7 +43,7 @@
 namespace fsg {
 namespace {
 
-constexpr int kLmMaxWarps = 8;
+constexpr int kLmMaxWarps = 16;
 
 // exp: the hardware approximation in FP32, IEEE in FP64
 __device__ __forceinline__ float lm_exp(float x) { return __expf(x); }
