@@ -1,10 +1,12 @@
 """Ragged batches for the per-bond and per-triplet kernels (Stillinger–Weber,
-Tersoff, Angular, ACSF): an isolated atom (no pairs, no triplets), a dimer
+Tersoff, Angular, ACSF, LMBTR): an isolated atom (no pairs, no triplets), a dimer
 (pairs, no triplets), a bent trimer, and a periodic diamond cell, in one
 batch, against the oracle in FP64.
 
 Tolerances: forces, energy, stress, F rows |Δ| ≤ 1e-9·(1 + |x|); objective
-1e-9 relative.
+1e-9 relative.  LMBTR, whose oracle forces are the reference's central
+differences of the descriptor: energies 1e-10·(1 + |E|), forces and stress
+1e-7 of their largest magnitude (grids and cutoff as in test_gpu_lmbtr.py).
 """
 import numpy as np
 import pytest
@@ -60,3 +62,23 @@ def test_ragged_batch_fp64(which):
         assert err <= 1e-9, (which, key, err)
     assert abs(rg["obj"] - ro["obj"]) <= 1e-9 * ro["obj"]
     assert np.all(np.abs(rg["forces"][0]) == 0.0)  # the isolated atom
+
+
+def test_ragged_batch_lmbtr_fp64():
+    from forcesmith_b200.gpu import GpuSession
+    from tests.test_gpu_lmbtr import SMOOTH, clear_cutoff, model as lmbtr_model
+    ds = ragged()
+    m = lmbtr_model(1, clear_cutoff(ds, 3.6, 3.95), SMOOTH, 8)
+    ds = label(ds, m.with_values(m.free_values() * 1.02), O.Oracle, 1.0, 0.2)
+    g = GpuSession(0, "fp64")
+    g.upload(ds)
+    g.set_model(m)
+    o = O.Oracle()
+    o.upload(ds)
+    o.set_model(m)
+    rg, ro = g.eval(1.0, 0.2), o.eval(1.0, 0.2)
+    assert np.max(np.abs(rg["energy"] - ro["energy"]) / (1.0 + np.abs(ro["energy"]))) <= 1e-10
+    assert np.abs(rg["forces"] - ro["forces"]).max() <= 1e-7 * np.abs(ro["forces"]).max()
+    assert np.abs(rg["stress"] - ro["stress"]).max() <= 1e-7 * np.abs(ro["stress"]).max()
+    assert np.all(np.abs(rg["forces"][0]) == 0.0)  # the isolated atom: no neighbours, u = 0
+    assert rg["energy"][0] == m.tables[1].values[-1]  # … and its energy is the bias
