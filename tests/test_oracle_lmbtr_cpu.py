@@ -195,3 +195,27 @@ def test_model_validation():
     for m in bad:
         with pytest.raises(FsError):
             o.set_model(m)
+
+
+def test_two_species_block_layout():
+    """LmbtrLayout (lmbtr.hpp:13-38, DescriptorLayout::index = base + chan ·
+    count + t): k2 blocks per neighbour species, then k3 blocks per species
+    pair in pair_ordinal order.  A species-0 atom with one species-0 and one
+    species-1 neighbour fills the k2 blocks of both species and only the k3
+    block of the pair (0, 1), ordinal 1 of {(0,0), (0,1), (1,1)}."""
+    sp = spec(normalize=False)
+    o = O.Oracle()
+    o.upload(cluster([[0, 0, 0], [2.2, 0.3, 0.0], [-0.5, 2.1, 0.4]], 100.0, types=[0, 0, 1]))
+    o.set_model(Model(FS_FAMILY_LMBTR, 2, [sp] + [Table.linear_head(np.zeros(lmbtr_size(sp, 2)))] * 2))
+    v = o.descriptor(0, 0, lmbtr_size(sp, 2))
+    n2, n3 = 6, 6
+    k2 = v[:2 * n2].reshape(2, n2)
+    k3 = v[2 * n2:].reshape(3, n3)
+    assert np.abs(k2[0]).max() > 0 and np.abs(k2[1]).max() > 0
+    assert np.abs(k3[1]).max() > 0 and np.abs(k3[0]).max() == 0 and np.abs(k3[2]).max() == 0
+    # species-0 block of k2 is the species-0 neighbour's Gaussian alone
+    r = np.linalg.norm([2.2, 0.3, 0.0])
+    x = np.linspace(0.0, 6.0, n2)
+    g = np.exp(-r / 3.0) / (0.4 * np.sqrt(2 * np.pi)) * np.exp(-(x - r) ** 2 / (2 * 0.4 ** 2))
+    g[np.abs(x - r) > 5 * 0.4] = 0.0
+    assert np.abs(k2[0] - g).max() <= 1e-14
