@@ -67,8 +67,9 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=50,
                    help="configurations in the CPU central-difference sample of cpu_baseline")
     p.add_argument("--small", action="store_true", help="small case for profiler captures")
-    p.add_argument("--leg", default="all", choices=["all", "de"],
-                   help="de: only the DE and surrogate legs (profiler captures of their kernels)")
+    p.add_argument("--leg", default="all", choices=["all", "de", "lmbtr"],
+                   help="de: only the DE and surrogate legs; lmbtr: only the LMBTR leg (profiler captures "
+                        "of their kernels)")
     p.add_argument("--surrogate-seeds", type=int, default=len(SURROGATE_SEEDS),
                    help="seeds of the surrogate comparison (the first N of 11, 12, 13)")
     p.add_argument("--de-generations", type=int, default=200,
@@ -765,6 +766,17 @@ def run_de_only(args):
     return 0
 
 
+def run_lmbtr_only(args):
+    """The LMBTR leg alone on one GPU (profiler captures): at most 10 timed
+    calls of each kind; --small: 100 configurations instead of 1000."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    steps = max(1, min(args.steps, 10))
+    print(json.dumps({"lmbtr": lmbtr_leg(local, steps=steps, n_cfg=100 if args.small else 1000)}))
+    return 0
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -938,6 +950,8 @@ def main():
         return run_reference(args)
     if args.leg == "de":
         return run_de_only(args)
+    if args.leg == "lmbtr":
+        return run_lmbtr_only(args)
     return run_ours(args)
 
 
