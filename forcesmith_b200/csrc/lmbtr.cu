@@ -617,8 +617,9 @@ int lm_size(const fs_gpu *h) {
   return nt * static_cast<int>(v[3]) + nt * (nt + 1) / 2 * static_cast<int>(v[7]);
 }
 
-// The longest neighbour list (an upper bound on the neighbours inside rcut),
-// from the list offsets; kept until the lists are rebuilt.
+// The longest neighbour list (an upper bound on the neighbours inside rcut).
+// The neighbour build records it; this recount from the list offsets (a
+// synchronising copy) is only a fallback for lists built without it.
 int lm_kmax(fs_gpu *h) {
   if (h->max_list >= 0) return FS_OK;
   std::vector<int32_t> st(static_cast<size_t>(h->n_atoms) + 1);

@@ -371,9 +371,11 @@ int build_neighbors(fs_gpu *h, double rcut) {
   FS_NB(cudaStreamSynchronize(h->stream));
   std::vector<int32_t> start(h->n_atoms + 1, 0);
   int64_t total = 0;
+  int longest = 0; // the longest list (the LMBTR kernel's per-warp neighbour slices)
   for (int64_t i = 0; i < h->n_atoms; ++i) {
     start[i] = static_cast<int32_t>(total);
     total += cnt[i];
+    longest = std::max(longest, cnt[i]);
     if (total > (int64_t(1) << 31) - 1) {
       release();
       return set_error(h, FS_ERR_UNSUPPORTED, "neighbour list: more than 2^31 pairs");
@@ -382,6 +384,7 @@ int build_neighbors(fs_gpu *h, double rcut) {
   start[h->n_atoms] = static_cast<int32_t>(total);
   for (int c = 0; c < n_cfg; ++c) h->cfg_host[c].pair0 = start[h->atom0[c]];
   h->n_pairs = total;
+  h->max_list = longest;
   std::vector<int32_t> order(n_cfg); // outlives the asynchronous upload below (synchronised at the end)
   {
     std::vector<int64_t> work(n_cfg, 0);
